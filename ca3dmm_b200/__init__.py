@@ -1,0 +1,281 @@
+"""ca3dmm_b200 -- CA3DMM's FP64 GEMM path, B200-native.
+
+The product is the C-ABI shared library ``libca3dmm_b200.so`` (headers in
+``include/``): the reference's ``ca3dmm_engine_*`` / ``cannon_engine_*`` /
+partition API on one GPU.  This module is the Python host mirror of that
+interface -- the same entry points, argument meaning and error behaviour
+(an engine that fails to initialise is ``None``; exec errors are reported by
+``last_error``) -- over ctypes.  Device memory is passed as raw pointers
+(``torch.Tensor.data_ptr()`` or any CUDA allocation).
+
+There is no CPU fallback: when the library is missing, ``lib()`` raises.
+"""
+import ctypes as C
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libca3dmm_b200.so")
+
+DEV_TYPE_HOST, DEV_TYPE_CUDA, DEV_TYPE_CUDA_MPI_DIRECT = 0, 1, 2
+GEMM_PLAIN, GEMM_OZAKI = 0, 1
+ERRORS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "device wait timed out",
+          4: "out of memory", 5: "no device"}
+
+_lib = None
+
+
+class Ca3dmmEngineS(C.Structure):
+    """Mirror of ``struct ca3dmm_engine`` (include/ca3dmm.h)."""
+    _fields_ = [(n, C.c_int) for n in (
+        "m", "n", "k", "mp", "np", "kp", "rp", "my_rank", "n_proc", "is_active",
+        "rank_m", "rank_n", "rank_k", "trans_A", "trans_B", "task_m_num", "task_m_id",
+        "task_n_num", "task_n_id", "task_k_num", "task_k_id", "is_BTB", "use_ag", "use_rsb",
+        "A_rd_srow", "A_rd_scol", "B_rd_srow", "B_rd_scol", "A_2dmm_srow", "A_2dmm_scol",
+        "B_2dmm_srow", "B_2dmm_scol", "C_2dmm_srow", "C_2dmm_scol", "C_out_srow", "C_out_scol",
+        "A_rd_nrow", "A_rd_ncol", "B_rd_nrow", "B_rd_ncol", "A_2dmm_nrow", "A_2dmm_ncol",
+        "B_2dmm_nrow", "B_2dmm_ncol", "C_2dmm_nrow", "C_2dmm_ncol", "C_out_nrow", "C_out_ncol",
+        "alloc_workbuf")] + [
+        ("AB_agv_recvcnts", C.POINTER(C.c_int)), ("AB_agv_displs", C.POINTER(C.c_int)),
+        ("C_rs_recvcnts", C.POINTER(C.c_int))] + [(n, C.c_void_p) for n in (
+            "A_rd_recv_h", "A_trans_h", "A_2dmm_h", "B_rd_recv_h", "B_trans_h", "B_2dmm_h",
+            "C_2dmm_h", "C_out_h", "A_rd_recv_d", "A_trans_d", "A_2dmm_d", "B_rd_recv_d",
+            "B_trans_d", "B_2dmm_d", "C_2dmm_d", "C_out_d", "workbuf_h", "workbuf_d")] + [
+        (n, C.c_size_t) for n in ("rdA_workbuf_bytes", "rdB_workbuf_bytes", "rdC_workbuf_bytes",
+                                  "cannon_workbuf_bytes", "self_workbuf_bytes")] + [
+        (n, C.c_void_p) for n in ("comm_AB_agv", "comm_C_rs", "comm_2dmm", "redist_A",
+                                  "redist_B", "redist_C", "cannon_engine")] + [
+        ("dev_type", C.c_int), ("print_timing", C.c_int)] + [
+        (n, C.c_double) for n in ("init_ms", "redist_ms", "agvAB_ms", "cannon_ms", "reduce_ms",
+                                  "hd_trans_ms", "exec_ms")] + [
+        ("n_exec", C.c_int), ("n_group", C.c_int), ("gemm_mode", C.c_int),
+        ("ozaki_slices", C.c_int), ("last_error", C.c_int), ("stream", C.c_void_p),
+        ("sync_exec", C.c_int), ("workbuf_bytes", C.c_size_t), ("impl", C.c_void_p)]
+
+
+class CannonEngineS(C.Structure):
+    """Mirror of ``struct cannon_engine`` (include/cannon.h), leading fields."""
+    _fields_ = [(n, C.c_int) for n in (
+        "m", "n", "k", "my_rank", "rank_row", "rank_col", "np_dim", "A_srow", "A_scol", "B_srow",
+        "B_scol", "C_srow", "C_scol", "A_nrow", "A_ncol", "B_nrow", "B_ncol", "C_nrow", "C_ncol",
+        "gemm_cycle", "max_A_blk_size", "max_B_blk_size", "max_C_blk_size", "alloc_workbuf")] + [
+        (n, C.POINTER(C.c_int)) for n in ("m_displs", "n_displs", "k_displs")] + [
+        (n, C.c_void_p) for n in ("A_recv_h", "A_stack_h", "B_recv_h", "B_stack_h", "A_recv_d",
+                                  "A_stack_d", "B_recv_d", "B_stack_d", "workbuf_h", "workbuf_d",
+                                  "A_gemm_h", "B_gemm_h")] + [
+        ("dev_type", C.c_int), ("comm", C.c_void_p)] + [
+        (n, C.c_double) for n in ("init_ms", "shift0_ms", "lshift_ms", "gemm_ms", "exec_ms",
+                                  "hd_trans_ms")] + [
+        ("n_exec", C.c_int), ("workbuf_bytes", C.c_size_t), ("impl", C.c_void_p),
+        ("last_error", C.c_int)]
+
+
+def lib():
+    """Load the shared library (raises if it has not been built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError("libca3dmm_b200.so is not built: run `python -m ca3dmm_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    i, p, d, sz = C.c_int, C.c_void_p, C.c_double, C.c_size_t
+    pi = C.POINTER(C.c_int)
+    EP = C.POINTER(Ca3dmmEngineS)
+    sig = {
+        "ca3dmm_vcomm_create": (i, [i, C.POINTER(p)]),
+        "ca3dmm_vcomm_free": (None, [C.POINTER(p)]),
+        "ca3dmm_vcomm_size": (i, [p]),
+        "calc_3d_decomposition_cannon": (None, [i, i, i, i, pi, pi, pi, pi]),
+        "calc_3d_decomposition_nk": (None, [i, i, i, pi, pi, pi]),
+        "calc_block_spos_size": (None, [i, i, i, pi, pi]),
+        "ca3dmm_engine_init": (None, [i] * 17 + [pi, p, i, C.POINTER(EP), C.POINTER(sz)]),
+        "ca3dmm_engine_init_BTB": (None, [i] * 10 + [pi, p, i, C.POINTER(EP), C.POINTER(sz)]),
+        "ca3dmm_engine_attach_workbuf": (None, [EP, p, p]),
+        "ca3dmm_engine_free": (None, [C.POINTER(EP)]),
+        "ca3dmm_engine_exec": (None, [EP, p, i, p, i, p, i]),
+        "ca3dmm_engine_reset_stat": (None, [EP]),
+        "ca3dmm_engine_print_stat": (None, [EP]),
+        "ca3dmm_engine_last_error": (i, [EP]),
+        "ca3dmm_engine_set_stream": (None, [EP, p, i]),
+        "ca3dmm_engine_set_gemm_mode": (i, [EP, i, i]),
+        "ca3dmm_engine_workbuf_bytes": (sz, [EP]),
+        "ca3dmm_engine_vrank_info": (i, [EP, i, pi]),
+        "cannon_engine_init": (None, [i, i, i, p, i, C.POINTER(C.POINTER(CannonEngineS)),
+                                      C.POINTER(sz)]),
+        "cannon_engine_attach_workbuf": (None, [C.POINTER(CannonEngineS), p, p]),
+        "cannon_engine_free": (None, [C.POINTER(C.POINTER(CannonEngineS))]),
+        "cannon_engine_exec": (None, [C.POINTER(CannonEngineS), d, d, p, p, p]),
+        "cannon_engine_reset_stat": (None, [C.POINTER(CannonEngineS)]),
+        "cannon_engine_print_stat": (None, [C.POINTER(CannonEngineS)]),
+        "dev_type_malloc": (p, [sz, i]),
+        "dev_type_free": (None, [p, i]),
+        "dev_type_memcpy": (None, [p, p, sz, i, i]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(L, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = L
+    return L
+
+
+class VComm:
+    """Virtual communicator of p ranks (the reference's MPI_Comm)."""
+
+    def __init__(self, p):
+        self.h = C.c_void_p()
+        if lib().ca3dmm_vcomm_create(int(p), C.byref(self.h)) != 0:
+            raise ValueError("invalid number of virtual ranks: %r" % (p,))
+        self.p = int(p)
+
+    def __del__(self):
+        try:
+            if self.h:
+                lib().ca3dmm_vcomm_free(C.byref(self.h))
+        except Exception:
+            pass
+
+
+def calc_3d_decomposition_cannon(p, m, n, k):
+    """src/partition.h:16-19 -> (mp, np, kp, rp)."""
+    o = [C.c_int() for _ in range(4)]
+    lib().calc_3d_decomposition_cannon(p, m, n, k, *[C.byref(x) for x in o])
+    return tuple(x.value for x in o)
+
+
+def calc_3d_decomposition_nk(p, n, k):
+    """src/partition.h:27-30 -> (np, kp, rp)."""
+    o = [C.c_int() for _ in range(3)]
+    lib().calc_3d_decomposition_nk(p, n, k, *[C.byref(x) for x in o])
+    return tuple(x.value for x in o)
+
+
+def calc_block_spos_size(length, nblk, iblk):
+    s, z = C.c_int(), C.c_int()
+    lib().calc_block_spos_size(length, nblk, iblk, C.byref(s), C.byref(z))
+    return s.value, z.value
+
+
+def _ptr(x):
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return x
+    return x.data_ptr()
+
+
+class Ca3dmmEngine:
+    """Python mirror of ca3dmm_engine_{init,init_BTB,attach_workbuf,exec,free}.
+
+    ``Ca3dmmEngine(m, n, k, trans_A, trans_B, p=..., proc_grid=None)`` folds
+    the reference's SPMD call onto one GPU: the source blocks are the whole
+    matrices and the output (``dst_C`` whole C unless a block is given) is
+    written by ``exec``.  ``gemm_mode`` selects plain FP64 DMMA or the
+    split-precision path.  ``workbuf`` may be a caller-owned device pointer
+    (then the engine does not allocate; size via ``workbuf_bytes``).
+    """
+
+    def __init__(self, m, n, k, trans_A=0, trans_B=0, p=1, proc_grid=None, dst_C=True,
+                 btb=False, dev_type=DEV_TYPE_CUDA, caller_workbuf=False):
+        L = lib()
+        self.comm = VComm(p)
+        self.m, self.n, self.k = m, n, k
+        self.btb = btb
+        self.e = C.POINTER(Ca3dmmEngineS)()
+        grid = (C.c_int * 3)(*proc_grid) if proc_grid is not None else None
+        wb = C.c_size_t(0)
+        wbp = C.byref(wb) if caller_workbuf else None
+        if dst_C is True:
+            dst = (0, m if not btb else n, 0, n)
+        elif dst_C is None or dst_C is False:
+            dst = (-1, -1, -1, -1)
+        else:
+            dst = tuple(dst_C)
+        if btb:
+            L.ca3dmm_engine_init_BTB(n, k, 0, k, 0, n, dst[0], dst[1], dst[2], dst[3],
+                                     grid, self.comm.h, dev_type, C.byref(self.e), wbp)
+        else:
+            a_r, a_c = (k, m) if trans_A else (m, k)
+            b_r, b_c = (n, k) if trans_B else (k, n)
+            L.ca3dmm_engine_init(m, n, k, int(trans_A), int(trans_B), 0, a_r, 0, a_c, 0, b_r, 0,
+                                 b_c, dst[0], dst[1], dst[2], dst[3], grid, self.comm.h,
+                                 dev_type, C.byref(self.e), wbp)
+        self.workbuf_bytes = wb.value if caller_workbuf else None
+
+    @property
+    def ok(self):
+        return bool(self.e)
+
+    @property
+    def s(self):
+        return self.e.contents
+
+    def attach_workbuf(self, workbuf_d, workbuf_h=None):
+        lib().ca3dmm_engine_attach_workbuf(self.e, _ptr(workbuf_h), _ptr(workbuf_d))
+
+    def set_gemm_mode(self, mode, slices=7):
+        return lib().ca3dmm_engine_set_gemm_mode(self.e, int(mode), int(slices))
+
+    def set_stream(self, stream, sync=1):
+        lib().ca3dmm_engine_set_stream(self.e, C.c_void_p(stream), int(sync))
+
+    def required_workbuf_bytes(self):
+        return lib().ca3dmm_engine_workbuf_bytes(self.e)
+
+    def exec(self, A, ldA, B, ldB, Cout=None, ldC=0):
+        lib().ca3dmm_engine_exec(self.e, _ptr(A), int(ldA), _ptr(B), int(ldB), _ptr(Cout),
+                                 int(ldC))
+        return lib().ca3dmm_engine_last_error(self.e)
+
+    def vrank_info(self, r):
+        out = (C.c_int * 34)()
+        rc = lib().ca3dmm_engine_vrank_info(self.e, int(r), out)
+        if rc:
+            raise ValueError("bad virtual rank %d" % r)
+        return list(out)
+
+    def reset_stat(self):
+        lib().ca3dmm_engine_reset_stat(self.e)
+
+    def print_stat(self):
+        lib().ca3dmm_engine_print_stat(self.e)
+
+    def free(self):
+        if self.e:
+            lib().ca3dmm_engine_free(C.byref(self.e))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class CannonEngine:
+    """Python mirror of cannon_engine_{init,exec,free} (np_dim^2 virtual ranks)."""
+
+    def __init__(self, m, n, k, p=1, dev_type=DEV_TYPE_CUDA):
+        self.comm = VComm(p)
+        self.e = C.POINTER(CannonEngineS)()
+        lib().cannon_engine_init(m, n, k, self.comm.h, dev_type, C.byref(self.e), None)
+
+    @property
+    def ok(self):
+        return bool(self.e)
+
+    @property
+    def s(self):
+        return self.e.contents
+
+    def exec(self, alpha, beta, A, B, Cm):
+        lib().cannon_engine_exec(self.e, float(alpha), float(beta), _ptr(A), _ptr(B), _ptr(Cm))
+        return self.e.contents.last_error
+
+    def free(self):
+        if self.e:
+            lib().cannon_engine_free(C.byref(self.e))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass

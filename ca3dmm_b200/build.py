@@ -1,0 +1,67 @@
+"""Build libca3dmm_b200.so in-tree: C host engine (gcc) + sm_100a kernels (nvcc).
+
+The library is the drop-in boundary: plain C ABI (include/*.h), no torch
+types.  Run `python -m ca3dmm_b200.build` or call build().
+"""
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(HERE)
+CSRC = os.path.join(HERE, "csrc")
+INC = os.path.join(ROOT, "include")
+OBJ = os.path.join(HERE, "_obj")
+LIB = os.path.join(HERE, "libca3dmm_b200.so")
+CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+NVCC = os.path.join(CUDA, "bin", "nvcc")
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+C_SOURCES = ["vcomm.c", "partition.c", "dev_type.c", "mat_redist.c", "cannon.c", "ca3dmm.c"]
+CU_SOURCES = ["k_dgemm.cu", "k_pack.cu", "k_ozaki.cu"]
+HEADERS = ["ca3dmm_kernels.h", "ca3dmm_ozaki.h", "ca3dmm_util.h", "k_common.cuh"]
+
+
+def _newer(target, deps):
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
+
+
+def _run(cmd):
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError("build step failed: " + os.path.basename(cmd[-1]))
+    return r
+
+
+def build(verbose=False):
+    os.makedirs(OBJ, exist_ok=True)
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [
+        os.path.join(INC, f) for f in os.listdir(INC) if f.endswith(".h")]
+    objs = []
+    for src in C_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(OBJ, src + ".o")
+        objs.append(o)
+        if _newer(o, [s] + hdrs):
+            _run(["gcc", "-O2", "-fPIC", "-std=gnu11", "-Wall", "-Wno-unused-function",
+                  "-I", INC, "-I", CSRC, "-I", os.path.join(CUDA, "include"), "-c", s, "-o", o])
+    for src in CU_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(OBJ, src + ".o")
+        objs.append(o)
+        if _newer(o, [s] + hdrs):
+            _run([NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
+                                  "-I", INC, "-I", CSRC, "-c", s, "-o", o])
+    if _newer(LIB, objs):
+        _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs + ["-lm"])
+    if verbose:
+        print("built", LIB)
+    return LIB
+
+
+if __name__ == "__main__":
+    build(verbose=True)

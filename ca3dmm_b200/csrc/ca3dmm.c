@@ -1,0 +1,877 @@
+/* CA3DMM engine on one B200: the reference's mp x np x kp virtual process
+ * grid folded into one host call (src/ca3dmm.c:23-1410).
+ *
+ * Init reproduces the reference's grid choice and per-rank block arithmetic
+ * (src/ca3dmm.c:47-356 general, :468-642 B^T*B) and turns the active grid
+ * into work groups: one group per (task_k, task_m, task_n) Cannon task, whose
+ * np_dim^2 ranks' cuboid GEMMs tile one group GEMM
+ *     C_g = op(A)[task m rows, slab k] * op(B)[slab k, task n cols].
+ * Exec runs, on one stream:
+ *   1. pack op(A) blocks (task_m x task_k) and op(B) blocks (task_k x task_n)
+ *      into the work buffer, transposing on the way when trans_A / trans_B
+ *      (src/ca3dmm.c:970-1060: redistribution + cublasDgeam; replication by
+ *      allgather, :1062-1167, becomes groups reading the same packed block);
+ *   2. one grouped GEMM launch over all groups (src/cannon.c:319-684), plain
+ *      FP64 DMMA or split precision;
+ *   3. the kp-slab FP64 reduction in slab order (src/ca3dmm.c:1287-1343), or a
+ *      direct write when kp == 1;
+ *   4. a block copy into dst_C when a dst_C block other than the whole C was
+ *      requested (src/ca3dmm.c:1348-1364).
+ */
+#include <math.h>
+#include <stdint.h>
+#include <string.h>
+#include <cuda_runtime_api.h>
+#include "ca3dmm_util.h"
+#include "ca3dmm_kernels.h"
+#include "ca3dmm_ozaki.h"
+#include "ca3dmm.h"
+
+#define ALIGN_BYTES 256
+
+typedef struct {
+    int tk, tm, tn;        /* task ids */
+    int m0, n0, k0;        /* first row of op(A) / column of op(B) / k index */
+    int mz, nz, kz;        /* group GEMM size */
+    int a_blk, b_blk;      /* packed block indices */
+} group_t;
+
+typedef struct {
+    int rows, cols, r0, c0;   /* block of op(X): rows x cols starting at (r0, c0) */
+    long long ld;             /* leading dimension of the packed copy */
+    size_t off;               /* byte offset of the packed copy in the work buffer */
+} blk_t;
+
+typedef struct {
+    int ngroup, nA, nB;
+    group_t *groups;
+    blk_t *A, *B;
+    /* work buffer layout (byte offsets) */
+    size_t off_status, off_packA, off_packB, off_copy, off_gemm, off_ozplan;
+    size_t off_A, off_B, off_slab, off_cout, off_oz, total;
+    size_t gemm_plan_bytes, oz_plan_bytes, oz_bytes;
+    long long slab_ld;        /* leading dimension of each C slab */
+    size_t slab_stride;       /* elements between slabs */
+    /* pinned host staging for plan uploads */
+    void *stage;
+    size_t stage_bytes;
+    int *status_h;
+    /* cached exec arguments the device plan was built for */
+    int plan_valid, c_ldA, c_ldB, c_ldC;
+    const void *c_A, *c_B;
+    void *c_dst;
+    int gemm_tiles;
+    /* dst_C block */
+    int has_dst, dst_srow, dst_nrow, dst_scol, dst_ncol;
+    cudaEvent_t ev[5];
+    int events_ok;
+    ca3dmm_oz_plan_t oz;
+} plan_t;
+
+
+/* Geometry of one virtual rank (same 34-int layout as the oracle):
+ * src/ca3dmm.c:146-185 (task ids), :212-261 (block ranges, C_out),
+ * :298-346 (replication split of the redistribution request),
+ * src/cannon.c:68-77 (Cannon block of the rank's in-group coordinates). */
+static void vrank_geometry(int m, int n, int k, int mp, int np, int kp, int rank, int is_btb,
+                           int *out)
+{
+    memset(out, 0, sizeof(int) * 34);
+    if (rank >= mp * np * kp) return;
+    out[0] = 1;
+    const int plane = mp * np;
+    const int rank_k = rank / plane, rank_mn = rank % plane;
+    int tmn = 1, tmi = 0, tnn = 1, tni = 0, group = plane;
+    if (!is_btb && mp > np) { tmn = mp / np; tmi = rank_mn / (np * np); group = np * np; }
+    if (!is_btb && np > mp) { tnn = np / mp; tni = rank_mn / (mp * mp); group = mp * mp; }
+    out[1] = rank_mn % mp; out[2] = rank_mn / mp; out[3] = rank_k;
+    out[4] = tmn; out[5] = tmi; out[6] = tnn; out[7] = tni; out[8] = kp; out[9] = rank_k;
+    int ms, mz, ns, nz, ks, kz;
+    calc_block_spos_size(m, tmn, tmi, &ms, &mz);
+    calc_block_spos_size(n, tnn, tni, &ns, &nz);
+    calc_block_spos_size(k, kp, rank_k, &ks, &kz);
+    const int side = (int) sqrt((double) group);
+    const int in_group = rank_mn % group, row = in_group / side, col = in_group % side;
+    int a_r, a_rz, a_c, a_cz, b_r, b_rz, b_c, b_cz, c_r, c_rz, c_c, c_cz;
+    calc_block_spos_size(mz, side, row, &a_r, &a_rz);
+    calc_block_spos_size(kz, side, col, &a_c, &a_cz);
+    calc_block_spos_size(kz, side, row, &b_r, &b_rz);
+    calc_block_spos_size(nz, side, col, &b_c, &b_cz);
+    calc_block_spos_size(mz, side, row, &c_r, &c_rz);
+    calc_block_spos_size(nz, side, col, &c_c, &c_cz);
+    out[10] = ms + a_r; out[11] = ks + a_c; out[12] = a_rz; out[13] = a_cz;
+    out[14] = ks + b_r; out[15] = ns + b_c; out[16] = b_rz; out[17] = b_cz;
+    out[18] = ms + c_r; out[19] = ns + c_c; out[20] = c_rz; out[21] = c_cz;
+    int o_c, o_cz;
+    calc_block_spos_size(c_cz, kp, rank_k, &o_c, &o_cz);
+    out[22] = out[18]; out[23] = out[19] + o_c; out[24] = c_rz; out[25] = o_cz;
+    memcpy(out + 26, out + 10, 4 * sizeof(int));
+    memcpy(out + 30, out + 14, 4 * sizeof(int));
+    if (!is_btb && tnn > 1) {
+        int s, z;
+        calc_block_spos_size(out[13], tnn, tni, &s, &z);
+        out[27] = out[11] + s; out[29] = z;
+    }
+    if (!is_btb && tmn > 1) {
+        int s, z;
+        calc_block_spos_size(out[17], tmn, tmi, &s, &z);
+        out[31] = out[15] + s; out[33] = z;
+    }
+}
+
+static size_t align_up(size_t x) { return (x + ALIGN_BYTES - 1) / ALIGN_BYTES * ALIGN_BYTES; }
+
+/* Byte layout of the device work buffer for the current gemm mode. */
+static void plan_layout(ca3dmm_engine_p e, plan_t *pl)
+{
+    size_t off = 0;
+    pl->off_status = off; off = align_up(off + 64);
+    pl->off_packA = off; off = align_up(off + sizeof(ca3dmm_pack_desc_t) * pl->nA);
+    pl->off_packB = off; off = align_up(off + sizeof(ca3dmm_pack_desc_t) * pl->nB);
+    pl->off_copy = off; off = align_up(off + sizeof(ca3dmm_pack_desc_t));
+    pl->gemm_plan_bytes = ca3dmm_dgemm_plan_bytes(pl->ngroup);
+    pl->off_gemm = off; off = align_up(off + pl->gemm_plan_bytes);
+    pl->oz_plan_bytes = ca3dmm_oz_plan_bytes(pl->ngroup);
+    pl->off_ozplan = off; off = align_up(off + pl->oz_plan_bytes);
+    size_t packs = 0;
+    pl->off_A = off;
+    for (int i = 0; i < pl->nA; i++) {
+        pl->A[i].off = off + packs;
+        packs += align_up(sizeof(double) * (size_t) pl->A[i].ld * (size_t) pl->A[i].cols);
+    }
+    off += packs;
+    packs = 0;
+    pl->off_B = off;
+    for (int i = 0; i < pl->nB; i++) {
+        pl->B[i].off = off + packs;
+        packs += align_up(sizeof(double) * (size_t) pl->B[i].ld * (size_t) pl->B[i].cols);
+    }
+    off += packs;
+    pl->slab_ld = ca3dmm_round_up(e->m, 2);
+    pl->slab_stride = (size_t) pl->slab_ld * (size_t) e->n;
+    pl->off_slab = off;
+    if (e->kp > 1) off = align_up(off + sizeof(double) * pl->slab_stride * (size_t) e->kp);
+    pl->off_cout = off;
+    off = align_up(off + sizeof(double) * (size_t) e->m * (size_t) e->n);
+    pl->off_oz = off;
+    pl->oz_bytes = 0;
+    if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
+        int am[1024], ak[1024], bn[1024], bk[1024];
+        int na = pl->nA < 1024 ? pl->nA : 1024, nb = pl->nB < 1024 ? pl->nB : 1024;
+        for (int i = 0; i < na; i++) { am[i] = pl->A[i].rows; ak[i] = pl->A[i].cols; }
+        for (int i = 0; i < nb; i++) { bk[i] = pl->B[i].rows; bn[i] = pl->B[i].cols; }
+        pl->oz_bytes = ca3dmm_oz_work_bytes(na, am, ak, nb, bk, bn, e->ozaki_slices);
+        off = align_up(off + pl->oz_bytes);
+    }
+    pl->total = off;
+}
+
+static int plan_build(ca3dmm_engine_p e)
+{
+    plan_t *pl = (plan_t *) calloc(1, sizeof(plan_t));
+    if (!pl) return CA3DMM_ENOMEM;
+    e->impl = pl;
+    const int tmn = e->mp > e->np && !e->is_BTB ? e->mp / e->np : 1;
+    const int tnn = e->np > e->mp && !e->is_BTB ? e->np / e->mp : 1;
+    const int kp = e->kp;
+    pl->nA = tmn * kp;
+    pl->nB = tnn * kp;
+    pl->ngroup = kp * tmn * tnn;
+    pl->groups = (group_t *) calloc((size_t) pl->ngroup, sizeof(group_t));
+    pl->A = (blk_t *) calloc((size_t) pl->nA, sizeof(blk_t));
+    pl->B = (blk_t *) calloc((size_t) pl->nB, sizeof(blk_t));
+    if (!pl->groups || !pl->A || !pl->B) return CA3DMM_ENOMEM;
+    for (int tk = 0; tk < kp; tk++) {
+        int ks, kz;
+        calc_block_spos_size(e->k, kp, tk, &ks, &kz);
+        for (int tm = 0; tm < tmn; tm++) {
+            int ms, mz;
+            calc_block_spos_size(e->m, tmn, tm, &ms, &mz);
+            blk_t *a = &pl->A[tk * tmn + tm];
+            a->rows = mz; a->cols = kz; a->r0 = ms; a->c0 = ks;
+            a->ld = ca3dmm_round_up(mz > 0 ? mz : 1, 2);
+        }
+        for (int tn = 0; tn < tnn; tn++) {
+            int ns, nz;
+            calc_block_spos_size(e->n, tnn, tn, &ns, &nz);
+            blk_t *b = &pl->B[tk * tnn + tn];
+            b->rows = kz; b->cols = nz; b->r0 = ks; b->c0 = ns;
+            b->ld = ca3dmm_round_up(kz > 0 ? kz : 1, 2);
+        }
+        for (int tm = 0; tm < tmn; tm++)
+            for (int tn = 0; tn < tnn; tn++) {
+                group_t *g = &pl->groups[(tk * tmn + tm) * tnn + tn];
+                g->tk = tk; g->tm = tm; g->tn = tn;
+                g->a_blk = tk * tmn + tm;
+                g->b_blk = tk * tnn + tn;
+                g->m0 = pl->A[g->a_blk].r0; g->mz = pl->A[g->a_blk].rows;
+                g->n0 = pl->B[g->b_blk].c0; g->nz = pl->B[g->b_blk].cols;
+                g->k0 = ks; g->kz = kz;
+            }
+    }
+    plan_layout(e, pl);
+    pl->stage_bytes = pl->off_ozplan + pl->oz_plan_bytes;
+    return CA3DMM_OK;
+}
+
+/* CUDA-side resources of the plan, created when a work buffer is attached so
+ * that init itself makes no CUDA call (it only sizes the work buffer). */
+static int plan_cuda_init(plan_t *pl)
+{
+    if (pl->stage) return CA3DMM_OK;
+    if (cudaMallocHost(&pl->stage, pl->stage_bytes) != cudaSuccess) {
+        pl->stage = NULL;
+        return CA3DMM_ECUDA;
+    }
+    if (cudaMallocHost((void **) &pl->status_h, 64) != cudaSuccess) {
+        pl->status_h = NULL;
+        return CA3DMM_ECUDA;
+    }
+    memset(pl->status_h, 0, 64);
+    pl->events_ok = 1;
+    for (int i = 0; i < 5; i++)
+        if (cudaEventCreate(&pl->ev[i]) != cudaSuccess) pl->events_ok = 0;
+    return CA3DMM_OK;
+}
+
+static void plan_free(plan_t *pl)
+{
+    if (!pl) return;
+    free(pl->groups);
+    free(pl->A);
+    free(pl->B);
+    if (pl->stage) cudaFreeHost(pl->stage);
+    if (pl->status_h) cudaFreeHost(pl->status_h);
+    if (pl->events_ok)
+        for (int i = 0; i < 5; i++) cudaEventDestroy(pl->ev[i]);
+    free(pl);
+}
+
+/* Reference-style grid selection for the general engine (src/ca3dmm.c:47-136). */
+static int choose_grid(int p, int m, int n, int k, const int *proc_grid, int *mp, int *np, int *kp,
+                       int *rp)
+{
+    int gen = 1;
+    if (proc_grid != NULL) {
+        *mp = proc_grid[0]; *np = proc_grid[1]; *kp = proc_grid[2];
+        *rp = p - (*mp) * (*np) * (*kp);
+        int hi = *mp > *np ? *mp : *np, lo = *mp < *np ? *mp : *np;
+        if (lo < 1 || (hi % lo) || (*rp < 0))
+            WARNING_PRINTF("Invalid process grid specified: mp, np, kp = %d, %d, %d\n", *mp, *np,
+                           *kp);
+        else
+            gen = 0;
+    }
+    if (gen) {
+        calc_3d_decomposition_cannon(p, m, n, k, mp, np, kp, rp);
+        int reduce_kp;
+        GET_ENV_INT_VAR(reduce_kp, "CA3DMM_REDUCE_KP", "reduce_kp", 0, 0, 1);
+        if (reduce_kp) {
+            /* fold a factor 3 (else 2) of kp into the smaller of mp / np when
+             * the divisibility rule still holds (src/ca3dmm.c:75-124) */
+            int f = (*kp >= 3 && *kp % 3 == 0) ? 3 : ((*kp >= 2 && *kp % 2 == 0) ? 2 : 0);
+            if (f) {
+                int *grow = (*mp <= *np) ? mp : np, *other = (*mp <= *np) ? np : mp;
+                int g = *grow * f;
+                int hi = g > *other ? g : *other, lo = g < *other ? g : *other;
+                if (hi % lo == 0) {
+                    *kp /= f;
+                    *grow = g;
+                }
+            }
+        }
+    }
+    if (*mp < 1 || *np < 1 || *kp < 1 || (*mp) * (*np) * (*kp) > p) {
+        ERROR_PRINTF("Invalid process grid generated: p = %d, mp, np, kp = %d, %d, %d\n", p, *mp,
+                     *np, *kp);
+        return CA3DMM_EINVAL;
+    }
+    return CA3DMM_OK;
+}
+
+static void fill_rank0_fields(ca3dmm_engine_p e)
+{
+    int g[34];
+    vrank_geometry(e->m, e->n, e->k, e->mp, e->np, e->kp, 0, e->is_BTB, g);
+    e->is_active = g[0];
+    e->rank_m = g[1]; e->rank_n = g[2]; e->rank_k = g[3];
+    e->task_m_num = g[4]; e->task_m_id = g[5];
+    e->task_n_num = g[6]; e->task_n_id = g[7];
+    e->task_k_num = g[8]; e->task_k_id = g[9];
+    e->A_2dmm_srow = g[10]; e->A_2dmm_scol = g[11]; e->A_2dmm_nrow = g[12]; e->A_2dmm_ncol = g[13];
+    e->B_2dmm_srow = g[14]; e->B_2dmm_scol = g[15]; e->B_2dmm_nrow = g[16]; e->B_2dmm_ncol = g[17];
+    e->C_2dmm_srow = g[18]; e->C_2dmm_scol = g[19]; e->C_2dmm_nrow = g[20]; e->C_2dmm_ncol = g[21];
+    e->A_rd_srow = g[26]; e->A_rd_scol = g[27]; e->A_rd_nrow = g[28]; e->A_rd_ncol = g[29];
+    e->B_rd_srow = g[30]; e->B_rd_scol = g[31]; e->B_rd_nrow = g[32]; e->B_rd_ncol = g[33];
+    /* rank 0's reduce-scatter and allgather count arrays (src/ca3dmm.c:246-261, :298-336) */
+    int tk = e->task_k_num > 0 ? e->task_k_num : 1;
+    e->C_rs_recvcnts = (int *) calloc((size_t) tk, sizeof(int));
+    int s, z, z0 = -1;
+    e->use_rsb = 1;
+    for (int i = 0; i < e->task_k_num; i++) {
+        calc_block_spos_size(e->C_2dmm_ncol, e->task_k_num, i, &s, &z);
+        if (z0 == -1) z0 = z;
+        if (z != z0) e->use_rsb = 0;
+        e->C_rs_recvcnts[i] = z * e->C_2dmm_nrow;
+    }
+    int tmn = e->task_m_num * e->task_n_num;
+    if (tmn < 1) tmn = 1;
+    e->AB_agv_recvcnts = (int *) calloc((size_t) tmn, sizeof(int));
+    e->AB_agv_displs = (int *) calloc((size_t) tmn + 1, sizeof(int));
+    if (e->task_n_num > 1 || e->task_m_num > 1) {
+        int nt = e->task_n_num > 1 ? e->task_n_num : e->task_m_num;
+        int ncol = e->task_n_num > 1 ? e->A_2dmm_ncol : e->B_2dmm_ncol;
+        int nrow = e->task_n_num > 1 ? e->A_2dmm_nrow : e->B_2dmm_nrow;
+        z0 = -1;
+        e->use_ag = 1;
+        for (int i = 0; i < nt; i++) {
+            calc_block_spos_size(ncol, nt, i, &s, &z);
+            if (z0 == -1) z0 = z;
+            if (z != z0) e->use_ag = 0;
+            e->AB_agv_recvcnts[i] = z * nrow;
+            e->AB_agv_displs[i + 1] = e->AB_agv_displs[i] + e->AB_agv_recvcnts[i];
+        }
+    }
+    e->C_out_srow = 0; e->C_out_scol = 0; e->C_out_nrow = e->m; e->C_out_ncol = e->n;
+}
+
+/* Shared tail of both init functions: plan, sizes, optional allocation. */
+static void finish_init(ca3dmm_engine_p e, int dst_srow, int dst_nrow, int dst_scol, int dst_ncol,
+                        ca3dmm_engine_p *engine_, size_t *workbuf_bytes, double t0)
+{
+    fill_rank0_fields(e);
+    /* rank 0's Cannon geometry, for callers that read engine->cannon_engine */
+    e->cannon_engine = (cannon_engine_p) calloc(1, sizeof(cannon_engine_s));
+    if (e->cannon_engine) {
+        cannon_engine_p ce = e->cannon_engine;
+        int side = (int) sqrt((double) (e->is_BTB ? e->mp * e->np
+                                                  : (e->mp > e->np ? e->np * e->np : e->mp * e->mp)));
+        if (side < 1) side = 1;
+        int ms, mz, ns, nz, ks, kz;
+        calc_block_spos_size(e->m, e->task_m_num, 0, &ms, &mz);
+        calc_block_spos_size(e->n, e->task_n_num, 0, &ns, &nz);
+        calc_block_spos_size(e->k, e->kp, 0, &ks, &kz);
+        ce->m = mz; ce->n = nz; ce->k = kz; ce->np_dim = side; ce->dev_type = e->dev_type;
+        ce->A_srow = e->A_2dmm_srow - ms; ce->A_scol = e->A_2dmm_scol - ks;
+        ce->A_nrow = e->A_2dmm_nrow; ce->A_ncol = e->A_2dmm_ncol;
+        ce->B_srow = e->B_2dmm_srow - ks; ce->B_scol = e->B_2dmm_scol - ns;
+        ce->B_nrow = e->B_2dmm_nrow; ce->B_ncol = e->B_2dmm_ncol;
+        ce->C_srow = e->C_2dmm_srow - ms; ce->C_scol = e->C_2dmm_scol - ns;
+        ce->C_nrow = e->C_2dmm_nrow; ce->C_ncol = e->C_2dmm_ncol;
+        ce->max_A_blk_size = (mz / side + 1) * (kz / side + 1);
+        ce->max_B_blk_size = (kz / side + 1) * (nz / side + 1);
+        ce->max_C_blk_size = (mz / side + 1) * (nz / side + 1);
+        ce->gemm_cycle = 1;
+    }
+    int gm;
+    GET_ENV_INT_VAR(gm, "CA3DMM_GEMM_MODE", "gemm_mode", 0, 0, 1);
+    e->gemm_mode = gm;
+    int sl;
+    GET_ENV_INT_VAR(sl, "CA3DMM_OZAKI_SLICES", "ozaki_slices", 7, 2, 8);
+    e->ozaki_slices = sl;
+    e->sync_exec = 1;
+    int rc = plan_build(e);
+    if (rc) {
+        ERROR_PRINTF("Failed to build the device plan (error %d)\n", rc);
+        ca3dmm_engine_free(&e);
+        return;
+    }
+    plan_t *pl = (plan_t *) e->impl;
+    if (!((dst_srow == -1) || (dst_nrow == -1) || (dst_scol == -1) || (dst_ncol == -1))) {
+        if (dst_srow < 0 || dst_scol < 0 || dst_nrow < 0 || dst_ncol < 0 ||
+            dst_srow + dst_nrow > e->m || dst_scol + dst_ncol > e->n) {
+            ERROR_PRINTF("Invalid dst_C block: (%d, %d) + %d x %d for a %d x %d C\n", dst_srow,
+                         dst_scol, dst_nrow, dst_ncol, e->m, e->n);
+            ca3dmm_engine_free(&e);
+            return;
+        }
+        pl->has_dst = 1;
+        pl->dst_srow = dst_srow; pl->dst_nrow = dst_nrow;
+        pl->dst_scol = dst_scol; pl->dst_ncol = dst_ncol;
+    }
+    e->n_group = pl->ngroup;
+    e->workbuf_bytes = pl->total;
+    e->self_workbuf_bytes = pl->total;
+    GET_ENV_INT_VAR(e->print_timing, "CA3DMM_PRINT_TIMING", "engine->print_timing", 0, 0, 1);
+    if (workbuf_bytes != NULL) {
+        e->alloc_workbuf = 0;
+        *workbuf_bytes = pl->total;
+    } else {
+        e->alloc_workbuf = 1;
+        void *wh = NULL, *wd = NULL;
+        MALLOC_ATTACH_WORKBUF(ca3dmm_engine_attach_workbuf, ca3dmm_engine_free, e, e->dev_type,
+                              pl->total, wh, wd);
+        if (e == NULL) return;
+    }
+    e->init_ms = 1000.0 * (ca3dmm_wtime_sec() - t0);
+    *engine_ = e;
+}
+
+void ca3dmm_engine_init(const int m, const int n, const int k, const int trans_A,
+                        const int trans_B, const int src_A_srow, const int src_A_nrow,
+                        const int src_A_scol, const int src_A_ncol, const int src_B_srow,
+                        const int src_B_nrow, const int src_B_scol, const int src_B_ncol,
+                        const int dst_C_srow, const int dst_C_nrow, const int dst_C_scol,
+                        const int dst_C_ncol, const int *proc_grid, MPI_Comm comm,
+                        dev_type_t dev_type, ca3dmm_engine_p *engine_, size_t *workbuf_bytes)
+{
+    if (engine_ == NULL) return;
+    *engine_ = NULL;
+    if (is_dev_type_valid(dev_type) == 0) {
+        ERROR_PRINTF("Invalid device type %d\n", dev_type);
+        return;
+    }
+    int p = ca3dmm_vcomm_size(comm);
+    if (p < 1) {
+        ERROR_PRINTF("Invalid communicator\n");
+        return;
+    }
+    if (m < 1 || n < 1 || k < 1) {
+        ERROR_PRINTF("Invalid matrix size m, n, k = %d, %d, %d\n", m, n, k);
+        return;
+    }
+    const int a_nrow = trans_A ? k : m, a_ncol = trans_A ? m : k;
+    const int b_nrow = trans_B ? n : k, b_ncol = trans_B ? k : n;
+    if (src_A_srow != 0 || src_A_scol != 0 || src_A_nrow != a_nrow || src_A_ncol != a_ncol ||
+        src_B_srow != 0 || src_B_scol != 0 || src_B_nrow != b_nrow || src_B_ncol != b_ncol) {
+        ERROR_PRINTF("Folded call: src_A / src_B must describe the whole %d x %d A and %d x %d B\n",
+                     a_nrow, a_ncol, b_nrow, b_ncol);
+        return;
+    }
+    double t0 = ca3dmm_wtime_sec();
+    ca3dmm_engine_p e = (ca3dmm_engine_p) calloc(1, sizeof(ca3dmm_engine_s));
+    if (!e) return;
+    e->m = m; e->n = n; e->k = k;
+    e->n_proc = p;
+    e->my_rank = 0;
+    e->trans_A = trans_A ? 1 : 0;
+    e->trans_B = trans_B ? 1 : 0;
+    e->dev_type = dev_type;
+    int mp, np, kp, rp;
+    if (choose_grid(p, m, n, k, proc_grid, &mp, &np, &kp, &rp)) {
+        ca3dmm_engine_free(&e);
+        return;
+    }
+    e->mp = mp; e->np = np; e->kp = kp; e->rp = rp;
+    e->is_BTB = 0;
+    finish_init(e, dst_C_srow, dst_C_nrow, dst_C_scol, dst_C_ncol, engine_, workbuf_bytes, t0);
+}
+
+void ca3dmm_engine_init_BTB(const int n, const int k, const int src_B_srow, const int src_B_nrow,
+                            const int src_B_scol, const int src_B_ncol, const int dst_C_srow,
+                            const int dst_C_nrow, const int dst_C_scol, const int dst_C_ncol,
+                            const int *proc_grid, MPI_Comm comm, dev_type_t dev_type,
+                            ca3dmm_engine_p *engine_, size_t *workbuf_bytes)
+{
+    if (engine_ == NULL) return;
+    *engine_ = NULL;
+    if (is_dev_type_valid(dev_type) == 0) {
+        ERROR_PRINTF("Invalid device type %d\n", dev_type);
+        return;
+    }
+    int p = ca3dmm_vcomm_size(comm);
+    if (p < 1 || n < 1 || k < 1) {
+        ERROR_PRINTF("Invalid communicator or size n, k = %d, %d\n", n, k);
+        return;
+    }
+    if (src_B_srow != 0 || src_B_scol != 0 || src_B_nrow != k || src_B_ncol != n) {
+        ERROR_PRINTF("Folded call: src_B must describe the whole %d x %d B\n", k, n);
+        return;
+    }
+    double t0 = ca3dmm_wtime_sec();
+    ca3dmm_engine_p e = (ca3dmm_engine_p) calloc(1, sizeof(ca3dmm_engine_s));
+    if (!e) return;
+    e->m = n; e->n = n; e->k = k;
+    e->n_proc = p;
+    e->dev_type = dev_type;
+    int mp, np, kp, rp, gen = 1;
+    if (proc_grid != NULL) {
+        mp = proc_grid[0]; np = proc_grid[1]; kp = proc_grid[2];
+        rp = p - mp * np * kp;
+        if ((mp != np) || (rp < 0))
+            WARNING_PRINTF("Invalid process grid specified: mp, np, kp = %d, %d, %d\n", mp, np, kp);
+        else
+            gen = 0;
+    }
+    if (gen) {
+        /* src/ca3dmm.c:492-502: n x n x k planner, then (default on) fold a
+         * factor 4 of kp into a 2 x 2 larger mn-plane */
+        calc_3d_decomposition_nk(p, n, k, &np, &kp, &rp);
+        int reduce_kp;
+        GET_ENV_INT_VAR(reduce_kp, "CA3DMM_REDUCE_KP", "reduce_kp", 1, 0, 1);
+        if (reduce_kp && kp >= 4 && kp % 4 == 0) {
+            kp /= 4;
+            np *= 2;
+        }
+    }
+    mp = np;
+    if (mp < 1 || np < 1 || kp < 1 || mp * np * kp > p) {
+        ERROR_PRINTF("3D decomposition function error: p = %d, mp, np, kp = %d, %d, %d\n", p, mp,
+                     np, kp);
+        free(e);
+        return;
+    }
+    e->mp = mp; e->np = np; e->kp = kp; e->rp = rp;
+    e->is_BTB = 1;
+    e->trans_A = 1;   /* op(A) = B^T, read from B */
+    e->trans_B = 0;
+    finish_init(e, dst_C_srow, dst_C_nrow, dst_C_scol, dst_C_ncol, engine_, workbuf_bytes, t0);
+}
+
+void ca3dmm_engine_attach_workbuf(ca3dmm_engine_p e, void *workbuf_h, void *workbuf_d)
+{
+    if (e == NULL) return;
+    plan_t *pl = (plan_t *) e->impl;
+    e->workbuf_h = workbuf_h;
+    e->workbuf_d = workbuf_d;
+    if (workbuf_d == NULL) {
+        ERROR_PRINTF("A device work buffer is required\n");
+        e->last_error = CA3DMM_EINVAL;
+        return;
+    }
+    if (plan_cuda_init(pl) != CA3DMM_OK) {
+        ERROR_PRINTF("Failed to create the engine's CUDA resources\n");
+        e->last_error = CA3DMM_ECUDA;
+        return;
+    }
+    char *w = (char *) workbuf_d;
+    e->A_rd_recv_d = w + pl->off_A;
+    e->A_trans_d = e->A_rd_recv_d;
+    e->A_2dmm_d = e->A_rd_recv_d;
+    e->B_rd_recv_d = w + pl->off_B;
+    e->B_trans_d = e->B_rd_recv_d;
+    e->B_2dmm_d = e->B_rd_recv_d;
+    e->C_2dmm_d = e->kp > 1 ? (void *) (w + pl->off_slab) : NULL;
+    e->C_out_d = w + pl->off_cout;
+    pl->plan_valid = 0;
+}
+
+void ca3dmm_engine_free(ca3dmm_engine_p *engine_)
+{
+    if (engine_ == NULL || *engine_ == NULL) return;
+    ca3dmm_engine_p e = *engine_;
+    free(e->AB_agv_recvcnts);
+    free(e->AB_agv_displs);
+    free(e->C_rs_recvcnts);
+    if (e->alloc_workbuf && e->workbuf_d) dev_type_free(e->workbuf_d, DEV_TYPE_CUDA);
+    free(e->cannon_engine);
+    plan_free((plan_t *) e->impl);
+    free(e);
+    *engine_ = NULL;
+}
+
+/* Build the per-call device plan into pinned staging and upload it. */
+static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B, int ldB,
+                       void *dst, int ldC, cudaStream_t st)
+{
+    plan_t *pl = (plan_t *) e->impl;
+    char *w = (char *) e->workbuf_d, *h = (char *) pl->stage;
+    ca3dmm_pack_desc_t *pa = (ca3dmm_pack_desc_t *) (h + pl->off_packA);
+    for (int i = 0; i < pl->nA; i++) {
+        blk_t *b = &pl->A[i];
+        ca3dmm_pack_desc_t *d = &pa[i];
+        memset(d, 0, sizeof(*d));
+        d->rows = b->rows; d->cols = b->cols; d->trans = e->trans_A; d->lds = ldA;
+        d->src_off = e->trans_A ? (long long) b->c0 + (long long) b->r0 * ldA
+                                : (long long) b->r0 + (long long) b->c0 * ldA;
+        d->dst_off = (long long) ((b->off) / sizeof(double));
+        d->ldd = b->ld;
+    }
+    ca3dmm_pack_desc_t *pb = (ca3dmm_pack_desc_t *) (h + pl->off_packB);
+    for (int i = 0; i < pl->nB; i++) {
+        blk_t *b = &pl->B[i];
+        ca3dmm_pack_desc_t *d = &pb[i];
+        memset(d, 0, sizeof(*d));
+        d->rows = b->rows; d->cols = b->cols; d->trans = e->trans_B; d->lds = ldB;
+        d->src_off = e->trans_B ? (long long) b->c0 + (long long) b->r0 * ldB
+                                : (long long) b->r0 + (long long) b->c0 * ldB;
+        d->dst_off = (long long) ((b->off) / sizeof(double));
+        d->ldd = b->ld;
+    }
+    /* output target of the GEMM (kp == 1) or of the reduction (kp > 1) */
+    int whole = pl->has_dst && pl->dst_srow == 0 && pl->dst_scol == 0 && pl->dst_nrow == e->m &&
+                pl->dst_ncol == e->n;
+    double *out = whole ? (double *) dst : (double *) (w + pl->off_cout);
+    long long ldo = whole ? ldC : e->m;
+    ca3dmm_pack_desc_t *pc = (ca3dmm_pack_desc_t *) (h + pl->off_copy);
+    memset(pc, 0, sizeof(*pc));
+    if (pl->has_dst && !whole) {
+        pc->rows = pl->dst_nrow; pc->cols = pl->dst_ncol; pc->lds = e->m; pc->ldd = ldC;
+        pc->src_off = (long long) pl->dst_srow + (long long) pl->dst_scol * e->m;
+    }
+    ca3dmm_dgemm_desc_t gd[4096];
+    if (pl->ngroup > 4096) return CA3DMM_EINVAL;
+    for (int i = 0; i < pl->ngroup; i++) {
+        group_t *g = &pl->groups[i];
+        ca3dmm_dgemm_desc_t *q = &gd[i];
+        q->A = (const double *) (w + pl->A[g->a_blk].off);
+        q->lda = pl->A[g->a_blk].ld;
+        q->B = (const double *) (w + pl->B[g->b_blk].off);
+        q->ldb = pl->B[g->b_blk].ld;
+        if (e->kp > 1) {
+            q->C = (double *) (w + pl->off_slab) + (size_t) g->tk * pl->slab_stride + g->m0 +
+                   (size_t) g->n0 * pl->slab_ld;
+            q->ldc = pl->slab_ld;
+        } else {
+            q->C = out + g->m0 + (size_t) g->n0 * ldo;
+            q->ldc = ldo;
+        }
+        q->m = g->mz; q->n = g->nz; q->k = g->kz;
+        q->alpha = 1.0; q->beta = 0.0;
+    }
+    int rc = ca3dmm_dgemm_plan_encode(gd, pl->ngroup, h + pl->off_gemm, &pl->gemm_tiles);
+    if (rc) return rc;
+    if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
+        ca3dmm_oz_blk_t ob[2048];
+        ca3dmm_oz_group_t og[4096];
+        if (pl->nA + pl->nB > 2048) return CA3DMM_EINVAL;
+        for (int i = 0; i < pl->nA; i++) {
+            ob[i].r0 = pl->A[i].r0; ob[i].c0 = pl->A[i].c0;
+            ob[i].rows = pl->A[i].rows; ob[i].cols = pl->A[i].cols;
+        }
+        for (int i = 0; i < pl->nB; i++) {
+            ob[pl->nA + i].r0 = pl->B[i].r0; ob[pl->nA + i].c0 = pl->B[i].c0;
+            ob[pl->nA + i].rows = pl->B[i].rows; ob[pl->nA + i].cols = pl->B[i].cols;
+        }
+        for (int i = 0; i < pl->ngroup; i++) {
+            og[i].a_blk = pl->groups[i].a_blk; og[i].b_blk = pl->groups[i].b_blk;
+            og[i].C = gd[i].C; og[i].ldc = gd[i].ldc;
+            og[i].m = gd[i].m; og[i].n = gd[i].n; og[i].k = gd[i].k;
+        }
+        rc = ca3dmm_oz_plan_encode(&pl->oz, e->ozaki_slices, pl->nA, ob, pl->nB, ob + pl->nA,
+                                   pl->ngroup, og, w + pl->off_oz, pl->oz_bytes,
+                                   h + pl->off_ozplan, w + pl->off_ozplan);
+        if (rc) return rc;
+    }
+    memset(h + pl->off_status, 0, 64);
+    if (cudaMemcpyAsync(w, h, pl->stage_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return CA3DMM_ECUDA;
+    pl->c_A = A; pl->c_B = B; pl->c_ldA = ldA; pl->c_ldB = ldB;
+    pl->c_dst = dst; pl->c_ldC = ldC;
+    pl->plan_valid = 1;
+    return CA3DMM_OK;
+}
+
+static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void *src_B, int ldB,
+                       void *dst_C, int ldC, cudaStream_t st)
+{
+    plan_t *pl = (plan_t *) e->impl;
+    char *w = (char *) e->workbuf_d;
+    if (e->is_BTB) { src_A = src_B; ldA = ldB; }
+    const int a_rows = e->trans_A ? e->k : e->m, b_rows = e->trans_B ? e->n : e->k;
+    if (!src_A || !src_B || ldA < a_rows || ldB < b_rows) {
+        ERROR_PRINTF("Invalid operands: ldA = %d (>= %d), ldB = %d (>= %d)\n", ldA, a_rows, ldB,
+                     b_rows);
+        return CA3DMM_EINVAL;
+    }
+    if (pl->has_dst && (dst_C == NULL || ldC < pl->dst_nrow)) {
+        ERROR_PRINTF("Invalid dst_C / ldC = %d (>= %d)\n", ldC, pl->dst_nrow);
+        return CA3DMM_EINVAL;
+    }
+    int rc;
+    if (!pl->plan_valid || pl->c_ldA != ldA || pl->c_ldB != ldB || pl->c_dst != dst_C ||
+        pl->c_ldC != ldC) {
+        rc = plan_upload(e, src_A, ldA, src_B, ldB, dst_C, ldC, st);
+        if (rc) return rc;
+    } else if (cudaMemsetAsync(w + pl->off_status, 0, 64, st) != cudaSuccess) {
+        return CA3DMM_ECUDA;
+    }
+    int timing = e->sync_exec && pl->events_ok;
+    if (timing) cudaEventRecord(pl->ev[0], st);
+    int max_r = 1, max_c = 1;
+    for (int i = 0; i < pl->nA; i++) {
+        if (pl->A[i].rows > max_r) max_r = pl->A[i].rows;
+        if (pl->A[i].cols > max_c) max_c = pl->A[i].cols;
+    }
+    if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
+        rc = ca3dmm_oz_run_pack(&pl->oz, src_A, ldA, e->trans_A, src_B, ldB, e->trans_B, st);
+        if (rc) return rc;
+    } else {
+        rc = ca3dmm_pack_launch((const double *) src_A, (double *) w,
+                                (const ca3dmm_pack_desc_t *) (w + pl->off_packA), pl->nA, max_r,
+                                max_c, e->trans_A, st);
+        if (rc) return rc;
+        max_r = 1; max_c = 1;
+        for (int i = 0; i < pl->nB; i++) {
+            if (pl->B[i].rows > max_r) max_r = pl->B[i].rows;
+            if (pl->B[i].cols > max_c) max_c = pl->B[i].cols;
+        }
+        rc = ca3dmm_pack_launch((const double *) src_B, (double *) w,
+                                (const ca3dmm_pack_desc_t *) (w + pl->off_packB), pl->nB, max_r,
+                                max_c, e->trans_B, st);
+        if (rc) return rc;
+    }
+    if (timing) cudaEventRecord(pl->ev[1], st);
+    int *status_d = (int *) (w + pl->off_status);
+    if (e->gemm_mode == CA3DMM_GEMM_OZAKI)
+        rc = ca3dmm_oz_run_gemm(&pl->oz, status_d, 5.0, st);
+    else
+        rc = ca3dmm_dgemm_launch(w + pl->off_gemm, pl->ngroup, pl->gemm_tiles, status_d, 5.0, st);
+    if (rc) return rc;
+    if (timing) cudaEventRecord(pl->ev[2], st);
+    int whole = pl->has_dst && pl->dst_srow == 0 && pl->dst_scol == 0 && pl->dst_nrow == e->m &&
+                pl->dst_ncol == e->n;
+    double *out = whole ? (double *) dst_C : (double *) (w + pl->off_cout);
+    long long ldo = whole ? ldC : e->m;
+    if (e->kp > 1) {
+        rc = ca3dmm_reduce_slabs_launch((const double *) (w + pl->off_slab),
+                                        (long long) pl->slab_stride, pl->slab_ld, e->kp, e->m,
+                                        e->n, out, ldo, st);
+        if (rc) return rc;
+    }
+    if (timing) cudaEventRecord(pl->ev[3], st);
+    if (pl->has_dst && !whole) {
+        rc = ca3dmm_pack_launch((const double *) (w + pl->off_cout), (double *) dst_C,
+                                (const ca3dmm_pack_desc_t *) (w + pl->off_copy), 1, pl->dst_nrow,
+                                pl->dst_ncol, 0, st);
+        if (rc) return rc;
+    }
+    if (timing) cudaEventRecord(pl->ev[4], st);
+    if (cudaMemcpyAsync(pl->status_h, status_d, sizeof(int), cudaMemcpyDeviceToHost, st) !=
+        cudaSuccess)
+        return CA3DMM_ECUDA;
+    if (e->sync_exec) {
+        if (cudaStreamSynchronize(st) != cudaSuccess) return CA3DMM_ECUDA;
+        if (pl->status_h[0] != 0) {
+            ERROR_PRINTF("Device status %d: a bounded wait ran out\n", pl->status_h[0]);
+            return CA3DMM_ETIMEOUT;
+        }
+        if (timing) {
+            float t_pack = 0, t_gemm = 0, t_red = 0, t_copy = 0;
+            cudaEventElapsedTime(&t_pack, pl->ev[0], pl->ev[1]);
+            cudaEventElapsedTime(&t_gemm, pl->ev[1], pl->ev[2]);
+            cudaEventElapsedTime(&t_red, pl->ev[2], pl->ev[3]);
+            cudaEventElapsedTime(&t_copy, pl->ev[3], pl->ev[4]);
+            e->redist_ms += t_pack + t_copy;
+            e->cannon_ms += t_gemm;
+            e->reduce_ms += t_red;
+            if (e->cannon_engine) {
+                e->cannon_engine->gemm_ms += t_gemm;
+                e->cannon_engine->exec_ms += t_gemm;
+                e->cannon_engine->n_exec++;
+            }
+            if (e->print_timing) {
+                INFO_PRINTF("Redistribute A & B time = %.2f ms\n", t_pack);
+                INFO_PRINTF("2D Cannon time          = %.2f ms\n", t_gemm);
+                INFO_PRINTF("Reduce-scatter C time   = %.2f ms\n", t_red);
+                INFO_PRINTF("Redistribute C time     = %.2f ms\n", t_copy);
+            }
+        }
+    }
+    return CA3DMM_OK;
+}
+
+void ca3dmm_engine_exec(ca3dmm_engine_p e, const void *src_A, const int ldA, const void *src_B,
+                        const int ldB, void *dst_C, const int ldC)
+{
+    if (e == NULL) {
+        ERROR_PRINTF("ca3dmm_engine not initialized\n");
+        return;
+    }
+    if (e->workbuf_d == NULL || ((plan_t *) e->impl)->stage == NULL) {
+        ERROR_PRINTF("ca3dmm_engine has no device work buffer attached\n");
+        e->last_error = CA3DMM_EINVAL;
+        return;
+    }
+    double t0 = ca3dmm_wtime_sec();
+    int rc = exec_device(e, src_A, ldA, src_B, ldB, dst_C, ldC, (cudaStream_t) e->stream);
+    e->last_error = rc;
+    if (rc) {
+        ERROR_PRINTF("ca3dmm_engine_exec failed (error %d)\n", rc);
+        return;
+    }
+    if (e->sync_exec) {
+        double ms = 1000.0 * (ca3dmm_wtime_sec() - t0);
+        e->exec_ms += ms;
+        e->n_exec++;
+        if (e->print_timing) INFO_PRINTF("CA3DMM exec time        = %.2f ms\n\n", ms);
+    }
+}
+
+void ca3dmm_engine_reset_stat(ca3dmm_engine_p e)
+{
+    if (e == NULL) return;
+    cannon_engine_reset_stat(e->cannon_engine);
+    e->redist_ms = 0.0;
+    e->agvAB_ms = 0.0;
+    e->cannon_ms = 0.0;
+    e->reduce_ms = 0.0;
+    e->hd_trans_ms = 0.0;
+    e->exec_ms = 0.0;
+    e->n_exec = 0;
+}
+
+void ca3dmm_engine_print_stat(ca3dmm_engine_p e)
+{
+    if (e == NULL) return;
+    if (e->n_exec == 0) {
+        WARNING_PRINTF("No ca3dmm_engine statistic data to print\n");
+        return;
+    }
+    printf("================== CA3DMM algorithm engine =================\n");
+    printf("* Initialization         : %.2f ms\n", e->init_ms);
+    printf("* Number of executions   : %d\n", e->n_exec);
+    printf("* Execution time (avg)   : %.2f ms\n", e->exec_ms / e->n_exec);
+    printf("  * Redistribute A, B, C : %.2f ms\n", e->redist_ms / e->n_exec);
+    printf("  * Allgather A or B     : %.2f ms\n", e->agvAB_ms / e->n_exec);
+    printf("  * 2D Cannon execution  : %.2f ms\n", e->cannon_ms / e->n_exec);
+    printf("  * Reduce-scatter C     : %.2f ms\n", e->reduce_ms / e->n_exec);
+    double gf = 2.0 * (double) e->m * (double) e->n * (double) e->k / (e->cannon_ms / e->n_exec) /
+                1e6;
+    printf("* GEMM throughput        : %.2f GFlops (%s)\n", gf,
+           e->gemm_mode == CA3DMM_GEMM_OZAKI ? "split precision" : "FP64 DMMA");
+    printf("============================================================\n");
+}
+
+int ca3dmm_engine_last_error(ca3dmm_engine_p e) { return e ? e->last_error : CA3DMM_EINVAL; }
+
+void ca3dmm_engine_set_stream(ca3dmm_engine_p e, void *stream, int sync)
+{
+    if (!e) return;
+    e->stream = stream;
+    e->sync_exec = sync ? 1 : 0;
+}
+
+int ca3dmm_engine_set_gemm_mode(ca3dmm_engine_p e, int mode, int slices)
+{
+    if (!e) return CA3DMM_EINVAL;
+    if (mode != CA3DMM_GEMM_PLAIN && mode != CA3DMM_GEMM_OZAKI) return CA3DMM_EINVAL;
+    if (mode == CA3DMM_GEMM_OZAKI && (slices < 2 || slices > 8)) return CA3DMM_EINVAL;
+    plan_t *pl = (plan_t *) e->impl;
+    int old_mode = e->gemm_mode, old_sl = e->ozaki_slices;
+    e->gemm_mode = mode;
+    if (mode == CA3DMM_GEMM_OZAKI) e->ozaki_slices = slices;
+    size_t old_total = pl->total;
+    plan_layout(e, pl);
+    if (e->workbuf_d != NULL && pl->total > old_total) {
+        if (!e->alloc_workbuf) {
+            /* the caller's buffer is too small: keep the old mode */
+            e->gemm_mode = old_mode;
+            e->ozaki_slices = old_sl;
+            plan_layout(e, pl);
+            return CA3DMM_ENOMEM;
+        }
+        void *nw = dev_type_malloc(pl->total, DEV_TYPE_CUDA);
+        if (!nw) {
+            e->gemm_mode = old_mode;
+            e->ozaki_slices = old_sl;
+            plan_layout(e, pl);
+            return CA3DMM_ENOMEM;
+        }
+        dev_type_free(e->workbuf_d, DEV_TYPE_CUDA);
+        ca3dmm_engine_attach_workbuf(e, NULL, nw);
+    }
+    if (pl->total < old_total) pl->total = old_total;   /* keep the larger layout's size */
+    e->workbuf_bytes = pl->total;
+    pl->plan_valid = 0;
+    return CA3DMM_OK;
+}
+
+size_t ca3dmm_engine_workbuf_bytes(ca3dmm_engine_p e) { return e ? e->workbuf_bytes : 0; }
+
+int ca3dmm_engine_vrank_info(ca3dmm_engine_p e, int vrank, int *out34)
+{
+    if (!e || !out34 || vrank < 0 || vrank >= e->n_proc) return CA3DMM_EINVAL;
+    vrank_geometry(e->m, e->n, e->k, e->mp, e->np, e->kp, vrank, e->is_BTB, out34);
+    return CA3DMM_OK;
+}

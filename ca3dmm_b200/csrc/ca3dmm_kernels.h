@@ -1,0 +1,76 @@
+/* Internal C ABI between the C host engine and the sm_100a kernels.
+ * Plain pointers and sizes only; every launcher returns 0 or a CA3DMM_E*
+ * error code and never exits the process. */
+#ifndef CA3DMM_KERNELS_H
+#define CA3DMM_KERNELS_H
+
+#include <stddef.h>
+#include <stdint.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+    CA3DMM_OK = 0,
+    CA3DMM_EINVAL = 1,       /* bad argument (size, alignment, mode) */
+    CA3DMM_ECUDA = 2,        /* a CUDA runtime / driver call failed */
+    CA3DMM_ETIMEOUT = 3,     /* a device-side bounded wait ran out */
+    CA3DMM_ENOMEM = 4,       /* work buffer too small / allocation failed */
+    CA3DMM_ENODEV = 5,       /* no sm_100 device or driver entry point missing */
+};
+
+/* ---- plain FP64 DMMA GEMM, grouped ---------------------------------------
+ * One problem: C = alpha * op(A) op(B) + beta * C, where the operands are
+ * already packed by the pack kernels:
+ *   A: op(A) stored M-major, element (i,l) at A[i + l*lda]   (lda even, A 16B-aligned)
+ *   B: op(B) stored K-major, element (l,j) at B[l + j*ldb]   (ldb even, B 16B-aligned)
+ *   C: column-major, element (i,j) at C[i + j*ldc]           (any ldc >= m)      */
+typedef struct {
+    const double *A; long long lda;
+    const double *B; long long ldb;
+    double *C; long long ldc;
+    int m, n, k;
+    double alpha, beta;
+} ca3dmm_dgemm_desc_t;
+
+/* Bytes of the device plan for nprob problems (tensor maps + problem records). */
+size_t ca3dmm_dgemm_plan_bytes(int nprob);
+/* Encode the plan into host memory `host_plan` (size plan_bytes); the caller
+ * copies it to device memory `dev_plan` before launching.  Tensor maps embed
+ * the device addresses of A and B.  Returns the total tile count. */
+int ca3dmm_dgemm_plan_encode(const ca3dmm_dgemm_desc_t *probs, int nprob, void *host_plan,
+                             int *total_tiles);
+/* Persistent grouped launch over every tile of every problem. */
+int ca3dmm_dgemm_launch(const void *dev_plan, int nprob, int total_tiles, int *dev_status,
+                        double timeout_s, cudaStream_t stream);
+
+/* ---- pack / transpose ----------------------------------------------------
+ * Batched block copies between column-major matrices.  Descriptor j copies a
+ * rows x cols block: dst[r + c*ldd] = trans ? src[c + r*lds] : src[r + c*lds],
+ * with src = src_base + src_off (elements) and dst = dst_base + dst_off. */
+typedef struct {
+    long long src_off, lds;
+    long long dst_off, ldd;
+    int rows, cols, trans, pad;
+} ca3dmm_pack_desc_t;
+
+int ca3dmm_pack_launch(const double *src_base, double *dst_base,
+                       const ca3dmm_pack_desc_t *dev_descs, int ndesc, int max_rows, int max_cols,
+                       int any_trans, cudaStream_t stream);
+
+/* ---- kp-slab reduction ---------------------------------------------------
+ * out[i + j*ldo] = sum_{s=0}^{nslab-1} slab[s*slab_stride + i + j*lds]
+ * (summed in slab order 0,1,...). */
+int ca3dmm_reduce_slabs_launch(const double *slab, long long slab_stride, long long lds,
+                               int nslab, int m, int n, double *out, long long ldo,
+                               cudaStream_t stream);
+
+/* ---- device properties (cached) ------------------------------------------ */
+int ca3dmm_device_sm_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

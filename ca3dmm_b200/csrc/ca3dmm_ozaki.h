@@ -1,0 +1,58 @@
+/* Internal C ABI of the split-precision (Ozaki scheme, INT8 slices) GEMM.
+ *
+ * For op(A) rows i and op(B) columns j of one operand block over its k range:
+ *   E_i = frexp exponent of max_l |a_il| (max|a| < 2^E_i; 0 for a zero row),
+ *   a_il = sum_{t<s} qa_t,il * 2^(E_i - 6 - 7t) + r,  qa_t = rint(...) in [-64, 64],
+ * likewise F_j for the columns of op(B).  Then
+ *   C_ij ~= sum_{d=0}^{s-1} 2^(E_i + F_j - 12 - 7d) * sum_{t+u=d} (qa_t qb_u)_ij
+ * where every inner sum is an exact INT32 tensor-core accumulation
+ * (|q| <= 64, so k (d+1) < 2^19 keeps it exact) and only the recombination
+ * over d is done in FP64, least significant diagonal first. */
+#ifndef CA3DMM_OZAKI_H
+#define CA3DMM_OZAKI_H
+
+#include <stddef.h>
+#include <cuda_runtime_api.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct { int r0, c0, rows, cols; } ca3dmm_oz_blk_t;   /* block of op(A) or op(B) */
+
+typedef struct {
+    int a_blk, b_blk;     /* operand blocks */
+    double *C;            /* output (column-major) */
+    long long ldc;
+    int m, n, k;
+} ca3dmm_oz_group_t;
+
+typedef struct {
+    int slices, nA, nB, ngroup;
+    int tiles;            /* total output tiles of the grouped INT8 launch */
+    int max_rows_a, max_k_a, max_cols_b, max_k_b;
+    void *dev_plan;       /* device copy of the plan (slice descriptors, tensor maps, groups) */
+    void *dev_work;       /* slices and exponents */
+} ca3dmm_oz_plan_t;
+
+size_t ca3dmm_oz_plan_bytes(int ngroup);
+size_t ca3dmm_oz_work_bytes(int nA, const int *a_rows, const int *a_k, int nB, const int *b_k,
+                            const int *b_cols, int slices);
+/* Build the plan into host memory host_plan (ca3dmm_oz_plan_bytes), which the
+ * caller uploads to dev_plan before running. */
+int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA, const ca3dmm_oz_blk_t *A,
+                          int nB, const ca3dmm_oz_blk_t *B, int ngroup,
+                          const ca3dmm_oz_group_t *G, void *dev_work, size_t work_bytes,
+                          void *host_plan, void *dev_plan);
+/* Exponent extraction + slicing of every A and B block straight from the
+ * caller's matrices (op(A)(i,l) = transA ? A[l + i*ldA] : A[i + l*ldA]). */
+int ca3dmm_oz_run_pack(const ca3dmm_oz_plan_t *oz, const void *A, int ldA, int transA,
+                       const void *B, int ldB, int transB, cudaStream_t stream);
+/* Grouped INT8 tcgen05 GEMM with FP64 recombination into each group's C. */
+int ca3dmm_oz_run_gemm(const ca3dmm_oz_plan_t *oz, int *dev_status, double timeout_s,
+                       cudaStream_t stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,72 @@
+/* Device-type helpers (src/dev_type.c:14-156), GPU-only. */
+#include <string.h>
+#include <cuda_runtime_api.h>
+#include "ca3dmm_util.h"
+#include "ca3dmm_kernels.h"
+#include "dev_type.h"
+
+int is_dev_type_valid(dev_type_t dev_type)
+{
+    return dev_type == DEV_TYPE_CUDA || dev_type == DEV_TYPE_CUDA_MPI_DIRECT;
+}
+
+void *dev_type_malloc(size_t bytes, dev_type_t dev_type)
+{
+    void *p = NULL;
+    if (bytes == 0) bytes = 256;
+    if (dev_type == DEV_TYPE_HOST) {
+        if (cudaMallocHost(&p, bytes) != cudaSuccess) p = NULL;
+    } else if (cudaMalloc(&p, bytes) != cudaSuccess) {
+        p = NULL;
+    }
+    return p;
+}
+
+void dev_type_free(void *mem, dev_type_t dev_type)
+{
+    if (mem == NULL) return;
+    if (dev_type == DEV_TYPE_HOST) cudaFreeHost(mem);
+    else cudaFree(mem);
+}
+
+void dev_type_memset(void *mem, int value, size_t bytes, dev_type_t dev_type)
+{
+    if (dev_type == DEV_TYPE_HOST) memset(mem, value, bytes);
+    else cudaMemset(mem, value, bytes);
+}
+
+void dev_type_memcpy(void *dst, const void *src, size_t bytes, dev_type_t dst_dev_type,
+                     dev_type_t src_dev_type)
+{
+    (void) dst_dev_type;
+    (void) src_dev_type;
+    if (cudaMemcpy(dst, src, bytes, cudaMemcpyDefault) != cudaSuccess)
+        ERROR_PRINTF("dev_type_memcpy of %zu bytes failed\n", bytes);
+}
+
+/* Row-major nrow x ncol block = column-major ncol x nrow block. */
+void dev_type_copy_mat_blk(size_t dt_size, const int nrow, const int ncol, const void *src,
+                           const int lds, void *dst, const int ldd, dev_type_t dev_type)
+{
+    if (nrow <= 0 || ncol <= 0) return;
+    if (dev_type == DEV_TYPE_HOST || dt_size != 8) {
+        /* 2D strided copy handles any element size and any memory type */
+        if (cudaMemcpy2D(dst, (size_t) ldd * dt_size, src, (size_t) lds * dt_size,
+                         (size_t) ncol * dt_size, (size_t) nrow, cudaMemcpyDefault) != cudaSuccess)
+            ERROR_PRINTF("dev_type_copy_mat_blk failed\n");
+        return;
+    }
+    ca3dmm_pack_desc_t d;
+    memset(&d, 0, sizeof(d));
+    d.lds = lds; d.ldd = ldd; d.rows = ncol; d.cols = nrow; d.trans = 0;
+    ca3dmm_pack_desc_t *dd = NULL;
+    if (cudaMalloc((void **) &dd, sizeof(d)) != cudaSuccess) {
+        ERROR_PRINTF("dev_type_copy_mat_blk: descriptor allocation failed\n");
+        return;
+    }
+    cudaMemcpy(dd, &d, sizeof(d), cudaMemcpyHostToDevice);
+    if (ca3dmm_pack_launch((const double *) src, (double *) dst, dd, 1, ncol, nrow, 0, 0))
+        ERROR_PRINTF("dev_type_copy_mat_blk: pack launch failed\n");
+    cudaDeviceSynchronize();
+    cudaFree(dd);
+}

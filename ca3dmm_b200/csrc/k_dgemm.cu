@@ -1,0 +1,372 @@
+// Plain FP64 GEMM on the sm_100a FP64 tensor path (DMMA, mma.sync m16n8k4 f64),
+// fed by TMA through a multi-stage mbarrier pipeline, as one persistent
+// grouped launch over every tile of every problem.
+//
+// Replaces the reference's per-Cannon-step cublasDgemm + stream sync
+// (src/cannon.c:410-418, :651-676; src/cuda_proxy.cu:211-230).  All virtual
+// ranks' cuboid GEMMs of one ca3dmm exec run in this single launch.
+//
+// Layout (per stage, 32 KiB, 1024-byte aligned):
+//   A tile: 128 (m) x 16 (k) doubles as 8 TMA boxes of 16 m x 16 k, each box
+//           16 rows (k) of 128 B (m), SWIZZLE_128B.
+//   B tile: 128 (n) x 16 (k) doubles as 1 TMA box, 128 rows (n) of 128 B (k),
+//           SWIZZLE_128B.
+// Fragment ownership is permuted so every fragment load is one conflict-free
+// 128-bit LDS:
+//   * MMA row r of an m16 tile  -> tile row 2r (r < 8) or 2(r-8)+1, so a0/a1 of
+//     m16n8k4 are the two doubles of one 16-byte chunk;
+//   * MMA column c of n8 tile j -> warp column 4c + j;
+//   * MMA k index t of k-step (q, b) -> tile k row 8q + 2t + b, so one 16-byte
+//     chunk of a B row holds the b0 fragments of two consecutive k-steps.
+// With the 128B swizzle (16-byte chunk index XOR row % 8) these choices put
+// every quarter-warp of a 128-bit load on 8 distinct chunks.
+#include <cuda.h>
+#include <cuda_runtime.h>
+#include <cstdio>
+#include <cstring>
+#include "k_common.cuh"
+#include "ca3dmm_kernels.h"
+
+namespace {
+
+constexpr int BM = 128, BN = 128, BK = 16;
+constexpr int STAGES = 5;
+constexpr int STAGE_BYTES = (BM + BN) * BK * 8;      // 32 KiB
+constexpr int A_BYTES = BM * BK * 8;                 // 16 KiB
+constexpr int CONSUMER_WARPS = 8;
+constexpr int THREADS = (CONSUMER_WARPS + 1) * 32;   // + 1 TMA producer warp
+constexpr int GROUP_M = 8;
+constexpr size_t SMEM_BYTES = (size_t) STAGES * STAGE_BYTES + 2 * STAGES * 8 + 1024;
+
+struct alignas(16) DProb {
+    double *C;
+    long long ldc;
+    int m, n, k;
+    int tiles_m, tiles_n, tile_begin;
+    double alpha, beta;
+    int vec_ok, pad;
+};
+
+__device__ __forceinline__ int find_problem(const DProb *probs, int nprob, int tile)
+{
+    int lo = 0, hi = nprob - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (probs[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void tile_coords(const DProb &p, int tile, int &tm, int &tn)
+{
+    int t = tile - p.tile_begin;
+    int group_size = GROUP_M * p.tiles_n;
+    int group = t / group_size;
+    int first_m = group * GROUP_M;
+    int gm = min(p.tiles_m - first_m, GROUP_M);
+    int r = t % group_size;
+    tm = first_m + r % gm;
+    tn = r / gm;
+}
+
+__device__ __forceinline__ void dmma(double (&d)[4], double a0, double a1, double b0)
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k4.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5}, {%6}, "
+        "{%0,%1,%2,%3};\n"
+        : "+d"(d[0]), "+d"(d[1]), "+d"(d[2]), "+d"(d[3])
+        : "d"(a0), "d"(a1), "d"(b0));
+}
+
+__device__ __forceinline__ void store_pair(const DProb &p, int m, int n, double v0, double v1)
+{
+    if (n >= p.n || m >= p.m) return;
+    double *c = p.C + (long long) m + (long long) n * p.ldc;
+    if (p.vec_ok && m + 1 < p.m) {
+        double2 o;
+        if (p.beta != 0.0) {
+            double2 old = *reinterpret_cast<const double2 *>(c);
+            o.x = p.alpha * v0 + p.beta * old.x;
+            o.y = p.alpha * v1 + p.beta * old.y;
+        } else {
+            o.x = p.alpha * v0;
+            o.y = p.alpha * v1;
+        }
+        *reinterpret_cast<double2 *>(c) = o;
+    } else {
+        c[0] = p.beta != 0.0 ? p.alpha * v0 + p.beta * c[0] : p.alpha * v0;
+        if (m + 1 < p.m) c[1] = p.beta != 0.0 ? p.alpha * v1 + p.beta * c[1] : p.alpha * v1;
+    }
+}
+
+__global__ void __maxnreg__(224)
+dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restrict__ probs,
+                   int nprob, int total_tiles, int *status, unsigned long long limit_ns)
+{
+    extern __shared__ uint8_t smem_raw[];
+    uint8_t *smem = reinterpret_cast<uint8_t *>(
+        (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
+    uint64_t *empty = full + STAGES;
+    __shared__ volatile int abort_flag;
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(&full[s], 1);
+            mbar_init(&empty[s], CONSUMER_WARPS);
+        }
+        abort_flag = 0;
+        fence_barrier_init();
+    }
+    __syncthreads();
+
+    if (warp == CONSUMER_WARPS) {
+        // ------------------------------------------------------------ producer
+        if (lane == 0) {
+            int stage = 0;
+            uint32_t phase = 0;
+            uint32_t issued_mask = 0, last_par = 0;
+            int last_p = -1;
+            for (int tile = blockIdx.x; tile < total_tiles && !abort_flag; tile += gridDim.x) {
+                int pi = find_problem(probs, nprob, tile);
+                const DProb &p = probs[pi];
+                const CUtensorMap *ta = tmaps + 2 * pi, *tb = ta + 1;
+                if (pi != last_p) {
+                    tmap_acquire(ta);
+                    tmap_acquire(tb);
+                    last_p = pi;
+                }
+                int tm, tn;
+                tile_coords(p, tile, tm, tn);
+                const int m0 = tm * BM, n0 = tn * BN;
+                const int ktiles = (p.k + BK - 1) / BK;
+                bool ok = true;
+                for (int kt = 0; kt < ktiles; ++kt) {
+                    if (!mbar_wait_bounded(&empty[stage], phase ^ 1, &abort_flag, status,
+                                           CA3DMM_DEV_TIMEOUT_PRODUCE, limit_ns)) {
+                        ok = false;
+                        break;
+                    }
+                    uint8_t *sA = smem + stage * STAGE_BYTES;
+                    uint8_t *sB = sA + A_BYTES;
+                    mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
+#pragma unroll
+                    for (int j = 0; j < BM / 16; ++j)
+                        tma_load_2d(sA + j * 2048, ta, m0 + 16 * j, kt * BK, &full[stage]);
+                    tma_load_2d(sB, tb, kt * BK, n0, &full[stage]);
+                    issued_mask |= 1u << stage;
+                    last_par = (last_par & ~(1u << stage)) | (phase << stage);
+                    if (++stage == STAGES) { stage = 0; phase ^= 1; }
+                }
+                if (!ok) break;
+            }
+            // Wait (bounded, ignoring the abort flag) for every copy still in
+            // flight so no TMA write lands in shared memory after exit.
+            for (int s = 0; s < STAGES; ++s) {
+                if (!(issued_mask & (1u << s))) continue;
+                uint32_t par = (last_par >> s) & 1u;
+                uint64_t t0 = global_timer_ns();
+                while (!mbar_try_wait(&full[s], par)) {
+                    if (global_timer_ns() - t0 > limit_ns) {
+                        atomicCAS(status, 0, CA3DMM_DEV_TIMEOUT_PRODUCE);
+                        break;
+                    }
+                }
+            }
+        }
+        return;
+    }
+
+    // ---------------------------------------------------------------- consumers
+    const int g = lane >> 2, t = lane & 3;
+    const int wm = warp >> 2, wn = warp & 3;
+    int stage = 0;
+    uint32_t phase = 0;
+    double acc[4][4][4];
+
+    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+        int pi = find_problem(probs, nprob, tile);
+        const DProb &p = probs[pi];
+        int tm, tn;
+        tile_coords(p, tile, tm, tn);
+        const int ktiles = (p.k + BK - 1) / BK;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j)
+#pragma unroll
+                for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
+
+        bool ok = true;
+        for (int kt = 0; kt < ktiles; ++kt) {
+            if (!mbar_wait_bounded(&full[stage], phase, &abort_flag, status,
+                                   CA3DMM_DEV_TIMEOUT_CONSUME, limit_ns)) {
+                ok = false;
+                break;
+            }
+            const uint8_t *sA = smem + stage * STAGE_BYTES;
+            const uint8_t *sB = sA + A_BYTES;
+#pragma unroll
+            for (int q = 0; q < 2; ++q) {
+                double2 bf[4];
+#pragma unroll
+                for (int j = 0; j < 4; ++j) {
+                    const int nl = wn * 32 + 4 * g + j;
+                    bf[j] = *reinterpret_cast<const double2 *>(
+                        sB + nl * 128 + (((4 * q + t) ^ (nl & 7)) << 4));
+                }
+#pragma unroll
+                for (int b = 0; b < 2; ++b) {
+                    const int kr = 8 * q + 2 * t + b;
+                    double2 af[4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        af[i] = *reinterpret_cast<const double2 *>(
+                            sA + (wm * 4 + i) * 2048 + kr * 128 + ((g ^ (kr & 7)) << 4));
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j)
+                            dmma(acc[i][j], af[i].x, af[i].y, b ? bf[j].y : bf[j].x);
+                }
+            }
+            __syncwarp();
+            if (lane == 0) mbar_arrive(&empty[stage]);
+            if (++stage == STAGES) { stage = 0; phase ^= 1; }
+        }
+        if (!ok) break;
+
+        const int mb = tm * BM + wm * 64 + 2 * g;
+        const int nb = tn * BN + wn * 32 + 8 * t;
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                store_pair(p, mb + 16 * i, nb + j, acc[i][j][0], acc[i][j][2]);
+                store_pair(p, mb + 16 * i, nb + 4 + j, acc[i][j][1], acc[i][j][3]);
+            }
+    }
+}
+
+typedef CUresult (*encode_tiled_fn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
+                                    const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
+                                    const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                    CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+encode_tiled_fn get_encode()
+{
+    static encode_tiled_fn fn = nullptr;
+    if (!fn) {
+        cudaDriverEntryPointQueryResult q;
+        void *p = nullptr;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
+                cudaSuccess ||
+            q != cudaDriverEntryPointSuccess)
+            return nullptr;
+        fn = reinterpret_cast<encode_tiled_fn>(p);
+    }
+    return fn;
+}
+
+}  // namespace
+
+extern "C" int ca3dmm_encode_tmap_2d(void *tmap, int dtype_bytes, const void *base,
+                                     unsigned long long dim0, unsigned long long dim1,
+                                     unsigned long long stride1_bytes, unsigned box0,
+                                     unsigned box1, int swizzle128)
+{
+    encode_tiled_fn enc = get_encode();
+    if (!enc) return CA3DMM_ENODEV;
+    if ((reinterpret_cast<uintptr_t>(base) & 15) || (stride1_bytes & 15)) return CA3DMM_EINVAL;
+    CUtensorMapDataType dt =
+        dtype_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_UINT8;
+    cuuint64_t dims[2] = {dim0, dim1};
+    cuuint64_t strides[1] = {stride1_bytes};
+    cuuint32_t box[2] = {box0, box1};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(reinterpret_cast<CUtensorMap *>(tmap), dt, 2, const_cast<void *>(base), dims,
+                     strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     swizzle128 ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? CA3DMM_OK : CA3DMM_EINVAL;
+}
+
+extern "C" size_t ca3dmm_dgemm_plan_bytes(int nprob)
+{
+    return (size_t) nprob * 2 * sizeof(CUtensorMap) + (size_t) nprob * sizeof(DProb);
+}
+
+extern "C" int ca3dmm_dgemm_plan_encode(const ca3dmm_dgemm_desc_t *probs, int nprob,
+                                        void *host_plan, int *total_tiles)
+{
+    CUtensorMap *tm = reinterpret_cast<CUtensorMap *>(host_plan);
+    DProb *dp = reinterpret_cast<DProb *>(tm + 2 * nprob);
+    int tiles = 0;
+    for (int i = 0; i < nprob; ++i) {
+        const ca3dmm_dgemm_desc_t &q = probs[i];
+        if (q.m < 0 || q.n < 0 || q.k < 0) return CA3DMM_EINVAL;
+        if ((q.lda & 1) || (q.ldb & 1) || q.lda < q.m || q.ldb < q.k) return CA3DMM_EINVAL;
+        memset(&tm[2 * i], 0, 2 * sizeof(CUtensorMap));
+        if (q.m > 0 && q.n > 0 && q.k > 0) {
+            int r = ca3dmm_encode_tmap_2d(&tm[2 * i], 8, q.A, (unsigned long long) q.m,
+                                          (unsigned long long) q.k,
+                                          (unsigned long long) q.lda * 8, 16, 16, 1);
+            if (r) return r;
+            r = ca3dmm_encode_tmap_2d(&tm[2 * i + 1], 8, q.B, (unsigned long long) q.k,
+                                      (unsigned long long) q.n, (unsigned long long) q.ldb * 8,
+                                      16, BN, 1);
+            if (r) return r;
+        }
+        DProb &d = dp[i];
+        memset(&d, 0, sizeof(d));
+        d.C = q.C;
+        d.ldc = q.ldc;
+        d.m = q.m; d.n = q.n; d.k = q.k;
+        d.alpha = q.alpha; d.beta = q.beta;
+        // k == 0 still needs the beta-scaling pass; give it one tile per block
+        // through the normal path (ktiles == 0 -> acc stays 0).
+        d.tiles_m = (q.m > 0 && q.n > 0) ? (q.m + BM - 1) / BM : 0;
+        d.tiles_n = (q.m > 0 && q.n > 0) ? (q.n + BN - 1) / BN : 0;
+        d.tile_begin = tiles;
+        d.vec_ok = ((reinterpret_cast<uintptr_t>(q.C) & 15) == 0) && ((q.ldc & 1) == 0);
+        tiles += d.tiles_m * d.tiles_n;
+    }
+    *total_tiles = tiles;
+    return CA3DMM_OK;
+}
+
+extern "C" int ca3dmm_dgemm_launch(const void *dev_plan, int nprob, int total_tiles,
+                                   int *dev_status, double timeout_s, cudaStream_t stream)
+{
+    if (total_tiles <= 0) return CA3DMM_OK;
+    static bool attr_done = false;
+    if (!attr_done) {
+        if (cudaFuncSetAttribute(dgemm_dmma_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int) SMEM_BYTES) != cudaSuccess)
+            return CA3DMM_ECUDA;
+        attr_done = true;
+    }
+    const CUtensorMap *tm = reinterpret_cast<const CUtensorMap *>(dev_plan);
+    const DProb *dp = reinterpret_cast<const DProb *>(tm + 2 * nprob);
+    int grid = ca3dmm_device_sm_count();
+    if (grid > total_tiles) grid = total_tiles;
+    unsigned long long limit = (unsigned long long) (timeout_s * 1e9);
+    dgemm_dmma_grouped<<<grid, THREADS, SMEM_BYTES, stream>>>(tm, dp, nprob, total_tiles,
+                                                               dev_status, limit);
+    return cudaGetLastError() == cudaSuccess ? CA3DMM_OK : CA3DMM_ECUDA;
+}
+
+extern "C" int ca3dmm_device_sm_count(void)
+{
+    static int sms[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
+    if (!sms[dev]) {
+        int v = 0;
+        if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
+            v = 148;
+        sms[dev] = v;
+    }
+    return sms[dev];
+}

@@ -1,0 +1,39 @@
+"""The C-ABI library loads and exports every function include/*.h declares."""
+import ctypes
+import os
+import re
+
+import ca3dmm_b200 as cb
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    names = set()
+    for f in os.listdir(os.path.join(ROOT, "include")):
+        if not f.endswith(".h"):
+            continue
+        text = open(os.path.join(ROOT, "include", f)).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        text = re.sub(r"#define[^\n]*(\\\n[^\n]*)*", "", text)
+        for m in re.finditer(r"^\s*[A-Za-z_][\w\s\*]*?\b([A-Za-z_][A-Za-z0-9_]*)\s*\(", text, flags=re.M):
+            name = m.group(1)
+            if name not in ("if", "while", "for", "sizeof", "return"):
+                names.add(name)
+    return sorted(names)
+
+
+def test_headers_declare_the_reference_api():
+    names = set(declared_functions())
+    for n in ("ca3dmm_engine_init", "ca3dmm_engine_init_BTB", "ca3dmm_engine_attach_workbuf",
+              "ca3dmm_engine_free", "ca3dmm_engine_exec", "ca3dmm_engine_reset_stat",
+              "ca3dmm_engine_print_stat", "cannon_engine_init", "cannon_engine_exec",
+              "calc_3d_decomposition_cannon", "calc_3d_decomposition_nk",
+              "mat_redist_engine_init", "mat_redist_engine_exec", "dev_type_malloc"):
+        assert n in names, n
+
+
+def test_library_exports_every_declared_symbol():
+    L = ctypes.CDLL(cb.LIB_PATH)
+    missing = [n for n in declared_functions() if not hasattr(L, n)]
+    assert not missing, missing

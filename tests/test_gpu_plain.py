@@ -1,0 +1,163 @@
+"""Plain FP64 DMMA path on the GPU against the double-double oracle."""
+import numpy as np
+import pytest
+
+import ca3dmm_b200 as cb
+from oracle import oracle as orc
+from tests._util import dev_zeros, from_dev, to_dev
+
+U = 2.0 ** -53
+pytestmark = pytest.mark.gpu
+
+
+def _dd_check(Cg, A, B, ta, tb, m, n, k, full=True):
+    if full:
+        hi, lo, ab = orc.dd_gemm(A, B, ta, tb, m, n, k)
+        err = orc.errors(Cg.ravel(order="F"), hi.ravel(order="F"), lo.ravel(order="F"),
+                         ab.ravel(order="F"))
+    else:
+        ii, jj = orc.sample_indices(m, n)
+        hi, lo, ab = orc.dd_entries(A, B, ta, tb, k, ii, jj)
+        err = orc.errors(Cg[ii, jj], hi, lo, ab)
+    # |C - T| <= gamma_k |A||B| with gamma_k ~ k u (blocked sums do better)
+    assert err["vs_absprod"] <= max(k, 1) * U, err
+    return err
+
+
+@pytest.mark.parametrize("m,n,k", [(1, 1, 1), (7, 5, 3), (63, 65, 129), (128, 128, 16),
+                                   (129, 257, 100), (300, 200, 1000), (1000, 999, 1001),
+                                   (256, 384, 4099)])
+def test_cannon_engine_gemm(cuda, m, n, k):
+    A = orc.gen_uniform(1, m, k)
+    B = orc.gen_uniform(2, k, n)
+    dA, _ = to_dev(A)
+    dB, _ = to_dev(B)
+    dC = dev_zeros(m * n)
+    ce = cb.CannonEngine(m, n, k, p=1)
+    assert ce.ok
+    assert ce.exec(1.0, 0.0, dA, dB, dC) == 0
+    _dd_check(from_dev(dC, m, n), A, B, 0, 0, m, n, k)
+
+
+def test_cannon_alpha_beta_and_unaligned(cuda):
+    m, n, k = 131, 77, 259           # odd m, k: operands are packed before TMA
+    A = orc.gen_uniform(3, m, k)
+    B = orc.gen_uniform(4, k, n)
+    C0 = orc.gen_uniform(5, m, n)
+    dA, _ = to_dev(A)
+    dB, _ = to_dev(B)
+    dC, _ = to_dev(C0)
+    ce = cb.CannonEngine(m, n, k, p=4)
+    assert ce.ok and ce.s.np_dim == 2
+    assert ce.exec(-0.5, 2.0, dA, dB, dC) == 0
+    got = from_dev(dC, m, n)
+    hi, lo, ab = orc.dd_gemm(A, B, 0, 0, m, n, k)
+    want = -0.5 * (hi + lo) + 2.0 * C0
+    assert np.max(np.abs(got - want) / (0.5 * ab + 2 * np.abs(C0))) <= k * U
+
+
+ENGINE_CASES = [  # m, n, k, p, ta, tb, grid
+    (256, 256, 256, 1, 0, 0, None),
+    (600, 500, 700, 6, 0, 0, None),
+    (600, 500, 700, 6, 1, 0, None),
+    (600, 500, 700, 6, 0, 1, None),
+    (600, 500, 700, 6, 1, 1, None),
+    (517, 1031, 2049, 16, 0, 0, (2, 4, 2)),
+    (1031, 517, 333, 12, 1, 0, None),
+    (64, 80, 20000, 8, 0, 0, None),
+    (5, 7, 3, 6, 0, 0, None),
+    (2048, 2048, 2048, 4, 0, 0, None),
+]
+
+
+@pytest.mark.parametrize("m,n,k,p,ta,tb,grid", ENGINE_CASES)
+def test_engine_vs_dd(cuda, m, n, k, p, ta, tb, grid):
+    A = orc.gen_uniform(11, *((k, m) if ta else (m, k)))
+    B = orc.gen_uniform(12, *((n, k) if tb else (k, n)))
+    dA, lda = to_dev(A, pad_ld=A.shape[0] + 3)
+    dB, ldb = to_dev(B)
+    dC = dev_zeros(m * n)
+    e = cb.Ca3dmmEngine(m, n, k, ta, tb, p=p, proc_grid=grid)
+    assert e.ok
+    assert e.exec(dA, lda, dB, ldb, dC, m) == 0
+    _dd_check(from_dev(dC, m, n), A, B, ta, tb, m, n, k, full=m * n * k <= 2e9)
+    # repeated exec reuses the plan and gives the same bits
+    got1 = from_dev(dC, m, n)
+    dC.zero_()
+    assert e.exec(dA, lda, dB, ldb, dC, m) == 0
+    assert np.array_equal(got1, from_dev(dC, m, n))
+
+
+@pytest.mark.parametrize("m,n,k,p,ta,tb", [(2048, 2048, 2048, 4, 0, 0), (700, 900, 1100, 24, 1, 0),
+                                           (333, 444, 555, 7, 0, 1)])
+def test_example_ab_validation_rule(cuda, m, n, k, p, ta, tb):
+    """examples/example_AB.c:222-313: deterministic fill, 0 entries over 1e-12."""
+    A = orc.gen_example_fill(*((k, m) if ta else (m, k)), 0.19, 0.24)
+    B = orc.gen_example_fill(*((n, k) if tb else (k, n)), 0.11, 0.12)
+    dA, lda = to_dev(A)
+    dB, ldb = to_dev(B)
+    dC = dev_zeros(m * n)
+    e = cb.Ca3dmmEngine(m, n, k, ta, tb, p=p)
+    assert e.ok and e.exec(dA, lda, dB, ldb, dC, m) == 0
+    Cg = from_dev(dC, m, n)
+    ii, jj = orc.sample_indices(m, n, nrand=20000)
+    hi, lo, ab = orc.dd_entries(A, B, ta, tb, k, ii, jj)
+    err = orc.errors(Cg[ii, jj], hi, lo, ab, tol=1e-12)
+    assert err["n_over_tol"] == 0, err
+    # the reference checks against cblas_dgemm; numpy's BLAS stands in here
+    ref = (A.T if ta else A) @ (B.T if tb else B)
+    assert np.max(np.abs(Cg - ref) / np.abs(ref)) <= 1e-12
+
+
+def test_btb_engine(cuda):
+    n, k, p = 96, 5000, 8
+    Bm = orc.gen_btb(3, k, n)
+    dB, ldb = to_dev(Bm)
+    dC = dev_zeros(n * n)
+    for grid in (None, (1, 1, 8), (2, 2, 2)):
+        e = cb.Ca3dmmEngine(n, n, k, p=p, btb=True, proc_grid=grid)
+        assert e.ok
+        assert e.exec(None, 0, dB, ldb, dC, n) == 0
+        _dd_check(from_dev(dC, n, n), Bm, Bm, 1, 0, n, n, k)
+
+
+def test_dst_block_and_c_out(cuda):
+    m, n, k = 300, 260, 410
+    A = orc.gen_uniform(21, m, k)
+    B = orc.gen_uniform(22, k, n)
+    dA, lda = to_dev(A)
+    dB, ldb = to_dev(B)
+    ref = A @ B
+    # a sub-block of C as the destination (row range 50..249, column range 10..139)
+    e = cb.Ca3dmmEngine(m, n, k, p=6, dst_C=(50, 200, 10, 130))
+    dC = dev_zeros(210 * 130)
+    assert e.ok and e.exec(dA, lda, dB, ldb, dC, 210) == 0
+    got = from_dev(dC, 200, 130, ld=210)
+    assert np.max(np.abs(got - ref[50:250, 10:140])) <= 1e-12 * np.max(np.abs(ref))
+    # no destination: the whole C stays in the engine's C_out buffer (ld = m)
+    e2 = cb.Ca3dmmEngine(m, n, k, p=6, dst_C=None)
+    assert e2.ok and e2.exec(dA, lda, dB, ldb, None, 0) == 0
+    import torch
+    s = e2.s
+    assert (s.C_out_srow, s.C_out_scol, s.C_out_nrow, s.C_out_ncol) == (0, 0, m, n)
+    out = torch.empty(m * n, dtype=torch.float64, device="cuda")
+    cb.lib().dev_type_memcpy(out.data_ptr(), s.C_out_d, m * n * 8, cb.DEV_TYPE_CUDA,
+                             cb.DEV_TYPE_CUDA)
+    assert np.max(np.abs(from_dev(out, m, n) - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+def test_caller_workbuf_and_bad_ld(cuda):
+    import torch
+    m, n, k = 200, 150, 300
+    A = orc.gen_uniform(31, m, k)
+    B = orc.gen_uniform(32, k, n)
+    dA, lda = to_dev(A)
+    dB, ldb = to_dev(B)
+    e = cb.Ca3dmmEngine(m, n, k, p=4, caller_workbuf=True)
+    assert e.ok and e.workbuf_bytes > 0
+    wb = torch.empty(e.workbuf_bytes // 8 + 1, dtype=torch.float64, device="cuda")
+    e.attach_workbuf(wb)
+    dC = dev_zeros(m * n)
+    assert e.exec(dA, lda, dB, ldb, dC, m) == 0
+    assert np.max(np.abs(from_dev(dC, m, n) - A @ B)) <= 1e-12 * np.max(np.abs(A @ B))
+    assert e.exec(dA, m - 1, dB, ldb, dC, m) == 1     # ldA < m is rejected, nothing runs
