@@ -644,8 +644,7 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
         if (rc) return rc;
     }
     memset(h + pl->off_status, 0, 64);
-    if (cudaMemcpyAsync(w, h, pl->stage_bytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
-        return CA3DMM_ECUDA;
+    CA3DMM_CUDA_TRY(cudaMemcpyAsync(w, h, pl->stage_bytes, cudaMemcpyHostToDevice, st));
     pl->c_A = A; pl->c_B = B; pl->c_ldA = ldA; pl->c_ldB = ldB;
     pl->c_dst = dst; pl->c_ldC = ldC;
     pl->plan_valid = 1;
@@ -727,11 +726,9 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
         if (rc) return rc;
     }
     if (timing) cudaEventRecord(pl->ev[4], st);
-    if (cudaMemcpyAsync(pl->status_h, status_d, sizeof(int), cudaMemcpyDeviceToHost, st) !=
-        cudaSuccess)
-        return CA3DMM_ECUDA;
+    CA3DMM_CUDA_TRY(cudaMemcpyAsync(pl->status_h, status_d, sizeof(int), cudaMemcpyDeviceToHost, st));
     if (e->sync_exec) {
-        if (cudaStreamSynchronize(st) != cudaSuccess) return CA3DMM_ECUDA;
+        CA3DMM_CUDA_TRY(cudaStreamSynchronize(st));
         if (pl->status_h[0] != 0) {
             ERROR_PRINTF("Device status %d: a bounded wait ran out\n", pl->status_h[0]);
             return CA3DMM_ETIMEOUT;

@@ -37,6 +37,17 @@
         }                                                                                  \
     } while (0)
 
+/* Evaluate a CUDA runtime call; on failure print where and why and return
+ * CA3DMM_ECUDA from the enclosing function. */
+#define CA3DMM_CUDA_TRY(call)                                                              \
+    do {                                                                                   \
+        cudaError_t err_ = (call);                                                         \
+        if (err_ != cudaSuccess) {                                                         \
+            ERROR_PRINTF("%s failed: %s\n", #call, cudaGetErrorString(err_));              \
+            return CA3DMM_ECUDA;                                                           \
+        }                                                                                  \
+    } while (0)
+
 static inline long long ca3dmm_round_up(long long x, long long a) { return (x + a - 1) / a * a; }
 
 double ca3dmm_wtime_sec(void);

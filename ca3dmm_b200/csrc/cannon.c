@@ -158,8 +158,7 @@ static int cannon_exec_device(cannon_engine_p e, double alpha, double beta, cons
         d.rows = m; d.cols = k; d.lds = lda; d.ldd = ca3dmm_round_up(m, 2);
         Ause = (const double *) e->A_recv_d;
         lda = d.ldd;
-        if (cudaMemcpy(w + cp->off_pack, &d, sizeof(d), cudaMemcpyHostToDevice) != cudaSuccess)
-            return CA3DMM_ECUDA;
+        CA3DMM_CUDA_TRY(cudaMemcpy(w + cp->off_pack, &d, sizeof(d), cudaMemcpyHostToDevice));
         int rc = ca3dmm_pack_launch(A, (double *) e->A_recv_d,
                                     (const ca3dmm_pack_desc_t *) (w + cp->off_pack), 1, m, k, 0, 0);
         if (rc) return rc;
@@ -170,8 +169,7 @@ static int cannon_exec_device(cannon_engine_p e, double alpha, double beta, cons
         d.rows = k; d.cols = n; d.lds = ldb; d.ldd = ca3dmm_round_up(k, 2);
         Buse = (const double *) e->B_recv_d;
         ldb = d.ldd;
-        if (cudaMemcpy(w + cp->off_pack + 64, &d, sizeof(d), cudaMemcpyHostToDevice) != cudaSuccess)
-            return CA3DMM_ECUDA;
+        CA3DMM_CUDA_TRY(cudaMemcpy(w + cp->off_pack + 64, &d, sizeof(d), cudaMemcpyHostToDevice));
         int rc = ca3dmm_pack_launch(B, (double *) e->B_recv_d,
                                     (const ca3dmm_pack_desc_t *) (w + cp->off_pack + 64), 1, k, n, 0, 0);
         if (rc) return rc;
@@ -184,16 +182,12 @@ static int cannon_exec_device(cannon_engine_p e, double alpha, double beta, cons
     int rc = ca3dmm_dgemm_plan_encode(&g, 1, h + 256, &tiles);
     if (rc) return rc;
     memset(h, 0, 256);
-    if (cudaMemcpy(w + cp->off_plan, h, 256 + ca3dmm_dgemm_plan_bytes(1), cudaMemcpyHostToDevice) !=
-        cudaSuccess)
-        return CA3DMM_ECUDA;
+    CA3DMM_CUDA_TRY(cudaMemcpy(w + cp->off_plan, h, 256 + ca3dmm_dgemm_plan_bytes(1), cudaMemcpyHostToDevice));
     cudaEventRecord(cp->ev[0], 0);
     rc = ca3dmm_dgemm_launch(w + cp->off_plan + 256, 1, tiles, (int *) (w + cp->off_plan), 5.0, 0);
     if (rc) return rc;
     cudaEventRecord(cp->ev[1], 0);
-    if (cudaMemcpy(cp->status_h, w + cp->off_plan, sizeof(int), cudaMemcpyDeviceToHost) !=
-        cudaSuccess)
-        return CA3DMM_ECUDA;
+    CA3DMM_CUDA_TRY(cudaMemcpy(cp->status_h, w + cp->off_plan, sizeof(int), cudaMemcpyDeviceToHost));
     if (cp->status_h[0]) return CA3DMM_ETIMEOUT;
     float ms = 0.f;
     cudaEventElapsedTime(&ms, cp->ev[0], cp->ev[1]);

@@ -8,6 +8,7 @@
 #pragma once
 #include <cstdint>
 #include <cuda_runtime.h>
+#include <cstdio>
 
 #define CA3DMM_DEV __device__ __forceinline__
 
@@ -116,5 +117,16 @@ CA3DMM_DEV void tmap_acquire(const void *tmap)
 {
     asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;" ::"l"(tmap) : "memory");
 }
+
+// Host: report a failed CUDA call with its error string, return CA3DMM_ECUDA.
+#define CA3DMM_CUDA_TRY(call)                                                              \
+    do {                                                                                   \
+        cudaError_t err_ = (call);                                                         \
+        if (err_ != cudaSuccess) {                                                         \
+            fprintf(stderr, "[ERROR] %s, %d: %s failed: %s\n", __FILE__, __LINE__, #call,   \
+                    cudaGetErrorString(err_));                                             \
+            return 2;                                                                      \
+        }                                                                                  \
+    } while (0)
 
 CA3DMM_DEV int lane_id() { return threadIdx.x & 31; }

@@ -34,7 +34,7 @@ constexpr int STAGES = 5;
 constexpr int STAGE_BYTES = (BM + BN) * BK * 8;      // 32 KiB
 constexpr int A_BYTES = BM * BK * 8;                 // 16 KiB
 constexpr int CONSUMER_WARPS = 8;
-constexpr int THREADS = (CONSUMER_WARPS + 1) * 32;   // + 1 TMA producer warp
+constexpr int THREADS = CONSUMER_WARPS * 32;         // thread 0 also issues the TMA loads
 constexpr int GROUP_M = 8;
 constexpr size_t SMEM_BYTES = (size_t) STAGES * STAGE_BYTES + 2 * STAGES * 8 + 1024;
 
@@ -99,7 +99,44 @@ __device__ __forceinline__ void store_pair(const DProb &p, int m, int n, double 
     }
 }
 
-__global__ void __maxnreg__(224)
+// Iterator over this CTA's (tile, k-tile) load sequence, used by the
+// producer thread.  Tiles with k == 0 carry no loads and are skipped.
+struct LoadCursor {
+    int tile, kt, ktiles, pi, m0, n0;
+    bool valid;
+    __device__ void seek(const DProb *probs, int nprob, int total_tiles, int stride)
+    {
+        while (tile < total_tiles) {
+            pi = find_problem(probs, nprob, tile);
+            const DProb &p = probs[pi];
+            ktiles = (p.k + BK - 1) / BK;
+            if (ktiles > 0) {
+                int tm, tn;
+                tile_coords(p, tile, tm, tn);
+                m0 = tm * BM;
+                n0 = tn * BN;
+                valid = true;
+                return;
+            }
+            tile += stride;
+        }
+        valid = false;
+    }
+    __device__ void advance(const DProb *probs, int nprob, int total_tiles, int stride)
+    {
+        if (++kt < ktiles) return;
+        kt = 0;
+        tile += stride;
+        seek(probs, nprob, total_tiles, stride);
+    }
+};
+
+// All 8 warps compute; thread 0 also drives the TMA pipeline.  Load L lands
+// in stage L % STAGES; before issuing it the producer waits for the release
+// of load L - STAGES.  Loads are issued STAGES-1 ahead of consumption, and the
+// refill after consuming load `it` waits on the release of load it - 1, which
+// every warp has usually finished, so the producer thread rarely stalls.
+__global__ void __launch_bounds__(THREADS, 1)
 dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restrict__ probs,
                    int nprob, int total_tiles, int *status, unsigned long long limit_ns)
 {
@@ -111,7 +148,8 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
     __shared__ volatile int abort_flag;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    if (threadIdx.x == 0) {
+    const bool producer = threadIdx.x == 0;
+    if (producer) {
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], CONSUMER_WARPS);
@@ -121,71 +159,48 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
     }
     __syncthreads();
 
-    if (warp == CONSUMER_WARPS) {
-        // ------------------------------------------------------------ producer
-        if (lane == 0) {
-            int stage = 0;
-            uint32_t phase = 0;
-            uint32_t issued_mask = 0, last_par = 0;
-            int last_p = -1;
-            for (int tile = blockIdx.x; tile < total_tiles && !abort_flag; tile += gridDim.x) {
-                int pi = find_problem(probs, nprob, tile);
-                const DProb &p = probs[pi];
-                const CUtensorMap *ta = tmaps + 2 * pi, *tb = ta + 1;
-                if (pi != last_p) {
-                    tmap_acquire(ta);
-                    tmap_acquire(tb);
-                    last_p = pi;
-                }
-                int tm, tn;
-                tile_coords(p, tile, tm, tn);
-                const int m0 = tm * BM, n0 = tn * BN;
-                const int ktiles = (p.k + BK - 1) / BK;
-                bool ok = true;
-                for (int kt = 0; kt < ktiles; ++kt) {
-                    if (!mbar_wait_bounded(&empty[stage], phase ^ 1, &abort_flag, status,
-                                           CA3DMM_DEV_TIMEOUT_PRODUCE, limit_ns)) {
-                        ok = false;
-                        break;
-                    }
-                    uint8_t *sA = smem + stage * STAGE_BYTES;
-                    uint8_t *sB = sA + A_BYTES;
-                    mbar_arrive_expect_tx(&full[stage], STAGE_BYTES);
-#pragma unroll
-                    for (int j = 0; j < BM / 16; ++j)
-                        tma_load_2d(sA + j * 2048, ta, m0 + 16 * j, kt * BK, &full[stage]);
-                    tma_load_2d(sB, tb, kt * BK, n0, &full[stage]);
-                    issued_mask |= 1u << stage;
-                    last_par = (last_par & ~(1u << stage)) | (phase << stage);
-                    if (++stage == STAGES) { stage = 0; phase ^= 1; }
-                }
-                if (!ok) break;
-            }
-            // Wait (bounded, ignoring the abort flag) for every copy still in
-            // flight so no TMA write lands in shared memory after exit.
-            for (int s = 0; s < STAGES; ++s) {
-                if (!(issued_mask & (1u << s))) continue;
-                uint32_t par = (last_par >> s) & 1u;
-                uint64_t t0 = global_timer_ns();
-                while (!mbar_try_wait(&full[s], par)) {
-                    if (global_timer_ns() - t0 > limit_ns) {
-                        atomicCAS(status, 0, CA3DMM_DEV_TIMEOUT_PRODUCE);
-                        break;
-                    }
-                }
-            }
+    LoadCursor lc;
+    uint32_t issued = 0;
+    int last_p = -1;
+    // Issue load number `issued` at the cursor (producer thread only).
+    auto issue_one = [&]() -> bool {
+        if (!lc.valid) return true;
+        const uint32_t s = issued % STAGES, ph = (issued / STAGES) & 1u;
+        if (!mbar_wait_bounded(&empty[s], ph ^ 1u, &abort_flag, status,
+                               CA3DMM_DEV_TIMEOUT_PRODUCE, limit_ns))
+            return false;
+        const CUtensorMap *ta = tmaps + 2 * lc.pi, *tb = ta + 1;
+        if (lc.pi != last_p) {
+            tmap_acquire(ta);
+            tmap_acquire(tb);
+            last_p = lc.pi;
         }
-        return;
+        uint8_t *sA = smem + s * STAGE_BYTES;
+        uint8_t *sB = sA + A_BYTES;
+        mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+#pragma unroll
+        for (int j = 0; j < BM / 16; ++j)
+            tma_load_2d(sA + j * 2048, ta, lc.m0 + 16 * j, lc.kt * BK, &full[s]);
+        tma_load_2d(sB, tb, lc.kt * BK, lc.n0, &full[s]);
+        ++issued;
+        lc.advance(probs, nprob, total_tiles, gridDim.x);
+        return true;
+    };
+    if (producer) {
+        lc.tile = blockIdx.x;
+        lc.kt = 0;
+        lc.seek(probs, nprob, total_tiles, gridDim.x);
+        for (int s = 0; s < STAGES - 1; ++s)
+            if (!issue_one()) break;
     }
 
-    // ---------------------------------------------------------------- consumers
     const int g = lane >> 2, t = lane & 3;
     const int wm = warp >> 2, wn = warp & 3;
-    int stage = 0;
-    uint32_t phase = 0;
+    uint32_t it = 0;   // loads consumed so far
     double acc[4][4][4];
+    bool ok = true;
 
-    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+    for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
         int pi = find_problem(probs, nprob, tile);
         const DProb &p = probs[pi];
         int tm, tn;
@@ -198,8 +213,8 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
 #pragma unroll
                 for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
 
-        bool ok = true;
-        for (int kt = 0; kt < ktiles; ++kt) {
+        for (int kt = 0; kt < ktiles; ++kt, ++it) {
+            const uint32_t stage = it % STAGES, phase = (it / STAGES) & 1u;
             if (!mbar_wait_bounded(&full[stage], phase, &abort_flag, status,
                                    CA3DMM_DEV_TIMEOUT_CONSUME, limit_ns)) {
                 ok = false;
@@ -233,7 +248,10 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
             }
             __syncwarp();
             if (lane == 0) mbar_arrive(&empty[stage]);
-            if (++stage == STAGES) { stage = 0; phase ^= 1; }
+            if (producer && !issue_one()) {
+                ok = false;
+                break;
+            }
         }
         if (!ok) break;
 
@@ -246,6 +264,22 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
                 store_pair(p, mb + 16 * i, nb + j, acc[i][j][0], acc[i][j][2]);
                 store_pair(p, mb + 16 * i, nb + 4 + j, acc[i][j][1], acc[i][j][3]);
             }
+    }
+
+    if (producer) {
+        // Wait (bounded, ignoring the abort flag) for every copy still in
+        // flight so no TMA write lands in shared memory after exit.
+        const uint32_t first = issued > STAGES ? issued - STAGES : 0;
+        for (uint32_t L = first; L < issued; ++L) {
+            const uint32_t s = L % STAGES, ph = (L / STAGES) & 1u;
+            uint64_t t0 = global_timer_ns();
+            while (!mbar_try_wait(&full[s], ph)) {
+                if (global_timer_ns() - t0 > limit_ns) {
+                    atomicCAS(status, 0, CA3DMM_DEV_TIMEOUT_PRODUCE);
+                    break;
+                }
+            }
+        }
     }
 }
 
@@ -342,9 +376,8 @@ extern "C" int ca3dmm_dgemm_launch(const void *dev_plan, int nprob, int total_ti
     if (total_tiles <= 0) return CA3DMM_OK;
     static bool attr_done = false;
     if (!attr_done) {
-        if (cudaFuncSetAttribute(dgemm_dmma_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int) SMEM_BYTES) != cudaSuccess)
-            return CA3DMM_ECUDA;
+        CA3DMM_CUDA_TRY(cudaFuncSetAttribute(
+            dgemm_dmma_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) SMEM_BYTES));
         attr_done = true;
     }
     const CUtensorMap *tm = reinterpret_cast<const CUtensorMap *>(dev_plan);
@@ -354,7 +387,8 @@ extern "C" int ca3dmm_dgemm_launch(const void *dev_plan, int nprob, int total_ti
     unsigned long long limit = (unsigned long long) (timeout_s * 1e9);
     dgemm_dmma_grouped<<<grid, THREADS, SMEM_BYTES, stream>>>(tm, dp, nprob, total_tiles,
                                                                dev_status, limit);
-    return cudaGetLastError() == cudaSuccess ? CA3DMM_OK : CA3DMM_ECUDA;
+    CA3DMM_CUDA_TRY(cudaGetLastError());
+    return CA3DMM_OK;
 }
 
 extern "C" int ca3dmm_device_sm_count(void)

@@ -7,6 +7,7 @@
 //     reduce-scatter with mpi_op_omp_sum (src/ca3dmm.c:1287-1343,
 //     src/mpi_op_omp.c:6-23), summing slabs in rank order.
 #include <cuda_runtime.h>
+#include "k_common.cuh"
 #include "ca3dmm_kernels.h"
 
 namespace {
@@ -105,7 +106,8 @@ extern "C" int ca3dmm_pack_launch(const double *src_base, double *dst_base,
     if (gy > 65535) return CA3DMM_EINVAL;
     dim3 grid(gx, gy, (unsigned) ndesc);
     pack_kernel<<<grid, 256, 0, stream>>>(src_base, dst_base, dev_descs);
-    return cudaGetLastError() == cudaSuccess ? CA3DMM_OK : CA3DMM_ECUDA;
+    CA3DMM_CUDA_TRY(cudaGetLastError());
+    return CA3DMM_OK;
 }
 
 extern "C" int ca3dmm_reduce_slabs_launch(const double *slab, long long slab_stride,
@@ -121,5 +123,6 @@ extern "C" int ca3dmm_reduce_slabs_launch(const double *slab, long long slab_str
     if (blocks > cap) blocks = cap;
     reduce_slabs_kernel<<<(unsigned) blocks, 256, 0, stream>>>(slab, slab_stride, lds, nslab, m, n,
                                                              out, ldo, vec);
-    return cudaGetLastError() == cudaSuccess ? CA3DMM_OK : CA3DMM_ECUDA;
+    CA3DMM_CUDA_TRY(cudaGetLastError());
+    return CA3DMM_OK;
 }
