@@ -109,6 +109,8 @@ def lib():
         "dev_type_malloc": (p, [sz, i]),
         "dev_type_free": (None, [p, i]),
         "dev_type_memcpy": (None, [p, p, sz, i, i]),
+        "ca3dmm_dgemm_kslab_noalloc": (i, [i, i, i, i, p, i, p, i, p, i, p]),
+        "ca3dmm_dgemm_kslab_noalloc_scratch_bytes": (sz, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
