@@ -639,8 +639,9 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
             og[i].m = gd[i].m; og[i].n = gd[i].n; og[i].k = gd[i].k;
         }
         rc = ca3dmm_oz_plan_encode(&pl->oz, e->ozaki_slices, pl->nA, ob, pl->nB, ob + pl->nA,
-                                   pl->ngroup, og, w + pl->off_oz, pl->oz_bytes,
-                                   h + pl->off_ozplan, w + pl->off_ozplan);
+                                   pl->ngroup, og, ldA, e->trans_A, ldB, e->trans_B,
+                                   w + pl->off_oz, pl->oz_bytes, h + pl->off_ozplan,
+                                   w + pl->off_ozplan);
         if (rc) return rc;
     }
     memset(h + pl->off_status, 0, 64);
@@ -683,7 +684,7 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
         if (pl->A[i].cols > max_c) max_c = pl->A[i].cols;
     }
     if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
-        rc = ca3dmm_oz_run_pack(&pl->oz, src_A, ldA, e->trans_A, src_B, ldB, e->trans_B, st);
+        rc = ca3dmm_oz_run_pack(&pl->oz, src_A, src_B, st);
         if (rc) return rc;
     } else {
         rc = ca3dmm_pack_launch((const double *) src_A, (double *) w,

@@ -30,7 +30,8 @@ typedef struct {
 typedef struct {
     int slices, nA, nB, ngroup;
     int tiles;            /* total output tiles of the grouped INT8 launch */
-    int max_rows_a, max_k_a, max_cols_b, max_k_b;
+    int max_rows, max_kpad;
+    long long n_exp;      /* exponents (ints) at the start of the work region */
     void *dev_plan;       /* device copy of the plan (slice descriptors, tensor maps, groups) */
     void *dev_work;       /* slices and exponents */
 } ca3dmm_oz_plan_t;
@@ -39,15 +40,18 @@ size_t ca3dmm_oz_plan_bytes(int ngroup);
 size_t ca3dmm_oz_work_bytes(int nA, const int *a_rows, const int *a_k, int nB, const int *b_k,
                             const int *b_cols, int slices);
 /* Build the plan into host memory host_plan (ca3dmm_oz_plan_bytes), which the
- * caller uploads to dev_plan before running. */
+ * caller uploads to dev_plan before running.  A blocks: (r0, c0) = (first row
+ * of op(A), first k), rows x cols = rows x kz; B blocks: (r0, c0) = (first k,
+ * first column of op(B)), rows x cols = kz x cols. */
 int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA, const ca3dmm_oz_blk_t *A,
                           int nB, const ca3dmm_oz_blk_t *B, int ngroup,
-                          const ca3dmm_oz_group_t *G, void *dev_work, size_t work_bytes,
-                          void *host_plan, void *dev_plan);
+                          const ca3dmm_oz_group_t *G, long long ldA, int transA, long long ldB,
+                          int transB, void *dev_work, size_t work_bytes, void *host_plan,
+                          void *dev_plan);
 /* Exponent extraction + slicing of every A and B block straight from the
  * caller's matrices (op(A)(i,l) = transA ? A[l + i*ldA] : A[i + l*ldA]). */
-int ca3dmm_oz_run_pack(const ca3dmm_oz_plan_t *oz, const void *A, int ldA, int transA,
-                       const void *B, int ldB, int transB, cudaStream_t stream);
+int ca3dmm_oz_run_pack(const ca3dmm_oz_plan_t *oz, const void *A, const void *B,
+                       cudaStream_t stream);
 /* Grouped INT8 tcgen05 GEMM with FP64 recombination into each group's C. */
 int ca3dmm_oz_run_gemm(const ca3dmm_oz_plan_t *oz, int *dev_status, double timeout_s,
                        cudaStream_t stream);
