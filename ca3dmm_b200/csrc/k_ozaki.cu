@@ -2,20 +2,30 @@
 //
 //  1. oz_exp_kernel    -- per row of op(A) / column of op(B) over the block's k
 //                         range: E = frexp exponent of max|x| (max|x| < 2^E).
-//  2. oz_slice_kernel  -- x = sum_t q_t 2^(E-6-7t) + r with q_t = rint(...) in
-//                         [-64, 64]; writes the s slices K-major (k contiguous),
-//                         transposing through shared memory when the source is
-//                         k-strided.  HBM-bound.
-//  3. oz_gemm_kernel   -- tcgen05.mma kind::i8, M=128 x N=64 x K=32, all s
-//                         diagonal accumulators D_d = sum_{t+u=d} Aq_t Bq_u^T held
-//                         in TMEM at once (s*64 <= 512 columns), so every 64-byte
-//                         k-block of every slice is loaded once (one 3D TMA box
-//                         per operand, SWIZZLE_64B) and feeds all s(s+1)/2 slice
-//                         products.  INT32 accumulation is exact while
-//                         (d+1) k 64^2 < 2^31.  The epilogue recombines
-//                         C = sum_{d=s-1..0} 2^(E_i+F_j-12-7d) D_d in FP64 from the
-//                         least significant diagonal up.
-// Warp roles of the GEMM: warp 0 TMA producer, warp 1 TMEM owner + MMA issuer,
+//  2. oz_slice_kernel  -- x = sum_t q_t 2^(E-7-8t) + r with |r| <= 2^(E-8s): the
+//                         integer N = rint(x 2^(8s-1-E)) written in balanced
+//                         base-256 digits q_t in [-128, 127] (E chosen so that
+//                         max|x| <= 2^E 127/128, which keeps the top digit in range).
+//                         The slices are written straight into the GEMM's shared
+//                         memory image: per 128-row (A) / 64-row (B) tile and
+//                         32-byte k-block, the s slices are contiguous, each a
+//                         K-major rows x 32-byte tile with the 32-byte swizzle
+//                         (16-byte chunk ^= (row >> 2) & 1) already applied.
+//                         HBM-bound; transposes through shared memory when the
+//                         source is k-strided.
+//  3. oz_gemm_kernel   -- tcgen05.mma kind::i8 (signed x signed), M=128 x K=32,
+//                         N = 64 per slice pair, up to four pairs of one A slice
+//                         fused into one N <= 256 MMA.  All s diagonal accumulators
+//                         D_d = sum_{t+u=d} Aq_t Bq_u^T live in TMEM at once
+//                         (s*64 <= 512 columns), so each 32-byte k-block of every
+//                         slice is brought in once -- two contiguous bulk copies
+//                         per stage -- and feeds all s(s+1)/2 slice products.
+//                         The k range is processed in chunks short enough for the
+//                         INT32 sums to stay exact (s kc 2^14 < 2^31); after each
+//                         chunk the epilogue adds 2^(E_i+F_j-14-8d) D_d, d = s-1
+//                         down to 0, into FP64 registers, and stores C after the
+//                         last chunk.
+// Warp roles of the GEMM: warp 0 copy producer, warp 1 TMEM owner + MMA issuer,
 // warps 2..5 epilogue (warp w reads TMEM lanes 32*(w%4)..+31).  All waits are
 // bounded; on timeout the kernel records a status, drains, frees TMEM, returns.
 #include <cuda.h>
@@ -34,11 +44,12 @@ extern "C" int ca3dmm_encode_tmap_2d(void *tmap, int dtype_bytes, const void *ba
 
 namespace {
 
-constexpr int OBM = 128, OBN = 64, OKB = 64;    // tile rows, tile cols, k bytes per stage
+constexpr int OBM = 128, OBN = 64, OKB = 32;    // tile rows, tile cols, k bytes per stage
 constexpr int OTHREADS = 192;
 constexpr int MAX_SLICES = 8;
-constexpr int A_SLICE_BYTES = OBM * OKB;        // 8 KiB
-constexpr int B_SLICE_BYTES = OBN * OKB;        // 4 KiB
+constexpr int MAX_STAGES = 8;
+constexpr int A_SLICE_BYTES = OBM * OKB;        // 4 KiB
+constexpr int B_SLICE_BYTES = OBN * OKB;        // 2 KiB
 constexpr int SMEM_BUDGET = 200 * 1024;
 constexpr int GROUP_M = 8;
 constexpr int EXP_BIAS = 2048;                   // stored exponent = E + bias, 0 = all-zero row
@@ -47,18 +58,20 @@ constexpr int EXP_BIAS = 2048;                   // stored exponent = E + bias, 
 // element (r,l) at src[src_off + r*rs + l*ls].
 struct SliceDesc {
     long long src_off, rs, ls;
-    long long q_off;        // byte offset of slice 0 in the work region
+    long long q_off;        // byte offset of the block's tiled slices in the work region
     long long e_off;        // int offset of the exponents in the work region
-    int rows, kz, kpad, pad;
+    int rows, kz, kpad;     // kpad = kz rounded up to OKB
+    int rows_pad, tile_rows, nkb;   // rows rounded up to tile_rows (128 for A, 64 for B)
 };
 
 struct OzGroup {
     double *C;
     long long ldc;
     int m, n, k;
-    int a_blk, b_blk;       // tensor map indices (B maps follow the A maps)
-    int tiles_m, tiles_n, tile_begin;
+    int nkb;                    // 32-byte k-blocks
+    int tiles_m, tiles_n, tile_begin, pad;
     long long ea_off, eb_off;   // exponent offsets (ints) of the A rows / B columns
+    long long qa_off, qb_off;   // byte offsets of the tiled slices
 };
 
 struct PlanHeader {
@@ -88,9 +101,11 @@ oz_exp_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ desc
         if (gr < d.rows && gl < d.kz) {
             const double v = fabs(__ldg(base + gr * d.rs + gl * d.ls));
             if (v != 0.0) {
+                // effective exponent: one more when the mantissa exceeds 127/128,
+                // so that max|x| <= 2^E * 127/128 and the top digit fits in int8
                 int ex;
-                frexp(v, &ex);
-                atomicMax(&smax[r], ex + EXP_BIAS);
+                const double mant = frexp(v, &ex);
+                atomicMax(&smax[r], ex + (mant > 0.9921875 ? 1 : 0) + EXP_BIAS);
             }
         }
     }
@@ -105,7 +120,7 @@ oz_slice_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ de
 {
     const SliceDesc d = descs[blockIdx.z];
     const int r0 = blockIdx.x * ST, l0 = blockIdx.y * ST;
-    if (r0 >= d.rows || l0 >= d.kpad) return;
+    if (r0 >= d.rows_pad || l0 >= d.kpad) return;
     __shared__ double tile[ST][ST + 1];
     const double *base = src + d.src_off;
     const bool rfast = d.rs == 1;
@@ -116,18 +131,15 @@ oz_slice_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ de
         tile[r][l] = (gr < d.rows && gl < d.kz) ? __ldg(base + gr * d.rs + gl * d.ls) : 0.0;
     }
     __syncthreads();
-    // thread -> (row r, 16 consecutive k)
+    // thread -> (row r, 16 consecutive k = one 16-byte chunk of a 32-byte k-block)
     const int r = threadIdx.x >> 2, c = (threadIdx.x & 3) * 16;
     const int gr = r0 + r, gl = l0 + c;
-    if (gr >= d.rows || gl >= d.kpad) return;
-    const unsigned eb = reinterpret_cast<const unsigned *>(work)[d.e_off + gr];
+    if (gr >= d.rows_pad || gl >= d.kpad) return;
+    const unsigned eb = gr < d.rows ? reinterpret_cast<const unsigned *>(work)[d.e_off + gr] : 0u;
     const int E = eb ? (int) eb - EXP_BIAS : 0;
-    double up[MAX_SLICES], dn[MAX_SLICES];
-#pragma unroll
-    for (int t = 0; t < MAX_SLICES; ++t) {
-        up[t] = ldexp(1.0, 6 + 7 * t - E);
-        dn[t] = ldexp(1.0, E - 6 - 7 * t);
-    }
+    // N = rint(x 2^(8s-1-E)) in balanced base-256 digits q_t in [-128, 127],
+    // least significant first: q = ((N + 128) mod 256) - 128, N = (N - q) / 256.
+    const double up = ldexp(1.0, 8 * slices - 1 - E);
     uint32_t q[MAX_SLICES][4];
 #pragma unroll
     for (int t = 0; t < MAX_SLICES; ++t)
@@ -135,34 +147,37 @@ oz_slice_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ de
         for (int w = 0; w < 4; ++w) q[t][w] = 0;
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
-        double x = tile[r][c + j];
+        long long N = __double2ll_rn(tile[r][c + j] * up);
 #pragma unroll
-        for (int t = 0; t < MAX_SLICES; ++t) {
+        for (int t = MAX_SLICES - 1; t >= 0; --t) {
             if (t < slices) {
-                const double qq = rint(x * up[t]);
-                x -= qq * dn[t];
-                const uint32_t byte = (uint32_t) ((int) qq) & 0xffu;
-                q[t][j >> 2] |= byte << (8 * (j & 3));
+                const long long dgt = ((N + 128) & 255) - 128;
+                N = (N - dgt) >> 8;
+                q[t][j >> 2] |= ((uint32_t) dgt & 0xffu) << (8 * (j & 3));
             }
         }
     }
-    unsigned char *dst = work + d.q_off + (long long) gr * d.kpad + gl;
-    const long long slice_bytes = (long long) d.rows * d.kpad;
+    // tiled, pre-swizzled destination
+    const int rt = gr / d.tile_rows, rr = gr % d.tile_rows;
+    const int kb = gl / OKB, chunk = (gl % OKB) >> 4;
+    const long long tile_bytes = (long long) d.tile_rows * OKB;
+    unsigned char *dst = work + d.q_off + ((long long) rt * d.nkb + kb) * slices * tile_bytes +
+                         rr * OKB + ((chunk ^ ((rr >> 2) & 1)) << 4);
 #pragma unroll
     for (int t = 0; t < MAX_SLICES; ++t)
         if (t < slices)
-            *reinterpret_cast<uint4 *>(dst + t * slice_bytes) =
+            *reinterpret_cast<uint4 *>(dst + t * tile_bytes) =
                 make_uint4(q[t][0], q[t][1], q[t][2], q[t][3]);
 }
 
 // ------------------------------------------------------------------ tcgen05 GEMM
-__device__ __forceinline__ void tma_load_3d(void *dst, const void *tmap, int x, int y, int z,
-                                            uint64_t *bar)
+// Contiguous global -> shared bulk copy completing on an mbarrier.
+__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
 {
     asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_u32(dst)),
-        "l"(tmap), "r"(x), "r"(y), "r"(z), "r"(smem_u32(bar))
+        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::
+            "r"(smem_u32(dst)),
+        "l"(src), "r"(bytes), "r"(smem_u32(bar))
         : "memory");
 }
 
@@ -187,27 +202,37 @@ __device__ __forceinline__ void tc_mma_i8(uint32_t tmem_d, uint64_t adesc, uint6
         : "memory");
 }
 
-// K-major, SWIZZLE_64B shared-memory operand descriptor: rows of 64 bytes,
-// 8-row groups 512 bytes apart (SBO), version 1, layout type 4.
-__device__ __forceinline__ uint64_t sdesc_k64(uint32_t saddr)
+// K-major, SWIZZLE_32B shared-memory operand descriptor: rows of 32 bytes,
+// 8-row groups 256 bytes apart (SBO), descriptor version 1, layout type 6.
+__device__ __forceinline__ uint64_t sdesc_k32(uint32_t saddr)
 {
     uint64_t d = 0;
     d |= (uint64_t) ((saddr & 0x3FFFFu) >> 4);
     d |= (uint64_t) 1 << 16;                 // LBO (unused for swizzled K-major)
-    d |= (uint64_t) (512 >> 4) << 32;        // SBO
+    d |= (uint64_t) (256 >> 4) << 32;        // SBO
     d |= (uint64_t) 1 << 46;                 // descriptor version (sm_100)
-    d |= (uint64_t) 4 << 61;                 // SWIZZLE_64B
+    d |= (uint64_t) 6 << 61;                 // SWIZZLE_32B
     return d;
 }
 
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, uint32_t (&v)[16])
+// Instruction descriptor: S32 accumulator, A and B signed 8-bit, both
+// K-major, M = 128, N = n.
+__device__ __forceinline__ uint32_t idesc_i8(int n)
+{
+    return (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t) (n >> 3) << 17) |
+           ((uint32_t) (OBM >> 4) << 24);
+}
+
+__device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32])
 {
     asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
-        "%14,%15}, [%16];"
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,"
+        "%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
         : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]),
           "=r"(v[7]), "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]),
-          "=r"(v[14]), "=r"(v[15])
+          "=r"(v[14]), "=r"(v[15]), "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]),
+          "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]), "=r"(v[24]), "=r"(v[25]),
+          "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
         : "r"(taddr));
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
@@ -241,22 +266,31 @@ __device__ __forceinline__ void group_tile(const OzGroup &p, int tile, int &tm, 
     tn = r / gm;
 }
 
+// number of exactly-accumulated k chunks of a tile with nkb k-blocks
+__device__ __forceinline__ int nchunks(int nkb, int kb_per_chunk)
+{
+    return nkb > 0 ? (nkb + kb_per_chunk - 1) / kb_per_chunk : 1;
+}
+
 __global__ void __launch_bounds__(OTHREADS, 1)
-oz_gemm_kernel(const CUtensorMap *__restrict__ tmaps, const OzGroup *__restrict__ groups,
-               int ngroup, int total_tiles, int slices, int nstage, const int *__restrict__ ework,
+oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, int slices,
+               int nstage, int kb_per_chunk, const unsigned char *__restrict__ work,
                int *status, unsigned long long limit_ns)
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     const int a_bytes = slices * A_SLICE_BYTES;
-    const int stage_bytes = slices * (A_SLICE_BYTES + B_SLICE_BYTES);
+    const int b_bytes = slices * B_SLICE_BYTES;
+    const int stage_bytes = a_bytes + b_bytes;
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + nstage * stage_bytes);
     uint64_t *empty = full + nstage;
     uint64_t *acc_full = empty + nstage;
     uint64_t *acc_empty = acc_full + 1;
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
+    __shared__ int col_exp_all[4][OBN];   // per epilogue warp (no cross-warp barrier)
+    const int *ework = reinterpret_cast<const int *>(work);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t tmem_cols = slices * OBN <= 256 ? 256u : 512u;
@@ -286,21 +320,16 @@ oz_gemm_kernel(const CUtensorMap *__restrict__ tmaps, const OzGroup *__restrict_
         // ---------------------------------------------------------- producer
         if (lane == 0) {
             uint32_t it = 0;
-            int last_g = -1;
             for (int tile = blockIdx.x; tile < total_tiles && !abort_flag; tile += gridDim.x) {
-                const int gi = find_group(groups, ngroup, tile);
-                const OzGroup &p = groups[gi];
-                const CUtensorMap *ta = tmaps + p.a_blk, *tb = tmaps + p.b_blk;
-                if (gi != last_g) {
-                    tmap_acquire(ta);
-                    tmap_acquire(tb);
-                    last_g = gi;
-                }
+                const OzGroup &p = groups[find_group(groups, ngroup, tile)];
                 int tm, tn;
                 group_tile(p, tile, tm, tn);
-                const int kblocks = (p.k + OKB - 1) / OKB;
+                const unsigned char *qa =
+                    work + p.qa_off + (long long) tm * p.nkb * a_bytes;
+                const unsigned char *qb =
+                    work + p.qb_off + (long long) tn * p.nkb * b_bytes;
                 bool ok = true;
-                for (int kb = 0; kb < kblocks; ++kb, ++it) {
+                for (int kb = 0; kb < p.nkb; ++kb, ++it) {
                     const uint32_t s = it % nstage, ph = (it / nstage) & 1u;
                     if (!mbar_wait_bounded(&empty[s], ph ^ 1u, &abort_flag, status,
                                            CA3DMM_DEV_TIMEOUT_PRODUCE, limit_ns)) {
@@ -309,8 +338,8 @@ oz_gemm_kernel(const CUtensorMap *__restrict__ tmaps, const OzGroup *__restrict_
                     }
                     uint8_t *sA = smem + s * stage_bytes;
                     mbar_arrive_expect_tx(&full[s], stage_bytes);
-                    tma_load_3d(sA, ta, kb * OKB, tm * OBM, 0, &full[s]);
-                    tma_load_3d(sA + a_bytes, tb, kb * OKB, tn * OBN, 0, &full[s]);
+                    bulk_load(sA, qa + (long long) kb * a_bytes, a_bytes, &full[s]);
+                    bulk_load(sA + a_bytes, qb + (long long) kb * b_bytes, b_bytes, &full[s]);
                 }
                 if (!ok) break;
             }
@@ -325,51 +354,56 @@ oz_gemm_kernel(const CUtensorMap *__restrict__ tmaps, const OzGroup *__restrict_
     } else if (warp == 1) {
         // ---------------------------------------------------------- MMA issuer
         if (lane == 0) {
-            const uint32_t idesc = (2u << 4) | (1u << 7) | (1u << 10) |
-                                   ((uint32_t) (OBN >> 3) << 17) | ((uint32_t) (OBM >> 4) << 24);
-            uint32_t it = 0, ti = 0;
+            uint32_t it = 0, ci = 0;
             bool ok = true;
-            for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x, ++ti) {
+            for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
                 const OzGroup &p = groups[find_group(groups, ngroup, tile)];
-                if (!mbar_wait_bounded(acc_empty, (ti & 1u) ^ 1u, &abort_flag, status,
-                                       CA3DMM_DEV_TIMEOUT_ACCUM, limit_ns)) {
-                    ok = false;
-                    break;
-                }
-                tc_fence_after();
-                const int kblocks = (p.k + OKB - 1) / OKB;
-                for (int kb = 0; kb < kblocks; ++kb, ++it) {
-                    const uint32_t s = it % nstage, ph = (it / nstage) & 1u;
-                    if (!mbar_wait_bounded(&full[s], ph, &abort_flag, status,
-                                           CA3DMM_DEV_TIMEOUT_CONSUME, limit_ns)) {
+                const int nch = nchunks(p.nkb, kb_per_chunk);
+                for (int ch = 0; ch < nch && ok; ++ch, ++ci) {
+                    if (!mbar_wait_bounded(acc_empty, (ci & 1u) ^ 1u, &abort_flag, status,
+                                           CA3DMM_DEV_TIMEOUT_ACCUM, limit_ns)) {
                         ok = false;
                         break;
                     }
                     tc_fence_after();
-                    const uint32_t sA = smem_u32(smem + s * stage_bytes);
-                    const uint32_t sB = sA + a_bytes;
-#pragma unroll
-                    for (int ks = 0; ks < OKB / 32; ++ks) {
+                    const int kb0 = ch * kb_per_chunk;
+                    const int kb1 = min(p.nkb, kb0 + kb_per_chunk);
+                    for (int kb = kb0; kb < kb1; ++kb, ++it) {
+                        const uint32_t s = it % nstage, ph = (it / nstage) & 1u;
+                        if (!mbar_wait_bounded(&full[s], ph, &abort_flag, status,
+                                               CA3DMM_DEV_TIMEOUT_CONSUME, limit_ns)) {
+                            ok = false;
+                            break;
+                        }
+                        tc_fence_after();
+                        const uint32_t sA = smem_u32(smem + s * stage_bytes);
+                        const uint32_t sB = sA + a_bytes;
+                        // For slice t of A the partner slices u = 0..s-1-t of B are
+                        // adjacent 64-row tiles in shared memory and their
+                        // accumulators D_{t+u} adjacent 64-column blocks in TMEM,
+                        // so one MMA with N = 64 * (#u) (<= 256) covers up to four
+                        // slice products.
                         for (int t = 0; t < slices; ++t) {
-                            const uint64_t ad = sdesc_k64(sA + t * A_SLICE_BYTES + ks * 32);
-                            for (int u = 0; u + t < slices; ++u) {
-                                const uint64_t bd = sdesc_k64(sB + u * B_SLICE_BYTES + ks * 32);
-                                const uint32_t acc = (kb > 0 || ks > 0 || t > 0) ? 1u : 0u;
-                                tc_mma_i8(tmem_base + (uint32_t) ((t + u) * OBN), ad, bd, idesc,
-                                          acc);
+                            const uint64_t ad = sdesc_k32(sA + t * A_SLICE_BYTES);
+                            for (int u0 = 0; u0 + t < slices; u0 += 4) {
+                                const int nu = min(4, slices - t - u0);
+                                const uint64_t bd = sdesc_k32(sB + u0 * B_SLICE_BYTES);
+                                const uint32_t acc = (kb > kb0 || t > 0) ? 1u : 0u;
+                                tc_mma_i8(tmem_base + (uint32_t) ((t + u0) * OBN), ad, bd,
+                                          idesc_i8(nu * OBN), acc);
                             }
                         }
+                        tc_commit(&empty[s]);
                     }
-                    tc_commit(&empty[s]);
+                    if (!ok) break;
+                    tc_commit(acc_full);
                 }
-                if (!ok) break;
-                tc_commit(acc_full);
             }
             if (!ok) {
                 // let every MMA already issued finish before TMEM is freed
                 tc_commit(acc_full);
                 uint64_t t0 = global_timer_ns();
-                while (!mbar_try_wait(acc_full, ti & 1u))
+                while (!mbar_try_wait(acc_full, ci & 1u))
                     if (global_timer_ns() - t0 > limit_ns) break;
             }
         }
@@ -378,55 +412,69 @@ oz_gemm_kernel(const CUtensorMap *__restrict__ tmaps, const OzGroup *__restrict_
         // ---------------------------------------------------------- epilogue
         const int q = warp & 3;                       // TMEM lane quarter of this warp
         const int row = q * 32 + lane;
-        uint32_t ti = 0;
-        for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x, ++ti) {
+        int *col_exp = col_exp_all[q];
+        uint32_t ci = 0;
+        bool ok = true;
+        for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
             const OzGroup &p = groups[find_group(groups, ngroup, tile)];
             int tm, tn;
             group_tile(p, tile, tm, tn);
-            if (!mbar_wait_bounded(acc_full, ti & 1u, &abort_flag, status, CA3DMM_DEV_TIMEOUT_EPI,
-                                   limit_ns))
-                break;
-            tc_fence_after();
             const int gr = tm * OBM + row;
-            const int ebase = gr < p.m ? ework[p.ea_off + gr] : 0;
-            const int Ei = ebase ? ebase - EXP_BIAS : 0;
-            for (int c0 = 0; c0 < OBN; c0 += 16) {
-                double acc[16];
+            const int eb = gr < p.m ? ework[p.ea_off + gr] : 0;
+            const int Ei = eb ? eb - EXP_BIAS : 0;
+            // column exponents of this tile into this warp's shared slots
+            __syncwarp();
+            for (int j = lane; j < OBN; j += 32) {
+                const int gc = tn * OBN + j;
+                const int fb = gc < p.n ? ework[p.eb_off + gc] : 0;
+                col_exp[j] = fb ? fb - EXP_BIAS : 0;
+            }
+            __syncwarp();
+            double acc[OBN];
 #pragma unroll
-                for (int j = 0; j < 16; ++j) acc[j] = 0.0;
-                int Fj[16];
-#pragma unroll
-                for (int j = 0; j < 16; ++j) {
-                    const int gc = tn * OBN + c0 + j;
-                    const int fb = gc < p.n ? ework[p.eb_off + gc] : 0;
-                    Fj[j] = fb ? fb - EXP_BIAS : 0;
+            for (int j = 0; j < OBN; ++j) acc[j] = 0.0;
+            const int nch = nchunks(p.nkb, kb_per_chunk);
+            for (int ch = 0; ch < nch; ++ch, ++ci) {
+                if (!mbar_wait_bounded(acc_full, ci & 1u, &abort_flag, status,
+                                       CA3DMM_DEV_TIMEOUT_EPI, limit_ns)) {
+                    ok = false;
+                    break;
                 }
-                for (int d = slices - 1; d >= 0; --d) {
-                    uint32_t v[16];
-                    tmem_ld16(tmem_base + ((uint32_t) (q * 32) << 16) + (uint32_t) (d * OBN + c0), v);
-                    if (p.k > 0) {
+                tc_fence_after();
+                if (p.nkb > 0) {
 #pragma unroll
-                        for (int j = 0; j < 16; ++j) {
-                            // |v| < 2^31, so v * 2^e is exact unless it leaves the
-                            // normal range, where ldexp rounds it once
-                            const int e = Ei + Fj[j] - 12 - 7 * d;
-                            const double x = (double) (int) v[j];
-                            acc[j] += (e >= -1022 + 31 && e <= 1023 - 31) ? x * pow2(e)
-                                                                          : ldexp(x, e);
+                    for (int h = 0; h < OBN / 32; ++h) {
+                        for (int d = slices - 1; d >= 0; --d) {
+                            uint32_t v[32];
+                            tmem_ld32(tmem_base + ((uint32_t) (q * 32) << 16) +
+                                          (uint32_t) (d * OBN + h * 32),
+                                      v);
+#pragma unroll
+                            for (int j = 0; j < 32; ++j) {
+                                // |v| < 2^31, so v * 2^e is exact unless it leaves
+                                // the normal range, where ldexp rounds it once
+                                const int e = Ei + col_exp[h * 32 + j] - 14 - 8 * d;
+                                const double x = (double) (int) v[j];
+                                acc[h * 32 + j] += (e >= -1022 + 31 && e <= 1023 - 31)
+                                                       ? x * pow2(e)
+                                                       : ldexp(x, e);
+                            }
                         }
                     }
                 }
-                if (gr < p.m) {
+                tc_fence_before();
+                __syncwarp();
+                if (lane == 0) mbar_arrive(acc_empty);
+            }
+            if (!ok) break;
+            if (gr < p.m) {
+                double *crow = p.C + gr;
 #pragma unroll
-                    for (int j = 0; j < 16; ++j) {
-                        const int gc = tn * OBN + c0 + j;
-                        if (gc < p.n) p.C[(long long) gr + (long long) gc * p.ldc] = acc[j];
-                    }
+                for (int j = 0; j < OBN; ++j) {
+                    const int gc = tn * OBN + j;
+                    if (gc < p.n) crow[(long long) gc * p.ldc] = acc[j];
                 }
             }
-            tc_fence_before();
-            __syncwarp();
-            if (lane == 0) mbar_arrive(acc_empty);
         }
     }
     tc_fence_before();
@@ -439,56 +487,23 @@ oz_gemm_kernel(const CUtensorMap *__restrict__ tmaps, const OzGroup *__restrict_
     }
 }
 
-typedef CUresult (*encode_tiled_fn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
-                                    const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,
-                                    const cuuint32_t *, CUtensorMapInterleave, CUtensorMapSwizzle,
-                                    CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-encode_tiled_fn get_encode()
-{
-    static encode_tiled_fn fn = nullptr;
-    if (!fn) {
-        cudaDriverEntryPointQueryResult q;
-        void *p = nullptr;
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
-                cudaSuccess ||
-            q != cudaDriverEntryPointSuccess)
-            return nullptr;
-        fn = reinterpret_cast<encode_tiled_fn>(p);
-    }
-    return fn;
-}
-
-// 3D map over one block's slices: dims {kz bytes, rows, slices}.
-int encode_slices(CUtensorMap *tm, const void *base, int kz, int rows, int kpad, int slices,
-                  int box_rows)
-{
-    encode_tiled_fn enc = get_encode();
-    if (!enc) return CA3DMM_ENODEV;
-    if ((reinterpret_cast<uintptr_t>(base) & 15) || (kpad & 15)) return CA3DMM_EINVAL;
-    cuuint64_t dims[3] = {(cuuint64_t) kz, (cuuint64_t) rows, (cuuint64_t) slices};
-    cuuint64_t strides[2] = {(cuuint64_t) kpad, (cuuint64_t) kpad * (cuuint64_t) rows};
-    cuuint32_t box[3] = {(cuuint32_t) OKB, (cuuint32_t) box_rows, (cuuint32_t) slices};
-    cuuint32_t estr[3] = {1, 1, 1};
-    CUresult r = enc(tm, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, const_cast<void *>(base), dims, strides,
-                     box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_64B,
-                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-    return r == CUDA_SUCCESS ? CA3DMM_OK : CA3DMM_EINVAL;
-}
-
 size_t align256(size_t x) { return (x + 255) / 256 * 256; }
 int kpad_of(int kz) { return (kz + OKB - 1) / OKB * OKB; }
+int rows_pad_of(int rows, int tr) { return (rows + tr - 1) / tr * tr; }
 
+// k chunk (bytes) over which every diagonal sum stays exact in INT32:
+// s * kc * 2^14 < 2^31 (|q| <= 128), rounded down to the 32-byte k step (the
+// oracle's orc_ozaki_kchunk uses the same rule).
+int kchunk_of(int s) { return (int) ((2147483647L / 16384L) / s / OKB * OKB); }
 
 // Device plan layout for g groups (at most 2g operand blocks):
-// [header 256 B][2g slice descriptors][2g tensor maps, 64-byte aligned][g groups]
+// [header 256 B][2g slice descriptors][g groups]
 struct PlanLayout {
-    size_t sd, tm, gr, total;
+    size_t sd, gr, total;
     explicit PlanLayout(int g)
     {
         sd = 256;
-        tm = (sd + (size_t) 2 * g * sizeof(SliceDesc) + 127) / 128 * 128;
-        gr = tm + (size_t) 2 * g * sizeof(CUtensorMap);
+        gr = (sd + (size_t) 2 * g * sizeof(SliceDesc) + 127) / 128 * 128;
         total = gr + (size_t) g * sizeof(OzGroup);
     }
 };
@@ -503,11 +518,13 @@ extern "C" size_t ca3dmm_oz_work_bytes(int nA, const int *a_rows, const int *a_k
     size_t e = 0, q = 0;
     for (int i = 0; i < nA; ++i) {
         e += (size_t) a_rows[i];
-        q += align256((size_t) slices * a_rows[i] * kpad_of(a_k[i] > 0 ? a_k[i] : 1));
+        q += align256((size_t) slices * rows_pad_of(a_rows[i], OBM) *
+                      kpad_of(a_k[i] > 0 ? a_k[i] : 1));
     }
     for (int i = 0; i < nB; ++i) {
         e += (size_t) b_cols[i];
-        q += align256((size_t) slices * b_cols[i] * kpad_of(b_k[i] > 0 ? b_k[i] : 1));
+        q += align256((size_t) slices * rows_pad_of(b_cols[i], OBN) *
+                      kpad_of(b_k[i] > 0 ? b_k[i] : 1));
     }
     return align256(e * sizeof(int)) + q + 256;
 }
@@ -524,9 +541,7 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
     memset(h, 0, L.total);
     PlanHeader *hd = reinterpret_cast<PlanHeader *>(h);
     SliceDesc *sd = reinterpret_cast<SliceDesc *>(h + L.sd);
-    CUtensorMap *tm = reinterpret_cast<CUtensorMap *>(h + L.tm);
     OzGroup *gr = reinterpret_cast<OzGroup *>(h + L.gr);
-    unsigned char *w = static_cast<unsigned char *>(dev_work);
     // exponents first: one int array, cleared before each run
     size_t ne = 0;
     for (int i = 0; i < nA; ++i) ne += A[i].rows;
@@ -539,11 +554,13 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
         const ca3dmm_oz_blk_t &b = isA ? A[i] : B[i - nA];
         const int rows = isA ? b.rows : b.cols;   // A: rows of op(A); B: columns of op(B)
         const int kz = isA ? b.cols : b.rows;
-        const int kpad = kpad_of(kz > 0 ? kz : 1);
         SliceDesc &d = sd[i];
         d.rows = rows;
         d.kz = kz;
-        d.kpad = kpad;
+        d.kpad = kpad_of(kz > 0 ? kz : 1);
+        d.tile_rows = isA ? OBM : OBN;
+        d.rows_pad = rows_pad_of(rows, d.tile_rows);
+        d.nkb = d.kpad / OKB;
         d.q_off = (long long) qoff;
         d.e_off = eoff;
         if (isA) {
@@ -557,30 +574,23 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
             d.ls = transB ? ldB : 1;
             d.src_off = (long long) b.c0 * d.rs + (long long) b.r0 * d.ls;
         }
-        if (rows > 0 && kz > 0) {
-            int rc = encode_slices(&tm[i], w + qoff, kz, rows, kpad, slices, isA ? OBM : OBN);
-            if (rc) return rc;
-        }
-        qoff += align256((size_t) slices * rows * kpad);
+        qoff += align256((size_t) slices * d.rows_pad * d.kpad);
         eoff += rows;
-        if (rows > max_rows) max_rows = rows;
-        if (kpad > max_kpad) max_kpad = kpad;
+        if (d.rows_pad > max_rows) max_rows = d.rows_pad;
+        if (d.kpad > max_kpad) max_kpad = d.kpad;
     }
     if (qoff > work_bytes) return CA3DMM_ENOMEM;
     int tiles = 0;
     for (int g = 0; g < ngroup; ++g) {
         OzGroup &o = gr[g];
+        const SliceDesc &da = sd[G[g].a_blk], &db = sd[nA + G[g].b_blk];
         o.C = G[g].C; o.ldc = G[g].ldc;
         o.m = G[g].m; o.n = G[g].n; o.k = G[g].k;
-        if ((long long) G[g].k * slices >= (1LL << 19)) {
-            fprintf(stderr, "[ERROR] split-precision GEMM: k = %d with %d slices exceeds the exact "
-                            "INT32 range (k * slices < 2^19); use more k slabs\n", G[g].k, slices);
-            return CA3DMM_EINVAL;
-        }
-        o.a_blk = G[g].a_blk;
-        o.b_blk = nA + G[g].b_blk;
-        o.ea_off = sd[o.a_blk].e_off;
-        o.eb_off = sd[o.b_blk].e_off;
+        o.nkb = G[g].k > 0 ? da.nkb : 0;
+        o.ea_off = da.e_off;
+        o.eb_off = db.e_off;
+        o.qa_off = da.q_off;
+        o.qb_off = db.q_off;
         o.tiles_m = (o.m > 0 && o.n > 0) ? (o.m + OBM - 1) / OBM : 0;
         o.tiles_n = (o.m > 0 && o.n > 0) ? (o.n + OBN - 1) / OBN : 0;
         o.tile_begin = tiles;
@@ -604,32 +614,21 @@ extern "C" int ca3dmm_oz_run_pack(const ca3dmm_oz_plan_t *oz, const void *A, con
         reinterpret_cast<const SliceDesc *>(static_cast<const unsigned char *>(oz->dev_plan) + L.sd);
     unsigned char *w = static_cast<unsigned char *>(oz->dev_work);
     CA3DMM_CUDA_TRY(cudaMemsetAsync(w, 0, (size_t) oz->n_exp * sizeof(int), stream));
-    const int nd = oz->nA + oz->nB;
-    dim3 ge((unsigned) ((oz->max_rows + ST - 1) / ST), (unsigned) ((oz->max_kpad + ST - 1) / ST),
-            (unsigned) nd);
-    if (ge.y > 65535 || nd > 65535) return CA3DMM_EINVAL;
-    // A blocks then B blocks: the kernels read their source from the right base
-    if (oz->nA > 0) {
-        dim3 ga(ge.x, ge.y, (unsigned) oz->nA);
-        oz_exp_kernel<<<ga, 256, 0, stream>>>(static_cast<const double *>(A), sd,
-                                              reinterpret_cast<unsigned *>(w));
+    const unsigned gx = (unsigned) ((oz->max_rows + ST - 1) / ST);
+    const unsigned gy = (unsigned) ((oz->max_kpad + ST - 1) / ST);
+    if (gy > 65535 || oz->nA > 65535 || oz->nB > 65535) return CA3DMM_EINVAL;
+    const double *src[2] = {static_cast<const double *>(A), static_cast<const double *>(B)};
+    const int cnt[2] = {oz->nA, oz->nB}, first[2] = {0, oz->nA};
+    for (int o = 0; o < 2; ++o) {
+        if (cnt[o] == 0) continue;
+        oz_exp_kernel<<<dim3(gx, gy, (unsigned) cnt[o]), 256, 0, stream>>>(
+            src[o], sd + first[o], reinterpret_cast<unsigned *>(w));
         CA3DMM_CUDA_TRY(cudaGetLastError());
     }
-    if (oz->nB > 0) {
-        dim3 gb(ge.x, ge.y, (unsigned) oz->nB);
-        oz_exp_kernel<<<gb, 256, 0, stream>>>(static_cast<const double *>(B), sd + oz->nA,
-                                              reinterpret_cast<unsigned *>(w));
-        CA3DMM_CUDA_TRY(cudaGetLastError());
-    }
-    if (oz->nA > 0) {
-        dim3 ga(ge.x, ge.y, (unsigned) oz->nA);
-        oz_slice_kernel<<<ga, 256, 0, stream>>>(static_cast<const double *>(A), sd, w, oz->slices);
-        CA3DMM_CUDA_TRY(cudaGetLastError());
-    }
-    if (oz->nB > 0) {
-        dim3 gb(ge.x, ge.y, (unsigned) oz->nB);
-        oz_slice_kernel<<<gb, 256, 0, stream>>>(static_cast<const double *>(B), sd + oz->nA, w,
-                                                oz->slices);
+    for (int o = 0; o < 2; ++o) {
+        if (cnt[o] == 0) continue;
+        oz_slice_kernel<<<dim3(gx, gy, (unsigned) cnt[o]), 256, 0, stream>>>(
+            src[o], sd + first[o], w, oz->slices);
         CA3DMM_CUDA_TRY(cudaGetLastError());
     }
     return CA3DMM_OK;
@@ -643,7 +642,7 @@ extern "C" int ca3dmm_oz_run_gemm(const ca3dmm_oz_plan_t *oz, int *dev_status, d
     const unsigned char *pl = static_cast<const unsigned char *>(oz->dev_plan);
     const int stage_bytes = oz->slices * (A_SLICE_BYTES + B_SLICE_BYTES);
     int nstage = SMEM_BUDGET / stage_bytes;
-    if (nstage > 4) nstage = 4;
+    if (nstage > MAX_STAGES) nstage = MAX_STAGES;
     if (nstage < 2) return CA3DMM_EINVAL;
     const size_t smem = (size_t) nstage * stage_bytes + (2 * nstage + 2) * 8 + 1024;
     CA3DMM_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel,
@@ -651,10 +650,10 @@ extern "C" int ca3dmm_oz_run_gemm(const ca3dmm_oz_plan_t *oz, int *dev_status, d
     int grid = ca3dmm_device_sm_count();
     if (grid > oz->tiles) grid = oz->tiles;
     const unsigned long long limit = (unsigned long long) (timeout_s * 1e9);
+    const int kb_per_chunk = kchunk_of(oz->slices) / OKB;
     oz_gemm_kernel<<<grid, OTHREADS, smem, stream>>>(
-        reinterpret_cast<const CUtensorMap *>(pl + L.tm),
         reinterpret_cast<const OzGroup *>(pl + L.gr), oz->ngroup, oz->tiles, oz->slices, nstage,
-        static_cast<const int *>(oz->dev_work), dev_status, limit);
+        kb_per_chunk, static_cast<const unsigned char *>(oz->dev_work), dev_status, limit);
     CA3DMM_CUDA_TRY(cudaGetLastError());
     return CA3DMM_OK;
 }

@@ -18,9 +18,10 @@
  *   5. Closed-form answers        -- the example_AB / example_BTB deterministic fills
  *                                    (examples/example_AB.c:107-128, example_BTB.c:70-80)
  *   6. Ozaki slicing restatement  -- the split-precision path's exponent scaling and
- *                                    round-to-nearest INT8 slicing, bit-exact
+ *                                    balanced base-256 INT8 slicing, bit-exact
  *   7. MLP cost-model reference   -- FP32 forward / backward / Adam for gradient checks
  */
+#include <limits.h>
 #include <math.h>
 #include <stdint.h>
 #include <stdlib.h>
@@ -195,29 +196,48 @@ void orc_fill_example_ab(double *X, int nrow, int ncol, double ci, double cj)
 
 /* ---------------------------------------------------------------------- */
 /* 6. Ozaki INT8 slicing (bit-exact restatement of the product's rule)     */
-/*    Per row i of op(A) over l in [0,k): E_i = frexp exponent of max|a_il| */
-/*    (max|a| < 2^E_i), E_i = 0 for an all-zero row.  Slice t (0-based) of  */
-/*    a: q_t = rint(r_t * 2^(6 + 7t - E_i)), r_0 = a, r_{t+1} = r_t -        */
-/*    q_t * 2^(E_i - 6 - 7t); |q_t| <= 64.                                  */
-/*    out_q[t * m * k + i * k + l] (K-major int8), out_e[i] = E_i.           */
+/*    Per row i of op(A) over l in [0,k): E_i = max over the row of the      */
+/*    effective exponent of a: e + 1 if the frexp mantissa of |a| exceeds    */
+/*    127/128, else e (so max|a| <= 2^E_i * 127/128); E_i = 0 for a zero row. */
+/*    N = rint(a 2^(8s-1-E)) is written in balanced base-256 digits          */
+/*    q_t in [-128, 127]:  N = sum_t q_t 256^(s-1-t), least significant digit */
+/*    first: q = ((N + 128) mod 256) - 128, N = (N - q) / 256.  Hence          */
+/*    a = sum_t q_t 2^(E-7-8t) + r with |r| <= 2^(E-8s).                      */
+/*    out_q[t * m * k + i * k + l] (K-major int8), out_e[i] = E_i.            */
 /* ---------------------------------------------------------------------- */
+static int eff_exponent(double v)
+{
+    if (v == 0.0) return INT_MIN;
+    int e;
+    double m = frexp(fabs(v), &e);
+    return m > 0.9921875 ? e + 1 : e;
+}
+
+static void slice_one(double a, int E, int s, int8_t *q, long stride)
+{
+    long long N = llrint(ldexp(a, 8 * s - 1 - E));
+    for (int t = s - 1; t >= 0; t--) {
+        long long d = ((N + 128) & 255) - 128;
+        q[t * stride] = (int8_t) d;
+        N = (N - d) / 256;
+    }
+}
+
+static int row_exponent(double mxe)
+{
+    return mxe == INT_MIN ? 0 : (int) mxe;
+}
+
 void orc_ozaki_slice_rows(const double *A, long lda, int tA, int m, int k, int s,
                           int8_t *out_q, int *out_e)
 {
     for (long i = 0; i < m; i++) {
-        double mx = 0.0;
-        for (long l = 0; l < k; l++) { double v = fabs(opA(A, lda, tA, i, l)); if (v > mx) mx = v; }
-        int E = 0;
-        if (mx > 0.0) frexp(mx, &E);
+        int mx = INT_MIN;
+        for (long l = 0; l < k; l++) { int e = eff_exponent(opA(A, lda, tA, i, l)); if (e > mx) mx = e; }
+        int E = row_exponent(mx);
         out_e[i] = E;
-        for (long l = 0; l < k; l++) {
-            double r = opA(A, lda, tA, i, l);
-            for (int t = 0; t < s; t++) {
-                double q = rint(ldexp(r, 6 + 7 * t - E));
-                out_q[(long) t * m * k + i * k + l] = (int8_t) q;
-                r -= ldexp(q, E - 6 - 7 * t);
-            }
-        }
+        for (long l = 0; l < k; l++)
+            slice_one(opA(A, lda, tA, i, l), E, s, out_q + i * k + l, (long) m * k);
     }
 }
 
@@ -226,41 +246,51 @@ void orc_ozaki_slice_cols(const double *B, long ldb, int tB, int k, int n, int s
                           int8_t *out_q, int *out_e)
 {
     for (long j = 0; j < n; j++) {
-        double mx = 0.0;
-        for (long l = 0; l < k; l++) { double v = fabs(opB(B, ldb, tB, l, j)); if (v > mx) mx = v; }
-        int E = 0;
-        if (mx > 0.0) frexp(mx, &E);
+        int mx = INT_MIN;
+        for (long l = 0; l < k; l++) { int e = eff_exponent(opB(B, ldb, tB, l, j)); if (e > mx) mx = e; }
+        int E = row_exponent(mx);
         out_e[j] = E;
-        for (long l = 0; l < k; l++) {
-            double r = opB(B, ldb, tB, l, j);
-            for (int t = 0; t < s; t++) {
-                double q = rint(ldexp(r, 6 + 7 * t - E));
-                out_q[(long) t * n * k + j * k + l] = (int8_t) q;
-                r -= ldexp(q, E - 6 - 7 * t);
-            }
-        }
+        for (long l = 0; l < k; l++)
+            slice_one(opB(B, ldb, tB, l, j), E, s, out_q + j * k + l, (long) n * k);
     }
 }
 
-/* Ozaki product from slices, for small sizes: diagonal d = t + u <= s - 1,
- * exact int64 sums per diagonal, then FP64 accumulation from the least
- * significant diagonal up (the product's order).  C is m x n col-major. */
+/* k range of one exactly-accumulated chunk: every diagonal sum
+ * sum_{t+u=d} sum_l q_t q_u must stay below 2^31 with |q q| <= 2^14, i.e.
+ * s * kc * 16384 < 2^31; kc is rounded down to the GEMM's 32-byte k step. */
+int orc_ozaki_kchunk(int s)
+{
+    long kc = (2147483647L / 16384L) / s;
+    return (int) (kc / 32 * 32);
+}
+
+/* Ozaki product from slices, for small sizes: per k chunk (orc_ozaki_kchunk),
+ * diagonals d = t + u <= s - 1 as exact integer sums, recombined into one
+ * running FP64 sum per entry: for each chunk in order, d = s-1 down to 0,
+ * acc += 2^(E_i + F_j - 14 - 8d) * D_d (the product's order).  C is m x n
+ * column-major. */
 void orc_ozaki_gemm(const int8_t *qa, const int *ea, const int8_t *qb, const int *eb,
                     int m, int n, int k, int s, double *C)
 {
+    const int kc = orc_ozaki_kchunk(s);
     #pragma omp parallel for collapse(2) schedule(static)
     for (long j = 0; j < n; j++)
         for (long i = 0; i < m; i++) {
             double acc = 0.0;
-            for (int d = s - 1; d >= 0; d--) {
-                long long sum = 0;
-                for (int t = 0; t <= d; t++) {
-                    int u = d - t;
-                    const int8_t *a = qa + (long) t * m * k + i * k;
-                    const int8_t *b = qb + (long) u * n * k + j * k;
-                    for (long l = 0; l < k; l++) sum += (long long) a[l] * b[l];
+            for (long c0 = 0; c0 < k || (k == 0 && c0 == 0); c0 += kc) {
+                long c1 = c0 + kc < k ? c0 + kc : k;
+                for (int d = s - 1; d >= 0; d--) {
+                    long long sum = 0;
+                    for (int t = 0; t <= d; t++) {
+                        int u = d - t;
+                        const int8_t *a = qa + (long) t * m * k + i * k;
+                        const int8_t *b = qb + (long) u * n * k + j * k;
+                        for (long l = c0; l < c1; l++)
+                            sum += (long long) a[l] * b[l];
+                    }
+                    acc += ldexp((double) sum, ea[i] + eb[j] - 14 - 8 * d);
                 }
-                acc += ldexp((double) sum, ea[i] + eb[j] - 12 - 7 * d);
+                if (k == 0) break;
             }
             C[i + j * m] = acc;
         }

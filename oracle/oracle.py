@@ -36,11 +36,14 @@ def lib():
         L.orc_errors.argtypes = [C.c_int, dp, dp, dp, dp, C.c_double, dp]
         L.orc_rank_geometry.argtypes = [C.c_int] * 8 + [ip]
         L.orc_block_spos_size.argtypes = [C.c_int, C.c_int, C.c_int, ip, ip]
-        L.orc_ozaki_slice_rows.argtypes = [dp, C.c_long, C.c_int, C.c_int, C.c_int, C.c_int, i8p,
+        u8p = C.POINTER(C.c_int8)
+        L.orc_ozaki_slice_rows.argtypes = [dp, C.c_long, C.c_int, C.c_int, C.c_int, C.c_int, u8p,
                                            ip]
-        L.orc_ozaki_slice_cols.argtypes = [dp, C.c_long, C.c_int, C.c_int, C.c_int, C.c_int, i8p,
+        L.orc_ozaki_slice_cols.argtypes = [dp, C.c_long, C.c_int, C.c_int, C.c_int, C.c_int, u8p,
                                            ip]
-        L.orc_ozaki_gemm.argtypes = [i8p, ip, i8p, ip, C.c_int, C.c_int, C.c_int, C.c_int, dp]
+        L.orc_ozaki_gemm.argtypes = [u8p, ip, u8p, ip, C.c_int, C.c_int, C.c_int, C.c_int, dp]
+        L.orc_ozaki_kchunk.argtypes = [C.c_int]
+        L.orc_ozaki_kchunk.restype = C.c_int
         fp = C.POINTER(C.c_float)
         L.orc_mlp_fwd_bwd.argtypes = [C.c_int] * 4 + [fp] * 9 + [fp] * 6
         L.orc_mlp_fwd_bwd.restype = C.c_float
@@ -167,6 +170,7 @@ def rank_geometry(m, n, k, mp, np_, kp, rank, is_btb=0):
 
 
 def ozaki_slices_rows(A, tA, m, k, s):
+    """Slices of the rows of op(A): (int8 [s, m, k], exponents [m])."""
     A = np.asfortranarray(A, dtype=np.float64)
     q = np.zeros((s, m, k), dtype=np.int8)
     e = np.zeros(m, dtype=np.int32)
@@ -186,13 +190,17 @@ def ozaki_slices_cols(B, tB, k, n, s):
     return q, e
 
 
+def ozaki_kchunk(s):
+    return lib().orc_ozaki_kchunk(int(s))
+
+
 def ozaki_gemm(qa, ea, qb, eb, m, n, k, s):
     Cm = np.zeros((m, n), order="F")
-    i8 = C.POINTER(C.c_int8)
+    u8 = C.POINTER(C.c_int8)
     ip = C.POINTER(C.c_int)
-    lib().orc_ozaki_gemm(np.ascontiguousarray(qa).ctypes.data_as(i8),
+    lib().orc_ozaki_gemm(np.ascontiguousarray(qa).ctypes.data_as(u8),
                          np.ascontiguousarray(ea, dtype=np.int32).ctypes.data_as(ip),
-                         np.ascontiguousarray(qb).ctypes.data_as(i8),
+                         np.ascontiguousarray(qb).ctypes.data_as(u8),
                          np.ascontiguousarray(eb, dtype=np.int32).ctypes.data_as(ip),
                          m, n, k, s, _d(Cm))
     return Cm

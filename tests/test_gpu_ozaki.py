@@ -1,10 +1,11 @@
 """Split-precision (Ozaki INT8 on tcgen05) path against the oracle.
 
 Bit-exact: with the slices computed by the oracle's restatement of the
-slicing rule and the same FP64 recombination order, every C entry of the
-device result equals the oracle's, slab by slab.  Accuracy: the error
-against the double-double truth shrinks by ~2^-7 per slice and at 8 slices
-is within 2x of the plain FP64 DMMA error on the exponent-spread inputs."""
+slicing rule, the same exact k chunks and the same FP64 recombination order,
+every C entry of the device result equals the oracle's, slab by slab.
+Accuracy: the error against the double-double truth shrinks by ~2^-8 per
+slice; at 7 slices (55 bits) it is no worse than the plain FP64 DMMA error
+on the exponent-spread inputs."""
 import numpy as np
 import pytest
 
@@ -63,7 +64,7 @@ def test_ozaki_bitexact_single_group(cuda, m, n, k, s):
     (400, 300, 900, 1, 0, 6, None, 6),
     (400, 300, 900, 0, 1, 6, None, 8),
     (333, 444, 555, 1, 1, 12, (2, 2, 3), 7),
-    (64, 80, 5000, 8, 0, 8, None, 8) if False else (64, 80, 5000, 0, 0, 8, None, 8),
+    (64, 80, 5000, 0, 0, 8, None, 8),
 ])
 def test_ozaki_bitexact_virtual_grid(cuda, m, n, k, ta, tb, p, grid, s):
     A = orc.gen_signed_exp(71, *((k, m) if ta else (m, k)))
@@ -88,7 +89,19 @@ def test_ozaki_error_shrinks_with_slices_and_matches_plain(cuda):
                          ab.ravel(order="F"))["normwise"]
     for s in (3, 4, 5, 6, 7):
         assert errs[s + 1] < errs[s] or errs[s + 1] <= e_plain, errs
-    assert errs[8] <= 2.0 * e_plain, (errs, e_plain)
+    assert errs[7] <= e_plain, (errs, e_plain)
+    assert errs[8] <= e_plain, (errs, e_plain)
+
+
+@pytest.mark.parametrize("s", [5, 8])
+def test_ozaki_k_chunks_bitexact(cuda, s):
+    """k longer than one exact INT32 chunk: chunked recombination matches."""
+    kc = orc.ozaki_kchunk(s)
+    m, n, k = 130, 70, 2 * kc + 77
+    A = orc.gen_signed_exp(101, m, k)
+    B = orc.gen_signed_exp(102, k, n)
+    got, _ = _run(A, B, m, n, k, 0, 0, 1, None, cb.GEMM_OZAKI, s)
+    assert np.array_equal(got, _oracle_ozaki(A, B, m, n, k, 0, 0, 1, s))
 
 
 def test_ozaki_btb(cuda):
