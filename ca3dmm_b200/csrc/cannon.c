@@ -14,6 +14,7 @@
 #include "ca3dmm_util.h"
 #include "ca3dmm_kernels.h"
 #include "cannon.h"
+#include "partition.h"
 
 typedef struct {
     size_t off_plan, off_pack, off_A, off_B, total;

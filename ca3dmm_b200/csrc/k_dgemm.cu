@@ -159,7 +159,7 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
     }
     __syncthreads();
 
-    LoadCursor lc;
+    LoadCursor lc = {};
     uint32_t issued = 0;
     int last_p = -1;
     // Issue load number `issued` at the cursor (producer thread only).

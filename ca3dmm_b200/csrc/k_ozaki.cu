@@ -25,8 +25,12 @@
 //                         chunk the epilogue adds 2^(E_i+F_j-14-8d) D_d, d = s-1
 //                         down to 0, into FP64 registers, and stores C after the
 //                         last chunk.
-// Warp roles of the GEMM: warp 0 copy producer, warp 1 TMEM owner + MMA issuer,
-// warps 2..5 epilogue (warp w reads TMEM lanes 32*(w%4)..+31).  All waits are
+// Warp roles of the GEMM: warp 0 copy producer, warps 1, 6, 7 MMA issuers, each
+// owning a contiguous interval of diagonals (disjoint TMEM columns; warp 1 also
+// owns the TMEM allocation), warps 2..5 epilogue (warp w reads TMEM lanes
+// 32*(w%4)..+31).  Each issuing warp needs ~150-190 cycles per tcgen05.mma, so
+// one issuer cannot keep the tensor core busy with M=128 MMAs; several issuers
+// with disjoint accumulators can.  All waits are
 // bounded; on timeout the kernel records a status, drains, frees TMEM, returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
@@ -45,7 +49,8 @@ extern "C" int ca3dmm_encode_tmap_2d(void *tmap, int dtype_bytes, const void *ba
 namespace {
 
 constexpr int OBM = 128, OBN = 64, OKB = 32;    // tile rows, tile cols, k bytes per stage
-constexpr int OTHREADS = 192;
+constexpr int OTHREADS = 256;                    // 8 warps
+constexpr int MAX_ISSUERS = 3;                   // MMA issuer warps 1, 6, 7
 constexpr int MAX_SLICES = 8;
 constexpr int MAX_STAGES = 8;
 constexpr int A_SLICE_BYTES = OBM * OKB;        // 4 KiB
@@ -274,7 +279,7 @@ __device__ __forceinline__ int nchunks(int nkb, int kb_per_chunk)
 
 __global__ void __launch_bounds__(OTHREADS, 1)
 oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, int slices,
-               int nstage, int kb_per_chunk, const unsigned char *__restrict__ work,
+               int nstage, int kb_per_chunk, int4 dsplit, const unsigned char *__restrict__ work,
                int *status, unsigned long long limit_ns)
 {
     extern __shared__ uint8_t smem_raw[];
@@ -289,7 +294,7 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
     uint64_t *acc_empty = acc_full + 1;
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
-    __shared__ int col_exp_all[4][OBN];   // per epilogue warp (no cross-warp barrier)
+    __shared__ double col_scale_all[4][OBN];   // 2^F_j per epilogue warp (no cross-warp barrier)
     const int *ework = reinterpret_cast<const int *>(work);
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -297,9 +302,9 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
     if (threadIdx.x == 0) {
         for (int s = 0; s < nstage; ++s) {
             mbar_init(&full[s], 1);
-            mbar_init(&empty[s], 1);
+            mbar_init(&empty[s], MAX_ISSUERS);     // one commit per MMA issuer
         }
-        mbar_init(acc_full, 1);
+        mbar_init(acc_full, MAX_ISSUERS);
         mbar_init(acc_empty, 4);
         abort_flag = 0;
         fence_barrier_init();
@@ -351,9 +356,14 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
                     if (global_timer_ns() - t0 > limit_ns) break;
             }
         }
-    } else if (warp == 1) {
-        // ---------------------------------------------------------- MMA issuer
+    } else if (warp == 1 || warp >= 6) {
+        // ---------------------------------------------------------- MMA issuers
         if (lane == 0) {
+            // this issuer's accumulators: diagonals [d0, d1) (possibly empty; an
+            // issuer without diagonals still commits, keeping barrier counts)
+            const int ii = warp == 1 ? 0 : warp - 5;
+            const int d0 = ii == 0 ? 0 : (ii == 1 ? dsplit.x : dsplit.y);
+            const int d1 = ii == 0 ? dsplit.x : (ii == 1 ? dsplit.y : slices);
             uint32_t it = 0, ci = 0;
             bool ok = true;
             for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
@@ -378,18 +388,21 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
                         tc_fence_after();
                         const uint32_t sA = smem_u32(smem + s * stage_bytes);
                         const uint32_t sB = sA + a_bytes;
-                        // For slice t of A the partner slices u = 0..s-1-t of B are
-                        // adjacent 64-row tiles in shared memory and their
-                        // accumulators D_{t+u} adjacent 64-column blocks in TMEM,
-                        // so one MMA with N = 64 * (#u) (<= 256) covers up to four
-                        // slice products.
+                        // For slice t of A the partner slices u of B are adjacent
+                        // 64-row tiles in shared memory and their accumulators
+                        // D_{t+u} adjacent 64-column blocks in TMEM, so one MMA with
+                        // N = 64 * (#u) (<= 256) covers up to four slice products.
+                        // At t = 0 the issuer's MMAs cover all its diagonals, which
+                        // is where a chunk's accumulation starts.
                         for (int t = 0; t < slices; ++t) {
+                            const int lo = max(t, d0);
+                            if (lo >= d1) continue;
                             const uint64_t ad = sdesc_k32(sA + t * A_SLICE_BYTES);
-                            for (int u0 = 0; u0 + t < slices; u0 += 4) {
-                                const int nu = min(4, slices - t - u0);
-                                const uint64_t bd = sdesc_k32(sB + u0 * B_SLICE_BYTES);
+                            for (int dd = lo; dd < d1; dd += 4) {
+                                const int nu = min(4, d1 - dd);
+                                const uint64_t bd = sdesc_k32(sB + (dd - t) * B_SLICE_BYTES);
                                 const uint32_t acc = (kb > kb0 || t > 0) ? 1u : 0u;
-                                tc_mma_i8(tmem_base + (uint32_t) ((t + u0) * OBN), ad, bd,
+                                tc_mma_i8(tmem_base + (uint32_t) (dd * OBN), ad, bd,
                                           idesc_i8(nu * OBN), acc);
                             }
                         }
@@ -400,7 +413,7 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
                 }
             }
             if (!ok) {
-                // let every MMA already issued finish before TMEM is freed
+                // let every MMA this thread issued finish before TMEM is freed
                 tc_commit(acc_full);
                 uint64_t t0 = global_timer_ns();
                 while (!mbar_try_wait(acc_full, ci & 1u))
@@ -412,7 +425,7 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
         // ---------------------------------------------------------- epilogue
         const int q = warp & 3;                       // TMEM lane quarter of this warp
         const int row = q * 32 + lane;
-        int *col_exp = col_exp_all[q];
+        double *col_scale = col_scale_all[q];
         uint32_t ci = 0;
         bool ok = true;
         for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
@@ -420,14 +433,17 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
             int tm, tn;
             group_tile(p, tile, tm, tn);
             const int gr = tm * OBM + row;
-            const int eb = gr < p.m ? ework[p.ea_off + gr] : 0;
+            const int gm = p.m, gn = p.n;
+            const long long ldc = p.ldc;
+            double *const Cg = p.C;
+            const int eb = gr < gm ? ework[p.ea_off + gr] : 0;
             const int Ei = eb ? eb - EXP_BIAS : 0;
-            // column exponents of this tile into this warp's shared slots
+            // column scales 2^F_j of this tile into this warp's shared slots
             __syncwarp();
             for (int j = lane; j < OBN; j += 32) {
                 const int gc = tn * OBN + j;
-                const int fb = gc < p.n ? ework[p.eb_off + gc] : 0;
-                col_exp[j] = fb ? fb - EXP_BIAS : 0;
+                const int fb = gc < gn ? ework[p.eb_off + gc] : 0;
+                col_scale[j] = pow2(fb ? fb - EXP_BIAS : 0);
             }
             __syncwarp();
             double acc[OBN];
@@ -442,23 +458,21 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
                 }
                 tc_fence_after();
                 if (p.nkb > 0) {
+                    for (int d = slices - 1; d >= 0; --d) {
+                        // D_d * 2^(E_i - 14 - 8d) * 2^(F_j): both factors are powers
+                        // of two and |D_d| < 2^31, so in the supported exponent
+                        // range each product is exact and equals the oracle's
+                        // ldexp(D_d, E_i + F_j - 14 - 8d)
+                        const double rs = pow2(Ei - 14 - 8 * d);
 #pragma unroll
-                    for (int h = 0; h < OBN / 32; ++h) {
-                        for (int d = slices - 1; d >= 0; --d) {
+                        for (int h = 0; h < OBN / 32; ++h) {
                             uint32_t v[32];
                             tmem_ld32(tmem_base + ((uint32_t) (q * 32) << 16) +
                                           (uint32_t) (d * OBN + h * 32),
                                       v);
 #pragma unroll
-                            for (int j = 0; j < 32; ++j) {
-                                // |v| < 2^31, so v * 2^e is exact unless it leaves
-                                // the normal range, where ldexp rounds it once
-                                const int e = Ei + col_exp[h * 32 + j] - 14 - 8 * d;
-                                const double x = (double) (int) v[j];
-                                acc[h * 32 + j] += (e >= -1022 + 31 && e <= 1023 - 31)
-                                                       ? x * pow2(e)
-                                                       : ldexp(x, e);
-                            }
+                            for (int j = 0; j < 32; ++j)
+                                acc[h * 32 + j] += ((double) (int) v[j] * rs) * col_scale[h * 32 + j];
                         }
                     }
                 }
@@ -467,12 +481,12 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
                 if (lane == 0) mbar_arrive(acc_empty);
             }
             if (!ok) break;
-            if (gr < p.m) {
-                double *crow = p.C + gr;
+            if (gr < gm) {
+                double *crow = Cg + gr;
 #pragma unroll
                 for (int j = 0; j < OBN; ++j) {
                     const int gc = tn * OBN + j;
-                    if (gc < p.n) crow[(long long) gc * p.ldc] = acc[j];
+                    if (gc < gn) crow[(long long) gc * ldc] = acc[j];
                 }
             }
         }
@@ -495,6 +509,47 @@ int rows_pad_of(int rows, int tr) { return (rows + tr - 1) / tr * tr; }
 // s * kc * 2^14 < 2^31 (|q| <= 128), rounded down to the 32-byte k step (the
 // oracle's orc_ozaki_kchunk uses the same rule).
 int kchunk_of(int s) { return (int) ((2147483647L / 16384L) / s / OKB * OKB); }
+
+// Boundaries of the MMA issuers' diagonal intervals [0, b1), [b1, b2),
+// [b2, s): minimise the largest per-issuer MMA count per k-step, then the
+// spread of MMA columns.
+int issuer_mmas(int s, int d0, int d1, int *units)
+{
+    int n = 0;
+    *units = 0;
+    for (int t = 0; t < s; ++t) {
+        const int lo = t > d0 ? t : d0;
+        if (lo >= d1) continue;
+        n += (d1 - lo + 3) / 4;
+        *units += d1 - lo;
+    }
+    return n;
+}
+
+int4 diagonal_split(int s)
+{
+    int4 best = make_int4(s, s, 0, 0);
+    int best_instr = 1 << 30, best_gap = 1 << 30;
+    for (int b1 = 0; b1 <= s; ++b1)
+        for (int b2 = b1; b2 <= s; ++b2) {
+            int u[3], n[3];
+            n[0] = issuer_mmas(s, 0, b1, &u[0]);
+            n[1] = issuer_mmas(s, b1, b2, &u[1]);
+            n[2] = issuer_mmas(s, b2, s, &u[2]);
+            const int mi = n[0] > n[1] ? (n[0] > n[2] ? n[0] : n[2]) : (n[1] > n[2] ? n[1] : n[2]);
+            int umax = u[0], umin = u[0];
+            for (int w = 1; w < 3; ++w) {
+                if (u[w] > umax) umax = u[w];
+                if (u[w] < umin) umin = u[w];
+            }
+            if (mi < best_instr || (mi == best_instr && umax - umin < best_gap)) {
+                best = make_int4(b1, b2, 0, 0);
+                best_instr = mi;
+                best_gap = umax - umin;
+            }
+        }
+    return best;
+}
 
 // Device plan layout for g groups (at most 2g operand blocks):
 // [header 256 B][2g slice descriptors][g groups]
@@ -653,7 +708,8 @@ extern "C" int ca3dmm_oz_run_gemm(const ca3dmm_oz_plan_t *oz, int *dev_status, d
     const int kb_per_chunk = kchunk_of(oz->slices) / OKB;
     oz_gemm_kernel<<<grid, OTHREADS, smem, stream>>>(
         reinterpret_cast<const OzGroup *>(pl + L.gr), oz->ngroup, oz->tiles, oz->slices, nstage,
-        kb_per_chunk, static_cast<const unsigned char *>(oz->dev_work), dev_status, limit);
+        kb_per_chunk, diagonal_split(oz->slices), static_cast<const unsigned char *>(oz->dev_work),
+        dev_status, limit);
     CA3DMM_CUDA_TRY(cudaGetLastError());
     return CA3DMM_OK;
 }
