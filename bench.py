@@ -43,6 +43,11 @@ def parse():
     ap.add_argument("--trans-a", type=int, default=0)
     ap.add_argument("--size", type=int, default=M)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="square", choices=["square", "grouped", "btb"],
+                    help="square: the headline 8000^3 engine exec; grouped: 256 uneven "
+                         "independent GEMMs in one graph-captured launch; btb: B^T B of a "
+                         "1048576 x 512 B on a 1x1x32 grid")
+    ap.add_argument("--nprob", type=int, default=256)
     return ap.parse_args()
 
 
@@ -212,9 +217,88 @@ def reference_arm(args, world, rank):
     print(json.dumps(line), flush=True)
 
 
+def grouped_problems(nprob, seed=2024):
+    """256 GEMMs, m, n, k = round(exp(U[ln 64, ln 4096])), random trans flags,
+    entries u * 2^e with u uniform in [-1, 1), e uniform in [-4, 4]."""
+    rng = np.random.default_rng(seed)
+    dims = np.exp(rng.uniform(np.log(64), np.log(4096), size=(nprob, 3))).round().astype(int)
+    ta = rng.integers(0, 2, nprob)
+    tb = rng.integers(0, 2, nprob)
+    return [(int(m), int(n), int(k), int(ta[i]), int(tb[i])) for i, (m, n, k) in enumerate(dims)]
+
+
+def run_grouped(args, world, rank, local):
+    """Configuration 4: one persistent grouped launch (captured in a CUDA graph)
+    against one plain DMMA launch per GEMM."""
+    import torch
+    import ca3dmm_b200 as cb
+    from oracle import oracle as orc
+    torch.cuda.set_device(local)
+    probs = grouped_problems(args.nprob)
+    flops = sum(2.0 * m * n * k for m, n, k, _, _ in probs)
+    dA, dB, dC, lda, ldb, ldc = [], [], [], [], [], []
+    for i, (m, n, k, ta, tb) in enumerate(probs):
+        A = orc.gen_signed_exp(3000 + i, *((k, m) if ta else (m, k)), emin=-4, emax=4, unit=True)
+        B = orc.gen_signed_exp(4000 + i, *((n, k) if tb else (k, n)), emin=-4, emax=4, unit=True)
+        dA.append(torch.from_numpy(A.ravel(order="F").copy()).cuda()); lda.append(A.shape[0])
+        dB.append(torch.from_numpy(B.ravel(order="F").copy()).cuda()); ldb.append(B.shape[0])
+        dC.append(torch.zeros(m * n, dtype=torch.float64, device="cuda")); ldc.append(m)
+    stream = torch.cuda.Stream()
+    res = {}
+
+    def timed(fn, steps):
+        # everything (library launches, graph replays, events) on `stream`
+        with torch.cuda.stream(stream):
+            for _ in range(max(args.warmup, 1)):
+                fn()
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            for _ in range(steps):
+                fn()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / steps
+
+    # one plain DMMA launch (pack + GEMM) per product
+    singles = [cb.GroupedGemm([m], [n], [k], [ta], [tb]) for m, n, k, ta, tb in probs]
+    for i, g in enumerate(singles):
+        g.set_stream(stream.cuda_stream, 0)
+
+    def run_singles():
+        for i, g in enumerate(singles):
+            g.exec([dA[i]], [lda[i]], [dB[i]], [ldb[i]], [dC[i]], [ldc[i]])
+    res["per_gemm_launches_ms"] = timed(run_singles, args.steps)
+    for mode, sl, key in ((cb.GEMM_PLAIN, 0, "grouped_plain"), (cb.GEMM_OZAKI, 7, "grouped_ozaki7")):
+        g = cb.GroupedGemm([p[0] for p in probs], [p[1] for p in probs], [p[2] for p in probs],
+                           [p[3] for p in probs], [p[4] for p in probs], mode=mode, slices=sl)
+        assert g.ok
+        assert g.exec(dA, lda, dB, ldb, dC, ldc) == 0
+        g.set_stream(stream.cuda_stream, 0)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=stream):
+            g.exec(dA, lda, dB, ldb, dC, ldc)
+        res[key + "_ms"] = timed(graph.replay, args.steps)
+        del graph
+    v = flops / (res["grouped_ozaki7_ms"] * 1e-3) / 1e12
+    out = {"metric": METRIC, "value": v, "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps,
+           "warmup": args.warmup, "ms_per_step": res["grouped_ozaki7_ms"],
+           "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic",
+           "config": {"workload": "%d independent GEMMs, m,n,k log-uniform in [64,4096], random "
+                                  "trans, one grouped launch in a CUDA graph" % len(probs),
+                      "total_flop": flops},
+           "legs_ms": res,
+           "legs_tflops": {k.replace("_ms", ""): flops / (t * 1e-3) / 1e12 for k, t in res.items()}}
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
+    if args.workload == "grouped" and args.impl == "ours":
+        run_grouped(args, world, rank, local)
+        return
     if args.impl == "reference":
         reference_arm(args, world, rank)
         return

@@ -111,6 +111,12 @@ def lib():
         "dev_type_memcpy": (None, [p, p, sz, i, i]),
         "ca3dmm_dgemm_kslab_noalloc": (i, [i, i, i, i, p, i, p, i, p, i, p]),
         "ca3dmm_dgemm_kslab_noalloc_scratch_bytes": (sz, []),
+        "ca3dmm_grouped_init": (i, [i, pi, pi, pi, pi, pi, i, i, C.POINTER(p), C.POINTER(sz)]),
+        "ca3dmm_grouped_attach_workbuf": (i, [p, p]),
+        "ca3dmm_grouped_set_stream": (None, [p, p, i]),
+        "ca3dmm_grouped_exec": (i, [p, C.POINTER(p), pi, C.POINTER(p), pi, C.POINTER(p), pi]),
+        "ca3dmm_grouped_last_ms": (d, [p]),
+        "ca3dmm_grouped_free": (None, [C.POINTER(p)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -275,6 +281,51 @@ class CannonEngine:
     def free(self):
         if self.e:
             lib().cannon_engine_free(C.byref(self.e))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class GroupedGemm:
+    """Python mirror of ca3dmm_grouped_{init,exec,free}: a batch of independent
+    C_i = op(A_i) op(B_i) run as one persistent grouped launch."""
+
+    def __init__(self, ms, ns, ks, trans_a=None, trans_b=None, mode=GEMM_PLAIN, slices=7):
+        L = lib()
+        npb = len(ms)
+        arr = lambda v: (C.c_int * npb)(*[int(x) for x in v])
+        self.n = npb
+        self.ms, self.ns, self.ks = list(ms), list(ns), list(ks)
+        self.ta = list(trans_a) if trans_a is not None else [0] * npb
+        self.tb = list(trans_b) if trans_b is not None else [0] * npb
+        self.h = C.c_void_p()
+        self.rc = L.ca3dmm_grouped_init(npb, arr(ms), arr(ns), arr(ks), arr(self.ta), arr(self.tb),
+                                        int(mode), int(slices), C.byref(self.h), None)
+
+    @property
+    def ok(self):
+        return self.rc == 0 and bool(self.h)
+
+    def set_stream(self, stream, sync=1):
+        lib().ca3dmm_grouped_set_stream(self.h, C.c_void_p(stream), int(sync))
+
+    def exec(self, A, ldA, B, ldB, Cs, ldC):
+        npb = self.n
+        P = C.c_void_p * npb
+        I = C.c_int * npb
+        return lib().ca3dmm_grouped_exec(self.h, P(*[_ptr(x) for x in A]), I(*ldA),
+                                         P(*[_ptr(x) for x in B]), I(*ldB),
+                                         P(*[_ptr(x) for x in Cs]), I(*ldC))
+
+    def last_ms(self):
+        return lib().ca3dmm_grouped_last_ms(self.h)
+
+    def free(self):
+        if self.h:
+            lib().ca3dmm_grouped_free(C.byref(self.h))
 
     def __del__(self):
         try:

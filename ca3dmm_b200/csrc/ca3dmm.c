@@ -61,11 +61,16 @@ typedef struct {
     const void *c_A, *c_B;
     void *c_dst;
     int gemm_tiles;
+    int pack_tiles_A, pack_tiles_B, pack_tiles_C;
     /* dst_C block */
     int has_dst, dst_srow, dst_nrow, dst_scol, dst_ncol;
     cudaEvent_t ev[5];
     int events_ok;
     ca3dmm_oz_plan_t oz;
+    ca3dmm_dgemm_desc_t *gd;      /* per-group GEMM descriptors (plan build scratch) */
+    ca3dmm_oz_blk_t *ob;
+    ca3dmm_oz_src_t *os;
+    ca3dmm_oz_group_t *og;
 } plan_t;
 
 
@@ -156,11 +161,14 @@ static void plan_layout(ca3dmm_engine_p e, plan_t *pl)
     pl->off_oz = off;
     pl->oz_bytes = 0;
     if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
-        int am[1024], ak[1024], bn[1024], bk[1024];
-        int na = pl->nA < 1024 ? pl->nA : 1024, nb = pl->nB < 1024 ? pl->nB : 1024;
-        for (int i = 0; i < na; i++) { am[i] = pl->A[i].rows; ak[i] = pl->A[i].cols; }
-        for (int i = 0; i < nb; i++) { bk[i] = pl->B[i].rows; bn[i] = pl->B[i].cols; }
-        pl->oz_bytes = ca3dmm_oz_work_bytes(na, am, ak, nb, bk, bn, e->ozaki_slices);
+        int *dims = (int *) malloc(sizeof(int) * 2 * (size_t) (pl->nA + pl->nB));
+        if (dims) {
+            int *am = dims, *ak = dims + pl->nA, *bk = dims + 2 * pl->nA, *bn = bk + pl->nB;
+            for (int i = 0; i < pl->nA; i++) { am[i] = pl->A[i].rows; ak[i] = pl->A[i].cols; }
+            for (int i = 0; i < pl->nB; i++) { bk[i] = pl->B[i].rows; bn[i] = pl->B[i].cols; }
+            pl->oz_bytes = ca3dmm_oz_work_bytes(pl->nA, am, ak, pl->nB, bk, bn, e->ozaki_slices);
+            free(dims);
+        }
         off = align_up(off + pl->oz_bytes);
     }
     pl->total = off;
@@ -180,7 +188,12 @@ static int plan_build(ca3dmm_engine_p e)
     pl->groups = (group_t *) calloc((size_t) pl->ngroup, sizeof(group_t));
     pl->A = (blk_t *) calloc((size_t) pl->nA, sizeof(blk_t));
     pl->B = (blk_t *) calloc((size_t) pl->nB, sizeof(blk_t));
-    if (!pl->groups || !pl->A || !pl->B) return CA3DMM_ENOMEM;
+    pl->gd = (ca3dmm_dgemm_desc_t *) calloc((size_t) pl->ngroup, sizeof(ca3dmm_dgemm_desc_t));
+    pl->ob = (ca3dmm_oz_blk_t *) calloc((size_t) (pl->nA + pl->nB), sizeof(ca3dmm_oz_blk_t));
+    pl->os = (ca3dmm_oz_src_t *) calloc((size_t) (pl->nA + pl->nB), sizeof(ca3dmm_oz_src_t));
+    pl->og = (ca3dmm_oz_group_t *) calloc((size_t) pl->ngroup, sizeof(ca3dmm_oz_group_t));
+    if (!pl->groups || !pl->A || !pl->B || !pl->gd || !pl->ob || !pl->os || !pl->og)
+        return CA3DMM_ENOMEM;
     for (int tk = 0; tk < kp; tk++) {
         int ks, kz;
         calc_block_spos_size(e->k, kp, tk, &ks, &kz);
@@ -240,6 +253,10 @@ static void plan_free(plan_t *pl)
     free(pl->groups);
     free(pl->A);
     free(pl->B);
+    free(pl->gd);
+    free(pl->ob);
+    free(pl->os);
+    free(pl->og);
     if (pl->stage) cudaFreeHost(pl->stage);
     if (pl->status_h) cudaFreeHost(pl->status_h);
     if (pl->events_ok)
@@ -577,6 +594,7 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
         d->dst_off = (long long) ((b->off) / sizeof(double));
         d->ldd = b->ld;
     }
+    pl->pack_tiles_A = ca3dmm_pack_tiles(pa, pl->nA);
     ca3dmm_pack_desc_t *pb = (ca3dmm_pack_desc_t *) (h + pl->off_packB);
     for (int i = 0; i < pl->nB; i++) {
         blk_t *b = &pl->B[i];
@@ -588,6 +606,7 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
         d->dst_off = (long long) ((b->off) / sizeof(double));
         d->ldd = b->ld;
     }
+    pl->pack_tiles_B = ca3dmm_pack_tiles(pb, pl->nB);
     /* output target of the GEMM (kp == 1) or of the reduction (kp > 1) */
     int whole = pl->has_dst && pl->dst_srow == 0 && pl->dst_scol == 0 && pl->dst_nrow == e->m &&
                 pl->dst_ncol == e->n;
@@ -599,8 +618,8 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
         pc->rows = pl->dst_nrow; pc->cols = pl->dst_ncol; pc->lds = e->m; pc->ldd = ldC;
         pc->src_off = (long long) pl->dst_srow + (long long) pl->dst_scol * e->m;
     }
-    ca3dmm_dgemm_desc_t gd[4096];
-    if (pl->ngroup > 4096) return CA3DMM_EINVAL;
+    pl->pack_tiles_C = ca3dmm_pack_tiles(pc, 1);
+    ca3dmm_dgemm_desc_t *gd = pl->gd;
     for (int i = 0; i < pl->ngroup; i++) {
         group_t *g = &pl->groups[i];
         ca3dmm_dgemm_desc_t *q = &gd[i];
@@ -622,9 +641,15 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
     int rc = ca3dmm_dgemm_plan_encode(gd, pl->ngroup, h + pl->off_gemm, &pl->gemm_tiles);
     if (rc) return rc;
     if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
-        ca3dmm_oz_blk_t ob[2048];
-        ca3dmm_oz_group_t og[4096];
-        if (pl->nA + pl->nB > 2048) return CA3DMM_EINVAL;
+        ca3dmm_oz_blk_t *ob = pl->ob;
+        ca3dmm_oz_src_t *os = pl->os;
+        ca3dmm_oz_group_t *og = pl->og;
+        for (int i = 0; i < pl->nA + pl->nB; i++) {
+            os[i].base = NULL;
+            os[i].ld = i < pl->nA ? ldA : ldB;
+            os[i].trans = i < pl->nA ? e->trans_A : e->trans_B;
+            os[i].pad = 0;
+        }
         for (int i = 0; i < pl->nA; i++) {
             ob[i].r0 = pl->A[i].r0; ob[i].c0 = pl->A[i].c0;
             ob[i].rows = pl->A[i].rows; ob[i].cols = pl->A[i].cols;
@@ -638,10 +663,9 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
             og[i].C = gd[i].C; og[i].ldc = gd[i].ldc;
             og[i].m = gd[i].m; og[i].n = gd[i].n; og[i].k = gd[i].k;
         }
-        rc = ca3dmm_oz_plan_encode(&pl->oz, e->ozaki_slices, pl->nA, ob, pl->nB, ob + pl->nA,
-                                   pl->ngroup, og, ldA, e->trans_A, ldB, e->trans_B,
-                                   w + pl->off_oz, pl->oz_bytes, h + pl->off_ozplan,
-                                   w + pl->off_ozplan);
+        rc = ca3dmm_oz_plan_encode(&pl->oz, e->ozaki_slices, pl->nA, ob, os, pl->nB,
+                                   ob + pl->nA, os + pl->nA, pl->ngroup, og, w + pl->off_oz,
+                                   pl->oz_bytes, h + pl->off_ozplan, w + pl->off_ozplan);
         if (rc) return rc;
     }
     memset(h + pl->off_status, 0, 64);
@@ -678,27 +702,17 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
     }
     int timing = e->sync_exec && pl->events_ok;
     if (timing) cudaEventRecord(pl->ev[0], st);
-    int max_r = 1, max_c = 1;
-    for (int i = 0; i < pl->nA; i++) {
-        if (pl->A[i].rows > max_r) max_r = pl->A[i].rows;
-        if (pl->A[i].cols > max_c) max_c = pl->A[i].cols;
-    }
     if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
         rc = ca3dmm_oz_run_pack(&pl->oz, src_A, src_B, st);
         if (rc) return rc;
     } else {
         rc = ca3dmm_pack_launch((const double *) src_A, (double *) w,
-                                (const ca3dmm_pack_desc_t *) (w + pl->off_packA), pl->nA, max_r,
-                                max_c, e->trans_A, st);
+                                (const ca3dmm_pack_desc_t *) (w + pl->off_packA), pl->nA,
+                                pl->pack_tiles_A, st);
         if (rc) return rc;
-        max_r = 1; max_c = 1;
-        for (int i = 0; i < pl->nB; i++) {
-            if (pl->B[i].rows > max_r) max_r = pl->B[i].rows;
-            if (pl->B[i].cols > max_c) max_c = pl->B[i].cols;
-        }
         rc = ca3dmm_pack_launch((const double *) src_B, (double *) w,
-                                (const ca3dmm_pack_desc_t *) (w + pl->off_packB), pl->nB, max_r,
-                                max_c, e->trans_B, st);
+                                (const ca3dmm_pack_desc_t *) (w + pl->off_packB), pl->nB,
+                                pl->pack_tiles_B, st);
         if (rc) return rc;
     }
     if (timing) cudaEventRecord(pl->ev[1], st);
@@ -722,8 +736,8 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
     if (timing) cudaEventRecord(pl->ev[3], st);
     if (pl->has_dst && !whole) {
         rc = ca3dmm_pack_launch((const double *) (w + pl->off_cout), (double *) dst_C,
-                                (const ca3dmm_pack_desc_t *) (w + pl->off_copy), 1, pl->dst_nrow,
-                                pl->dst_ncol, 0, st);
+                                (const ca3dmm_pack_desc_t *) (w + pl->off_copy), 1,
+                                pl->pack_tiles_C, st);
         if (rc) return rc;
     }
     if (timing) cudaEventRecord(pl->ev[4], st);

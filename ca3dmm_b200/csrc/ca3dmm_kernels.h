@@ -53,12 +53,19 @@ int ca3dmm_dgemm_launch(const void *dev_plan, int nprob, int total_tiles, int *d
 typedef struct {
     long long src_off, lds;
     long long dst_off, ldd;
-    int rows, cols, trans, pad;
+    int rows, cols, trans;
+    int tile_begin;          /* first 64 x 64 tile of this block (set by ca3dmm_pack_tiles) */
 } ca3dmm_pack_desc_t;
 
+/* Assign each descriptor its range of 64 x 64 tiles; returns the total. */
+int ca3dmm_pack_tiles(ca3dmm_pack_desc_t *descs, int ndesc);
+/* One launch over the flat tile list of all descriptors (any mix of sizes and
+ * transposes).  Element offsets are taken from src_base / dst_base; with a
+ * NULL base the offset is an absolute address divided by 8 (batches whose
+ * blocks live in unrelated allocations). */
 int ca3dmm_pack_launch(const double *src_base, double *dst_base,
-                       const ca3dmm_pack_desc_t *dev_descs, int ndesc, int max_rows, int max_cols,
-                       int any_trans, cudaStream_t stream);
+                       const ca3dmm_pack_desc_t *dev_descs, int ndesc, int total_tiles,
+                       cudaStream_t stream);
 
 /* ---- kp-slab reduction ---------------------------------------------------
  * out[i + j*ldo] = sum_{s=0}^{nslab-1} slab[s*slab_stride + i + j*lds]

@@ -20,6 +20,16 @@ extern "C" {
 
 typedef struct { int r0, c0, rows, cols; } ca3dmm_oz_blk_t;   /* block of op(A) or op(B) */
 
+/* Where one operand block's source lives: op(X)(r, l) of the block's matrix
+ * is read with leading dimension ld and transpose flag trans.  base == NULL:
+ * offsets are relative to the pointer passed to ca3dmm_oz_run_pack (engine);
+ * otherwise base is the block's matrix itself (batched problems). */
+typedef struct {
+    const void *base;
+    long long ld;
+    int trans, pad;
+} ca3dmm_oz_src_t;
+
 typedef struct {
     int a_blk, b_blk;     /* operand blocks */
     double *C;            /* output (column-major) */
@@ -31,6 +41,7 @@ typedef struct {
     int slices, nA, nB, ngroup;
     int tiles;            /* total output tiles of the grouped INT8 launch */
     int max_rows, max_kpad;
+    int slice_tiles_a, slice_tiles_b;   /* 64 x 64 slicing tiles of the A / B blocks */
     long long n_exp;      /* exponents (ints) at the start of the work region */
     void *dev_plan;       /* device copy of the plan (slice descriptors, tensor maps, groups) */
     void *dev_work;       /* slices and exponents */
@@ -44,10 +55,9 @@ size_t ca3dmm_oz_work_bytes(int nA, const int *a_rows, const int *a_k, int nB, c
  * of op(A), first k), rows x cols = rows x kz; B blocks: (r0, c0) = (first k,
  * first column of op(B)), rows x cols = kz x cols. */
 int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA, const ca3dmm_oz_blk_t *A,
-                          int nB, const ca3dmm_oz_blk_t *B, int ngroup,
-                          const ca3dmm_oz_group_t *G, long long ldA, int transA, long long ldB,
-                          int transB, void *dev_work, size_t work_bytes, void *host_plan,
-                          void *dev_plan);
+                          const ca3dmm_oz_src_t *srcA, int nB, const ca3dmm_oz_blk_t *B,
+                          const ca3dmm_oz_src_t *srcB, int ngroup, const ca3dmm_oz_group_t *G,
+                          void *dev_work, size_t work_bytes, void *host_plan, void *dev_plan);
 /* Exponent extraction + slicing of every A and B block straight from the
  * caller's matrices (op(A)(i,l) = transA ? A[l + i*ldA] : A[i + l*ldA]). */
 int ca3dmm_oz_run_pack(const ca3dmm_oz_plan_t *oz, const void *A, const void *B,

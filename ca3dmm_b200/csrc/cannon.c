@@ -159,9 +159,10 @@ static int cannon_exec_device(cannon_engine_p e, double alpha, double beta, cons
         d.rows = m; d.cols = k; d.lds = lda; d.ldd = ca3dmm_round_up(m, 2);
         Ause = (const double *) e->A_recv_d;
         lda = d.ldd;
+        int tiles = ca3dmm_pack_tiles(&d, 1);
         CA3DMM_CUDA_TRY(cudaMemcpy(w + cp->off_pack, &d, sizeof(d), cudaMemcpyHostToDevice));
         int rc = ca3dmm_pack_launch(A, (double *) e->A_recv_d,
-                                    (const ca3dmm_pack_desc_t *) (w + cp->off_pack), 1, m, k, 0, 0);
+                                    (const ca3dmm_pack_desc_t *) (w + cp->off_pack), 1, tiles, 0);
         if (rc) return rc;
     }
     if (!tma_ok(B, ldb) && k > 0 && n > 0) {
@@ -170,9 +171,11 @@ static int cannon_exec_device(cannon_engine_p e, double alpha, double beta, cons
         d.rows = k; d.cols = n; d.lds = ldb; d.ldd = ca3dmm_round_up(k, 2);
         Buse = (const double *) e->B_recv_d;
         ldb = d.ldd;
+        int tiles = ca3dmm_pack_tiles(&d, 1);
         CA3DMM_CUDA_TRY(cudaMemcpy(w + cp->off_pack + 64, &d, sizeof(d), cudaMemcpyHostToDevice));
         int rc = ca3dmm_pack_launch(B, (double *) e->B_recv_d,
-                                    (const ca3dmm_pack_desc_t *) (w + cp->off_pack + 64), 1, k, n, 0, 0);
+                                    (const ca3dmm_pack_desc_t *) (w + cp->off_pack + 64), 1, tiles,
+                                    0);
         if (rc) return rc;
     }
     ca3dmm_dgemm_desc_t g;

@@ -59,13 +59,14 @@ void dev_type_copy_mat_blk(size_t dt_size, const int nrow, const int ncol, const
     ca3dmm_pack_desc_t d;
     memset(&d, 0, sizeof(d));
     d.lds = lds; d.ldd = ldd; d.rows = ncol; d.cols = nrow; d.trans = 0;
+    int tiles = ca3dmm_pack_tiles(&d, 1);
     ca3dmm_pack_desc_t *dd = NULL;
     if (cudaMalloc((void **) &dd, sizeof(d)) != cudaSuccess) {
         ERROR_PRINTF("dev_type_copy_mat_blk: descriptor allocation failed\n");
         return;
     }
     cudaMemcpy(dd, &d, sizeof(d), cudaMemcpyHostToDevice);
-    if (ca3dmm_pack_launch((const double *) src, (double *) dst, dd, 1, ncol, nrow, 0, 0))
+    if (ca3dmm_pack_launch((const double *) src, (double *) dst, dd, 1, tiles, 0))
         ERROR_PRINTF("dev_type_copy_mat_blk: pack launch failed\n");
     cudaDeviceSynchronize();
     cudaFree(dd);

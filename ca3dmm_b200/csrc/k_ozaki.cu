@@ -67,6 +67,8 @@ struct SliceDesc {
     long long e_off;        // int offset of the exponents in the work region
     int rows, kz, kpad;     // kpad = kz rounded up to OKB
     int rows_pad, tile_rows, nkb;   // rows rounded up to tile_rows (128 for A, 64 for B)
+    int tile_begin;         // first 64 x 64 slicing tile of this block (per operand)
+    int pad;
 };
 
 struct OzGroup {
@@ -87,48 +89,71 @@ struct PlanHeader {
 // ------------------------------------------------------------------ slicing
 constexpr int ST = 64;   // slicing tile edge (rows x k)
 
-__global__ void __launch_bounds__(256)
-oz_exp_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ descs,
-              unsigned *__restrict__ ework)
+__device__ __forceinline__ int find_slice_desc(const SliceDesc *d, int n, int tile)
 {
-    const SliceDesc d = descs[blockIdx.z];
-    const int r0 = blockIdx.x * ST, l0 = blockIdx.y * ST;
-    if (r0 >= d.rows || l0 >= d.kz) return;
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (d[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ const double *slice_src(const double *base, long long off)
+{
+    // with a NULL base the offset is an absolute address / 8 (batched sources)
+    return reinterpret_cast<const double *>(reinterpret_cast<uintptr_t>(base) +
+                                            (uintptr_t) off * sizeof(double));
+}
+
+// Persistent over the flat list of 64 x 64 (rows x k) tiles of every block.
+__global__ void __launch_bounds__(256)
+oz_exp_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ descs, int ndesc,
+              int total_tiles, unsigned *__restrict__ ework)
+{
     __shared__ int smax[ST];
-    if (threadIdx.x < ST) smax[threadIdx.x] = 0;
-    __syncthreads();
-    const double *base = src + d.src_off;
-    const bool rfast = d.rs == 1;   // consecutive threads walk the contiguous index
-    for (int e = threadIdx.x; e < ST * ST; e += blockDim.x) {
-        const int a = e % ST, b = e / ST;
-        const int r = rfast ? a : b, l = rfast ? b : a;
-        const int gr = r0 + r, gl = l0 + l;
-        if (gr < d.rows && gl < d.kz) {
-            const double v = fabs(__ldg(base + gr * d.rs + gl * d.ls));
-            if (v != 0.0) {
-                // effective exponent: one more when the mantissa exceeds 127/128,
-                // so that max|x| <= 2^E * 127/128 and the top digit fits in int8
-                int ex;
-                const double mant = frexp(v, &ex);
-                atomicMax(&smax[r], ex + (mant > 0.9921875 ? 1 : 0) + EXP_BIAS);
+    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+        const SliceDesc d = descs[find_slice_desc(descs, ndesc, tile)];
+        const int local = tile - d.tile_begin, tx = (d.rows_pad + ST - 1) / ST;
+        const int r0 = (local % tx) * ST, l0 = (local / tx) * ST;
+        __syncthreads();
+        if (threadIdx.x < ST) smax[threadIdx.x] = 0;
+        __syncthreads();
+        const double *base = slice_src(src, d.src_off);
+        const bool rfast = d.rs == 1;   // consecutive threads walk the contiguous index
+        for (int e = threadIdx.x; e < ST * ST; e += blockDim.x) {
+            const int a = e % ST, b = e / ST;
+            const int r = rfast ? a : b, l = rfast ? b : a;
+            const int gr = r0 + r, gl = l0 + l;
+            if (gr < d.rows && gl < d.kz) {
+                const double v = fabs(__ldg(base + gr * d.rs + gl * d.ls));
+                if (v != 0.0) {
+                    // effective exponent: one more when the mantissa exceeds 127/128,
+                    // so that max|x| <= 2^E * 127/128 and the top digit fits in int8
+                    int ex;
+                    const double mant = frexp(v, &ex);
+                    atomicMax(&smax[r], ex + (mant > 0.9921875 ? 1 : 0) + EXP_BIAS);
+                }
             }
         }
+        __syncthreads();
+        if (threadIdx.x < ST && r0 + threadIdx.x < d.rows && smax[threadIdx.x] > 0)
+            atomicMax(ework + d.e_off + r0 + threadIdx.x, (unsigned) smax[threadIdx.x]);
     }
-    __syncthreads();
-    if (threadIdx.x < ST && r0 + threadIdx.x < d.rows && smax[threadIdx.x] > 0)
-        atomicMax(ework + d.e_off + r0 + threadIdx.x, (unsigned) smax[threadIdx.x]);
 }
 
 __global__ void __launch_bounds__(256)
-oz_slice_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ descs,
-                unsigned char *__restrict__ work, int slices)
+oz_slice_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ descs, int ndesc,
+                int total_tiles, unsigned char *__restrict__ work, int slices)
 {
-    const SliceDesc d = descs[blockIdx.z];
-    const int r0 = blockIdx.x * ST, l0 = blockIdx.y * ST;
-    if (r0 >= d.rows_pad || l0 >= d.kpad) return;
     __shared__ double tile[ST][ST + 1];
-    const double *base = src + d.src_off;
+  for (int gtile = blockIdx.x; gtile < total_tiles; gtile += gridDim.x) {
+    const SliceDesc d = descs[find_slice_desc(descs, ndesc, gtile)];
+    const int local = gtile - d.tile_begin, tx = (d.rows_pad + ST - 1) / ST;
+    const int r0 = (local % tx) * ST, l0 = (local / tx) * ST;
+    const double *base = slice_src(src, d.src_off);
     const bool rfast = d.rs == 1;
+    __syncthreads();
     for (int e = threadIdx.x; e < ST * ST; e += blockDim.x) {
         const int a = e % ST, b = e / ST;
         const int r = rfast ? a : b, l = rfast ? b : a;
@@ -139,7 +164,7 @@ oz_slice_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ de
     // thread -> (row r, 16 consecutive k = one 16-byte chunk of a 32-byte k-block)
     const int r = threadIdx.x >> 2, c = (threadIdx.x & 3) * 16;
     const int gr = r0 + r, gl = l0 + c;
-    if (gr >= d.rows_pad || gl >= d.kpad) return;
+    if (gr >= d.rows_pad || gl >= d.kpad) continue;
     const unsigned eb = gr < d.rows ? reinterpret_cast<const unsigned *>(work)[d.e_off + gr] : 0u;
     const int E = eb ? (int) eb - EXP_BIAS : 0;
     // N = rint(x 2^(8s-1-E)) in balanced base-256 digits q_t in [-128, 127],
@@ -173,6 +198,7 @@ oz_slice_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ de
         if (t < slices)
             *reinterpret_cast<uint4 *>(dst + t * tile_bytes) =
                 make_uint4(q[t][0], q[t][1], q[t][2], q[t][3]);
+  }
 }
 
 // ------------------------------------------------------------------ tcgen05 GEMM
@@ -585,9 +611,10 @@ extern "C" size_t ca3dmm_oz_work_bytes(int nA, const int *a_rows, const int *a_k
 }
 
 extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
-                                     const ca3dmm_oz_blk_t *A, int nB, const ca3dmm_oz_blk_t *B,
-                                     int ngroup, const ca3dmm_oz_group_t *G, long long ldA,
-                                     int transA, long long ldB, int transB, void *dev_work,
+                                     const ca3dmm_oz_blk_t *A, const ca3dmm_oz_src_t *srcA,
+                                     int nB, const ca3dmm_oz_blk_t *B,
+                                     const ca3dmm_oz_src_t *srcB, int ngroup,
+                                     const ca3dmm_oz_group_t *G, void *dev_work,
                                      size_t work_bytes, void *host_plan, void *dev_plan)
 {
     if (slices < 2 || slices > MAX_SLICES || nA + nB > 2 * ngroup) return CA3DMM_EINVAL;
@@ -604,6 +631,7 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
     size_t qoff = align256(ne * sizeof(int));
     long long eoff = 0;
     int max_rows = 1, max_kpad = 1;
+    int tiles_op[2] = {0, 0};
     for (int i = 0; i < nA + nB; ++i) {
         const bool isA = i < nA;
         const ca3dmm_oz_blk_t &b = isA ? A[i] : B[i - nA];
@@ -618,17 +646,22 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
         d.nkb = d.kpad / OKB;
         d.q_off = (long long) qoff;
         d.e_off = eoff;
+        const ca3dmm_oz_src_t &src = isA ? srcA[i] : srcB[i - nA];
         if (isA) {
-            // op(A)(r, l) = transA ? A[l + r ldA] : A[r + l ldA]; block at (b.r0, b.c0)
-            d.rs = transA ? ldA : 1;
-            d.ls = transA ? 1 : ldA;
+            // op(A)(r, l) = trans ? A[l + r ld] : A[r + l ld]; block at (b.r0, b.c0)
+            d.rs = src.trans ? src.ld : 1;
+            d.ls = src.trans ? 1 : src.ld;
             d.src_off = (long long) b.r0 * d.rs + (long long) b.c0 * d.ls;
         } else {
-            // column j of op(B) over l: transB ? B[j + l ldB] : B[l + j ldB]; block at (l0 = b.r0, j0 = b.c0)
-            d.rs = transB ? 1 : ldB;
-            d.ls = transB ? ldB : 1;
+            // column j of op(B) over l: trans ? B[j + l ld] : B[l + j ld]; block at (l0 = b.r0, j0 = b.c0)
+            d.rs = src.trans ? 1 : src.ld;
+            d.ls = src.trans ? src.ld : 1;
             d.src_off = (long long) b.c0 * d.rs + (long long) b.r0 * d.ls;
         }
+        if (src.base) d.src_off += (long long) (reinterpret_cast<uintptr_t>(src.base) / sizeof(double));
+        d.tile_begin = tiles_op[isA ? 0 : 1];
+        if (rows > 0 && kz > 0)
+            tiles_op[isA ? 0 : 1] += ((d.rows_pad + ST - 1) / ST) * ((d.kpad + ST - 1) / ST);
         qoff += align256((size_t) slices * d.rows_pad * d.kpad);
         eoff += rows;
         if (d.rows_pad > max_rows) max_rows = d.rows_pad;
@@ -655,6 +688,8 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
     hd->nslice_desc = nA + nB; hd->tiles = tiles;
     oz->slices = slices; oz->nA = nA; oz->nB = nB; oz->ngroup = ngroup; oz->tiles = tiles;
     oz->max_rows = max_rows; oz->max_kpad = max_kpad;
+    oz->slice_tiles_a = tiles_op[0];
+    oz->slice_tiles_b = tiles_op[1];
     oz->n_exp = (long long) ne;
     oz->dev_plan = dev_plan;
     oz->dev_work = dev_work;
@@ -669,21 +704,20 @@ extern "C" int ca3dmm_oz_run_pack(const ca3dmm_oz_plan_t *oz, const void *A, con
         reinterpret_cast<const SliceDesc *>(static_cast<const unsigned char *>(oz->dev_plan) + L.sd);
     unsigned char *w = static_cast<unsigned char *>(oz->dev_work);
     CA3DMM_CUDA_TRY(cudaMemsetAsync(w, 0, (size_t) oz->n_exp * sizeof(int), stream));
-    const unsigned gx = (unsigned) ((oz->max_rows + ST - 1) / ST);
-    const unsigned gy = (unsigned) ((oz->max_kpad + ST - 1) / ST);
-    if (gy > 65535 || oz->nA > 65535 || oz->nB > 65535) return CA3DMM_EINVAL;
     const double *src[2] = {static_cast<const double *>(A), static_cast<const double *>(B)};
     const int cnt[2] = {oz->nA, oz->nB}, first[2] = {0, oz->nA};
+    const int tiles[2] = {oz->slice_tiles_a, oz->slice_tiles_b};
+    const int cap = ca3dmm_device_sm_count() * 8;
     for (int o = 0; o < 2; ++o) {
-        if (cnt[o] == 0) continue;
-        oz_exp_kernel<<<dim3(gx, gy, (unsigned) cnt[o]), 256, 0, stream>>>(
-            src[o], sd + first[o], reinterpret_cast<unsigned *>(w));
+        if (cnt[o] == 0 || tiles[o] == 0) continue;
+        oz_exp_kernel<<<tiles[o] < cap ? tiles[o] : cap, 256, 0, stream>>>(
+            src[o], sd + first[o], cnt[o], tiles[o], reinterpret_cast<unsigned *>(w));
         CA3DMM_CUDA_TRY(cudaGetLastError());
     }
     for (int o = 0; o < 2; ++o) {
-        if (cnt[o] == 0) continue;
-        oz_slice_kernel<<<dim3(gx, gy, (unsigned) cnt[o]), 256, 0, stream>>>(
-            src[o], sd + first[o], w, oz->slices);
+        if (cnt[o] == 0 || tiles[o] == 0) continue;
+        oz_slice_kernel<<<tiles[o] < cap ? tiles[o] : cap, 256, 0, stream>>>(
+            src[o], sd + first[o], cnt[o], tiles[o], w, oz->slices);
         CA3DMM_CUDA_TRY(cudaGetLastError());
     }
     return CA3DMM_OK;

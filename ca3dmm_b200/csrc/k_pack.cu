@@ -12,49 +12,60 @@
 
 namespace {
 
-constexpr int TT = 32;   // transpose tile edge
+constexpr int PT = 64;   // pack tile edge
 
-// One CTA per (descriptor, 2D tile).  blockIdx.z = descriptor index.
-// Copy path: tile of 256 rows x 8 columns, 256 threads, thread = row.
-// Transpose path: 32 x 32 tile through shared memory (+1 pad), 32 x 8 threads.
+__device__ __forceinline__ int find_desc(const ca3dmm_pack_desc_t *d, int n, int tile)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (d[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Persistent over the flat list of 64 x 64 tiles of every descriptor.
+// Copy: thread -> (row, 16 columns), reads and writes run down the columns.
+// Transpose: through a padded shared tile; reads run along the source's
+// contiguous index, writes along the destination's.
 __global__ void __launch_bounds__(256)
 pack_kernel(const double *__restrict__ src_base, double *__restrict__ dst_base,
-            const ca3dmm_pack_desc_t *__restrict__ descs)
+            const ca3dmm_pack_desc_t *__restrict__ descs, int ndesc, int total_tiles)
 {
-    const ca3dmm_pack_desc_t d = descs[blockIdx.z];
-    const double *src = src_base + d.src_off;
-    double *dst = dst_base + d.dst_off;
-    if (!d.trans) {
-        const int r = blockIdx.x * 256 + threadIdx.x;
-        const int c0 = blockIdx.y * 8;
-        if (r >= d.rows || c0 >= d.cols) return;
-        const int cn = min(8, d.cols - c0);
-        double v[8];
+    __shared__ double tile[PT][PT + 1];
+    for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+        const ca3dmm_pack_desc_t d = descs[find_desc(descs, ndesc, t)];
+        const int local = t - d.tile_begin;
+        const int tx = (d.rows + PT - 1) / PT;
+        const int r0 = (local % tx) * PT, c0 = (local / tx) * PT;
+        const double *src = reinterpret_cast<const double *>(
+            reinterpret_cast<uintptr_t>(src_base) + (uintptr_t) d.src_off * sizeof(double));
+        double *dst = reinterpret_cast<double *>(reinterpret_cast<uintptr_t>(dst_base) +
+                                                 (uintptr_t) d.dst_off * sizeof(double));
+        if (!d.trans) {
+            const int r = r0 + (threadIdx.x & 63), cb = c0 + (threadIdx.x >> 6) * 16;
+            if (r < d.rows) {
+                double v[16];
 #pragma unroll
-        for (int c = 0; c < 8; ++c)
-            if (c < cn) v[c] = __ldg(src + r + (long long) (c0 + c) * d.lds);
+                for (int c = 0; c < 16; ++c)
+                    if (cb + c < d.cols) v[c] = __ldg(src + r + (long long) (cb + c) * d.lds);
 #pragma unroll
-        for (int c = 0; c < 8; ++c)
-            if (c < cn) dst[r + (long long) (c0 + c) * d.ldd] = v[c];
-        return;
-    }
-    // dst (rows x cols) = transpose of the src block (cols x rows).
-    __shared__ double tile[TT][TT + 1];
-    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;   // 32 x 8
-    const int r0 = blockIdx.x * TT, c0 = blockIdx.y * TT;     // in dst coordinates
-    if (r0 >= d.rows || c0 >= d.cols) return;
-    // Reads run along the source's contiguous index (dst column c), writes
-    // along the destination's (dst row r); both are coalesced.
-#pragma unroll
-    for (int k = 0; k < TT; k += 8) {
-        const int c = c0 + tx, r = r0 + ty + k;
-        if (c < d.cols && r < d.rows) tile[ty + k][tx] = __ldg(src + c + (long long) r * d.lds);
-    }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < TT; k += 8) {
-        const int r = r0 + tx, c = c0 + ty + k;
-        if (r < d.rows && c < d.cols) dst[r + (long long) c * d.ldd] = tile[tx][ty + k];
+                for (int c = 0; c < 16; ++c)
+                    if (cb + c < d.cols) dst[r + (long long) (cb + c) * d.ldd] = v[c];
+            }
+            continue;
+        }
+        // dst (rows x cols) = transpose of the source block (cols x rows)
+        __syncthreads();
+        for (int e = threadIdx.x; e < PT * PT; e += blockDim.x) {
+            const int c = c0 + (e & 63), r = r0 + (e >> 6);
+            if (c < d.cols && r < d.rows) tile[e >> 6][e & 63] = __ldg(src + c + (long long) r * d.lds);
+        }
+        __syncthreads();
+        for (int e = threadIdx.x; e < PT * PT; e += blockDim.x) {
+            const int r = r0 + (e & 63), c = c0 + (e >> 6);
+            if (r < d.rows && c < d.cols) dst[r + (long long) c * d.ldd] = tile[e & 63][e >> 6];
+        }
     }
 }
 
@@ -89,23 +100,25 @@ reduce_slabs_kernel(const double *__restrict__ slab, long long slab_stride, long
 
 }  // namespace
 
-extern "C" int ca3dmm_pack_launch(const double *src_base, double *dst_base,
-                                  const ca3dmm_pack_desc_t *dev_descs, int ndesc, int max_rows,
-                                  int max_cols, int any_trans, cudaStream_t stream)
+extern "C" int ca3dmm_pack_tiles(ca3dmm_pack_desc_t *descs, int ndesc)
 {
-    if (ndesc <= 0 || max_rows <= 0 || max_cols <= 0) return CA3DMM_OK;
-    if (ndesc > 65535) return CA3DMM_EINVAL;
-    // grid covers the larger of the copy tiling (256 x 8) and the transpose
-    // tiling (32 x 32); blocks outside a descriptor's extent exit at once.
-    unsigned gx = (unsigned) ((max_rows + 255) / 256), gy = (unsigned) ((max_cols + 7) / 8);
-    if (any_trans) {
-        unsigned tx = (unsigned) ((max_rows + TT - 1) / TT), ty = (unsigned) ((max_cols + TT - 1) / TT);
-        if (tx > gx) gx = tx;
-        if (ty > gy) gy = ty;
+    int tiles = 0;
+    for (int j = 0; j < ndesc; ++j) {
+        descs[j].tile_begin = tiles;
+        if (descs[j].rows > 0 && descs[j].cols > 0)
+            tiles += ((descs[j].rows + PT - 1) / PT) * ((descs[j].cols + PT - 1) / PT);
     }
-    if (gy > 65535) return CA3DMM_EINVAL;
-    dim3 grid(gx, gy, (unsigned) ndesc);
-    pack_kernel<<<grid, 256, 0, stream>>>(src_base, dst_base, dev_descs);
+    return tiles;
+}
+
+extern "C" int ca3dmm_pack_launch(const double *src_base, double *dst_base,
+                                  const ca3dmm_pack_desc_t *dev_descs, int ndesc, int total_tiles,
+                                  cudaStream_t stream)
+{
+    if (ndesc <= 0 || total_tiles <= 0) return CA3DMM_OK;
+    int grid = ca3dmm_device_sm_count() * 8;
+    if (grid > total_tiles) grid = total_tiles;
+    pack_kernel<<<grid, 256, 0, stream>>>(src_base, dst_base, dev_descs, ndesc, total_tiles);
     CA3DMM_CUDA_TRY(cudaGetLastError());
     return CA3DMM_OK;
 }

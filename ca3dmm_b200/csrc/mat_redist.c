@@ -114,12 +114,13 @@ void mat_redist_engine_exec(mat_redist_engine_p e, const void *src_blk, const in
     d.lds = src_ld;
     d.ldd = dst_ld;
     d.src_off = (long long) (e->req_srow - e->src_srow) * src_ld + (e->req_scol - e->src_scol);
+    int tiles = ca3dmm_pack_tiles(&d, 1);
     if (cudaMemcpy(e->workbuf_d, &d, sizeof(d), cudaMemcpyHostToDevice) != cudaSuccess) {
         e->last_error = CA3DMM_ECUDA;
         return;
     }
     int rc = ca3dmm_pack_launch((const double *) src_blk, (double *) dst_blk,
-                                (const ca3dmm_pack_desc_t *) e->workbuf_d, 1, d.rows, d.cols, 0, 0);
+                                (const ca3dmm_pack_desc_t *) e->workbuf_d, 1, tiles, 0);
     if (rc == CA3DMM_OK && cudaDeviceSynchronize() != cudaSuccess) rc = CA3DMM_ECUDA;
     e->last_error = rc;
     if (rc) ERROR_PRINTF("mat_redist_engine_exec failed (error %d)\n", rc);
