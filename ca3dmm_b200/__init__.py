@@ -49,7 +49,16 @@ class Ca3dmmEngineS(C.Structure):
                                   "hd_trans_ms", "exec_ms")] + [
         ("n_exec", C.c_int), ("n_group", C.c_int), ("gemm_mode", C.c_int),
         ("ozaki_slices", C.c_int), ("last_error", C.c_int), ("stream", C.c_void_p),
-        ("sync_exec", C.c_int), ("workbuf_bytes", C.c_size_t), ("impl", C.c_void_p)]
+        ("sync_exec", C.c_int), ("workbuf_bytes", C.c_size_t), ("impl", C.c_void_p),
+        ("raster", C.c_int)]
+
+
+class TuneCfg(C.Structure):
+    """Mirror of ca3dmm_tune_cfg_t (include/ca3dmm_tune.h)."""
+    _fields_ = [("gemm_mode", C.c_int), ("slices", C.c_int), ("kp", C.c_int), ("raster", C.c_int)]
+
+
+NFEAT = 12
 
 
 class CannonEngineS(C.Structure):
@@ -117,6 +126,26 @@ def lib():
         "ca3dmm_grouped_exec": (i, [p, C.POINTER(p), pi, C.POINTER(p), pi, C.POINTER(p), pi]),
         "ca3dmm_grouped_last_ms": (d, [p]),
         "ca3dmm_grouped_free": (None, [C.POINTER(p)]),
+        "ca3dmm_engine_set_raster": (i, [EP, i]),
+        "ca3dmm_tune_features": (i, [i, i, i, i, i, C.POINTER(TuneCfg), C.c_float,
+                                     C.POINTER(C.c_float)]),
+        "ca3dmm_tune_measure": (i, [i, i, i, i, i, p, i, p, i, p, i, C.POINTER(TuneCfg), i,
+                                    C.POINTER(C.c_float)]),
+        "ca3dmm_autotune": (i, [i, i, i, i, i, p, i, p, i, p, i, C.POINTER(TuneCfg), i, C.c_float,
+                                p, i, i, pi, C.POINTER(C.c_float)]),
+        "ca3dmm_mlp_create": (i, [i, i, i, C.c_ulonglong, C.POINTER(p)]),
+        "ca3dmm_mlp_free": (None, [C.POINTER(p)]),
+        "ca3dmm_mlp_nparams": (i, [p]),
+        "ca3dmm_mlp_get_params": (i, [p, C.POINTER(C.c_float)]),
+        "ca3dmm_mlp_set_params": (i, [p, C.POINTER(C.c_float)]),
+        "ca3dmm_mlp_set_normalisation": (i, [p, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+        "ca3dmm_mlp_fwd_bwd": (i, [p, C.POINTER(C.c_float), C.POINTER(C.c_float), i,
+                                   C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+        "ca3dmm_mlp_train": (i, [p, C.POINTER(C.c_float), C.POINTER(C.c_float), i, i, i,
+                                 C.c_float, C.c_ulonglong, C.POINTER(C.c_float)]),
+        "ca3dmm_mlp_predict": (i, [p, C.POINTER(C.c_float), i, C.POINTER(C.c_float)]),
+        "ca3dmm_mlp_save": (i, [p, C.c_char_p]),
+        "ca3dmm_mlp_load": (i, [C.c_char_p, C.POINTER(p)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -332,3 +361,115 @@ class GroupedGemm:
             self.free()
         except Exception:
             pass
+
+
+def _fp(a):
+    import numpy as np
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    return a, a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+def tune_features(m, n, k, ta, tb, cfg, spread):
+    import numpy as np
+    out = np.zeros(NFEAT, dtype=np.float32)
+    c = TuneCfg(*cfg)
+    rc = lib().ca3dmm_tune_features(m, n, k, ta, tb, C.byref(c), float(spread),
+                                    out.ctypes.data_as(C.POINTER(C.c_float)))
+    if rc:
+        raise ValueError("bad features request")
+    return out
+
+
+class CostModel:
+    """Python mirror of ca3dmm_mlp_*: the FP32 MLP cost model trained and run by
+    the library's CUDA kernels."""
+
+    def __init__(self, nin=NFEAT, h1=64, h2=64, seed=1, path=None):
+        self.h = C.c_void_p()
+        if path is not None:
+            rc = lib().ca3dmm_mlp_load(path.encode(), C.byref(self.h))
+        else:
+            rc = lib().ca3dmm_mlp_create(nin, h1, h2, seed, C.byref(self.h))
+        if rc:
+            raise RuntimeError("cost model creation failed: %d" % rc)
+
+    @property
+    def nparams(self):
+        return lib().ca3dmm_mlp_nparams(self.h)
+
+    def params(self):
+        import numpy as np
+        out = np.zeros(self.nparams, dtype=np.float32)
+        lib().ca3dmm_mlp_get_params(self.h, out.ctypes.data_as(C.POINTER(C.c_float)))
+        return out
+
+    def set_params(self, p):
+        a, ptr = _fp(p)
+        return lib().ca3dmm_mlp_set_params(self.h, ptr)
+
+    def fwd_bwd(self, X, y):
+        import numpy as np
+        X, xp = _fp(X)
+        y, yp = _fp(y)
+        loss = C.c_float()
+        g = np.zeros(self.nparams, dtype=np.float32)
+        rc = lib().ca3dmm_mlp_fwd_bwd(self.h, xp, yp, len(y), C.byref(loss),
+                                      g.ctypes.data_as(C.POINTER(C.c_float)))
+        if rc:
+            raise RuntimeError("fwd_bwd failed: %d" % rc)
+        return loss.value, g
+
+    def train(self, X, y, epochs=200, batch=256, lr=3e-3, seed=7):
+        X, xp = _fp(X)
+        y, yp = _fp(y)
+        loss = C.c_float()
+        rc = lib().ca3dmm_mlp_train(self.h, xp, yp, len(y), epochs, batch, lr, seed, C.byref(loss))
+        if rc:
+            raise RuntimeError("training failed: %d" % rc)
+        return loss.value
+
+    def predict(self, X):
+        import numpy as np
+        X, xp = _fp(X)
+        out = np.zeros(X.shape[0], dtype=np.float32)
+        rc = lib().ca3dmm_mlp_predict(self.h, xp, X.shape[0], out.ctypes.data_as(C.POINTER(C.c_float)))
+        if rc:
+            raise RuntimeError("predict failed: %d" % rc)
+        return out
+
+    def save(self, path):
+        return lib().ca3dmm_mlp_save(self.h, path.encode())
+
+    def free(self):
+        if self.h:
+            lib().ca3dmm_mlp_free(C.byref(self.h))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+def autotune(m, n, k, ta, tb, A, ldA, B, ldB, Cm, ldC, cands, spread=0.0, model=None, topk=2,
+             reps=2):
+    """Run ca3dmm_autotune; returns (best index, measured ms per candidate or -1)."""
+    import numpy as np
+    arr = (TuneCfg * len(cands))(*[TuneCfg(*c) for c in cands])
+    best = C.c_int()
+    ms = np.zeros(len(cands), dtype=np.float32)
+    rc = lib().ca3dmm_autotune(m, n, k, ta, tb, _ptr(A), ldA, _ptr(B), ldB, _ptr(Cm), ldC, arr,
+                               len(cands), float(spread), model.h if model is not None else None,
+                               int(topk), int(reps), C.byref(best),
+                               ms.ctypes.data_as(C.POINTER(C.c_float)))
+    if rc:
+        raise RuntimeError("autotune failed: %d" % rc)
+    return best.value, ms
+
+
+def measure(m, n, k, ta, tb, A, ldA, B, ldB, Cm, ldC, cfg, reps=2):
+    t = C.c_float()
+    c = TuneCfg(*cfg)
+    rc = lib().ca3dmm_tune_measure(m, n, k, ta, tb, _ptr(A), ldA, _ptr(B), ldB, _ptr(Cm), ldC,
+                                   C.byref(c), int(reps), C.byref(t))
+    return (t.value if rc == 0 else None)

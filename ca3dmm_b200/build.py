@@ -18,8 +18,8 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 C_SOURCES = ["vcomm.c", "partition.c", "dev_type.c", "mat_redist.c", "cannon.c", "ca3dmm.c",
-             "grouped.c"]
-CU_SOURCES = ["k_dgemm.cu", "k_pack.cu", "k_ozaki.cu", "k_noalloc.cu"]
+             "grouped.c", "autotune.c"]
+CU_SOURCES = ["k_dgemm.cu", "k_pack.cu", "k_ozaki.cu", "k_noalloc.cu", "k_mlp.cu"]
 HEADERS = ["ca3dmm_kernels.h", "ca3dmm_ozaki.h", "ca3dmm_util.h", "k_common.cuh"]
 
 

@@ -387,6 +387,7 @@ static void finish_init(ca3dmm_engine_p e, int dst_srow, int dst_nrow, int dst_s
     GET_ENV_INT_VAR(sl, "CA3DMM_OZAKI_SLICES", "ozaki_slices", 7, 2, 8);
     e->ozaki_slices = sl;
     e->sync_exec = 1;
+    e->raster = 8;
     int rc = plan_build(e);
     if (rc) {
         ERROR_PRINTF("Failed to build the device plan (error %d)\n", rc);
@@ -637,6 +638,7 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
         }
         q->m = g->mz; q->n = g->nz; q->k = g->kz;
         q->alpha = 1.0; q->beta = 0.0;
+        q->raster = e->raster;
     }
     int rc = ca3dmm_dgemm_plan_encode(gd, pl->ngroup, h + pl->off_gemm, &pl->gemm_tiles);
     if (rc) return rc;
@@ -662,6 +664,7 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
             og[i].a_blk = pl->groups[i].a_blk; og[i].b_blk = pl->groups[i].b_blk;
             og[i].C = gd[i].C; og[i].ldc = gd[i].ldc;
             og[i].m = gd[i].m; og[i].n = gd[i].n; og[i].k = gd[i].k;
+            og[i].raster = e->raster;
         }
         rc = ca3dmm_oz_plan_encode(&pl->oz, e->ozaki_slices, pl->nA, ob, os, pl->nB,
                                    ob + pl->nA, os + pl->nA, pl->ngroup, og, w + pl->off_oz,
@@ -880,6 +883,14 @@ int ca3dmm_engine_set_gemm_mode(ca3dmm_engine_p e, int mode, int slices)
 }
 
 size_t ca3dmm_engine_workbuf_bytes(ca3dmm_engine_p e) { return e ? e->workbuf_bytes : 0; }
+
+int ca3dmm_engine_set_raster(ca3dmm_engine_p e, int raster)
+{
+    if (!e || (raster != 4 && raster != 8 && raster != 16)) return CA3DMM_EINVAL;
+    e->raster = raster;
+    ((plan_t *) e->impl)->plan_valid = 0;
+    return CA3DMM_OK;
+}
 
 int ca3dmm_engine_vrank_info(ca3dmm_engine_p e, int vrank, int *out34)
 {

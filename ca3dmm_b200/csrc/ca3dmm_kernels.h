@@ -33,6 +33,7 @@ typedef struct {
     double *C; long long ldc;
     int m, n, k;
     double alpha, beta;
+    int raster;          /* tile rows per raster band (0 = default 8) */
 } ca3dmm_dgemm_desc_t;
 
 /* Bytes of the device plan for nprob problems (tensor maps + problem records). */

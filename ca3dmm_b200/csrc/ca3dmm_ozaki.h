@@ -35,6 +35,7 @@ typedef struct {
     double *C;            /* output (column-major) */
     long long ldc;
     int m, n, k;
+    int raster;           /* tile rows per raster band (0 = default) */
 } ca3dmm_oz_group_t;
 
 typedef struct {

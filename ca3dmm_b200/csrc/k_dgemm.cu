@@ -44,7 +44,7 @@ struct alignas(16) DProb {
     int m, n, k;
     int tiles_m, tiles_n, tile_begin;
     double alpha, beta;
-    int vec_ok, pad;
+    int vec_ok, raster;
 };
 
 __device__ __forceinline__ int find_problem(const DProb *probs, int nprob, int tile)
@@ -60,10 +60,10 @@ __device__ __forceinline__ int find_problem(const DProb *probs, int nprob, int t
 __device__ __forceinline__ void tile_coords(const DProb &p, int tile, int &tm, int &tn)
 {
     int t = tile - p.tile_begin;
-    int group_size = GROUP_M * p.tiles_n;
+    int group_size = p.raster * p.tiles_n;
     int group = t / group_size;
-    int first_m = group * GROUP_M;
-    int gm = min(p.tiles_m - first_m, GROUP_M);
+    int first_m = group * p.raster;
+    int gm = min(p.tiles_m - first_m, p.raster);
     int r = t % group_size;
     tm = first_m + r % gm;
     tn = r / gm;
@@ -364,6 +364,7 @@ extern "C" int ca3dmm_dgemm_plan_encode(const ca3dmm_dgemm_desc_t *probs, int np
         d.tiles_n = (q.m > 0 && q.n > 0) ? (q.n + BN - 1) / BN : 0;
         d.tile_begin = tiles;
         d.vec_ok = ((reinterpret_cast<uintptr_t>(q.C) & 15) == 0) && ((q.ldc & 1) == 0);
+        d.raster = q.raster > 0 ? q.raster : GROUP_M;
         tiles += d.tiles_m * d.tiles_n;
     }
     *total_tiles = tiles;

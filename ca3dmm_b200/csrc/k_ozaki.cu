@@ -76,7 +76,7 @@ struct OzGroup {
     long long ldc;
     int m, n, k;
     int nkb;                    // 32-byte k-blocks
-    int tiles_m, tiles_n, tile_begin, pad;
+    int tiles_m, tiles_n, tile_begin, raster;
     long long ea_off, eb_off;   // exponent offsets (ints) of the A rows / B columns
     long long qa_off, qb_off;   // byte offsets of the tiled slices
 };
@@ -289,9 +289,9 @@ __device__ __forceinline__ int find_group(const OzGroup *g, int n, int tile)
 __device__ __forceinline__ void group_tile(const OzGroup &p, int tile, int &tm, int &tn)
 {
     int t = tile - p.tile_begin;
-    int gs = GROUP_M * p.tiles_n;
-    int first = (t / gs) * GROUP_M;
-    int gm = min(p.tiles_m - first, GROUP_M);
+    int gs = p.raster * p.tiles_n;
+    int first = (t / gs) * p.raster;
+    int gm = min(p.tiles_m - first, p.raster);
     int r = t % gs;
     tm = first + r % gm;
     tn = r / gm;
@@ -682,6 +682,7 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
         o.tiles_m = (o.m > 0 && o.n > 0) ? (o.m + OBM - 1) / OBM : 0;
         o.tiles_n = (o.m > 0 && o.n > 0) ? (o.n + OBN - 1) / OBN : 0;
         o.tile_begin = tiles;
+        o.raster = G[g].raster > 0 ? G[g].raster : GROUP_M;
         tiles += o.tiles_m * o.tiles_n;
     }
     hd->nA = nA; hd->nB = nB; hd->ngroup = ngroup; hd->slices = slices;

@@ -117,6 +117,7 @@ struct ca3dmm_engine {
     int sync_exec;                  /* 1: exec returns with C complete (reference behaviour) */
     size_t workbuf_bytes;           /* device work buffer size */
     void *impl;                     /* opaque device plan */
+    int raster;                     /* GEMM tile rows per raster band (tuning knob) */
 };
 typedef struct ca3dmm_engine ca3dmm_engine_s;
 typedef struct ca3dmm_engine *ca3dmm_engine_p;
@@ -169,6 +170,8 @@ void ca3dmm_engine_set_stream(ca3dmm_engine_p engine, void *stream, int sync);
  * ca3dmm_engine_workbuf_bytes reports). */
 int ca3dmm_engine_set_gemm_mode(ca3dmm_engine_p engine, int mode, int slices);
 size_t ca3dmm_engine_workbuf_bytes(ca3dmm_engine_p engine);
+/* Tile rows per raster band of the GEMM launches (4, 8 or 16; L2 reuse). */
+int ca3dmm_engine_set_raster(ca3dmm_engine_p engine, int raster);
 /* Geometry of any virtual rank, same 34-int layout as the CPU oracle's
  * orc_rank_geometry: is_active, rank_m/n/k, task_{m,n,k}_{num,id},
  * A_2dmm/B_2dmm/C_2dmm/C_out/A_rd/B_rd (srow, scol, nrow, ncol). */

@@ -244,3 +244,30 @@ def cpu_ca3dmm(A, B, tA, tB, m, n, k, mp, np_, kp):
     for s in slabs[1:]:
         out = out + s
     return out
+
+
+# ---------------------------------------------------------------- MLP reference
+def mlp_split(params, nin, h1, h2):
+    p = np.asarray(params, dtype=np.float32)
+    o = 0
+    out = []
+    for size in (h1 * nin, h1, h2 * h1, h2, h2, 1):
+        out.append(p[o:o + size].copy())
+        o += size
+    return out
+
+
+def mlp_fwd_bwd(params, X, y, nin, h1, h2):
+    """CPU FP32 reference of the cost-model MLP (oracle.c section 7):
+    returns (loss, yhat, flat gradients in the parameter layout)."""
+    W1, b1, W2, b2, W3, b3 = mlp_split(params, nin, h1, h2)
+    X = np.ascontiguousarray(X, dtype=np.float32)
+    y = np.ascontiguousarray(y, dtype=np.float32)
+    B = X.shape[0]
+    g = [np.zeros_like(a) for a in (W1, b1, W2, b2, W3, b3)]
+    yhat = np.zeros(B, dtype=np.float32)
+    fp = lambda a: a.ctypes.data_as(C.POINTER(C.c_float))
+    loss = lib().orc_mlp_fwd_bwd(B, nin, h1, h2, fp(X), fp(y), fp(W1), fp(b1), fp(W2), fp(b2),
+                                 fp(W3), fp(b3), fp(yhat), fp(g[0]), fp(g[1]), fp(g[2]), fp(g[3]),
+                                 fp(g[4]), fp(g[5]))
+    return float(loss), yhat, np.concatenate(g)
