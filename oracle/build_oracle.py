@@ -5,9 +5,13 @@
                                -- the reference's own grid planner and balanced
                                   split, compiled unmodified from its sources
                                   (src/partition.c, src/utils.c) when the
-                                  reference tree is present.  The rest of the
-                                  reference needs MPI and CBLAS, which this
-                                  image lacks, so only these two files build.
+                                  reference tree is present;
+  oracle/_ref/libref_ca3dmm.so -- the reference's whole CPU path (src/ca3dmm.c,
+                                  cannon.c, mat_redist.c, partition.c, utils.c,
+                                  dev_type.c, mpi_op_omp.c), compiled unmodified
+                                  against vmpi (oracle/vmpi: MPI ranks as host
+                                  threads) and the OpenBLAS shipped in this
+                                  image, plus the driver oracle/vmpi/ref_driver.c.
 """
 import os
 import subprocess
@@ -43,7 +47,35 @@ def build():
         deps = [os.path.join(refsrc, f) for f in ("partition.c", "utils.c", "partition.h", "utils.h")]
         if _newer(rlib, deps):
             _run(["gcc", "-O2", "-fPIC", "-shared", "-I", refsrc, deps[0], deps[1], "-o", rlib, "-lm"])
+        openblas = find_openblas()
+        if openblas:
+            vdir = os.path.join(HERE, "vmpi")
+            srcs = [os.path.join(refsrc, f) for f in ("ca3dmm.c", "cannon.c", "mat_redist.c",
+                                                        "partition.c", "utils.c", "dev_type.c",
+                                                        "mpi_op_omp.c")]
+            mine = [os.path.join(vdir, f) for f in ("vmpi.c", "ref_driver.c")]
+            hdrs = [os.path.join(vdir, f) for f in ("mpi.h", "cblas.h", "lapacke.h")]
+            clib = os.path.join(out, "libref_ca3dmm.so")
+            if _newer(clib, srcs + mine + hdrs):
+                d, f = os.path.split(openblas)
+                _run(["gcc", "-O2", "-fPIC", "-shared", "-fopenmp", "-DUSE_OPENBLAS",
+                      "-Wno-implicit-function-declaration", "-I", vdir, "-I", refsrc] + srcs + mine +
+                     ["-o", clib, "-L", d, "-l:" + f, "-Wl,--disable-new-dtags", "-Wl,-rpath," + d,
+                      "-Wl,-Bsymbolic",
+                      "-lpthread", "-lm"])
     return lib
+
+
+def find_openblas():
+    """The OpenBLAS build with unprefixed CBLAS symbols shipped in this image."""
+    import glob
+    import site
+    for sp in site.getsitepackages():
+        for pat in ("opencv_python_headless.libs/libopenblas*.so*", "*/libopenblas*.so*"):
+            hits = sorted(glob.glob(os.path.join(sp, pat)))
+            if hits:
+                return hits[0]
+    return None
 
 
 if __name__ == "__main__":

@@ -271,3 +271,50 @@ def mlp_fwd_bwd(params, X, y, nin, h1, h2):
                                  fp(W3), fp(b3), fp(yhat), fp(g[0]), fp(g[1]), fp(g[2]), fp(g[3]),
                                  fp(g[4]), fp(g[5]))
     return float(loss), yhat, np.concatenate(g)
+
+
+# ---------------------------------------------------------------- reference CPU path
+_ref = None
+
+
+def ref_lib():
+    """The reference's own CPU path compiled under vmpi (oracle/_ref), or None."""
+    global _ref
+    if _ref is None:
+        path = os.path.join(HERE, "_ref", "libref_ca3dmm.so")
+        if not os.path.exists(path):
+            return None
+        L = C.CDLL(path)
+        dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
+        L.ref_ca3dmm.argtypes = [C.c_int] * 7 + [ip, dp, dp, dp, C.c_int, dp, ip, ip, C.c_double]
+        L.ref_fault_run.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double]
+        _ref = L
+    return _ref
+
+
+def ref_ca3dmm(p, m, n, k, ta, tb, A, B, grid=None, ntest=1, btb=False, timeout=300.0):
+    """Run the unmodified reference (DEV_TYPE_HOST, OpenBLAS) on p vmpi rank threads
+    the way examples/example_AB.c does.  Returns (C, times [ntest x 2] of rank 0:
+    total exec ms and matmul-only ms, per-rank geometry [p x 34], (mp, np, kp, rp))."""
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("reference CPU path not built (oracle/_ref)")
+    A = np.asfortranarray(A if A is not None else np.zeros((1, 1)), dtype=np.float64)
+    B = np.asfortranarray(B, dtype=np.float64)
+    cm = n if btb else m
+    Cm = np.zeros((cm, n), order="F")
+    times = np.zeros((max(ntest, 1), 2))
+    geom = np.zeros((p, 34), dtype=np.int32)
+    gout = np.zeros(4, dtype=np.int32)
+    g = (C.c_int * 3)(*grid) if grid is not None else None
+    ip = C.POINTER(C.c_int)
+    rc = L.ref_ca3dmm(p, m, n, k, int(ta), int(tb), int(btb), g, _d(A), _d(B), _d(Cm), ntest,
+                      _d(times), geom.ctypes.data_as(ip), gout.ctypes.data_as(ip), float(timeout))
+    if rc:
+        raise RuntimeError("reference run failed")
+    return Cm, times, geom, tuple(int(x) for x in gout)
+
+
+def ref_fault_run(p, dead_rank, m=64, timeout=1.0):
+    """One rank returns at once; the others must stop by timeout (nonzero)."""
+    return ref_lib().ref_fault_run(p, dead_rank, m, float(timeout))
