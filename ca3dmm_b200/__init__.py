@@ -15,6 +15,9 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libca3dmm_b200.so")
+# MLP trained on B200 timings of the 18 standard candidates (costmodel.CANDS)
+# over 2000 shapes log-uniform in [128, 16384]^3
+DEFAULT_COST_MODEL = os.path.join(HERE, "data", "costmodel_b200.txt")
 
 DEV_TYPE_HOST, DEV_TYPE_CUDA, DEV_TYPE_CUDA_MPI_DIRECT = 0, 1, 2
 GEMM_PLAIN, GEMM_OZAKI = 0, 1
@@ -146,6 +149,7 @@ def lib():
         "ca3dmm_mlp_predict": (i, [p, C.POINTER(C.c_float), i, C.POINTER(C.c_float)]),
         "ca3dmm_mlp_save": (i, [p, C.c_char_p]),
         "ca3dmm_mlp_load": (i, [C.c_char_p, C.POINTER(p)]),
+        "ca3dmm_kernel_launches": (C.c_ulonglong, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -170,6 +174,11 @@ class VComm:
                 lib().ca3dmm_vcomm_free(C.byref(self.h))
         except Exception:
             pass
+
+
+def kernel_launches():
+    """Kernels the library has launched since it was loaded (host count)."""
+    return int(lib().ca3dmm_kernel_launches())
 
 
 def calc_3d_decomposition_cannon(p, m, n, k):
@@ -392,6 +401,11 @@ class CostModel:
             rc = lib().ca3dmm_mlp_create(nin, h1, h2, seed, C.byref(self.h))
         if rc:
             raise RuntimeError("cost model creation failed: %d" % rc)
+
+    @classmethod
+    def default(cls):
+        """The shipped model (DEFAULT_COST_MODEL)."""
+        return cls(path=DEFAULT_COST_MODEL)
 
     @property
     def nparams(self):

@@ -1,0 +1,138 @@
+"""Cost-model study: collect autotuner timings, train the MLP on the GPU with
+the library's own CUDA kernels, and evaluate it against exhaustive search.
+
+  python -m ca3dmm_b200.costmodel --train 2000 --test 500 --out DIR
+
+Shapes: m, n, k log-uniform in [lo, hi] (default [128, 16384]), random
+transposes, entries sign * (1 + u) * 2^e with e uniform in [-E, E], E drawn
+per shape from {0, 4, 8} (the exponent-spread feature).  Candidates: plain
+FP64 DMMA and split precision with 7 or 8 slices, each with k-slab splits
+kp in {1, 2, 4} and tile raster bands of 8 or 16 rows (18 configurations).
+Every candidate is timed on every shape (exhaustive) through
+ca3dmm_tune_measure; the MLP is trained on log2(ms) of the training shapes
+and evaluated on the held-out shapes by
+  * regret = t(choice) / t(best) - 1 of the model's top-1 (no timing) and of
+    the best of its top-2 (two timings),
+  * search time saved = 1 - (time to time the top-2) / (time to time all),
+against the untuned default (plain, kp = 1, raster 8).
+"""
+import argparse
+import json
+import os
+import time
+
+import numpy as np
+
+import ca3dmm_b200 as cb
+
+CANDS = [(mode, sl, kp, r) for (mode, sl) in ((0, 0), (1, 7), (1, 8)) for kp in (1, 2, 4)
+         for r in (8, 16)]
+DEFAULT = CANDS.index((0, 0, 1, 8))
+
+
+def shapes(count, seed, lo, hi):
+    rng = np.random.default_rng(seed)
+    d = np.exp(rng.uniform(np.log(lo), np.log(hi), size=(count, 3))).round().astype(int)
+    ta = rng.integers(0, 2, count)
+    tb = rng.integers(0, 2, count)
+    em = rng.choice([0, 4, 8], count)
+    return [(int(a), int(b), int(c), int(x), int(y), int(e)) for (a, b, c), x, y, e in
+            zip(d, ta, tb, em)]
+
+
+def fill(buf, rows, cols, emax, gen):
+    import torch
+    n = rows * cols
+    v = buf[:n]
+    u = torch.rand(n, dtype=torch.float64, device="cuda", generator=gen)
+    e = torch.randint(-emax, emax + 1, (n,), device="cuda", generator=gen).double()
+    s = torch.randint(0, 2, (n,), device="cuda", generator=gen).double() * 2 - 1
+    v.copy_(s * (1 + u) * torch.pow(2.0, e))
+    return float(2 * emax + 1)
+
+
+def collect(shape_list, maxdim, reps=1, log_every=100):
+    import torch
+    gen = torch.Generator(device="cuda")
+    gen.manual_seed(1234)
+    A = torch.empty(maxdim * maxdim, dtype=torch.float64, device="cuda")
+    B = torch.empty(maxdim * maxdim, dtype=torch.float64, device="cuda")
+    C = torch.empty(maxdim * maxdim, dtype=torch.float64, device="cuda")
+    feats, times = [], []
+    t0 = time.time()
+    for si, (m, n, k, ta, tb, em) in enumerate(shape_list):
+        ar, ac = (k, m) if ta else (m, k)
+        br, bc = (n, k) if tb else (k, n)
+        spread = fill(A, ar, ac, em, gen)
+        fill(B, br, bc, em, gen)
+        row_f, row_t = [], []
+        for c in CANDS:
+            if c[2] > k:
+                ms = float("nan")
+            else:
+                ms = cb.measure(m, n, k, ta, tb, A, ar, B, br, C, m, c, reps=reps)
+                ms = float("nan") if ms is None else ms
+            row_f.append(cb.tune_features(m, n, k, ta, tb, c, spread))
+            row_t.append(ms)
+        feats.append(np.stack(row_f))
+        times.append(np.array(row_t))
+        if log_every and (si + 1) % log_every == 0:
+            print("collected %d shapes in %.0f s" % (si + 1, time.time() - t0), flush=True)
+    return np.stack(feats), np.stack(times)
+
+
+def evaluate(model, F, T):
+    ns, nc, nf = F.shape
+    pred = model.predict(F.reshape(-1, nf)).reshape(ns, nc)
+    ok = np.all(np.isfinite(T), axis=1)
+    r1, r2, rdef, saved = [], [], [], []
+    for i in np.nonzero(ok)[0]:
+        best = np.min(T[i])
+        order = np.argsort(pred[i])
+        r1.append(T[i, order[0]] / best - 1)
+        r2.append(min(T[i, order[0]], T[i, order[1]]) / best - 1)
+        rdef.append(T[i, DEFAULT] / best - 1)
+        saved.append(1 - (T[i, order[0]] + T[i, order[1]]) / np.sum(T[i]))
+    q = lambda v: {"mean": float(np.mean(v)), "median": float(np.median(v)),
+                   "p90": float(np.percentile(v, 90)), "max": float(np.max(v))}
+    return {"shapes": int(len(r1)), "regret_model_top1": q(r1), "regret_model_top2": q(r2),
+            "regret_untuned_default": q(rdef), "search_time_saved_top2": q(saved)}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--train", type=int, default=2000)
+    ap.add_argument("--test", type=int, default=500)
+    ap.add_argument("--lo", type=int, default=128)
+    ap.add_argument("--hi", type=int, default=16384)
+    ap.add_argument("--epochs", type=int, default=300)
+    ap.add_argument("--out", default="gpurun_out")
+    a = ap.parse_args()
+    os.makedirs(a.out, exist_ok=True)
+    tr = shapes(a.train, 11, a.lo, a.hi)
+    te = shapes(a.test, 22, a.lo, a.hi)
+    t0 = time.time()
+    Ftr, Ttr = collect(tr, a.hi)
+    Fte, Tte = collect(te, a.hi)
+    t_collect = time.time() - t0
+    np.savez_compressed(os.path.join(a.out, "costmodel_timings.npz"), Ftr=Ftr, Ttr=Ttr, Fte=Fte,
+                        Tte=Tte)
+    ok = np.isfinite(Ttr.ravel())
+    X = Ftr.reshape(-1, Ftr.shape[-1])[ok]
+    y = np.log2(Ttr.ravel()[ok]).astype(np.float32)
+    model = cb.CostModel(seed=3)
+    t1 = time.time()
+    loss = model.train(X, y, epochs=a.epochs, batch=512, lr=2e-3)
+    t_train = time.time() - t1
+    model.save(os.path.join(a.out, "costmodel_b200.txt"))
+    res = {"train_shapes": a.train, "test_shapes": a.test, "range": [a.lo, a.hi],
+           "candidates": CANDS, "collect_s": t_collect, "train_s": t_train,
+           "train_loss_log2ms": loss, "test": evaluate(model, Fte, Tte),
+           "train": evaluate(model, Ftr, Ttr)}
+    with open(os.path.join(a.out, "costmodel_eval.json"), "w") as f:
+        json.dump(res, f, indent=1)
+    print(json.dumps(res), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -54,3 +54,17 @@ def test_autotune_exhaustive_and_model(cuda):
     cm = cb.CostModel(seed=11)
     best2, ms2 = cb.autotune(m, n, k, 0, 0, dA, lda, dB, ldb, dC, m, cands, model=cm, topk=2)
     assert int(np.sum(ms2 > 0)) == 2 and ms2[best2] > 0
+
+
+def test_shipped_model_predicts_like_the_oracle(cuda):
+    """The shipped model, loaded and run by the library's kernels, ranks the
+    held-out study shapes exactly as the oracle's FP32 forward does."""
+    from tests.test_costmodel_eval import TIMINGS, load_model
+    nin, h1, h2, mu, sd, params = load_model()
+    F = np.load(TIMINGS)["Fte"][:100]
+    X = F.reshape(-1, nin)
+    cm = cb.CostModel.default()
+    got = cm.predict(X)
+    Xn = ((X - mu) / sd).astype(np.float32)
+    _, want, _ = orc.mlp_fwd_bwd(params, Xn, np.zeros(len(Xn), np.float32), nin, h1, h2)
+    assert np.allclose(got, want, rtol=1e-4, atol=1e-4), np.max(np.abs(got - want))
