@@ -31,6 +31,7 @@ sys.path.insert(0, ROOT)
 
 M = N = K = 8000
 P = 24
+GRID = (4, 2, 3)
 METRIC = "FP64-accurate TFLOP/s (2mnk/t): split-precision vs plain DMMA, equal error"
 
 
@@ -48,6 +49,8 @@ def parse():
                          "independent GEMMs in one graph-captured launch; btb: B^T B of a "
                          "1048576 x 512 B on a 1x1x32 grid")
     ap.add_argument("--nprob", type=int, default=256)
+    ap.add_argument("--no-slice-sweep", action="store_true",
+                    help="skip timing the other split-precision slice counts")
     return ap.parse_args()
 
 
@@ -129,43 +132,38 @@ def make_inputs(n, trans_a):
     return A, B
 
 
-def error_vs_dd(Cdev, A, B, ta, n, nsample=2048):
-    """Sampled errors of the device result against the double-double oracle."""
-    import torch
+def cpu_cores():
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def ref_cpu_run(A, B, ta, n, ntest):
+    """The reference's own CPU path (src/ca3dmm.c, DEV_TYPE_HOST, OpenBLAS),
+    compiled unmodified under the thread-backed MPI subset: P rank threads
+    with one BLAS thread each, driven as examples/example_AB.c drives it (one
+    warm-up exec, then `ntest` timed execs).  Returns exec ms per timed exec
+    of rank 0, or None when the reference build is absent."""
     from oracle import oracle as orc
-    ii, jj = orc.sample_indices(n, n, nrand=nsample, nlines=1)
-    hi, lo, ab = orc.dd_entries(A, B, ta, 0, n, ii, jj)
-    idx = torch.from_numpy(ii + jj * n).cuda()
-    vals = Cdev[idx].cpu().numpy()
-    return orc.errors(vals, hi, lo, ab)
-
-
-def run_leg(eng, dA, dB, dC, n, steps, warmup, stream):
-    import torch
-    for _ in range(warmup):
-        rc = eng.exec(dA, n, dB, n, dC, n)
-        if rc:
-            raise RuntimeError("exec failed: %d" % rc)
-    torch.cuda.synchronize()
-    eng.reset_stat()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    # the engine runs synchronously on the legacy default stream; events on it
-    ev0.record(stream)
-    for _ in range(steps):
-        eng.exec(dA, n, dB, n, dC, n)
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    ms = ev0.elapsed_time(ev1) / steps
-    s = eng.s
-    return {"ms_per_step": ms, "gemm_ms": s.cannon_ms / max(s.n_exec, 1),
-            "pack_ms": s.redist_ms / max(s.n_exec, 1), "reduce_ms": s.reduce_ms / max(s.n_exec, 1)}
+    if orc.ref_lib() is None:
+        return None
+    _, times, _, _ = orc.ref_ca3dmm(P, n, n, n, ta, 0, A, B, grid=GRID, ntest=ntest, timeout=600.0)
+    return list(times[:, 0])
 
 
 def cpu_baseline(A, B, ta, n, budget_s=20.0):
-    """The oracle's CPU restatement of the virtual-rank algorithm (BLAS local
-    GEMMs, numpy) on a bounded sample: the k-slab 0 cuboids of the 4x2x3
-    grid, i.e. one third of the 8000^3 work, repeated while under budget."""
+    """CPU baseline on this host: the reference's own CPU path when it was
+    built (kind "reference"), else the oracle's numpy restatement of the
+    virtual-rank algorithm on k-slab 0 (kind "port")."""
     from oracle import oracle as orc
+    flops = 2.0 * n * n * n
+    ms = ref_cpu_run(A, B, ta, n, 1)
+    if ms is not None:
+        return {"value": flops / (ms[0] * 1e-3) / 1e12, "unit": "TFLOP/s",
+                "cores": min(P, cpu_cores()), "kind": "reference",
+                "sample": "one full %d^3 exec (after one warm-up) of the reference's CPU path, "
+                          "24 rank threads on grid 4x2x3, 1 OpenBLAS thread per rank" % n}
     cores = os.cpu_count()
     try:
         from threadpoolctl import threadpool_info
@@ -190,30 +188,45 @@ def cpu_baseline(A, B, ta, n, budget_s=20.0):
 
 
 def reference_arm(args, world, rank):
+    """The reference's CPU implementation of the path on this host's cores
+    (rank 0 only): each step is one full ca3dmm_engine_exec of the reference
+    over the same 8000^3 inputs and 4x2x3 grid."""
     if rank != 0:
         return
     n = args.size
     A, B = make_inputs(n, args.trans_a)
     steps, warm = max(args.steps, 1), max(args.warmup, 0)
-    base = None
-    for _ in range(warm):
-        cpu_baseline(A, B, args.trans_a, n, budget_s=4.0)
-    vals = []
-    for _ in range(steps):
-        base = cpu_baseline(A, B, args.trans_a, n, budget_s=4.0)
-        vals.append(base["value"])
-    v = float(np.median(vals))
-    base["value"] = v
+    flops = 2.0 * n * n * n
+    ms = ref_cpu_run(A, B, args.trans_a, n, warm + steps)
+    if ms is not None:
+        t = float(np.mean(ms[warm:]))
+        v = flops / (t * 1e-3) / 1e12
+        base = {"value": v, "unit": "TFLOP/s", "cores": min(P, cpu_cores()), "kind": "reference",
+                "sample": "%d full %d^3 execs of the reference's CPU path (24 rank threads, grid "
+                          "4x2x3, 1 OpenBLAS thread per rank) after %d warm-up" % (steps, n, warm + 1)}
+        note = ("reference src/ca3dmm.c CPU path (DEV_TYPE_HOST, OpenBLAS 0.3.31) compiled "
+                "unmodified; MPI ranks are threads of one process")
+    else:
+        vals = []
+        for _ in range(warm):
+            cpu_baseline(A, B, args.trans_a, n, budget_s=4.0)
+        for _ in range(steps):
+            base = cpu_baseline(A, B, args.trans_a, n, budget_s=4.0)
+            vals.append(base["value"])
+        v = float(np.median(vals))
+        base["value"] = v
+        t = flops / (v * 1e12) * 1e3
+        note = "reference build absent: the oracle's restatement of its CPU path"
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "TFLOP/s",
-            "n_gpus": args.gpus, "steps": steps, "warmup": warm,
-            "ms_per_step": 2.0 * n * n * n / (v * 1e12) * 1e3, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": t,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
             "config": {"workload": "ca3dmm_exec M=N=K=%d transA=%d grid 4x2x3 (24 virtual ranks)"
                                    % (n, args.trans_a), "l2": "inputs larger than L2"},
             "cpu_baseline": base,
             "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
-            "note": "reference CPU path restated by the oracle (MPI + BLAS cannot be built here)"}
+            "note": note}
     print(json.dumps(line), flush=True)
 
 
@@ -293,6 +306,70 @@ def run_grouped(args, world, rank, local):
     print(json.dumps(out), flush=True)
 
 
+BTB_K, BTB_N, BTB_P, BTB_GRID = 1048576, 512, 32, (1, 1, 32)
+
+
+def make_btb(k, n, seed=303):
+    """B (k x n, column-major) with column j ~ N(0, 1) * 10^u_j, u_j uniform in
+    [-3, 3], from a seeded torch generator (the tall-skinny Gram workload)."""
+    import torch
+    g = torch.Generator().manual_seed(seed)
+    z = torch.randn(n, k, dtype=torch.float64, generator=g)
+    u = torch.rand(n, dtype=torch.float64, generator=g) * 6.0 - 3.0
+    z.mul_(torch.pow(10.0, u)[:, None])
+    return z.numpy().T          # Fortran-ordered view of the (n, k) row-major buffer
+
+
+def workload(args):
+    if args.workload == "btb":
+        B = make_btb(BTB_K, BTB_N)
+        return {"m": BTB_N, "n": BTB_N, "k": BTB_K, "ta": 0, "btb": True, "p": BTB_P,
+                "grid": BTB_GRID, "A": None, "B": B,
+                "label": "btb %dx%d grid 1x1x32" % (BTB_K, BTB_N),
+                "desc": "ca3dmm_exec B^T B, B %dx%d, columns N(0,1)*10^u, u in [-3,3], 32 virtual "
+                        "ranks on grid 1x1x32 (kp-slab reduction on device)" % (BTB_K, BTB_N),
+                "l2": "B is 4.3 GB, larger than L2, no flush"}
+    n = args.size
+    A, B = make_inputs(n, args.trans_a)
+    return {"m": n, "n": n, "k": n, "ta": args.trans_a, "btb": False, "p": P, "grid": GRID,
+            "A": A, "B": B, "label": "square %d^3 grid 4x2x3" % n,
+            "desc": "ca3dmm_exec M=N=K=%d transA=%d transB=0, 24 virtual ranks, grid 4x2x3 "
+                    "(cuboid 2000x4000x2667), entries sign*(1+u)*2^e, e in [-8,8]"
+                    % (n, args.trans_a),
+            "l2": "inputs larger than L2 (512 MB per operand), no flush"}
+
+
+def sampled_error(Cdev, wl, nsample=2048):
+    """Errors of sampled device entries against the double-double oracle."""
+    import torch
+    from oracle import oracle as orc
+    m, n, k = wl["m"], wl["n"], wl["k"]
+    if wl["btb"]:
+        ii, jj = orc.sample_indices(n, n, nrand=256, nlines=0)
+        hi, lo, ab = orc.dd_entries(wl["B"], wl["B"], 1, 0, k, ii, jj)
+    else:
+        ii, jj = orc.sample_indices(m, n, nrand=nsample, nlines=1)
+        hi, lo, ab = orc.dd_entries(wl["A"], wl["B"], wl["ta"], 0, k, ii, jj)
+    idx = torch.from_numpy(ii + jj * m).cuda()
+    return orc.errors(Cdev[idx].cpu().numpy(), hi, lo, ab)
+
+
+def btb_cpu_baseline(wl, rows=131072):
+    """The reference's CPU B^T B on the first `rows` rows of B (same 32-rank
+    1x1x32 grid, one warm-up and one timed exec)."""
+    from oracle import oracle as orc
+    if orc.ref_lib() is None:
+        return None
+    n = wl["n"]
+    Bs = np.asfortranarray(wl["B"][:rows, :])
+    _, times, _, _ = orc.ref_ca3dmm(BTB_P, n, n, rows, 0, 0, None, Bs, grid=BTB_GRID, ntest=1,
+                                   btb=True, timeout=600.0)
+    return {"value": 2.0 * n * n * rows / (times[0, 0] * 1e-3) / 1e12, "unit": "TFLOP/s",
+            "cores": min(BTB_P, cpu_cores()), "kind": "reference",
+            "sample": "B^T B of the first %d of %d rows, reference CPU path, 32 rank threads on "
+                      "grid 1x1x32" % (rows, wl["k"])}
+
+
 def main():
     args = parse()
     world, rank, local = dist_setup(args)
@@ -309,36 +386,76 @@ def main():
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     import ca3dmm_b200 as cb
-    n = args.size
-    A, B = make_inputs(n, args.trans_a)
-    dA = torch.from_numpy(A.ravel(order="F").copy()).cuda()
-    dB = torch.from_numpy(B.ravel(order="F").copy()).cuda()
-    dC = torch.zeros(n * n, dtype=torch.float64, device="cuda")
+    wl = workload(args)
+    m, n, k, ta, btb = wl["m"], wl["n"], wl["k"], wl["ta"], wl["btb"]
+    lda = (k if ta else m) if not btb else 0
+    ldb = k
+    hA = None if btb else torch.from_numpy(wl["A"].ravel(order="F")).pin_memory()
+    hB = torch.from_numpy(wl["B"].ravel(order="F")).pin_memory()
+    dA = None if btb else hA.cuda()
+    dB = hB.cuda()
+    dC = torch.zeros(m * n, dtype=torch.float64, device="cuda")
     stream = torch.cuda.default_stream()
-    flops = 2.0 * n * n * n
+    flops = 2.0 * m * n * k
+
+    def engine():
+        return cb.Ca3dmmEngine(m, n, k, ta, 0, p=wl["p"], proc_grid=wl["grid"], btb=btb)
+
+    def leg(eng, steps, warmup):
+        for _ in range(warmup):
+            if eng.exec(dA, lda, dB, ldb, dC, m):
+                raise RuntimeError("exec failed")
+        torch.cuda.synchronize()
+        eng.reset_stat()
+        evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+        # the engine runs synchronously on the legacy default stream; events on it
+        evs[0].record(stream)
+        for i in range(steps):
+            eng.exec(dA, lda, dB, ldb, dC, m)
+            evs[i + 1].record(stream)
+        torch.cuda.synchronize()
+        st = eng.s
+        per = [evs[i].elapsed_time(evs[i + 1]) for i in range(steps)]
+        return {"ms_per_step": evs[0].elapsed_time(evs[-1]) / steps,
+                "ms_median": float(np.median(per)), "ms_min": float(min(per)),
+                "gemm_ms": st.cannon_ms / max(st.n_exec, 1),
+                "pack_ms": st.redist_ms / max(st.n_exec, 1),
+                "reduce_ms": st.reduce_ms / max(st.n_exec, 1)}
 
     legs = {}
-    eng_plain = cb.Ca3dmmEngine(n, n, n, args.trans_a, 0, p=P)
+    eng_plain = engine()
     assert eng_plain.ok, "engine init failed"
     eng_plain.set_gemm_mode(cb.GEMM_PLAIN)
-    eng_oz = None
     oz_slices = int(os.environ.get("CA3DMM_BENCH_SLICES", "7"))
-    try:
-        e = cb.Ca3dmmEngine(n, n, n, args.trans_a, 0, p=P)
-        if e.ok and e.set_gemm_mode(cb.GEMM_OZAKI, oz_slices) == 0 and \
-                e.exec(dA, n, dB, n, dC, n) == 0:
-            eng_oz = e
-    except Exception:
-        eng_oz = None
-
-    # plain leg
-    legs["plain"] = run_leg(eng_plain, dA, dB, dC, n, 1, args.warmup, stream)
-    legs["plain"]["err"] = error_vs_dd(dC, A, B, args.trans_a, n)
-    if eng_oz is not None:
-        legs["ozaki"] = run_leg(eng_oz, dA, dB, dC, n, 1, args.warmup, stream)
-        legs["ozaki"]["err"] = error_vs_dd(dC, A, B, args.trans_a, n)
-    head = "ozaki" if eng_oz is not None else "plain"
-    eng = eng_oz if eng_oz is not None else eng_plain
+    eng_oz = engine()
+    if not (eng_oz.ok and eng_oz.set_gemm_mode(cb.GEMM_OZAKI, oz_slices) == 0 and
+            eng_oz.exec(dA, lda, dB, ldb, dC, m) == 0):
+        raise RuntimeError("split-precision engine failed")
+    legs["plain"] = leg(eng_plain, 1, args.warmup)
+    legs["plain"]["err"] = sampled_error(dC, wl)
+    legs["ozaki"] = leg(eng_oz, 1, args.warmup)
+    legs["ozaki"]["err"] = sampled_error(dC, wl)
+    legs["ozaki"]["slices"] = oz_slices
+    if not btb and not args.no_slice_sweep:
+        # the other slice counts: time and error of each (one timed exec)
+        sweep = {}
+        for sc in (3, 4, 5, 6, 8):
+            if sc == oz_slices:
+                continue
+            e2 = engine()
+            if e2.ok and e2.set_gemm_mode(cb.GEMM_OZAKI, sc) == 0:
+                r = leg(e2, 2, 1)
+                r["err"] = sampled_error(dC, wl)
+                r["tflops"] = flops / (r["ms_per_step"] * 1e-3) / 1e12
+                sweep[str(sc)] = r
+            e2.free()
+        legs["ozaki_slice_sweep"] = sweep
+    # the split-precision leg is the headline only while its error stays within
+    # twice the plain FP64 error (normwise and relative to |A||B|)
+    eo, ep = legs["ozaki"]["err"], legs["plain"]["err"]
+    head = "ozaki" if (eo["normwise"] <= 2 * ep["normwise"] and
+                       eo["vs_absprod"] <= 2 * ep["vs_absprod"]) else "plain"
+    eng = eng_oz if head == "ozaki" else eng_plain
 
     # timed region (headline leg), clocks sampled meanwhile
     sampler = ClockSampler(local)
@@ -347,7 +464,9 @@ def main():
     torch.cuda.synchronize()
     sampler.start()
     time.sleep(0.3)
-    res = run_leg(eng, dA, dB, dC, n, args.steps, 0, stream)
+    l0 = cb.kernel_launches()
+    res = leg(eng, args.steps, 0)
+    launches = cb.kernel_launches() - l0
     clocks = sampler.stop()
     ms = res["ms_per_step"]
     if world > 1:
@@ -355,28 +474,26 @@ def main():
         torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
         ms = float(t.item())
     value = world * flops / (ms * 1e-3) / 1e12
-    # also time the other leg over the same number of steps (reported beside)
-    other = "plain" if head == "ozaki" else None
-    if other:
-        r2 = run_leg(eng_plain, dA, dB, dC, n, max(2, args.steps // 2), 1, stream)
-        legs["plain"].update(r2)
+    other = "plain" if head == "ozaki" else "ozaki"
+    legs[other].update(leg(eng_plain if other == "plain" else eng_oz, max(2, args.steps // 2), 1))
+    legs[head].update(res)
 
-    # e2e: the same exec through the C ABI with host buffers, copies timed
-    hA = torch.from_numpy(A.ravel(order="F").copy()).pin_memory()
-    hB = torch.from_numpy(B.ravel(order="F").copy()).pin_memory()
-    hC = torch.empty(n * n, dtype=torch.float64).pin_memory()
+    # e2e: the same exec through the C ABI with pinned host buffers, copies timed
+    hC = torch.empty(m * n, dtype=torch.float64).pin_memory()
     e2e_steps = max(2, min(args.steps, 5))
-    for _ in range(1):
-        dA.copy_(hA, non_blocking=True); dB.copy_(hB, non_blocking=True)
-        eng.exec(dA, n, dB, n, dC, n); hC.copy_(dC)
+
+    def e2e_step():
+        if dA is not None:
+            dA.copy_(hA, non_blocking=True)
+        dB.copy_(hB, non_blocking=True)
+        eng.exec(dA, lda, dB, ldb, dC, m)
+        hC.copy_(dC, non_blocking=True)
+    e2e_step()
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     ev0.record(stream)
     for _ in range(e2e_steps):
-        dA.copy_(hA, non_blocking=True)
-        dB.copy_(hB, non_blocking=True)
-        eng.exec(dA, n, dB, n, dC, n)
-        hC.copy_(dC, non_blocking=True)
+        e2e_step()
     ev1.record(stream)
     torch.cuda.synchronize()
     e2e_ms = ev0.elapsed_time(ev1) / e2e_steps
@@ -386,41 +503,42 @@ def main():
         e2e_ms = float(t.item())
 
     peaks = measured_peaks()
-    traffic = ncu_traffic()
+    traffic = ncu_traffic().get(wl["label"], {})
     gemm_ms = res["gemm_ms"]
     if head == "ozaki":
         s = eng.s.ozaki_slices
         ops = flops * s * (s + 1) / 2           # INT8 ops of the slice products
         peak = 2.0 * peaks.get("bf16_tflops", 1590.0)
-        roof = {"bound": "tensor", "achieved": ops / (gemm_ms * 1e-3) / 1e12, "peak": peak,
-                "unit": "TFLOP/s", "peak_source": "2 x measured dense bf16 (INT8 dense rate)",
-                "traffic": traffic.get("ozaki_gemm")}
+        roof = {"bound": "tensor", "kernel": "oz_gemm_kernel",
+                "achieved": ops / (gemm_ms * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
+                "peak_source": "of measured: 2 x measured dense bf16 (dense INT8 rate is twice "
+                               "the bf16 rate)" if "bf16_tflops" in peaks else "of fallback",
+                "traffic": traffic.get("oz_gemm_kernel")}
     else:
         sm_mhz = peaks.get("sm_max_mhz", 1965.0)
         peak = 148 * 128 * sm_mhz * 1e6 / 1e12
-        roof = {"bound": "tensor", "achieved": flops / (gemm_ms * 1e-3) / 1e12, "peak": peak,
-                "unit": "TFLOP/s",
+        roof = {"bound": "tensor", "kernel": "dgemm_dmma_grouped",
+                "achieved": flops / (gemm_ms * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
                 "peak_source": "nominal FP64 DMMA rate 148 SM x 128 flop/clk x max SM clock",
-                "traffic": traffic.get("dgemm_dmma")}
+                "traffic": traffic.get("dgemm_dmma_grouped")}
     roof["frac"] = roof["achieved"] / roof["peak"]
-    launches_per_step = 4 if head == "plain" else 5
+    in_bytes = (0 if dA is None else dA.numel() * 8) + dB.numel() * 8
     out = {
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": "ca3dmm_exec M=N=K=%d transA=%d transB=0, 24 virtual ranks, grid "
-                               "4x2x3 (cuboid 2000x4000x2667), entries sign*(1+u)*2^e, e in [-8,8]"
-                               % (n, args.trans_a),
-                   "gemm": head, "ozaki_slices": eng.s.ozaki_slices if head == "ozaki" else None,
-                   "l2": "inputs larger than L2 (512 MB per operand), no flush"},
+        "config": {"workload": wl["desc"], "gemm": head,
+                   "ozaki_slices": eng.s.ozaki_slices if head == "ozaki" else None,
+                   "l2": wl["l2"]},
         "legs": legs, "roofline": roof, "clocks": clocks,
         "e2e": {"value": world * flops / (e2e_ms * 1e-3) / 1e12, "unit": "TFLOP/s",
-                "h2d_bytes_per_step": 2 * n * n * 8, "d2h_bytes_per_step": n * n * 8},
-        "gpu_launches": launches_per_step * args.steps,
+                "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": m * n * 8},
+        "gpu_launches": int(launches),
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        out["cpu_baseline"] = cpu_baseline(A, B, args.trans_a, n)
+        out["cpu_baseline"] = btb_cpu_baseline(wl) if btb else \
+            cpu_baseline(wl["A"], wl["B"], ta, n)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:

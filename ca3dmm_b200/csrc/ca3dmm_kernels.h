@@ -78,6 +78,9 @@ int ca3dmm_reduce_slabs_launch(const double *slab, long long slab_stride, long l
 /* ---- device properties (cached) ------------------------------------------ */
 int ca3dmm_device_sm_count(void);
 
+/* Adds n to the library's count of kernel launches (ca3dmm_kernel_launches). */
+void ca3dmm_note_launch(int n);
+
 #ifdef __cplusplus
 }
 #endif

@@ -389,6 +389,7 @@ extern "C" int ca3dmm_dgemm_launch(const void *dev_plan, int nprob, int total_ti
     dgemm_dmma_grouped<<<grid, THREADS, SMEM_BYTES, stream>>>(tm, dp, nprob, total_tiles,
                                                                dev_status, limit);
     CA3DMM_CUDA_TRY(cudaGetLastError());
+    ca3dmm_note_launch(1);
     return CA3DMM_OK;
 }
 

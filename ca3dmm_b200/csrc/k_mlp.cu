@@ -134,6 +134,7 @@ int forward(ca3dmm_mlp *m, int B)
     dense_fwd<<<blocks((long long) B * m->h2), 256>>>(m->a1, W2, b2, m->a2, B, m->h1, m->h2, 1);
     dense_fwd<<<blocks(B), 256>>>(m->a2, W3, b3, m->out, B, m->h2, 1, 0);
     CA3DMM_CUDA_TRY(cudaGetLastError());
+    ca3dmm_note_launch(3);
     return CA3DMM_OK;
 }
 
@@ -155,6 +156,7 @@ int fwd_bwd(ca3dmm_mlp *m, int B)
     dense_wgrad<<<blocks(m->h1 * m->nin + m->h1), 256>>>(m->d1, m->X, gW1, gb1, B, m->nin, m->h1);
     (void) W1;
     CA3DMM_CUDA_TRY(cudaGetLastError());
+    ca3dmm_note_launch(6);
     return CA3DMM_OK;
 }
 
@@ -318,6 +320,7 @@ extern "C" int ca3dmm_mlp_train(ca3dmm_mlp_p m, const float *X, const float *y, 
             adam_step<<<blocks(m->np), 256>>>(m->params, m->grads, m->m1, m->m2, m->np, lr, b1, b2,
                                               eps, c1, c2);
             if (cudaGetLastError() != cudaSuccess) rc = CA3DMM_ECUDA;
+            ca3dmm_note_launch(1);
         }
     }
     if (!rc) {

@@ -714,12 +714,14 @@ extern "C" int ca3dmm_oz_run_pack(const ca3dmm_oz_plan_t *oz, const void *A, con
         oz_exp_kernel<<<tiles[o] < cap ? tiles[o] : cap, 256, 0, stream>>>(
             src[o], sd + first[o], cnt[o], tiles[o], reinterpret_cast<unsigned *>(w));
         CA3DMM_CUDA_TRY(cudaGetLastError());
+        ca3dmm_note_launch(1);
     }
     for (int o = 0; o < 2; ++o) {
         if (cnt[o] == 0 || tiles[o] == 0) continue;
         oz_slice_kernel<<<tiles[o] < cap ? tiles[o] : cap, 256, 0, stream>>>(
             src[o], sd + first[o], cnt[o], tiles[o], w, oz->slices);
         CA3DMM_CUDA_TRY(cudaGetLastError());
+        ca3dmm_note_launch(1);
     }
     return CA3DMM_OK;
 }
@@ -746,5 +748,6 @@ extern "C" int ca3dmm_oz_run_gemm(const ca3dmm_oz_plan_t *oz, int *dev_status, d
         kb_per_chunk, diagonal_split(oz->slices), static_cast<const unsigned char *>(oz->dev_work),
         dev_status, limit);
     CA3DMM_CUDA_TRY(cudaGetLastError());
+    ca3dmm_note_launch(1);
     return CA3DMM_OK;
 }

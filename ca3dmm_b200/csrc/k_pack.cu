@@ -6,6 +6,7 @@
 //   * the kp-slab FP64 reduction -- the on-device form of the C
 //     reduce-scatter with mpi_op_omp_sum (src/ca3dmm.c:1287-1343,
 //     src/mpi_op_omp.c:6-23), summing slabs in rank order.
+#include <atomic>
 #include <cuda_runtime.h>
 #include "k_common.cuh"
 #include "ca3dmm_kernels.h"
@@ -100,6 +101,18 @@ reduce_slabs_kernel(const double *__restrict__ slab, long long slab_stride, long
 
 }  // namespace
 
+static std::atomic<unsigned long long> g_kernel_launches{0};
+
+extern "C" void ca3dmm_note_launch(int n)
+{
+    g_kernel_launches.fetch_add((unsigned long long) n, std::memory_order_relaxed);
+}
+
+extern "C" unsigned long long ca3dmm_kernel_launches(void)
+{
+    return g_kernel_launches.load(std::memory_order_relaxed);
+}
+
 extern "C" int ca3dmm_pack_tiles(ca3dmm_pack_desc_t *descs, int ndesc)
 {
     int tiles = 0;
@@ -120,6 +133,7 @@ extern "C" int ca3dmm_pack_launch(const double *src_base, double *dst_base,
     if (grid > total_tiles) grid = total_tiles;
     pack_kernel<<<grid, 256, 0, stream>>>(src_base, dst_base, dev_descs, ndesc, total_tiles);
     CA3DMM_CUDA_TRY(cudaGetLastError());
+    ca3dmm_note_launch(1);
     return CA3DMM_OK;
 }
 
@@ -137,5 +151,6 @@ extern "C" int ca3dmm_reduce_slabs_launch(const double *slab, long long slab_str
     reduce_slabs_kernel<<<(unsigned) blocks, 256, 0, stream>>>(slab, slab_stride, lds, nslab, m, n,
                                                              out, ldo, vec);
     CA3DMM_CUDA_TRY(cudaGetLastError());
+    ca3dmm_note_launch(1);
     return CA3DMM_OK;
 }

@@ -159,6 +159,11 @@ void ca3dmm_engine_print_stat(ca3dmm_engine_p engine);
 
 /* ---- added entry points (no counterpart in the reference) ---- */
 
+/* Kernels this library has launched since it was loaded, counted on the
+ * host at each launch (a launch recorded into a CUDA graph counts once, at
+ * capture; its replays do not). */
+unsigned long long ca3dmm_kernel_launches(void);
+
 /* First error of the last call on this engine (0 = none). */
 int ca3dmm_engine_last_error(ca3dmm_engine_p engine);
 /* Run exec on `stream` (cudaStream_t); sync = 0 makes exec asynchronous and

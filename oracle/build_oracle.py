@@ -58,7 +58,8 @@ def build():
             clib = os.path.join(out, "libref_ca3dmm.so")
             if _newer(clib, srcs + mine + hdrs):
                 d, f = os.path.split(openblas)
-                _run(["gcc", "-O2", "-fPIC", "-shared", "-fopenmp", "-DUSE_OPENBLAS",
+                pre = ["-DVMPI_SCIPY_OPENBLAS"] if "scipy_openblas" in f else []
+                _run(["gcc", "-O2", "-fPIC", "-shared", "-fopenmp", "-DUSE_OPENBLAS"] + pre + [
                       "-Wno-implicit-function-declaration", "-I", vdir, "-I", refsrc] + srcs + mine +
                      ["-o", clib, "-L", d, "-l:" + f, "-Wl,--disable-new-dtags", "-Wl,-rpath," + d,
                       "-Wl,-Bsymbolic",
@@ -67,11 +68,14 @@ def build():
 
 
 def find_openblas():
-    """The OpenBLAS build with unprefixed CBLAS symbols shipped in this image."""
+    """An LP64 OpenBLAS shipped in this image: the scipy wheel's build
+    (0.3.31, scipy_-prefixed exports, Skylake-X kernels) first, else one with
+    plain CBLAS names."""
     import glob
     import site
     for sp in site.getsitepackages():
-        for pat in ("opencv_python_headless.libs/libopenblas*.so*", "*/libopenblas*.so*"):
+        for pat in ("scipy.libs/libscipy_openblas-*.so", "opencv_python_headless.libs/libopenblas*.so*",
+                    "*/libopenblas*.so*"):
             hits = sorted(glob.glob(os.path.join(sp, pat)))
             if hits:
                 return hits[0]

@@ -11,6 +11,7 @@
 #include <string.h>
 #include <omp.h>
 #include "mpi.h"
+#include "cblas.h"
 #include "ca3dmm.h"
 
 typedef struct {
