@@ -43,7 +43,7 @@ typedef struct {
     int tiles;            /* total output tiles of the grouped INT8 launch */
     int max_rows, max_kpad;
     int slice_tiles_a, slice_tiles_b;   /* 64 x 64 slicing tiles of the A / B blocks */
-    long long n_exp;      /* exponents (ints) at the start of the work region */
+    long long n_exp;      /* rows with an exponent: E (int) then max bits (u64) arrays open the work region */
     void *dev_plan;       /* device copy of the plan (slice descriptors, tensor maps, groups) */
     void *dev_work;       /* slices and exponents */
 } ca3dmm_oz_plan_t;

@@ -26,12 +26,14 @@
 //                         down to 0, into FP64 registers, and stores C after the
 //                         last chunk.
 // Warp roles of the GEMM: warp 0 copy producer, warps 1, 6, 7 MMA issuers, each
-// owning a contiguous interval of diagonals (disjoint TMEM columns; warp 1 also
-// owns the TMEM allocation), warps 2..5 epilogue (warp w reads TMEM lanes
-// 32*(w%4)..+31).  Each issuing warp needs ~150-190 cycles per tcgen05.mma, so
-// one issuer cannot keep the tensor core busy with M=128 MMAs; several issuers
-// with disjoint accumulators can.  All waits are
-// bounded; on timeout the kernel records a status, drains, frees TMEM, returns.
+// owning a set of A slices (warp 1 also owns the TMEM allocation), warps 2..5
+// epilogue (warp w reads TMEM lanes 32*(w%4)..+31).  Each issuing thread needs
+// ~150-190 cycles per tcgen05.mma, so one issuer cannot keep the tensor core
+// busy; the A slices are dealt out so that no issuer has more than four MMAs
+// per k-block (s <= 8).  Issuers of different slices add into
+// the same diagonal accumulators, so every MMA accumulates and the epilogue
+// zeroes each accumulator after reading it.  All waits are bounded; on
+// timeout the kernel records a status, drains, frees TMEM, returns.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <climits>
@@ -106,99 +108,168 @@ __device__ __forceinline__ const double *slice_src(const double *base, long long
                                             (uintptr_t) off * sizeof(double));
 }
 
-// Persistent over the flat list of 64 x 64 (rows x k) tiles of every block.
+// Work region: [E + EXP_BIAS per row, int][max |x| per row as its IEEE bit
+// pattern, u64][tiled slices].  Both prefix arrays are cleared before a run.
+__host__ __device__ inline size_t exp_bytes(long long n_exp)
+{
+    return ((size_t) n_exp * sizeof(int) + 255) / 256 * 256;
+}
+__host__ __device__ inline size_t maxbits_bytes(long long n_exp)
+{
+    return ((size_t) n_exp * sizeof(unsigned long long) + 255) / 256 * 256;
+}
+
+// Pass 1, persistent over the flat list of 64 x 64 (rows x k) tiles of every
+// block: per row, the largest |x| as its bit pattern (for non-negative doubles
+// the bit pattern orders like the value).  The effective exponent
+// E(x) = min{E : |x| <= 2^E 127/128} is non-decreasing in |x|, so the row's
+// exponent max_l E(x_l) is E(max_l |x_l|), formed once per row in pass 2.
 __global__ void __launch_bounds__(256)
 oz_exp_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ descs, int ndesc,
-              int total_tiles, unsigned *__restrict__ ework)
+              int total_tiles, unsigned long long *__restrict__ mwork)
 {
-    __shared__ int smax[ST];
+    __shared__ unsigned long long part[4][ST];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
         const SliceDesc d = descs[find_slice_desc(descs, ndesc, tile)];
         const int local = tile - d.tile_begin, tx = (d.rows_pad + ST - 1) / ST;
         const int r0 = (local % tx) * ST, l0 = (local / tx) * ST;
-        __syncthreads();
-        if (threadIdx.x < ST) smax[threadIdx.x] = 0;
-        __syncthreads();
+        const int rn = min(ST, d.rows - r0), ln = min(ST, d.kz - l0);
+        if (rn <= 0 || ln <= 0) continue;               // padding tile (uniform)
+        const double *base = slice_src(src, d.src_off) + (long long) r0 * d.rs + (long long) l0 * d.ls;
+        if (d.rs == 1) {
+            // rows contiguous: thread (row r, k phase g) walks k = g, g + 4, ...
+            const int r = threadIdx.x & (ST - 1), g = threadIdx.x >> 6;
+            unsigned long long m = 0;
+            if (r < rn) {
+#pragma unroll
+                for (int j = 0; j < ST / 4; ++j) {
+                    const int l = g + 4 * j;
+                    if (l < ln) {
+                        const unsigned long long v =
+                            (unsigned long long) __double_as_longlong(__ldg(base + r + (long long) l * d.ls)) &
+                            0x7fffffffffffffffull;
+                        m = v > m ? v : m;
+                    }
+                }
+            }
+            __syncthreads();                             // part[] of the previous tile is read
+            part[g][r] = m;
+            __syncthreads();
+            if (threadIdx.x < rn) {
+                unsigned long long v = part[0][threadIdx.x];
+#pragma unroll
+                for (int q = 1; q < 4; ++q) v = part[q][threadIdx.x] > v ? part[q][threadIdx.x] : v;
+                if (v) atomicMax(mwork + d.e_off + r0 + threadIdx.x, v);
+            }
+        } else {
+            // k contiguous: warp w reads rows w, w + 8, ... (64 consecutive k each)
+            unsigned long long m[ST / 8];
+#pragma unroll
+            for (int j = 0; j < ST / 8; ++j) {
+                const int r = warp + 8 * j;
+                unsigned long long v0 = 0, v1 = 0;
+                if (r < rn) {
+                    const double *row = base + (long long) r * d.rs;
+                    if (lane < ln)
+                        v0 = (unsigned long long) __double_as_longlong(__ldg(row + (long long) lane * d.ls));
+                    if (lane + 32 < ln)
+                        v1 = (unsigned long long) __double_as_longlong(__ldg(row + (long long) (lane + 32) * d.ls));
+                }
+                v0 &= 0x7fffffffffffffffull;
+                v1 &= 0x7fffffffffffffffull;
+                m[j] = v1 > v0 ? v1 : v0;
+            }
+#pragma unroll
+            for (int j = 0; j < ST / 8; ++j) {
+                unsigned long long v = m[j];
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
+                    v = w > v ? w : v;
+                }
+                const int r = warp + 8 * j;
+                if (lane == 0 && r < rn && v) atomicMax(mwork + d.e_off + r0 + r, v);
+            }
+        }
+    }
+}
+
+// Pass 2: slices of one 64 x 64 tile through shared memory.  Thread (row r,
+// 16-byte k chunk c) forms N = rint(x 2^(8S-1-E)) for its 16 elements; the
+// balanced digits q_t in [-128, 127] of N (least significant first:
+// q = ((N + 128) mod 256) - 128, N = (N - q) / 256) are exactly the bytes of
+// N + 0x80..80 (S bytes of 0x80) with the top bit flipped, because adding 128
+// to every digit of a balanced representation gives the unsigned base-256
+// representation of N + 0x80..80 (|N| < 2^(8S-1) 127/128 keeps it in range).
+// Slice t holds digit S-1-t.  The 16 bytes of each slice are gathered with
+// byte permutes and stored with the 32-byte swizzle of the GEMM's operand tile.
+template <int S>
+__global__ void __launch_bounds__(256)
+oz_slice_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ descs, int ndesc,
+                int total_tiles, unsigned char *__restrict__ work,
+                const unsigned long long *__restrict__ mwork)
+{
+    __shared__ double tile[ST][ST + 1];
+    int *ework = reinterpret_cast<int *>(work);
+    for (int gtile = blockIdx.x; gtile < total_tiles; gtile += gridDim.x) {
+        const SliceDesc d = descs[find_slice_desc(descs, ndesc, gtile)];
+        const int local = gtile - d.tile_begin, tx = (d.rows_pad + ST - 1) / ST;
+        const int r0 = (local % tx) * ST, l0 = (local / tx) * ST;
         const double *base = slice_src(src, d.src_off);
-        const bool rfast = d.rs == 1;   // consecutive threads walk the contiguous index
+        const bool rfast = d.rs == 1;
+        __syncthreads();
         for (int e = threadIdx.x; e < ST * ST; e += blockDim.x) {
             const int a = e % ST, b = e / ST;
             const int r = rfast ? a : b, l = rfast ? b : a;
             const int gr = r0 + r, gl = l0 + l;
-            if (gr < d.rows && gl < d.kz) {
-                const double v = fabs(__ldg(base + gr * d.rs + gl * d.ls));
-                if (v != 0.0) {
-                    // effective exponent: one more when the mantissa exceeds 127/128,
-                    // so that max|x| <= 2^E * 127/128 and the top digit fits in int8
-                    int ex;
-                    const double mant = frexp(v, &ex);
-                    atomicMax(&smax[r], ex + (mant > 0.9921875 ? 1 : 0) + EXP_BIAS);
-                }
-            }
+            tile[r][l] = (gr < d.rows && gl < d.kz) ? __ldg(base + gr * d.rs + gl * d.ls) : 0.0;
         }
         __syncthreads();
-        if (threadIdx.x < ST && r0 + threadIdx.x < d.rows && smax[threadIdx.x] > 0)
-            atomicMax(ework + d.e_off + r0 + threadIdx.x, (unsigned) smax[threadIdx.x]);
-    }
-}
-
-__global__ void __launch_bounds__(256)
-oz_slice_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ descs, int ndesc,
-                int total_tiles, unsigned char *__restrict__ work, int slices)
-{
-    __shared__ double tile[ST][ST + 1];
-  for (int gtile = blockIdx.x; gtile < total_tiles; gtile += gridDim.x) {
-    const SliceDesc d = descs[find_slice_desc(descs, ndesc, gtile)];
-    const int local = gtile - d.tile_begin, tx = (d.rows_pad + ST - 1) / ST;
-    const int r0 = (local % tx) * ST, l0 = (local / tx) * ST;
-    const double *base = slice_src(src, d.src_off);
-    const bool rfast = d.rs == 1;
-    __syncthreads();
-    for (int e = threadIdx.x; e < ST * ST; e += blockDim.x) {
-        const int a = e % ST, b = e / ST;
-        const int r = rfast ? a : b, l = rfast ? b : a;
-        const int gr = r0 + r, gl = l0 + l;
-        tile[r][l] = (gr < d.rows && gl < d.kz) ? __ldg(base + gr * d.rs + gl * d.ls) : 0.0;
-    }
-    __syncthreads();
-    // thread -> (row r, 16 consecutive k = one 16-byte chunk of a 32-byte k-block)
-    const int r = threadIdx.x >> 2, c = (threadIdx.x & 3) * 16;
-    const int gr = r0 + r, gl = l0 + c;
-    if (gr >= d.rows_pad || gl >= d.kpad) continue;
-    const unsigned eb = gr < d.rows ? reinterpret_cast<const unsigned *>(work)[d.e_off + gr] : 0u;
-    const int E = eb ? (int) eb - EXP_BIAS : 0;
-    // N = rint(x 2^(8s-1-E)) in balanced base-256 digits q_t in [-128, 127],
-    // least significant first: q = ((N + 128) mod 256) - 128, N = (N - q) / 256.
-    const double up = ldexp(1.0, 8 * slices - 1 - E);
-    uint32_t q[MAX_SLICES][4];
+        // thread -> (row r, 16 consecutive k); a warp covers 32 rows of one chunk
+        const int r = threadIdx.x & (ST - 1), c = (threadIdx.x >> 6) * 16;
+        const int gr = r0 + r, gl = l0 + c;
+        if (gr >= d.rows_pad || gl >= d.kpad) continue;
+        const unsigned long long mb = gr < d.rows ? mwork[d.e_off + gr] : 0ull;
+        int E = 0;
+        if (mb) {
+            int ex;
+            const double mant = frexp(__longlong_as_double((long long) mb), &ex);
+            E = ex + (mant > 0.9921875 ? 1 : 0);
+        }
+        if (l0 == 0 && c == 0 && gr < d.rows) ework[d.e_off + gr] = mb ? E + EXP_BIAS : 0;
+        // x 2^(8S-1-E) as two exact power-of-two factors (each inside the normal range)
+        const int sh = 8 * S - 1 - E;
+        const double up1 = ldexp(1.0, sh / 2), up2 = ldexp(1.0, sh - sh / 2);
+        constexpr unsigned long long BIAS = 0x8080808080808080ull >> (64 - 8 * S);
+        uint32_t lo[16], hi[16];
 #pragma unroll
-    for (int t = 0; t < MAX_SLICES; ++t)
+        for (int j = 0; j < 16; ++j) {
+            const long long N = __double2ll_rn(tile[r][c + j] * up1 * up2);
+            const unsigned long long U = (unsigned long long) N + BIAS;
+            lo[j] = (uint32_t) U;
+            hi[j] = (uint32_t) (U >> 32);
+        }
+        const int rt = gr / d.tile_rows, rr = gr % d.tile_rows;
+        const int kb = gl / OKB, chunk = (gl % OKB) >> 4;
+        const long long tile_bytes = (long long) d.tile_rows * OKB;
+        unsigned char *dst = work + d.q_off + ((long long) rt * d.nkb + kb) * S * tile_bytes +
+                             rr * OKB + ((chunk ^ ((rr >> 2) & 1)) << 4);
 #pragma unroll
-        for (int w = 0; w < 4; ++w) q[t][w] = 0;
+        for (int t = 0; t < S; ++t) {
+            const int b = S - 1 - t, bb = b & 3;
+            const uint32_t *w = b < 4 ? lo : hi;
+            const uint32_t sel = (uint32_t) bb | ((uint32_t) (bb + 4) << 4);
+            uint32_t out[4];
 #pragma unroll
-    for (int j = 0; j < 16; ++j) {
-        long long N = __double2ll_rn(tile[r][c + j] * up);
-#pragma unroll
-        for (int t = MAX_SLICES - 1; t >= 0; --t) {
-            if (t < slices) {
-                const long long dgt = ((N + 128) & 255) - 128;
-                N = (N - dgt) >> 8;
-                q[t][j >> 2] |= ((uint32_t) dgt & 0xffu) << (8 * (j & 3));
+            for (int q = 0; q < 4; ++q) {
+                const uint32_t p01 = __byte_perm(w[4 * q], w[4 * q + 1], sel);
+                const uint32_t p23 = __byte_perm(w[4 * q + 2], w[4 * q + 3], sel);
+                out[q] = __byte_perm(p01, p23, 0x5410) ^ 0x80808080u;
             }
+            *reinterpret_cast<uint4 *>(dst + t * tile_bytes) = make_uint4(out[0], out[1], out[2], out[3]);
         }
     }
-    // tiled, pre-swizzled destination
-    const int rt = gr / d.tile_rows, rr = gr % d.tile_rows;
-    const int kb = gl / OKB, chunk = (gl % OKB) >> 4;
-    const long long tile_bytes = (long long) d.tile_rows * OKB;
-    unsigned char *dst = work + d.q_off + ((long long) rt * d.nkb + kb) * slices * tile_bytes +
-                         rr * OKB + ((chunk ^ ((rr >> 2) & 1)) << 4);
-#pragma unroll
-    for (int t = 0; t < MAX_SLICES; ++t)
-        if (t < slices)
-            *reinterpret_cast<uint4 *>(dst + t * tile_bytes) =
-                make_uint4(q[t][0], q[t][1], q[t][2], q[t][3]);
-  }
 }
 
 // ------------------------------------------------------------------ tcgen05 GEMM
@@ -268,6 +339,26 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, uint32_t (&v)[32])
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 }
 
+// Zero 32 consecutive TMEM columns of this warp's 32 lanes.
+__device__ __forceinline__ void tmem_zero32(uint32_t taddr)
+{
+    const uint32_t z = 0;
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x32.b32 [%0], {%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,"
+        "%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1,%1};" ::"r"(taddr),
+        "r"(z)
+        : "memory");
+}
+
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
+
+// Exact int32 -> double without the conversion unit: the double with high word
+// 0x43300000 and low word v ^ 2^31 is 2^52 + v + 2^31.
+__device__ __forceinline__ double i32_to_f64(uint32_t v)
+{
+    return __hiloint2double(0x43300000, (int) (v ^ 0x80000000u)) - 4503601774854144.0;
+}
+
 // 2^e as a double: built from the exponent bits in the normal range (exact),
 // ldexp outside it.
 __device__ __forceinline__ double pow2(int e)
@@ -305,7 +396,7 @@ __device__ __forceinline__ int nchunks(int nkb, int kb_per_chunk)
 
 __global__ void __launch_bounds__(OTHREADS, 1)
 oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, int slices,
-               int nstage, int kb_per_chunk, int4 dsplit, const unsigned char *__restrict__ work,
+               int nstage, int kb_per_chunk, int4 tsplit, const unsigned char *__restrict__ work,
                int *status, unsigned long long limit_ns)
 {
     extern __shared__ uint8_t smem_raw[];
@@ -346,6 +437,16 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
     __syncthreads();
     tc_fence_after();
     const uint32_t tmem_base = tmem_slot;
+    // the MMAs only ever accumulate: the epilogue warps clear the accumulators
+    // here and again after draining each chunk
+    if (warp >= 2 && warp <= 5) {
+        const uint32_t lane_base = (uint32_t) ((warp & 3) * 32) << 16;
+        for (int c = 0; c < slices * OBN; c += 32) tmem_zero32(tmem_base + lane_base + (uint32_t) c);
+        tmem_wait_st();
+    }
+    tc_fence_before();
+    __syncthreads();
+    tc_fence_after();
 
     if (warp == 0) {
         // ---------------------------------------------------------- producer
@@ -385,11 +486,10 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
     } else if (warp == 1 || warp >= 6) {
         // ---------------------------------------------------------- MMA issuers
         if (lane == 0) {
-            // this issuer's accumulators: diagonals [d0, d1) (possibly empty; an
-            // issuer without diagonals still commits, keeping barrier counts)
+            // this issuer's A slices (bit t of the mask; possibly none: an idle
+            // issuer still commits, keeping the barrier counts)
             const int ii = warp == 1 ? 0 : warp - 5;
-            const int d0 = ii == 0 ? 0 : (ii == 1 ? dsplit.x : dsplit.y);
-            const int d1 = ii == 0 ? dsplit.x : (ii == 1 ? dsplit.y : slices);
+            const unsigned tmask = (unsigned) (ii == 0 ? tsplit.x : (ii == 1 ? tsplit.y : tsplit.z));
             uint32_t it = 0, ci = 0;
             bool ok = true;
             for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
@@ -404,6 +504,7 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
                     tc_fence_after();
                     const int kb0 = ch * kb_per_chunk;
                     const int kb1 = min(p.nkb, kb0 + kb_per_chunk);
+                    (void) kb0;
                     for (int kb = kb0; kb < kb1; ++kb, ++it) {
                         const uint32_t s = it % nstage, ph = (it / nstage) & 1u;
                         if (!mbar_wait_bounded(&full[s], ph, &abort_flag, status,
@@ -414,22 +515,20 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
                         tc_fence_after();
                         const uint32_t sA = smem_u32(smem + s * stage_bytes);
                         const uint32_t sB = sA + a_bytes;
-                        // For slice t of A the partner slices u of B are adjacent
-                        // 64-row tiles in shared memory and their accumulators
-                        // D_{t+u} adjacent 64-column blocks in TMEM, so one MMA with
-                        // N = 64 * (#u) (<= 256) covers up to four slice products.
-                        // At t = 0 the issuer's MMAs cover all its diagonals, which
-                        // is where a chunk's accumulation starts.
+                        // For slice t of A the partner slices u = 0 .. s-1-t of B are
+                        // adjacent 64-row tiles in shared memory and their
+                        // accumulators D_{t+u} adjacent 64-column blocks in TMEM, so
+                        // one MMA with N = 64 * (#u) (<= 256) covers up to four slice
+                        // products.  Issuers of different A slices add into the same
+                        // diagonals; integer accumulation makes the order immaterial.
                         for (int t = 0; t < slices; ++t) {
-                            const int lo = max(t, d0);
-                            if (lo >= d1) continue;
+                            if (!((tmask >> t) & 1u)) continue;
                             const uint64_t ad = sdesc_k32(sA + t * A_SLICE_BYTES);
-                            for (int dd = lo; dd < d1; dd += 4) {
-                                const int nu = min(4, d1 - dd);
-                                const uint64_t bd = sdesc_k32(sB + (dd - t) * B_SLICE_BYTES);
-                                const uint32_t acc = (kb > kb0 || t > 0) ? 1u : 0u;
-                                tc_mma_i8(tmem_base + (uint32_t) (dd * OBN), ad, bd,
-                                          idesc_i8(nu * OBN), acc);
+                            for (int u = 0; u < slices - t; u += 4) {
+                                const int nu = min(4, slices - t - u);
+                                const uint64_t bd = sdesc_k32(sB + u * B_SLICE_BYTES);
+                                tc_mma_i8(tmem_base + (uint32_t) ((t + u) * OBN), ad, bd,
+                                          idesc_i8(nu * OBN), 1u);
                             }
                         }
                         tc_commit(&empty[s]);
@@ -485,22 +584,25 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
                 tc_fence_after();
                 if (p.nkb > 0) {
                     for (int d = slices - 1; d >= 0; --d) {
-                        // D_d * 2^(E_i - 14 - 8d) * 2^(F_j): both factors are powers
-                        // of two and |D_d| < 2^31, so in the supported exponent
-                        // range each product is exact and equals the oracle's
-                        // ldexp(D_d, E_i + F_j - 14 - 8d)
+                        // acc_j += D_d 2^(E_i - 14 - 8d), the term exact (|D_d| < 2^31,
+                        // power-of-two scale), one rounding per addition; the column
+                        // factor 2^F_j is applied at the store.  Scaling a rounded
+                        // sum by a power of two is exact, so in the normal range this
+                        // equals the oracle's sum of ldexp(D_d, E_i + F_j - 14 - 8d).
                         const double rs = pow2(Ei - 14 - 8 * d);
 #pragma unroll
                         for (int h = 0; h < OBN / 32; ++h) {
                             uint32_t v[32];
-                            tmem_ld32(tmem_base + ((uint32_t) (q * 32) << 16) +
-                                          (uint32_t) (d * OBN + h * 32),
-                                      v);
+                            const uint32_t ta = tmem_base + ((uint32_t) (q * 32) << 16) +
+                                                (uint32_t) (d * OBN + h * 32);
+                            tmem_ld32(ta, v);
+                            tmem_zero32(ta);
 #pragma unroll
                             for (int j = 0; j < 32; ++j)
-                                acc[h * 32 + j] += ((double) (int) v[j] * rs) * col_scale[h * 32 + j];
+                                acc[h * 32 + j] = fma(i32_to_f64(v[j]), rs, acc[h * 32 + j]);
                         }
                     }
+                    tmem_wait_st();
                 }
                 tc_fence_before();
                 __syncwarp();
@@ -512,7 +614,7 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
 #pragma unroll
                 for (int j = 0; j < OBN; ++j) {
                     const int gc = tn * OBN + j;
-                    if (gc < gn) crow[(long long) gc * ldc] = acc[j];
+                    if (gc < gn) crow[(long long) gc * ldc] = acc[j] * col_scale[j];
                 }
             }
         }
@@ -536,45 +638,33 @@ int rows_pad_of(int rows, int tr) { return (rows + tr - 1) / tr * tr; }
 // oracle's orc_ozaki_kchunk uses the same rule).
 int kchunk_of(int s) { return (int) ((2147483647L / 16384L) / s / OKB * OKB); }
 
-// Boundaries of the MMA issuers' diagonal intervals [0, b1), [b1, b2),
-// [b2, s): minimise the largest per-issuer MMA count per k-step, then the
-// spread of MMA columns.
-int issuer_mmas(int s, int d0, int d1, int *units)
+// A slices of the three MMA issuers (bit masks): slice t needs
+// ceil((s - t) / 4) MMAs per k-block; minimise the largest per-issuer MMA count
+// (each issuing thread needs ~150-190 cycles per tcgen05.mma), then the spread
+// of slice products.
+int4 slice_split(int s)
 {
-    int n = 0;
-    *units = 0;
-    for (int t = 0; t < s; ++t) {
-        const int lo = t > d0 ? t : d0;
-        if (lo >= d1) continue;
-        n += (d1 - lo + 3) / 4;
-        *units += d1 - lo;
-    }
-    return n;
-}
-
-int4 diagonal_split(int s)
-{
-    int4 best = make_int4(s, s, 0, 0);
-    int best_instr = 1 << 30, best_gap = 1 << 30;
-    for (int b1 = 0; b1 <= s; ++b1)
-        for (int b2 = b1; b2 <= s; ++b2) {
-            int u[3], n[3];
-            n[0] = issuer_mmas(s, 0, b1, &u[0]);
-            n[1] = issuer_mmas(s, b1, b2, &u[1]);
-            n[2] = issuer_mmas(s, b2, s, &u[2]);
-            const int mi = n[0] > n[1] ? (n[0] > n[2] ? n[0] : n[2]) : (n[1] > n[2] ? n[1] : n[2]);
-            int umax = u[0], umin = u[0];
-            for (int w = 1; w < 3; ++w) {
-                if (u[w] > umax) umax = u[w];
-                if (u[w] < umin) umin = u[w];
-            }
-            if (mi < best_instr || (mi == best_instr && umax - umin < best_gap)) {
-                best = make_int4(b1, b2, 0, 0);
-                best_instr = mi;
-                best_gap = umax - umin;
-            }
+    int best_m[3] = {0, 0, 0}, best_instr = 1 << 30, best_gap = 1 << 30;
+    int pow3 = 1;
+    for (int t = 0; t < s; ++t) pow3 *= 3;
+    for (int code = 0; code < pow3; ++code) {
+        int m[3] = {0, 0, 0}, n[3] = {0, 0, 0}, u[3] = {0, 0, 0}, c = code;
+        for (int t = 0; t < s; ++t, c /= 3) {
+            const int w = c % 3;
+            m[w] |= 1 << t;
+            n[w] += (s - t + 3) / 4;
+            u[w] += s - t;
         }
-    return best;
+        const int mi = n[0] > n[1] ? (n[0] > n[2] ? n[0] : n[2]) : (n[1] > n[2] ? n[1] : n[2]);
+        const int umax = u[0] > u[1] ? (u[0] > u[2] ? u[0] : u[2]) : (u[1] > u[2] ? u[1] : u[2]);
+        const int umin = u[0] < u[1] ? (u[0] < u[2] ? u[0] : u[2]) : (u[1] < u[2] ? u[1] : u[2]);
+        if (mi < best_instr || (mi == best_instr && umax - umin < best_gap)) {
+            best_instr = mi;
+            best_gap = umax - umin;
+            best_m[0] = m[0]; best_m[1] = m[1]; best_m[2] = m[2];
+        }
+    }
+    return make_int4(best_m[0], best_m[1], best_m[2], 0);
 }
 
 // Device plan layout for g groups (at most 2g operand blocks):
@@ -607,7 +697,7 @@ extern "C" size_t ca3dmm_oz_work_bytes(int nA, const int *a_rows, const int *a_k
         q += align256((size_t) slices * rows_pad_of(b_cols[i], OBN) *
                       kpad_of(b_k[i] > 0 ? b_k[i] : 1));
     }
-    return align256(e * sizeof(int)) + q + 256;
+    return exp_bytes((long long) e) + maxbits_bytes((long long) e) + q + 256;
 }
 
 extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
@@ -628,7 +718,7 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
     size_t ne = 0;
     for (int i = 0; i < nA; ++i) ne += A[i].rows;
     for (int i = 0; i < nB; ++i) ne += B[i].cols;
-    size_t qoff = align256(ne * sizeof(int));
+    size_t qoff = exp_bytes((long long) ne) + maxbits_bytes((long long) ne);
     long long eoff = 0;
     int max_rows = 1, max_kpad = 1;
     int tiles_op[2] = {0, 0};
@@ -704,7 +794,8 @@ extern "C" int ca3dmm_oz_run_pack(const ca3dmm_oz_plan_t *oz, const void *A, con
     const SliceDesc *sd =
         reinterpret_cast<const SliceDesc *>(static_cast<const unsigned char *>(oz->dev_plan) + L.sd);
     unsigned char *w = static_cast<unsigned char *>(oz->dev_work);
-    CA3DMM_CUDA_TRY(cudaMemsetAsync(w, 0, (size_t) oz->n_exp * sizeof(int), stream));
+    unsigned long long *mwork = reinterpret_cast<unsigned long long *>(w + exp_bytes(oz->n_exp));
+    CA3DMM_CUDA_TRY(cudaMemsetAsync(w, 0, exp_bytes(oz->n_exp) + maxbits_bytes(oz->n_exp), stream));
     const double *src[2] = {static_cast<const double *>(A), static_cast<const double *>(B)};
     const int cnt[2] = {oz->nA, oz->nB}, first[2] = {0, oz->nA};
     const int tiles[2] = {oz->slice_tiles_a, oz->slice_tiles_b};
@@ -712,14 +803,24 @@ extern "C" int ca3dmm_oz_run_pack(const ca3dmm_oz_plan_t *oz, const void *A, con
     for (int o = 0; o < 2; ++o) {
         if (cnt[o] == 0 || tiles[o] == 0) continue;
         oz_exp_kernel<<<tiles[o] < cap ? tiles[o] : cap, 256, 0, stream>>>(
-            src[o], sd + first[o], cnt[o], tiles[o], reinterpret_cast<unsigned *>(w));
+            src[o], sd + first[o], cnt[o], tiles[o], mwork);
         CA3DMM_CUDA_TRY(cudaGetLastError());
         ca3dmm_note_launch(1);
     }
     for (int o = 0; o < 2; ++o) {
         if (cnt[o] == 0 || tiles[o] == 0) continue;
-        oz_slice_kernel<<<tiles[o] < cap ? tiles[o] : cap, 256, 0, stream>>>(
-            src[o], sd + first[o], cnt[o], tiles[o], w, oz->slices);
+        const unsigned grid = tiles[o] < cap ? tiles[o] : cap;
+        switch (oz->slices) {
+#define CA3DMM_SLICE_CASE(S)                                                                       \
+    case S:                                                                                        \
+        oz_slice_kernel<S><<<grid, 256, 0, stream>>>(src[o], sd + first[o], cnt[o], tiles[o], w,   \
+                                                     mwork);                                       \
+        break;
+            CA3DMM_SLICE_CASE(2) CA3DMM_SLICE_CASE(3) CA3DMM_SLICE_CASE(4) CA3DMM_SLICE_CASE(5)
+            CA3DMM_SLICE_CASE(6) CA3DMM_SLICE_CASE(7) CA3DMM_SLICE_CASE(8)
+#undef CA3DMM_SLICE_CASE
+            default: return CA3DMM_EINVAL;
+        }
         CA3DMM_CUDA_TRY(cudaGetLastError());
         ca3dmm_note_launch(1);
     }
@@ -745,7 +846,7 @@ extern "C" int ca3dmm_oz_run_gemm(const ca3dmm_oz_plan_t *oz, int *dev_status, d
     const int kb_per_chunk = kchunk_of(oz->slices) / OKB;
     oz_gemm_kernel<<<grid, OTHREADS, smem, stream>>>(
         reinterpret_cast<const OzGroup *>(pl + L.gr), oz->ngroup, oz->tiles, oz->slices, nstage,
-        kb_per_chunk, diagonal_split(oz->slices), static_cast<const unsigned char *>(oz->dev_work),
+        kb_per_chunk, slice_split(oz->slices), static_cast<const unsigned char *>(oz->dev_work),
         dev_status, limit);
     CA3DMM_CUDA_TRY(cudaGetLastError());
     ca3dmm_note_launch(1);
