@@ -655,10 +655,18 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
         for (int i = 0; i < pl->nA; i++) {
             ob[i].r0 = pl->A[i].r0; ob[i].c0 = pl->A[i].c0;
             ob[i].rows = pl->A[i].rows; ob[i].cols = pl->A[i].cols;
+            ob[i].alias = -1;
+            /* B^T B: the op(A) block Bt(r0.., c0..) holds the elements of the B
+             * block B(c0.., r0..); slice it once */
+            for (int j = 0; e->is_BTB && j < pl->nB && ob[i].alias < 0; j++)
+                if (pl->B[j].r0 == pl->A[i].c0 && pl->B[j].rows == pl->A[i].cols &&
+                    pl->B[j].c0 == pl->A[i].r0 && pl->B[j].cols == pl->A[i].rows)
+                    ob[i].alias = j;
         }
         for (int i = 0; i < pl->nB; i++) {
             ob[pl->nA + i].r0 = pl->B[i].r0; ob[pl->nA + i].c0 = pl->B[i].c0;
             ob[pl->nA + i].rows = pl->B[i].rows; ob[pl->nA + i].cols = pl->B[i].cols;
+            ob[pl->nA + i].alias = -1;
         }
         for (int i = 0; i < pl->ngroup; i++) {
             og[i].a_blk = pl->groups[i].a_blk; og[i].b_blk = pl->groups[i].b_blk;

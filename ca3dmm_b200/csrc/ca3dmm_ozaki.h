@@ -1,13 +1,14 @@
 /* Internal C ABI of the split-precision (Ozaki scheme, INT8 slices) GEMM.
  *
  * For op(A) rows i and op(B) columns j of one operand block over its k range:
- *   E_i = frexp exponent of max_l |a_il| (max|a| < 2^E_i; 0 for a zero row),
- *   a_il = sum_{t<s} qa_t,il * 2^(E_i - 6 - 7t) + r,  qa_t = rint(...) in [-64, 64],
+ *   E_i = min{E : max_l |a_il| <= 2^E 127/128} (0 for a zero row),
+ *   rint(a_il 2^(8s-1-E_i)) = sum_{t<s} qa_t,il 256^(s-1-t), balanced digits
+ *   qa_t in [-128, 127], so a_il = sum_t qa_t,il 2^(E_i-7-8t) + r, |r| <= 2^(E_i-8s),
  * likewise F_j for the columns of op(B).  Then
- *   C_ij ~= sum_{d=0}^{s-1} 2^(E_i + F_j - 12 - 7d) * sum_{t+u=d} (qa_t qb_u)_ij
- * where every inner sum is an exact INT32 tensor-core accumulation
- * (|q| <= 64, so k (d+1) < 2^19 keeps it exact) and only the recombination
- * over d is done in FP64, least significant diagonal first. */
+ *   C_ij ~= sum_{d=s-1..0} 2^(E_i + F_j - 14 - 8d) * sum_{t+u=d} (qa_t qb_u)_ij
+ * where every inner sum is an exact INT32 tensor-core accumulation over k
+ * chunks with s kc 2^14 < 2^31, and only the recombination over d (most
+ * significant product last) and over chunks is done in FP64. */
 #ifndef CA3DMM_OZAKI_H
 #define CA3DMM_OZAKI_H
 
@@ -18,7 +19,10 @@
 extern "C" {
 #endif
 
-typedef struct { int r0, c0, rows, cols; } ca3dmm_oz_blk_t;   /* block of op(A) or op(B) */
+/* Block of op(A) or op(B).  alias >= 0 (A blocks only): this block is the
+ * transpose of B block `alias` (same elements: B^T B), so it reuses that
+ * block's slices and exponents instead of being sliced. */
+typedef struct { int r0, c0, rows, cols, alias; } ca3dmm_oz_blk_t;
 
 /* Where one operand block's source lives: op(X)(r, l) of the block's matrix
  * is read with leading dimension ld and transpose flag trans.  base == NULL:

@@ -221,9 +221,11 @@ static int build_plan(ca3dmm_grouped_p g, const double *const *A, const int *ldA
     } else {
         for (int i = 0; i < np; i++) {
             g->ob[i].r0 = 0; g->ob[i].c0 = 0; g->ob[i].rows = g->m[i]; g->ob[i].cols = g->k[i];
+            g->ob[i].alias = -1;
             g->os[i].base = A[i]; g->os[i].ld = ldA[i]; g->os[i].trans = g->ta[i];
             g->ob[np + i].r0 = 0; g->ob[np + i].c0 = 0;
             g->ob[np + i].rows = g->k[i]; g->ob[np + i].cols = g->n[i];
+            g->ob[np + i].alias = -1;
             g->os[np + i].base = B[i]; g->os[np + i].ld = ldB[i]; g->os[np + i].trans = g->tb[i];
             g->og[i].a_blk = i; g->og[i].b_blk = i;
             g->og[i].C = C[i]; g->og[i].ldc = ldC[i];

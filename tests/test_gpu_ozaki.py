@@ -104,16 +104,23 @@ def test_ozaki_k_chunks_bitexact(cuda, s):
     assert np.array_equal(got, _oracle_ozaki(A, B, m, n, k, 0, 0, 1, s))
 
 
-def test_ozaki_btb(cuda):
-    n, k, p = 96, 4000, 8
+@pytest.mark.parametrize("n,k,p,grid,s", [
+    (96, 4000, 8, (1, 1, 8), 8),
+    (100, 3000, 8, (1, 1, 8), 7),     # 128-row A tiles over 64-row B tiles: padded half
+    (50, 2000, 4, (1, 1, 4), 6),      # fewer rows than one B tile
+    (200, 1500, 8, None, 7),          # the reference's default B^T B grid (fold)
+    (130, 1000, 16, (2, 2, 4), 5),
+])
+def test_ozaki_btb(cuda, n, k, p, grid, s):
+    """B^T B: the op(A) = B^T blocks reuse the slices of the B blocks."""
     Bm = orc.gen_btb(5, k, n)
     dB, ldb = to_dev(Bm)
     dC = dev_zeros(n * n)
-    e = cb.Ca3dmmEngine(n, n, k, p=p, btb=True, proc_grid=(1, 1, 8))
-    assert e.ok and e.set_gemm_mode(cb.GEMM_OZAKI, 8) == 0
+    e = cb.Ca3dmmEngine(n, n, k, p=p, btb=True, proc_grid=grid)
+    assert e.ok and e.set_gemm_mode(cb.GEMM_OZAKI, s) == 0
     assert e.exec(None, 0, dB, ldb, dC, n) == 0
     got = from_dev(dC, n, n)
-    want = _oracle_ozaki(Bm, Bm, n, n, k, 1, 0, 8, 8)
+    want = _oracle_ozaki(Bm, Bm, n, n, k, 1, 0, e.s.kp, s)
     assert np.array_equal(got, want)
 
 
