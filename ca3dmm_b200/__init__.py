@@ -150,6 +150,7 @@ def lib():
         "ca3dmm_mlp_save": (i, [p, C.c_char_p]),
         "ca3dmm_mlp_load": (i, [C.c_char_p, C.POINTER(p)]),
         "ca3dmm_kernel_launches": (C.c_ulonglong, []),
+        "ca3dmm_engine_exec_host": (i, [EP, p, i, p, i, p, i]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -206,7 +207,9 @@ def _ptr(x):
         return None
     if isinstance(x, int):
         return x
-    return x.data_ptr()
+    if hasattr(x, "data_ptr"):
+        return x.data_ptr()
+    return x.ctypes.data          # numpy array (host memory)
 
 
 class Ca3dmmEngine:
@@ -271,6 +274,12 @@ class Ca3dmmEngine:
         lib().ca3dmm_engine_exec(self.e, _ptr(A), int(ldA), _ptr(B), int(ldB), _ptr(Cout),
                                  int(ldC))
         return lib().ca3dmm_engine_last_error(self.e)
+
+    def exec_host(self, A, ldA, B, ldB, Cout, ldC):
+        """ca3dmm_engine_exec_host: host (preferably page-locked) buffers in and
+        out, copies overlapped with the computation."""
+        return lib().ca3dmm_engine_exec_host(self.e, _ptr(A), int(ldA), _ptr(B), int(ldB),
+                                             _ptr(Cout), int(ldC))
 
     def vrank_info(self, r):
         out = (C.c_int * 34)()

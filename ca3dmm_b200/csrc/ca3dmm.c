@@ -71,7 +71,29 @@ typedef struct {
     ca3dmm_oz_blk_t *ob;
     ca3dmm_oz_src_t *os;
     ca3dmm_oz_group_t *og;
+    struct host_exec *hx;         /* state of ca3dmm_engine_exec_host (lazily created) */
 } plan_t;
+
+/* ca3dmm_engine_exec_host: device staging of A, B and C and the row-band
+ * pipeline.  Band c covers output rows [r0, r1) inside one task_m block; its
+ * op(A) rows are copied in, packed or sliced, multiplied (one tile range per
+ * (slab, task_n) group: the GEMM kernels number tiles in raster bands of
+ * `raster` 128-row tile rows, so a band of raster * 128 rows is contiguous),
+ * reduced over the slabs and copied out while the next band's rows arrive. */
+#define HX_MAX_BANDS 64
+struct host_exec {
+    double *dA, *dB, *dC;
+    long long lda, ldb, ldc;
+    cudaStream_t s_in, s_out;
+    cudaEvent_t ev_b, ev_a[HX_MAX_BANDS], ev_c[HX_MAX_BANDS];
+    int nband, r0[HX_MAX_BANDS], r1[HX_MAX_BANDS];
+    ca3dmm_tile_ranges_t rng[HX_MAX_BANDS];
+    void *desc_h, *desc_d;        /* per-band A descriptors (pack or slicing) */
+    size_t desc_stride;
+    int ndesc, ntile[HX_MAX_BANDS];
+    int built_mode, built_slices, built_raster;
+    int ok;                       /* streams and events created */
+};
 
 
 /* Geometry of one virtual rank (same 34-int layout as the oracle):
@@ -257,6 +279,24 @@ static void plan_free(plan_t *pl)
     free(pl->ob);
     free(pl->os);
     free(pl->og);
+    if (pl->hx) {
+        struct host_exec *x = pl->hx;
+        cudaFree(x->dA);
+        cudaFree(x->dB);
+        cudaFree(x->dC);
+        cudaFree(x->desc_d);
+        if (x->desc_h) cudaFreeHost(x->desc_h);
+        if (x->ok) {
+            cudaStreamDestroy(x->s_in);
+            cudaStreamDestroy(x->s_out);
+            cudaEventDestroy(x->ev_b);
+            for (int i = 0; i < HX_MAX_BANDS; i++) {
+                cudaEventDestroy(x->ev_a[i]);
+                cudaEventDestroy(x->ev_c[i]);
+            }
+        }
+        free(x);
+    }
     if (pl->stage) cudaFreeHost(pl->stage);
     if (pl->status_h) cudaFreeHost(pl->status_h);
     if (pl->events_ok)
@@ -809,6 +849,305 @@ void ca3dmm_engine_exec(ca3dmm_engine_p e, const void *src_A, const int ldA, con
         e->n_exec++;
         if (e->print_timing) INFO_PRINTF("CA3DMM exec time        = %.2f ms\n\n", ms);
     }
+}
+
+/* ---------------------------------------------------------------------------
+ * ca3dmm_engine_exec_host: host buffers in and out, copies overlapped with the
+ * computation band by band (see struct host_exec). */
+
+static int hx_create(ca3dmm_engine_p e, struct host_exec **out)
+{
+    plan_t *pl = (plan_t *) e->impl;
+    if (pl->hx) { *out = pl->hx; return CA3DMM_OK; }
+    struct host_exec *x = (struct host_exec *) calloc(1, sizeof(struct host_exec));
+    if (!x) return CA3DMM_ENOMEM;
+    pl->hx = x;
+    x->built_mode = -1;
+    const int a_rows = e->trans_A ? e->k : e->m, a_cols = e->trans_A ? e->m : e->k;
+    const int b_rows = e->trans_B ? e->n : e->k, b_cols = e->trans_B ? e->k : e->n;
+    x->lda = ca3dmm_round_up(a_rows > 0 ? a_rows : 1, 2);
+    x->ldb = ca3dmm_round_up(b_rows > 0 ? b_rows : 1, 2);
+    x->ldc = ca3dmm_round_up(pl->dst_nrow > 0 ? pl->dst_nrow : 1, 2);
+    if (!e->is_BTB &&
+        cudaMalloc((void **) &x->dA, sizeof(double) * (size_t) x->lda * (size_t) (a_cols > 0 ? a_cols : 1)) != cudaSuccess)
+        return CA3DMM_ENOMEM;
+    if (cudaMalloc((void **) &x->dB, sizeof(double) * (size_t) x->ldb * (size_t) (b_cols > 0 ? b_cols : 1)) != cudaSuccess)
+        return CA3DMM_ENOMEM;
+    if (cudaMalloc((void **) &x->dC, sizeof(double) * (size_t) x->ldc * (size_t) (pl->dst_ncol > 0 ? pl->dst_ncol : 1)) != cudaSuccess)
+        return CA3DMM_ENOMEM;
+    if (cudaStreamCreateWithFlags(&x->s_in, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&x->s_out, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&x->ev_b, cudaEventDisableTiming) != cudaSuccess)
+        return CA3DMM_ECUDA;
+    for (int i = 0; i < HX_MAX_BANDS; i++)
+        if (cudaEventCreateWithFlags(&x->ev_a[i], cudaEventDisableTiming) != cudaSuccess ||
+            cudaEventCreateWithFlags(&x->ev_c[i], cudaEventDisableTiming) != cudaSuccess)
+            return CA3DMM_ECUDA;
+    x->ok = 1;
+    *out = x;
+    return CA3DMM_OK;
+}
+
+/* Output row bands and, per band, the GEMM tile ranges and the descriptors
+ * that pack or slice its op(A) rows.  Returns the band count (0 or 1: no
+ * pipelining for this layout). */
+static int hx_build_bands(ca3dmm_engine_p e, struct host_exec *x, cudaStream_t st)
+{
+    plan_t *pl = (plan_t *) e->impl;
+    const int tmn = e->mp > e->np && !e->is_BTB ? e->mp / e->np : 1;
+    const int tnn = e->np > e->mp && !e->is_BTB ? e->np / e->mp : 1;
+    const int whole = pl->has_dst && pl->dst_srow == 0 && pl->dst_scol == 0 &&
+                      pl->dst_nrow == e->m && pl->dst_ncol == e->n;
+    const int ozaki = e->gemm_mode == CA3DMM_GEMM_OZAKI;
+    x->nband = 0;
+    x->built_mode = e->gemm_mode;
+    x->built_slices = e->ozaki_slices;
+    x->built_raster = e->raster;
+    if (e->is_BTB || !whole || e->kp * tnn > CA3DMM_MAX_RANGES) return 0;
+    const int raster = e->raster > 0 ? e->raster : 8;
+    const int bn = ozaki ? 64 : 128;
+    int *tb = (int *) malloc(sizeof(int) * (size_t) pl->ngroup);
+    if (!tb) return 0;
+    for (int g = 0, t = 0; g < pl->ngroup; g++) {
+        const group_t *gg = &pl->groups[g];
+        tb[g] = t;
+        if (gg->mz > 0 && gg->nz > 0) t += ((gg->mz + 127) / 128) * ((gg->nz + bn - 1) / bn);
+    }
+    int band_rows = raster * 128;
+    for (;;) {
+        int cnt = 0;
+        for (int tm = 0; tm < tmn; tm++) cnt += (pl->A[tm].rows + band_rows - 1) / band_rows;
+        if (cnt <= HX_MAX_BANDS) break;
+        band_rows *= 2;
+    }
+    const size_t one = ozaki ? ca3dmm_oz_desc_bytes() : sizeof(ca3dmm_pack_desc_t);
+    x->ndesc = e->kp;
+    x->desc_stride = align_up(one * (size_t) e->kp);
+    if (!x->desc_h) {
+        /* room for either mode's descriptors */
+        const size_t p1 = align_up(sizeof(ca3dmm_pack_desc_t) * (size_t) e->kp);
+        const size_t p2 = align_up(ca3dmm_oz_desc_bytes() * (size_t) e->kp);
+        const size_t cap = (p1 > p2 ? p1 : p2) * HX_MAX_BANDS;
+        if (cudaMallocHost(&x->desc_h, cap) != cudaSuccess) { x->desc_h = NULL; free(tb); return 0; }
+        if (cudaMalloc(&x->desc_d, cap) != cudaSuccess) { x->desc_d = NULL; free(tb); return 0; }
+    }
+    int *blocks = (int *) malloc(sizeof(int) * (size_t) e->kp);
+    if (!blocks) { free(tb); return 0; }
+    int bad = 0;
+    for (int tm = 0; tm < tmn && !bad; tm++) {
+        const blk_t *a0 = &pl->A[tm];              /* the same rows in every slab */
+        for (int r = 0; r < a0->rows && !bad; r += band_rows) {
+            const int c = x->nband++;
+            const int rend = r + band_rows < a0->rows ? r + band_rows : a0->rows;
+            x->r0[c] = a0->r0 + r;
+            x->r1[c] = a0->r0 + rend;
+            ca3dmm_tile_ranges_t *rg = &x->rng[c];
+            memset(rg, 0, sizeof(*rg));
+            const int row_lo = r / 128, nrow_t = band_rows / 128;
+            for (int tk = 0; tk < e->kp; tk++)
+                for (int tn = 0; tn < tnn; tn++) {
+                    const int g = (tk * tmn + tm) * tnn + tn;
+                    const group_t *gg = &pl->groups[g];
+                    if (gg->mz <= 0 || gg->nz <= 0) continue;
+                    const int tiles_m = (gg->mz + 127) / 128, tiles_n = (gg->nz + bn - 1) / bn;
+                    const int row_hi = row_lo + nrow_t < tiles_m ? row_lo + nrow_t : tiles_m;
+                    if (row_hi <= row_lo) continue;
+                    rg->begin[rg->n] = tb[g] + row_lo * tiles_n;
+                    rg->len[rg->n] = (row_hi - row_lo) * tiles_n;
+                    rg->n++;
+                }
+            char *dh = (char *) x->desc_h + (size_t) c * x->desc_stride;
+            for (int tk = 0; tk < e->kp; tk++) blocks[tk] = tk * tmn + tm;
+            if (ozaki) {
+                bad = ca3dmm_oz_encode_rows((char *) pl->stage + pl->off_ozplan, pl->ngroup, blocks,
+                                            e->kp, r, rend, dh, &x->ntile[c]);
+            } else {
+                ca3dmm_pack_desc_t *pd = (ca3dmm_pack_desc_t *) dh;
+                for (int tk = 0; tk < e->kp; tk++) {
+                    const blk_t *b = &pl->A[blocks[tk]];
+                    ca3dmm_pack_desc_t *d = &pd[tk];
+                    memset(d, 0, sizeof(*d));
+                    d->rows = rend - r; d->cols = b->cols; d->trans = e->trans_A; d->lds = x->lda;
+                    d->src_off = e->trans_A ? (long long) b->c0 + (long long) (b->r0 + r) * x->lda
+                                            : (long long) (b->r0 + r) + (long long) b->c0 * x->lda;
+                    d->dst_off = (long long) (b->off / sizeof(double)) + r;
+                    d->ldd = b->ld;
+                }
+                x->ntile[c] = ca3dmm_pack_tiles(pd, e->kp);
+            }
+        }
+    }
+    free(blocks);
+    free(tb);
+    if (bad) { x->nband = 0; return 0; }
+    if (cudaMemcpyAsync(x->desc_d, x->desc_h, x->desc_stride * (size_t) x->nband,
+                        cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        x->nband = 0;
+        return 0;
+    }
+    return x->nband;
+}
+
+static int hx_copy_in_B(ca3dmm_engine_p e, struct host_exec *x, const void *B_h, int ldB)
+{
+    const int b_rows = e->trans_B ? e->n : e->k, b_cols = e->trans_B ? e->k : e->n;
+    if (b_rows > 0 && b_cols > 0)
+        CA3DMM_CUDA_TRY(cudaMemcpy2DAsync(x->dB, sizeof(double) * (size_t) x->ldb, B_h,
+                                          sizeof(double) * (size_t) ldB, sizeof(double) * (size_t) b_rows,
+                                          (size_t) b_cols, cudaMemcpyHostToDevice, x->s_in));
+    return CA3DMM_OK;
+}
+
+/* op(A) rows [r0, r1) into the staging copy of A. */
+static int hx_copy_in_A_rows(ca3dmm_engine_p e, struct host_exec *x, const double *A_h, int ldA,
+                             int r0, int r1)
+{
+    if (r1 <= r0 || e->k <= 0) return CA3DMM_OK;
+    if (e->trans_A)     /* A is k x m: op(A) rows are columns of A */
+        CA3DMM_CUDA_TRY(cudaMemcpy2DAsync(x->dA + (size_t) r0 * x->lda, sizeof(double) * (size_t) x->lda,
+                                          A_h + (size_t) r0 * ldA, sizeof(double) * (size_t) ldA,
+                                          sizeof(double) * (size_t) e->k, (size_t) (r1 - r0),
+                                          cudaMemcpyHostToDevice, x->s_in));
+    else
+        CA3DMM_CUDA_TRY(cudaMemcpy2DAsync(x->dA + r0, sizeof(double) * (size_t) x->lda, A_h + r0,
+                                          sizeof(double) * (size_t) ldA, sizeof(double) * (size_t) (r1 - r0),
+                                          (size_t) e->k, cudaMemcpyHostToDevice, x->s_in));
+    return CA3DMM_OK;
+}
+
+static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_h, int ldB,
+                     void *C_h, int ldC)
+{
+    plan_t *pl = (plan_t *) e->impl;
+    const int a_rows = e->trans_A ? e->k : e->m, b_rows = e->trans_B ? e->n : e->k;
+    if (!B_h || ldB < b_rows || (!e->is_BTB && (!A_h || ldA < a_rows))) {
+        ERROR_PRINTF("Invalid host operands: ldA = %d (>= %d), ldB = %d (>= %d)\n", ldA, a_rows, ldB,
+                     b_rows);
+        return CA3DMM_EINVAL;
+    }
+    if (!pl->has_dst || C_h == NULL || ldC < pl->dst_nrow) {
+        ERROR_PRINTF("exec_host needs a dst_C block and a host C with ldC >= %d\n", pl->dst_nrow);
+        return CA3DMM_EINVAL;
+    }
+    struct host_exec *x;
+    int rc = hx_create(e, &x);
+    if (rc) return rc;
+    cudaStream_t st = (cudaStream_t) e->stream;
+    const double *dAsrc = e->is_BTB ? x->dB : x->dA;
+    const long long ldAsrc = e->is_BTB ? x->ldb : x->lda;
+    /* device plan for the staging buffers (rebuilt only when they change) */
+    if (!pl->plan_valid || pl->c_ldA != ldAsrc || pl->c_ldB != x->ldb || pl->c_dst != x->dC ||
+        pl->c_ldC != x->ldc) {
+        rc = plan_upload(e, dAsrc, (int) ldAsrc, x->dB, (int) x->ldb, x->dC, (int) x->ldc, st);
+        if (rc) return rc;
+        x->built_mode = -1;
+    }
+    if (x->built_mode != e->gemm_mode || x->built_slices != e->ozaki_slices ||
+        x->built_raster != e->raster)
+        hx_build_bands(e, x, st);
+    /* the inputs may not be overwritten before the previous exec's reads are done */
+    CA3DMM_CUDA_TRY(cudaStreamSynchronize(st));
+    const int dn = pl->dst_nrow, dc = pl->dst_ncol;
+    if (x->nband < 2) {
+        /* serial: copy in, the device exec, copy out */
+        rc = hx_copy_in_B(e, x, B_h, ldB);
+        if (!rc && !e->is_BTB) rc = hx_copy_in_A_rows(e, x, (const double *) A_h, ldA, 0, e->m);
+        if (rc) return rc;
+        CA3DMM_CUDA_TRY(cudaEventRecord(x->ev_b, x->s_in));
+        CA3DMM_CUDA_TRY(cudaStreamWaitEvent(st, x->ev_b, 0));
+        const int sync = e->sync_exec;
+        e->sync_exec = 1;
+        rc = exec_device(e, dAsrc, (int) ldAsrc, x->dB, (int) x->ldb, x->dC, (int) x->ldc, st);
+        e->sync_exec = sync;
+        if (rc) return rc;
+        if (dn > 0 && dc > 0)
+            CA3DMM_CUDA_TRY(cudaMemcpy2DAsync(C_h, sizeof(double) * (size_t) ldC, x->dC,
+                                              sizeof(double) * (size_t) x->ldc, sizeof(double) * (size_t) dn,
+                                              (size_t) dc, cudaMemcpyDeviceToHost, st));
+        CA3DMM_CUDA_TRY(cudaStreamSynchronize(st));
+        return CA3DMM_OK;
+    }
+    char *w = (char *) e->workbuf_d;
+    int *status_d = (int *) (w + pl->off_status);
+    CA3DMM_CUDA_TRY(cudaMemsetAsync(status_d, 0, 64, st));
+    /* copies in: all of B, then the op(A) rows band by band */
+    rc = hx_copy_in_B(e, x, B_h, ldB);
+    if (rc) return rc;
+    CA3DMM_CUDA_TRY(cudaEventRecord(x->ev_b, x->s_in));
+    for (int c = 0; c < x->nband; c++) {
+        rc = hx_copy_in_A_rows(e, x, (const double *) A_h, ldA, x->r0[c], x->r1[c]);
+        if (rc) return rc;
+        CA3DMM_CUDA_TRY(cudaEventRecord(x->ev_a[c], x->s_in));
+    }
+    const int ozaki = e->gemm_mode == CA3DMM_GEMM_OZAKI;
+    CA3DMM_CUDA_TRY(cudaStreamWaitEvent(st, x->ev_b, 0));
+    if (ozaki) {
+        rc = ca3dmm_oz_clear(&pl->oz, st);
+        if (!rc) rc = ca3dmm_oz_slice_side(&pl->oz, 1, x->dB, st);
+    } else {
+        rc = ca3dmm_pack_launch(x->dB, (double *) w, (const ca3dmm_pack_desc_t *) (w + pl->off_packB),
+                                pl->nB, pl->pack_tiles_B, st);
+    }
+    if (rc) return rc;
+    for (int c = 0; c < x->nband; c++) {
+        const void *dd = (const char *) x->desc_d + (size_t) c * x->desc_stride;
+        CA3DMM_CUDA_TRY(cudaStreamWaitEvent(st, x->ev_a[c], 0));
+        if (ozaki) {
+            rc = ca3dmm_oz_slice_descs(&pl->oz, x->dA, dd, x->ndesc, x->ntile[c], st);
+            if (!rc) rc = ca3dmm_oz_run_gemm_ranges(&pl->oz, &x->rng[c], status_d, 5.0, st);
+        } else {
+            rc = ca3dmm_pack_launch(x->dA, (double *) w, (const ca3dmm_pack_desc_t *) dd, x->ndesc,
+                                    x->ntile[c], st);
+            if (!rc)
+                rc = ca3dmm_dgemm_launch_ranges(w + pl->off_gemm, pl->ngroup, &x->rng[c], status_d,
+                                                5.0, st);
+        }
+        if (!rc && e->kp > 1)
+            rc = ca3dmm_reduce_slabs_launch((const double *) (w + pl->off_slab) + x->r0[c],
+                                            (long long) pl->slab_stride, pl->slab_ld, e->kp,
+                                            x->r1[c] - x->r0[c], e->n, x->dC + x->r0[c], x->ldc, st);
+        if (rc) return rc;
+        CA3DMM_CUDA_TRY(cudaEventRecord(x->ev_c[c], st));
+        CA3DMM_CUDA_TRY(cudaStreamWaitEvent(x->s_out, x->ev_c[c], 0));
+        CA3DMM_CUDA_TRY(cudaMemcpy2DAsync((double *) C_h + x->r0[c], sizeof(double) * (size_t) ldC,
+                                          x->dC + x->r0[c], sizeof(double) * (size_t) x->ldc,
+                                          sizeof(double) * (size_t) (x->r1[c] - x->r0[c]), (size_t) e->n,
+                                          cudaMemcpyDeviceToHost, x->s_out));
+    }
+    CA3DMM_CUDA_TRY(cudaMemcpyAsync(pl->status_h, status_d, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CA3DMM_CUDA_TRY(cudaStreamSynchronize(st));
+    CA3DMM_CUDA_TRY(cudaStreamSynchronize(x->s_out));
+    if (pl->status_h[0] != 0) {
+        ERROR_PRINTF("Device status %d: a bounded wait ran out\n", pl->status_h[0]);
+        return CA3DMM_ETIMEOUT;
+    }
+    return CA3DMM_OK;
+}
+
+int ca3dmm_engine_exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_h, int ldB,
+                            void *C_h, int ldC)
+{
+    if (e == NULL) {
+        ERROR_PRINTF("ca3dmm_engine not initialized\n");
+        return CA3DMM_EINVAL;
+    }
+    if (e->workbuf_d == NULL || ((plan_t *) e->impl)->stage == NULL) {
+        ERROR_PRINTF("ca3dmm_engine has no device work buffer attached\n");
+        e->last_error = CA3DMM_EINVAL;
+        return CA3DMM_EINVAL;
+    }
+    double t0 = ca3dmm_wtime_sec();
+    int rc = exec_host(e, A_h, ldA, B_h, ldB, C_h, ldC);
+    e->last_error = rc;
+    if (rc) {
+        ERROR_PRINTF("ca3dmm_engine_exec_host failed (error %d)\n", rc);
+        return rc;
+    }
+    double ms = 1000.0 * (ca3dmm_wtime_sec() - t0);
+    e->exec_ms += ms;
+    e->n_exec++;
+    if (e->print_timing) INFO_PRINTF("CA3DMM exec (host buffers) time = %.2f ms\n\n", ms);
+    return CA3DMM_OK;
 }
 
 void ca3dmm_engine_reset_stat(ca3dmm_engine_p e)

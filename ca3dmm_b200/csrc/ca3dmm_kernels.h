@@ -43,9 +43,21 @@ size_t ca3dmm_dgemm_plan_bytes(int nprob);
  * the device addresses of A and B.  Returns the total tile count. */
 int ca3dmm_dgemm_plan_encode(const ca3dmm_dgemm_desc_t *probs, int nprob, void *host_plan,
                              int *total_tiles);
+/* Up to CA3DMM_MAX_RANGES contiguous ranges [begin, begin + len) of a grouped
+ * plan's tile list (each problem's tiles are numbered in raster bands of
+ * `raster` tile rows, so a band of output rows is one range per problem). */
+#define CA3DMM_MAX_RANGES 8
+typedef struct {
+    int n;
+    int begin[CA3DMM_MAX_RANGES], len[CA3DMM_MAX_RANGES];
+} ca3dmm_tile_ranges_t;
+
 /* Persistent grouped launch over every tile of every problem. */
 int ca3dmm_dgemm_launch(const void *dev_plan, int nprob, int total_tiles, int *dev_status,
                         double timeout_s, cudaStream_t stream);
+/* The same over the tiles of `ranges` only. */
+int ca3dmm_dgemm_launch_ranges(const void *dev_plan, int nprob, const ca3dmm_tile_ranges_t *ranges,
+                               int *dev_status, double timeout_s, cudaStream_t stream);
 
 /* ---- pack / transpose ----------------------------------------------------
  * Batched block copies between column-major matrices.  Descriptor j copies a

@@ -14,6 +14,7 @@
 
 #include <stddef.h>
 #include <cuda_runtime_api.h>
+#include "ca3dmm_kernels.h"
 
 #ifdef __cplusplus
 extern "C" {
@@ -70,6 +71,25 @@ int ca3dmm_oz_run_pack(const ca3dmm_oz_plan_t *oz, const void *A, const void *B,
 /* Grouped INT8 tcgen05 GEMM with FP64 recombination into each group's C. */
 int ca3dmm_oz_run_gemm(const ca3dmm_oz_plan_t *oz, int *dev_status, double timeout_s,
                        cudaStream_t stream);
+
+/* Pieces of run_pack for pipelined execution: clear the exponent arrays
+ * (once per exec, before any slicing); slice one operand side (0: every A
+ * block, 1: every B block); or slice an explicit list of descriptors in device
+ * memory, e.g. the A blocks restricted to a band of rows built by
+ * ca3dmm_oz_encode_rows from the host copy of the plan (r0 a multiple of the
+ * 128-row A tile, rows counted inside each listed A block; *ntiles receives
+ * the slicing tile count). */
+int ca3dmm_oz_clear(const ca3dmm_oz_plan_t *oz, cudaStream_t stream);
+int ca3dmm_oz_slice_side(const ca3dmm_oz_plan_t *oz, int which, const void *src,
+                         cudaStream_t stream);
+size_t ca3dmm_oz_desc_bytes(void);
+int ca3dmm_oz_encode_rows(const void *host_plan, int ngroup, const int *blocks, int count, int r0,
+                          int r1, void *out_descs, int *ntiles);
+int ca3dmm_oz_slice_descs(const ca3dmm_oz_plan_t *oz, const void *src, const void *dev_descs,
+                          int ndesc, int ntiles, cudaStream_t stream);
+/* The GEMM over the tiles of `ranges` only (ca3dmm_kernels.h). */
+int ca3dmm_oz_run_gemm_ranges(const ca3dmm_oz_plan_t *oz, const ca3dmm_tile_ranges_t *ranges,
+                              int *dev_status, double timeout_s, cudaStream_t stream);
 
 #ifdef __cplusplus
 }

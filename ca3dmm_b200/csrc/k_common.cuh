@@ -22,6 +22,27 @@ enum {
     CA3DMM_DEV_TIMEOUT_QUEUE   = 5,   // persistent work queue wait ran out
 };
 
+// Virtual tile v of a persistent launch -> tile index of the plan: v walks the
+// ranges in order (a launch over the whole list is one range [0, total)).
+template <typename R>
+CA3DMM_DEV int range_tile(const R &r, int v)
+{
+#pragma unroll 1
+    for (int i = 0; i < r.n; ++i) {
+        if (v < r.len[i]) return r.begin[i] + v;
+        v -= r.len[i];
+    }
+    return -1;
+}
+
+template <typename R>
+inline int range_total(const R &r)
+{
+    int t = 0;
+    for (int i = 0; i < r.n; ++i) t += r.len[i];
+    return t;
+}
+
 CA3DMM_DEV uint32_t smem_u32(const void *p)
 {
     return static_cast<uint32_t>(__cvta_generic_to_shared(p));

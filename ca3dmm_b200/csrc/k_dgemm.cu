@@ -102,17 +102,19 @@ __device__ __forceinline__ void store_pair(const DProb &p, int m, int n, double 
 // Iterator over this CTA's (tile, k-tile) load sequence, used by the
 // producer thread.  Tiles with k == 0 carry no loads and are skipped.
 struct LoadCursor {
-    int tile, kt, ktiles, pi, m0, n0;
+    int tile, kt, ktiles, pi, m0, n0;   // tile: virtual index into the launch's ranges
     bool valid;
-    __device__ void seek(const DProb *probs, int nprob, int total_tiles, int stride)
+    __device__ void seek(const DProb *probs, int nprob, const ca3dmm_tile_ranges_t &rg,
+                         int total_tiles, int stride)
     {
         while (tile < total_tiles) {
-            pi = find_problem(probs, nprob, tile);
+            const int t = range_tile(rg, tile);
+            pi = find_problem(probs, nprob, t);
             const DProb &p = probs[pi];
             ktiles = (p.k + BK - 1) / BK;
             if (ktiles > 0) {
                 int tm, tn;
-                tile_coords(p, tile, tm, tn);
+                tile_coords(p, t, tm, tn);
                 m0 = tm * BM;
                 n0 = tn * BN;
                 valid = true;
@@ -122,12 +124,13 @@ struct LoadCursor {
         }
         valid = false;
     }
-    __device__ void advance(const DProb *probs, int nprob, int total_tiles, int stride)
+    __device__ void advance(const DProb *probs, int nprob, const ca3dmm_tile_ranges_t &rg,
+                            int total_tiles, int stride)
     {
         if (++kt < ktiles) return;
         kt = 0;
         tile += stride;
-        seek(probs, nprob, total_tiles, stride);
+        seek(probs, nprob, rg, total_tiles, stride);
     }
 };
 
@@ -138,7 +141,8 @@ struct LoadCursor {
 // every warp has usually finished, so the producer thread rarely stalls.
 __global__ void __launch_bounds__(THREADS, 1)
 dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restrict__ probs,
-                   int nprob, int total_tiles, int *status, unsigned long long limit_ns)
+                   int nprob, const ca3dmm_tile_ranges_t rg, int total_tiles, int *status,
+                   unsigned long long limit_ns)
 {
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
@@ -183,13 +187,13 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
             tma_load_2d(sA + j * 2048, ta, lc.m0 + 16 * j, lc.kt * BK, &full[s]);
         tma_load_2d(sB, tb, lc.kt * BK, lc.n0, &full[s]);
         ++issued;
-        lc.advance(probs, nprob, total_tiles, gridDim.x);
+        lc.advance(probs, nprob, rg, total_tiles, gridDim.x);
         return true;
     };
     if (producer) {
         lc.tile = blockIdx.x;
         lc.kt = 0;
-        lc.seek(probs, nprob, total_tiles, gridDim.x);
+        lc.seek(probs, nprob, rg, total_tiles, gridDim.x);
         for (int s = 0; s < STAGES - 1; ++s)
             if (!issue_one()) break;
     }
@@ -200,7 +204,8 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
     double acc[4][4][4];
     bool ok = true;
 
-    for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
+    for (int v = blockIdx.x; v < total_tiles && ok; v += gridDim.x) {
+        const int tile = range_tile(rg, v);
         int pi = find_problem(probs, nprob, tile);
         const DProb &p = probs[pi];
         int tm, tn;
@@ -374,6 +379,19 @@ extern "C" int ca3dmm_dgemm_plan_encode(const ca3dmm_dgemm_desc_t *probs, int np
 extern "C" int ca3dmm_dgemm_launch(const void *dev_plan, int nprob, int total_tiles,
                                    int *dev_status, double timeout_s, cudaStream_t stream)
 {
+    ca3dmm_tile_ranges_t rg;
+    memset(&rg, 0, sizeof(rg));
+    rg.n = 1;
+    rg.len[0] = total_tiles;
+    return ca3dmm_dgemm_launch_ranges(dev_plan, nprob, &rg, dev_status, timeout_s, stream);
+}
+
+extern "C" int ca3dmm_dgemm_launch_ranges(const void *dev_plan, int nprob,
+                                          const ca3dmm_tile_ranges_t *ranges, int *dev_status,
+                                          double timeout_s, cudaStream_t stream)
+{
+    if (!ranges || ranges->n < 0 || ranges->n > CA3DMM_MAX_RANGES) return CA3DMM_EINVAL;
+    const int total_tiles = range_total(*ranges);
     if (total_tiles <= 0) return CA3DMM_OK;
     static bool attr_done = false;
     if (!attr_done) {
@@ -386,7 +404,7 @@ extern "C" int ca3dmm_dgemm_launch(const void *dev_plan, int nprob, int total_ti
     int grid = ca3dmm_device_sm_count();
     if (grid > total_tiles) grid = total_tiles;
     unsigned long long limit = (unsigned long long) (timeout_s * 1e9);
-    dgemm_dmma_grouped<<<grid, THREADS, SMEM_BYTES, stream>>>(tm, dp, nprob, total_tiles,
+    dgemm_dmma_grouped<<<grid, THREADS, SMEM_BYTES, stream>>>(tm, dp, nprob, *ranges, total_tiles,
                                                                dev_status, limit);
     CA3DMM_CUDA_TRY(cudaGetLastError());
     ca3dmm_note_launch(1);

@@ -400,7 +400,8 @@ __device__ __forceinline__ int nchunks(int nkb, int kb_per_chunk)
 // measured 1.45x faster than the same loops over a runtime count.
 template <int S>
 __global__ void __launch_bounds__(OTHREADS, 1)
-oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, int nstage,
+oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, const ca3dmm_tile_ranges_t rg,
+               int total_tiles, int nstage,
                int kb_per_chunk, int4 tsplit, const unsigned char *__restrict__ work,
                int *status, unsigned long long limit_ns)
 {
@@ -458,7 +459,8 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
         // ---------------------------------------------------------- producer
         if (lane == 0) {
             uint32_t it = 0;
-            for (int tile = blockIdx.x; tile < total_tiles && !abort_flag; tile += gridDim.x) {
+            for (int v = blockIdx.x; v < total_tiles && !abort_flag; v += gridDim.x) {
+                const int tile = range_tile(rg, v);
                 const OzGroup &p = groups[find_group(groups, ngroup, tile)];
                 int tm, tn;
                 group_tile(p, tile, tm, tn);
@@ -512,8 +514,8 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
             const unsigned tmask = (unsigned) (ii == 0 ? tsplit.x : (ii == 1 ? tsplit.y : tsplit.z));
             uint32_t it = 0, ci = 0;
             bool ok = true;
-            for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
-                const OzGroup &p = groups[find_group(groups, ngroup, tile)];
+            for (int v = blockIdx.x; v < total_tiles && ok; v += gridDim.x) {
+                const OzGroup &p = groups[find_group(groups, ngroup, range_tile(rg, v))];
                 const int nch = nchunks(p.nkb, kb_per_chunk);
                 for (int ch = 0; ch < nch && ok; ++ch, ++ci) {
                     if (!mbar_wait_bounded(acc_empty, (ci & 1u) ^ 1u, &abort_flag, status,
@@ -575,7 +577,8 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, int total_tiles, 
         double *col_scale = col_scale_all[q];
         uint32_t ci = 0;
         bool ok = true;
-        for (int tile = blockIdx.x; tile < total_tiles && ok; tile += gridDim.x) {
+        for (int v = blockIdx.x; v < total_tiles && ok; v += gridDim.x) {
+            const int tile = range_tile(rg, v);
             const OzGroup &p = groups[find_group(groups, ngroup, tile)];
             int tm, tn;
             group_tile(p, tile, tm, tn);
@@ -819,50 +822,137 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
     return CA3DMM_OK;
 }
 
+extern "C" int ca3dmm_oz_clear(const ca3dmm_oz_plan_t *oz, cudaStream_t stream)
+{
+    CA3DMM_CUDA_TRY(cudaMemsetAsync(oz->dev_work, 0, exp_bytes(oz->n_exp) + maxbits_bytes(oz->n_exp),
+                                    stream));
+    return CA3DMM_OK;
+}
+
+static int launch_exp(const ca3dmm_oz_plan_t *oz, const void *src, const SliceDesc *descs,
+                      int ndesc, int ntiles, cudaStream_t stream)
+{
+    if (ndesc <= 0 || ntiles <= 0) return CA3DMM_OK;
+    unsigned char *w = static_cast<unsigned char *>(oz->dev_work);
+    unsigned long long *mwork = reinterpret_cast<unsigned long long *>(w + exp_bytes(oz->n_exp));
+    const int cap = ca3dmm_device_sm_count() * 8;
+    oz_exp_kernel<<<ntiles < cap ? ntiles : cap, 256, 0, stream>>>(
+        static_cast<const double *>(src), descs, ndesc, ntiles, mwork);
+    CA3DMM_CUDA_TRY(cudaGetLastError());
+    ca3dmm_note_launch(1);
+    return CA3DMM_OK;
+}
+
+static int launch_slice(const ca3dmm_oz_plan_t *oz, const void *src, const SliceDesc *descs,
+                        int ndesc, int ntiles, cudaStream_t stream)
+{
+    if (ndesc <= 0 || ntiles <= 0) return CA3DMM_OK;
+    unsigned char *w = static_cast<unsigned char *>(oz->dev_work);
+    const unsigned long long *mwork =
+        reinterpret_cast<const unsigned long long *>(w + exp_bytes(oz->n_exp));
+    const int cap = ca3dmm_device_sm_count() * 8;
+    const unsigned grid = ntiles < cap ? ntiles : cap;
+    const double *x = static_cast<const double *>(src);
+    switch (oz->slices) {
+#define CA3DMM_SLICE_CASE(S)                                                                       \
+    case S:                                                                                        \
+        oz_slice_kernel<S><<<grid, 256, 0, stream>>>(x, descs, ndesc, ntiles, w, mwork);          \
+        break;
+        CA3DMM_SLICE_CASE(2) CA3DMM_SLICE_CASE(3) CA3DMM_SLICE_CASE(4) CA3DMM_SLICE_CASE(5)
+        CA3DMM_SLICE_CASE(6) CA3DMM_SLICE_CASE(7) CA3DMM_SLICE_CASE(8)
+#undef CA3DMM_SLICE_CASE
+        default: return CA3DMM_EINVAL;
+    }
+    CA3DMM_CUDA_TRY(cudaGetLastError());
+    ca3dmm_note_launch(1);
+    return CA3DMM_OK;
+}
+
 extern "C" int ca3dmm_oz_run_pack(const ca3dmm_oz_plan_t *oz, const void *A, const void *B,
                                   cudaStream_t stream)
 {
     const PlanLayout L(oz->ngroup);
     const SliceDesc *sd =
         reinterpret_cast<const SliceDesc *>(static_cast<const unsigned char *>(oz->dev_plan) + L.sd);
-    unsigned char *w = static_cast<unsigned char *>(oz->dev_work);
-    unsigned long long *mwork = reinterpret_cast<unsigned long long *>(w + exp_bytes(oz->n_exp));
-    CA3DMM_CUDA_TRY(cudaMemsetAsync(w, 0, exp_bytes(oz->n_exp) + maxbits_bytes(oz->n_exp), stream));
-    const double *src[2] = {static_cast<const double *>(A), static_cast<const double *>(B)};
-    const int cnt[2] = {oz->nA, oz->nB}, first[2] = {0, oz->nA};
-    const int tiles[2] = {oz->slice_tiles_a, oz->slice_tiles_b};
-    const int cap = ca3dmm_device_sm_count() * 8;
-    for (int o = 0; o < 2; ++o) {
-        if (cnt[o] == 0 || tiles[o] == 0) continue;
-        oz_exp_kernel<<<tiles[o] < cap ? tiles[o] : cap, 256, 0, stream>>>(
-            src[o], sd + first[o], cnt[o], tiles[o], mwork);
-        CA3DMM_CUDA_TRY(cudaGetLastError());
-        ca3dmm_note_launch(1);
+    int rc = ca3dmm_oz_clear(oz, stream);
+    if (!rc) rc = launch_exp(oz, A, sd, oz->nA, oz->slice_tiles_a, stream);
+    if (!rc) rc = launch_exp(oz, B, sd + oz->nA, oz->nB, oz->slice_tiles_b, stream);
+    if (!rc) rc = launch_slice(oz, A, sd, oz->nA, oz->slice_tiles_a, stream);
+    if (!rc) rc = launch_slice(oz, B, sd + oz->nA, oz->nB, oz->slice_tiles_b, stream);
+    return rc;
+}
+
+extern "C" int ca3dmm_oz_slice_side(const ca3dmm_oz_plan_t *oz, int which, const void *src,
+                                    cudaStream_t stream)
+{
+    const PlanLayout L(oz->ngroup);
+    const SliceDesc *sd =
+        reinterpret_cast<const SliceDesc *>(static_cast<const unsigned char *>(oz->dev_plan) + L.sd);
+    const SliceDesc *d = which ? sd + oz->nA : sd;
+    const int nd = which ? oz->nB : oz->nA;
+    const int nt = which ? oz->slice_tiles_b : oz->slice_tiles_a;
+    int rc = launch_exp(oz, src, d, nd, nt, stream);
+    if (!rc) rc = launch_slice(oz, src, d, nd, nt, stream);
+    return rc;
+}
+
+extern "C" size_t ca3dmm_oz_desc_bytes(void) { return sizeof(SliceDesc); }
+
+extern "C" int ca3dmm_oz_encode_rows(const void *host_plan, int ngroup, const int *blocks,
+                                     int count, int r0, int r1, void *out_descs, int *ntiles)
+{
+    const PlanLayout L(ngroup);
+    const unsigned char *h = static_cast<const unsigned char *>(host_plan);
+    const PlanHeader *hd = reinterpret_cast<const PlanHeader *>(h);
+    const SliceDesc *sd = reinterpret_cast<const SliceDesc *>(h + L.sd);
+    SliceDesc *out = static_cast<SliceDesc *>(out_descs);
+    if (!blocks || count < 0 || r0 < 0 || r1 < r0) return CA3DMM_EINVAL;
+    int tiles = 0;
+    for (int i = 0; i < count; ++i) {
+        if (blocks[i] < 0 || blocks[i] >= hd->nA) return CA3DMM_EINVAL;
+        const SliceDesc &d = sd[blocks[i]];
+        if (r0 % d.tile_rows) return CA3DMM_EINVAL;
+        SliceDesc c = d;
+        const int hi = r1 < d.rows ? r1 : d.rows;
+        c.rows = hi > r0 ? hi - r0 : 0;
+        c.rows_pad = rows_pad_of(c.rows, d.tile_rows);
+        c.src_off = d.src_off + (long long) r0 * d.rs;
+        c.q_off = d.q_off + (long long) (r0 / d.tile_rows) * d.nkb * hd->slices * d.tile_rows * OKB;
+        c.e_off = d.e_off + r0;
+        c.tile_begin = tiles;
+        if (c.rows > 0 && c.kz > 0) tiles += ((c.rows_pad + ST - 1) / ST) * ((c.kpad + ST - 1) / ST);
+        out[i] = c;
     }
-    for (int o = 0; o < 2; ++o) {
-        if (cnt[o] == 0 || tiles[o] == 0) continue;
-        const unsigned grid = tiles[o] < cap ? tiles[o] : cap;
-        switch (oz->slices) {
-#define CA3DMM_SLICE_CASE(S)                                                                       \
-    case S:                                                                                        \
-        oz_slice_kernel<S><<<grid, 256, 0, stream>>>(src[o], sd + first[o], cnt[o], tiles[o], w,   \
-                                                     mwork);                                       \
-        break;
-            CA3DMM_SLICE_CASE(2) CA3DMM_SLICE_CASE(3) CA3DMM_SLICE_CASE(4) CA3DMM_SLICE_CASE(5)
-            CA3DMM_SLICE_CASE(6) CA3DMM_SLICE_CASE(7) CA3DMM_SLICE_CASE(8)
-#undef CA3DMM_SLICE_CASE
-            default: return CA3DMM_EINVAL;
-        }
-        CA3DMM_CUDA_TRY(cudaGetLastError());
-        ca3dmm_note_launch(1);
-    }
+    *ntiles = tiles;
     return CA3DMM_OK;
+}
+
+extern "C" int ca3dmm_oz_slice_descs(const ca3dmm_oz_plan_t *oz, const void *src,
+                                     const void *dev_descs, int ndesc, int ntiles,
+                                     cudaStream_t stream)
+{
+    const SliceDesc *d = static_cast<const SliceDesc *>(dev_descs);
+    int rc = launch_exp(oz, src, d, ndesc, ntiles, stream);
+    if (!rc) rc = launch_slice(oz, src, d, ndesc, ntiles, stream);
+    return rc;
 }
 
 extern "C" int ca3dmm_oz_run_gemm(const ca3dmm_oz_plan_t *oz, int *dev_status, double timeout_s,
                                   cudaStream_t stream)
 {
-    if (oz->tiles <= 0) return CA3DMM_OK;
+    ca3dmm_tile_ranges_t rg;
+    memset(&rg, 0, sizeof(rg));
+    rg.n = 1;
+    rg.len[0] = oz->tiles;
+    return ca3dmm_oz_run_gemm_ranges(oz, &rg, dev_status, timeout_s, stream);
+}
+
+extern "C" int ca3dmm_oz_run_gemm_ranges(const ca3dmm_oz_plan_t *oz, const ca3dmm_tile_ranges_t *rg,
+                                         int *dev_status, double timeout_s, cudaStream_t stream)
+{
+    if (!rg || rg->n < 0 || rg->n > CA3DMM_MAX_RANGES) return CA3DMM_EINVAL;
+    const int vtiles = range_total(*rg);
+    if (vtiles <= 0) return CA3DMM_OK;
     const PlanLayout L(oz->ngroup);
     const unsigned char *pl = static_cast<const unsigned char *>(oz->dev_plan);
     const int stage_bytes = oz->slices * (A_SLICE_BYTES + B_SLICE_BYTES);
@@ -871,7 +961,7 @@ extern "C" int ca3dmm_oz_run_gemm(const ca3dmm_oz_plan_t *oz, int *dev_status, d
     if (nstage < 2) return CA3DMM_EINVAL;
     const size_t smem = (size_t) nstage * stage_bytes + (2 * nstage + 2) * 8 + 1024;
     int grid = ca3dmm_device_sm_count();
-    if (grid > oz->tiles) grid = oz->tiles;
+    if (grid > vtiles) grid = vtiles;
     const unsigned long long limit = (unsigned long long) (timeout_s * 1e9);
     const int kb_per_chunk = kchunk_of(oz->slices) / OKB;
     const OzGroup *groups = reinterpret_cast<const OzGroup *>(pl + L.gr);
@@ -883,7 +973,7 @@ extern "C" int ca3dmm_oz_run_gemm(const ca3dmm_oz_plan_t *oz, int *dev_status, d
         CA3DMM_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel<S>,                                    \
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,          \
                                              (int) smem));                                         \
-        oz_gemm_kernel<S><<<grid, OTHREADS, smem, stream>>>(groups, oz->ngroup, oz->tiles, nstage, \
+        oz_gemm_kernel<S><<<grid, OTHREADS, smem, stream>>>(groups, oz->ngroup, *rg, vtiles, nstage, \
                                                            kb_per_chunk, split, work, dev_status,  \
                                                            limit);                                 \
         break;

@@ -159,6 +159,17 @@ void ca3dmm_engine_print_stat(ca3dmm_engine_p engine);
 
 /* ---- added entry points (no counterpart in the reference) ---- */
 
+/* ca3dmm_engine_exec with HOST buffers: the same operands and output as
+ * ca3dmm_engine_exec (a dst_C block is required), in host memory; page-locked
+ * memory lets the copies run asynchronously.  The engine copies B in, then
+ * op(A) in bands of output rows, and computes and copies C out band by band,
+ * so that the host-device copies overlap the computation.  Device staging of
+ * the size of A, B and C is allocated on the first call and kept until
+ * ca3dmm_engine_free.  Synchronous; returns 0 or a CA3DMM_E* code (also in
+ * ca3dmm_engine_last_error).  B^T B: A_h is ignored. */
+int ca3dmm_engine_exec_host(ca3dmm_engine_p engine, const void *A_h, int ldA, const void *B_h,
+                            int ldB, void *C_h, int ldC);
+
 /* Kernels this library has launched since it was loaded, counted on the
  * host at each launch (a launch recorded into a CUDA graph counts once, at
  * capture; its replays do not). */
