@@ -71,6 +71,8 @@ typedef struct {
     ca3dmm_oz_blk_t *ob;
     ca3dmm_oz_src_t *os;
     ca3dmm_oz_group_t *og;
+    ca3dmm_oz_unit_t *ou;
+    int oz_fused;                 /* split mode adds its kp slabs into C itself */
     struct host_exec *hx;         /* state of ca3dmm_engine_exec_host (lazily created) */
 } plan_t;
 
@@ -214,7 +216,8 @@ static int plan_build(ca3dmm_engine_p e)
     pl->ob = (ca3dmm_oz_blk_t *) calloc((size_t) (pl->nA + pl->nB), sizeof(ca3dmm_oz_blk_t));
     pl->os = (ca3dmm_oz_src_t *) calloc((size_t) (pl->nA + pl->nB), sizeof(ca3dmm_oz_src_t));
     pl->og = (ca3dmm_oz_group_t *) calloc((size_t) pl->ngroup, sizeof(ca3dmm_oz_group_t));
-    if (!pl->groups || !pl->A || !pl->B || !pl->gd || !pl->ob || !pl->os || !pl->og)
+    pl->ou = (ca3dmm_oz_unit_t *) calloc((size_t) pl->ngroup, sizeof(ca3dmm_oz_unit_t));
+    if (!pl->groups || !pl->A || !pl->B || !pl->gd || !pl->ob || !pl->os || !pl->og || !pl->ou)
         return CA3DMM_ENOMEM;
     for (int tk = 0; tk < kp; tk++) {
         int ks, kz;
@@ -279,6 +282,7 @@ static void plan_free(plan_t *pl)
     free(pl->ob);
     free(pl->os);
     free(pl->og);
+    free(pl->ou);
     if (pl->hx) {
         struct host_exec *x = pl->hx;
         cudaFree(x->dA);
@@ -708,15 +712,43 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
             ob[pl->nA + i].rows = pl->B[i].rows; ob[pl->nA + i].cols = pl->B[i].cols;
             ob[pl->nA + i].alias = -1;
         }
+        /* The kp slabs of one (task_m, task_n) block form one work unit that
+         * adds its slabs into the output in slab order (no slab buffers, no
+         * reduction launch) -- when the chained units still give every SM
+         * several output tiles; otherwise (e.g. B^T B with a small C) each
+         * slab is its own unit and the slab reduction runs after the GEMM. */
+        const int tmn = e->mp > e->np && !e->is_BTB ? e->mp / e->np : 1;
+        const int tnn = e->np > e->mp && !e->is_BTB ? e->np / e->mp : 1;
+        long long unit_tiles = 0;
+        for (int u = 0; u < tmn * tnn; u++) {
+            const group_t *g = &pl->groups[u];
+            unit_tiles += (long long) ((g->mz + 127) / 128) * ((g->nz + 63) / 64);
+        }
+        pl->oz_fused = e->kp > 1 && unit_tiles >= 8LL * ca3dmm_device_sm_count();
         for (int i = 0; i < pl->ngroup; i++) {
-            og[i].a_blk = pl->groups[i].a_blk; og[i].b_blk = pl->groups[i].b_blk;
-            og[i].C = gd[i].C; og[i].ldc = gd[i].ldc;
+            const group_t *g = &pl->groups[i];
+            og[i].a_blk = g->a_blk; og[i].b_blk = g->b_blk;
+            if (pl->oz_fused) {
+                og[i].C = out + g->m0 + (size_t) g->n0 * ldo;
+                og[i].ldc = ldo;
+            } else {
+                og[i].C = gd[i].C;
+                og[i].ldc = gd[i].ldc;
+            }
             og[i].m = gd[i].m; og[i].n = gd[i].n; og[i].k = gd[i].k;
             og[i].raster = e->raster;
         }
+        ca3dmm_oz_unit_t *un = pl->ou;
+        for (int u = 0; u < tmn * tnn; u++) {
+            un[u].group = u;             /* (tk = 0, tm, tn) = tm * tnn + tn */
+            un[u].nsub = e->kp;
+            un[u].sub_stride = tmn * tnn;
+        }
         rc = ca3dmm_oz_plan_encode(&pl->oz, e->ozaki_slices, pl->nA, ob, os, pl->nB,
-                                   ob + pl->nA, os + pl->nA, pl->ngroup, og, w + pl->off_oz,
-                                   pl->oz_bytes, h + pl->off_ozplan, w + pl->off_ozplan);
+                                   ob + pl->nA, os + pl->nA, pl->ngroup, og,
+                                   pl->oz_fused ? tmn * tnn : 0, pl->oz_fused ? un : NULL,
+                                   w + pl->off_oz, pl->oz_bytes, h + pl->off_ozplan,
+                                   w + pl->off_ozplan);
         if (rc) return rc;
     }
     memset(h + pl->off_status, 0, 64);
@@ -778,7 +810,7 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
                 pl->dst_ncol == e->n;
     double *out = whole ? (double *) dst_C : (double *) (w + pl->off_cout);
     long long ldo = whole ? ldC : e->m;
-    if (e->kp > 1) {
+    if (e->kp > 1 && !(e->gemm_mode == CA3DMM_GEMM_OZAKI && pl->oz_fused)) {
         rc = ca3dmm_reduce_slabs_launch((const double *) (w + pl->off_slab),
                                         (long long) pl->slab_stride, pl->slab_ld, e->kp, e->m,
                                         e->n, out, ldo, st);
@@ -903,12 +935,17 @@ static int hx_build_bands(ca3dmm_engine_p e, struct host_exec *x, cudaStream_t s
     x->built_mode = e->gemm_mode;
     x->built_slices = e->ozaki_slices;
     x->built_raster = e->raster;
-    if (e->is_BTB || !whole || e->kp * tnn > CA3DMM_MAX_RANGES) return 0;
+    if (e->is_BTB || !whole || ((ozaki && pl->oz_fused) ? 1 : e->kp) * tnn > CA3DMM_MAX_RANGES)
+        return 0;
     const int raster = e->raster > 0 ? e->raster : 8;
     const int bn = ozaki ? 64 : 128;
+    /* tile numbering of the GEMM plans: per group (plain) or per unit of
+     * (task_m, task_n) with its kp slabs chained (split precision) */
     int *tb = (int *) malloc(sizeof(int) * (size_t) pl->ngroup);
     if (!tb) return 0;
-    for (int g = 0, t = 0; g < pl->ngroup; g++) {
+    const int chained = ozaki && pl->oz_fused;
+    const int nnum = chained ? tmn * tnn : pl->ngroup;
+    for (int g = 0, t = 0; g < nnum; g++) {
         const group_t *gg = &pl->groups[g];
         tb[g] = t;
         if (gg->mz > 0 && gg->nz > 0) t += ((gg->mz + 127) / 128) * ((gg->nz + bn - 1) / bn);
@@ -944,7 +981,7 @@ static int hx_build_bands(ca3dmm_engine_p e, struct host_exec *x, cudaStream_t s
             ca3dmm_tile_ranges_t *rg = &x->rng[c];
             memset(rg, 0, sizeof(*rg));
             const int row_lo = r / 128, nrow_t = band_rows / 128;
-            for (int tk = 0; tk < e->kp; tk++)
+            for (int tk = 0; tk < (chained ? 1 : e->kp); tk++)
                 for (int tn = 0; tn < tnn; tn++) {
                     const int g = (tk * tmn + tm) * tnn + tn;
                     const group_t *gg = &pl->groups[g];
@@ -1102,7 +1139,7 @@ static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_
                 rc = ca3dmm_dgemm_launch_ranges(w + pl->off_gemm, pl->ngroup, &x->rng[c], status_d,
                                                 5.0, st);
         }
-        if (!rc && e->kp > 1)
+        if (!rc && e->kp > 1 && !(ozaki && pl->oz_fused))
             rc = ca3dmm_reduce_slabs_launch((const double *) (w + pl->off_slab) + x->r0[c],
                                             (long long) pl->slab_stride, pl->slab_ld, e->kp,
                                             x->r1[c] - x->r0[c], e->n, x->dC + x->r0[c], x->ldc, st);

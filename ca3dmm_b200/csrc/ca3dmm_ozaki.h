@@ -43,9 +43,18 @@ typedef struct {
     int raster;           /* tile rows per raster band (0 = default) */
 } ca3dmm_oz_group_t;
 
+/* Work unit: nsub groups (group, group + sub_stride, ...) of equal m x n that
+ * write the same C block (the k-slabs of one output block); each output tile
+ * runs the groups in order, the first storing C and the others adding to it,
+ * so the slab sum needs no separate reduction.  Without units every group is
+ * its own unit. */
 typedef struct {
-    int slices, nA, nB, ngroup;
-    int tiles;            /* total output tiles of the grouped INT8 launch */
+    int group, nsub, sub_stride;
+} ca3dmm_oz_unit_t;
+
+typedef struct {
+    int slices, nA, nB, ngroup, nunit, max_nsub;
+    int tiles;            /* output tiles of the grouped INT8 launch (numbered per unit) */
     int max_rows, max_kpad;
     int slice_tiles_a, slice_tiles_b;   /* 64 x 64 slicing tiles of the A / B blocks */
     long long n_exp;      /* rows with an exponent: E (int) then max bits (u64) arrays open the work region */
@@ -63,7 +72,8 @@ size_t ca3dmm_oz_work_bytes(int nA, const int *a_rows, const int *a_k, int nB, c
 int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA, const ca3dmm_oz_blk_t *A,
                           const ca3dmm_oz_src_t *srcA, int nB, const ca3dmm_oz_blk_t *B,
                           const ca3dmm_oz_src_t *srcB, int ngroup, const ca3dmm_oz_group_t *G,
-                          void *dev_work, size_t work_bytes, void *host_plan, void *dev_plan);
+                          int nunit, const ca3dmm_oz_unit_t *units, void *dev_work,
+                          size_t work_bytes, void *host_plan, void *dev_plan);
 /* Exponent extraction + slicing of every A and B block straight from the
  * caller's matrices (op(A)(i,l) = transA ? A[l + i*ldA] : A[i + l*ldA]). */
 int ca3dmm_oz_run_pack(const ca3dmm_oz_plan_t *oz, const void *A, const void *B,

@@ -232,7 +232,7 @@ static int build_plan(ca3dmm_grouped_p g, const double *const *A, const int *ldA
             g->og[i].m = g->m[i]; g->og[i].n = g->n[i]; g->og[i].k = g->k[i];
         }
         int rc = ca3dmm_oz_plan_encode(&g->oz, g->slices, np, g->ob, g->os, np, g->ob + np,
-                                       g->os + np, np, g->og, w + g->off_oz, g->oz_bytes,
+                                       g->os + np, np, g->og, 0, NULL, w + g->off_oz, g->oz_bytes,
                                        h + g->off_ozplan, w + g->off_ozplan);
         if (rc) return rc;
     }

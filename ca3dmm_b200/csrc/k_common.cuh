@@ -24,15 +24,20 @@ enum {
 
 // Virtual tile v of a persistent launch -> tile index of the plan: v walks the
 // ranges in order (a launch over the whole list is one range [0, total)).
+// (fully unrolled over the fixed capacity, so the parameter struct is read
+// with constant indices and never copied to local memory)
 template <typename R>
 CA3DMM_DEV int range_tile(const R &r, int v)
 {
-#pragma unroll 1
-    for (int i = 0; i < r.n; ++i) {
-        if (v < r.len[i]) return r.begin[i] + v;
-        v -= r.len[i];
+    int t = -1;
+#pragma unroll
+    for (int i = 0; i < (int) (sizeof(r.len) / sizeof(r.len[0])); ++i) {
+        if (t < 0 && i < r.n) {
+            if (v < r.len[i]) t = r.begin[i] + v;
+            else v -= r.len[i];
+        }
     }
-    return -1;
+    return t;
 }
 
 template <typename R>

@@ -84,9 +84,20 @@ struct OzGroup {
     long long qa_off, qb_off;   // byte offsets of the tiled slices
 };
 
+// A work unit is a chain of nsub groups (group, group + sub_stride, ...) that
+// write the same C block: the kp k-slabs of one (task_m, task_n) block.  Its
+// tiles are numbered once and every CTA owns a fixed set of tile numbers; the
+// CTA runs all its tiles for slab 0 (storing C), then all for slab 1 (adding
+// to the C it wrote), and so on -- the reference's slab-sum order, with the
+// operand locality of slab-by-slab processing.
+struct OzUnit {
+    int tile_begin, tiles_m, tiles_n, raster;
+    int group, nsub, sub_stride, pad;
+};
+
 struct PlanHeader {
     int nA, nB, ngroup, slices;
-    int nslice_desc, tiles, pad0, pad1;
+    int nslice_desc, tiles, nunit, pad1;
 };
 
 // ------------------------------------------------------------------ slicing
@@ -378,6 +389,27 @@ __device__ __forceinline__ int find_group(const OzGroup *g, int n, int tile)
     return lo;
 }
 
+__device__ __forceinline__ int find_unit(const OzUnit *u, int n, int tile)
+{
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        int mid = (lo + hi + 1) >> 1;
+        if (u[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+__device__ __forceinline__ void unit_tile(const OzUnit &p, int tile, int &tm, int &tn)
+{
+    int t = tile - p.tile_begin;
+    int gs = p.raster * p.tiles_n;
+    int first = (t / gs) * p.raster;
+    int gm = min(p.tiles_m - first, p.raster);
+    int r = t % gs;
+    tm = first + r % gm;
+    tn = r / gm;
+}
+
 __device__ __forceinline__ void group_tile(const OzGroup &p, int tile, int &tm, int &tn)
 {
     int t = tile - p.tile_begin;
@@ -400,7 +432,8 @@ __device__ __forceinline__ int nchunks(int nkb, int kb_per_chunk)
 // measured 1.45x faster than the same loops over a runtime count.
 template <int S>
 __global__ void __launch_bounds__(OTHREADS, 1)
-oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, const ca3dmm_tile_ranges_t rg,
+oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ units, int nunit,
+               int nsub_max, const ca3dmm_tile_ranges_t rg,
                int total_tiles, int nstage,
                int kb_per_chunk, int4 tsplit, const unsigned char *__restrict__ work,
                int *status, unsigned long long limit_ns)
@@ -459,17 +492,20 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, const ca3dmm_tile
         // ---------------------------------------------------------- producer
         if (lane == 0) {
             uint32_t it = 0;
-            for (int v = blockIdx.x; v < total_tiles && !abort_flag; v += gridDim.x) {
+            bool ok = true;
+          for (int sub = 0; sub < nsub_max && ok; ++sub)
+            for (int v = blockIdx.x; v < total_tiles && ok && !abort_flag; v += gridDim.x) {
                 const int tile = range_tile(rg, v);
-                const OzGroup &p = groups[find_group(groups, ngroup, tile)];
+                const OzUnit &U = units[find_unit(units, nunit, tile)];
                 int tm, tn;
-                group_tile(p, tile, tm, tn);
+                unit_tile(U, tile, tm, tn);
+              if (sub < U.nsub) {
+                const OzGroup &p = groups[U.group + sub * U.sub_stride];
                 const unsigned char *qa =
                     p.a_from_b ? work + p.qa_off + (long long) (2 * tm) * p.nkb * b_bytes
                                : work + p.qa_off + (long long) tm * p.nkb * a_bytes;
                 const unsigned char *qb =
                     work + p.qb_off + (long long) tn * p.nkb * b_bytes;
-                bool ok = true;
                 for (int kb = 0; kb < p.nkb; ++kb, ++it) {
                     const uint32_t s = it % nstage, ph = (it / nstage) & 1u;
                     if (!mbar_wait_bounded(&empty[s], ph ^ 1u, &abort_flag, status,
@@ -495,7 +531,7 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, const ca3dmm_tile
                     }
                     bulk_load(sA + a_bytes, qb + (long long) kb * b_bytes, b_bytes, &full[s]);
                 }
-                if (!ok) break;
+              }
             }
             // drain copies in flight (bounded, abort flag ignored)
             const uint32_t first = it > (uint32_t) nstage ? it - nstage : 0;
@@ -514,8 +550,11 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, const ca3dmm_tile
             const unsigned tmask = (unsigned) (ii == 0 ? tsplit.x : (ii == 1 ? tsplit.y : tsplit.z));
             uint32_t it = 0, ci = 0;
             bool ok = true;
+          for (int sub = 0; sub < nsub_max && ok; ++sub)
             for (int v = blockIdx.x; v < total_tiles && ok; v += gridDim.x) {
-                const OzGroup &p = groups[find_group(groups, ngroup, range_tile(rg, v))];
+                const OzUnit &U = units[find_unit(units, nunit, range_tile(rg, v))];
+              if (sub < U.nsub) {
+                const OzGroup &p = groups[U.group + sub * U.sub_stride];
                 const int nch = nchunks(p.nkb, kb_per_chunk);
                 for (int ch = 0; ch < nch && ok; ++ch, ++ci) {
                     if (!mbar_wait_bounded(acc_empty, (ci & 1u) ^ 1u, &abort_flag, status,
@@ -560,6 +599,7 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, const ca3dmm_tile
                     if (!ok) break;
                     tc_commit(acc_full);
                 }
+              }
             }
             if (!ok) {
                 // let every MMA this thread issued finish before TMEM is freed
@@ -577,11 +617,14 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, const ca3dmm_tile
         double *col_scale = col_scale_all[q];
         uint32_t ci = 0;
         bool ok = true;
+      for (int sub = 0; sub < nsub_max && ok; ++sub)
         for (int v = blockIdx.x; v < total_tiles && ok; v += gridDim.x) {
             const int tile = range_tile(rg, v);
-            const OzGroup &p = groups[find_group(groups, ngroup, tile)];
+            const OzUnit &U = units[find_unit(units, nunit, tile)];
             int tm, tn;
-            group_tile(p, tile, tm, tn);
+            unit_tile(U, tile, tm, tn);
+          if (sub < U.nsub) {
+            const OzGroup &p = groups[U.group + sub * U.sub_stride];
             const int gr = tm * OBM + row;
             const int gm = p.m, gn = p.n;
             const long long ldc = p.ldc;
@@ -635,13 +678,29 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, int ngroup, const ca3dmm_tile
             }
             if (!ok) break;
             if (gr < gm) {
-                double *crow = Cg + gr;
+                // slab 0 stores; later slabs of the chain add in slab order (this
+                // thread wrote the value it reads)
+                double *crow = Cg + gr + (long long) (tn * OBN) * ldc;
+                const int nj = min(OBN, gn - tn * OBN);
+                if (sub == 0) {
 #pragma unroll
-                for (int j = 0; j < OBN; ++j) {
-                    const int gc = tn * OBN + j;
-                    if (gc < gn) crow[(long long) gc * ldc] = acc[j] * col_scale[j];
+                    for (int j = 0; j < OBN; ++j)
+                        if (j < nj) crow[(long long) j * ldc] = acc[j] * col_scale[j];
+                } else {
+#pragma unroll
+                    for (int j0 = 0; j0 < OBN; j0 += 8) {
+                        double c[8];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j)
+                            c[j] = j0 + j < nj ? crow[(long long) (j0 + j) * ldc] : 0.0;
+#pragma unroll
+                        for (int j = 0; j < 8; ++j)
+                            if (j0 + j < nj)
+                                crow[(long long) (j0 + j) * ldc] = c[j] + acc[j0 + j] * col_scale[j0 + j];
+                    }
                 }
             }
+          }
         }
     }
     tc_fence_before();
@@ -692,15 +751,16 @@ int4 slice_split(int s)
     return make_int4(best_m[0], best_m[1], best_m[2], 0);
 }
 
-// Device plan layout for g groups (at most 2g operand blocks):
-// [header 256 B][2g slice descriptors][g groups]
+// Device plan layout for g groups (at most 2g operand blocks, g units):
+// [header 256 B][2g slice descriptors][g groups][g units]
 struct PlanLayout {
-    size_t sd, gr, total;
+    size_t sd, gr, un, total;
     explicit PlanLayout(int g)
     {
         sd = 256;
         gr = (sd + (size_t) 2 * g * sizeof(SliceDesc) + 127) / 128 * 128;
-        total = gr + (size_t) g * sizeof(OzGroup);
+        un = (gr + (size_t) g * sizeof(OzGroup) + 127) / 128 * 128;
+        total = un + (size_t) g * sizeof(OzUnit);
     }
 };
 
@@ -729,10 +789,12 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
                                      const ca3dmm_oz_blk_t *A, const ca3dmm_oz_src_t *srcA,
                                      int nB, const ca3dmm_oz_blk_t *B,
                                      const ca3dmm_oz_src_t *srcB, int ngroup,
-                                     const ca3dmm_oz_group_t *G, void *dev_work,
+                                     const ca3dmm_oz_group_t *G, int nunit,
+                                     const ca3dmm_oz_unit_t *units, void *dev_work,
                                      size_t work_bytes, void *host_plan, void *dev_plan)
 {
     if (slices < 2 || slices > MAX_SLICES || nA + nB > 2 * ngroup) return CA3DMM_EINVAL;
+    if (units && (nunit < 1 || nunit > ngroup)) return CA3DMM_EINVAL;
     const PlanLayout L(ngroup);
     unsigned char *h = static_cast<unsigned char *>(host_plan);
     memset(h, 0, L.total);
@@ -810,9 +872,32 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
         o.raster = G[g].raster > 0 ? G[g].raster : GROUP_M;
         tiles += o.tiles_m * o.tiles_n;
     }
+    // work units: one per group, or the caller's chains of equal-shaped groups
+    OzUnit *un = reinterpret_cast<OzUnit *>(h + L.un);
+    const int nu = units ? nunit : ngroup;
+    tiles = 0;
+    for (int u = 0; u < nu; ++u) {
+        const int g0 = units ? units[u].group : u;
+        const int ns = units ? units[u].nsub : 1, st = units ? units[u].sub_stride : 0;
+        if (g0 < 0 || ns < 1 || g0 + (ns - 1) * st >= ngroup || (ns > 1 && st < 1))
+            return CA3DMM_EINVAL;
+        for (int j = 1; j < ns; ++j)
+            if (gr[g0 + j * st].m != gr[g0].m || gr[g0 + j * st].n != gr[g0].n)
+                return CA3DMM_EINVAL;
+        OzUnit &w = un[u];
+        w.group = g0; w.nsub = ns; w.sub_stride = st; w.pad = 0;
+        w.tiles_m = gr[g0].tiles_m;
+        w.tiles_n = gr[g0].tiles_n;
+        w.raster = gr[g0].raster;
+        w.tile_begin = tiles;
+        tiles += w.tiles_m * w.tiles_n;
+    }
     hd->nA = nA; hd->nB = nB; hd->ngroup = ngroup; hd->slices = slices;
-    hd->nslice_desc = nA + nB; hd->tiles = tiles;
+    hd->nslice_desc = nA + nB; hd->tiles = tiles; hd->nunit = nu;
     oz->slices = slices; oz->nA = nA; oz->nB = nB; oz->ngroup = ngroup; oz->tiles = tiles;
+    oz->nunit = nu;
+    oz->max_nsub = 1;
+    for (int u = 0; u < nu; ++u) oz->max_nsub = un[u].nsub > oz->max_nsub ? un[u].nsub : oz->max_nsub;
     oz->max_rows = max_rows; oz->max_kpad = max_kpad;
     oz->slice_tiles_a = tiles_op[0];
     oz->slice_tiles_b = tiles_op[1];
@@ -965,6 +1050,7 @@ extern "C" int ca3dmm_oz_run_gemm_ranges(const ca3dmm_oz_plan_t *oz, const ca3dm
     const unsigned long long limit = (unsigned long long) (timeout_s * 1e9);
     const int kb_per_chunk = kchunk_of(oz->slices) / OKB;
     const OzGroup *groups = reinterpret_cast<const OzGroup *>(pl + L.gr);
+    const OzUnit *units = reinterpret_cast<const OzUnit *>(pl + L.un);
     const unsigned char *work = static_cast<const unsigned char *>(oz->dev_work);
     const int4 split = slice_split(oz->slices);
     switch (oz->slices) {
@@ -973,7 +1059,9 @@ extern "C" int ca3dmm_oz_run_gemm_ranges(const ca3dmm_oz_plan_t *oz, const ca3dm
         CA3DMM_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel<S>,                                    \
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,          \
                                              (int) smem));                                         \
-        oz_gemm_kernel<S><<<grid, OTHREADS, smem, stream>>>(groups, oz->ngroup, *rg, vtiles, nstage, \
+        oz_gemm_kernel<S><<<grid, OTHREADS, smem, stream>>>(groups, units, oz->nunit,             \
+                                                           oz->max_nsub, *rg, vtiles,              \
+                                                           nstage,                                 \
                                                            kb_per_chunk, split, work, dev_status,  \
                                                            limit);                                 \
         break;

@@ -93,6 +93,17 @@ def test_ozaki_error_shrinks_with_slices_and_matches_plain(cuda):
     assert errs[8] <= e_plain, (errs, e_plain)
 
 
+def test_ozaki_chained_slabs_bitexact(cuda):
+    """A C large enough that each output tile runs its kp slabs in one CTA and
+    adds them into C in slab order (no slab buffers): still bit-exact."""
+    m, n, k = 3200, 3000, 400
+    A = orc.gen_signed_exp(111, m, k)
+    B = orc.gen_signed_exp(112, k, n)
+    got, (mp, np_, kp) = _run(A, B, m, n, k, 0, 0, 6, (2, 1, 3), cb.GEMM_OZAKI, 7)
+    assert kp == 3
+    assert np.array_equal(got, _oracle_ozaki(A, B, m, n, k, 0, 0, kp, 7))
+
+
 @pytest.mark.parametrize("s", [5, 8])
 def test_ozaki_k_chunks_bitexact(cuda, s):
     """k longer than one exact INT32 chunk: chunked recombination matches."""
