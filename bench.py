@@ -38,7 +38,7 @@ METRIC = "FP64-accurate TFLOP/s (2mnk/t): split-precision vs plain DMMA, equal e
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--steps", type=int, default=40)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--trans-a", type=int, default=0)
@@ -62,7 +62,9 @@ def dist_setup(args):
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons during the timed region."""
+    """nvidia-smi clocks / throttle reasons during the timed region: samples
+    every 100 ms in a reader thread; mark() brackets the timed region and only
+    the samples read between the marks are summarised."""
 
     Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
@@ -77,7 +79,7 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.Q,
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "100"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
@@ -90,7 +92,10 @@ class ClockSampler:
             if len(parts) >= 9:
                 self.samples.append(parts)
 
-    def stop(self):
+    def mark(self):
+        return len(self.samples)
+
+    def stop(self, i0=0, i1=None):
         if self.proc is None:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
         self.proc.terminate()
@@ -98,17 +103,18 @@ class ClockSampler:
             self.proc.wait(timeout=5)
         except Exception:
             self.proc.kill()
-        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
-        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        window = self.samples[i0:i1] if i1 is not None and i1 > i0 else self.samples[i0:i0 + 1]
+        sm = [float(s[1]) for s in window if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in window if s[2].replace(".", "").isdigit()]
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
         reasons = set()
-        for s in self.samples:
+        for s in window:
             for nm, v in zip(names, s[5:9]):
                 if v.strip().lower() == "active":
                     reasons.add(nm)
         return {"sm_mhz": float(np.median(sm)) if sm else None,
                 "sm_max_mhz": max(mx) if mx else None, "reasons": sorted(reasons),
-                "samples": len(self.samples)}
+                "samples": len(window)}
 
 
 def max_over_ranks(ms, world, device="cuda"):
@@ -480,10 +486,12 @@ def main():
     torch.cuda.synchronize()
     sampler.start()
     time.sleep(0.3)
+    i0 = sampler.mark()
     l0 = cb.kernel_launches()
     res = leg(eng, args.steps, 0)
     launches = cb.kernel_launches() - l0
-    clocks = sampler.stop()
+    time.sleep(0.15)                      # the sample covering the region's end
+    clocks = sampler.stop(i0, sampler.mark())
     ms = max_over_ranks(res["ms_per_step"], world)
     value = whole_job_tflops(flops, world, ms)
     other = "plain" if head == "ozaki" else "ozaki"

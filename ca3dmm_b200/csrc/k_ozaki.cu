@@ -141,7 +141,6 @@ oz_exp_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ desc
               int total_tiles, unsigned long long *__restrict__ mwork)
 {
     __shared__ unsigned long long part[4][ST];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
         const SliceDesc d = descs[find_slice_desc(descs, ndesc, tile)];
         const int local = tile - d.tile_begin, tx = (d.rows_pad + ST - 1) / ST;
@@ -174,8 +173,10 @@ oz_exp_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ desc
                 for (int q = 1; q < 4; ++q) v = part[q][threadIdx.x] > v ? part[q][threadIdx.x] : v;
                 if (v) atomicMax(mwork + d.e_off + r0 + threadIdx.x, v);
             }
-        } else {
-            // k contiguous: warp w reads rows w, w + 8, ... (64 consecutive k each)
+        } else if (d.rs >= 65536) {
+            // k contiguous, rows at least 512 KB apart: warp w reads whole rows w,
+            // w + 8, ... (64 consecutive k; one row, so one page, per load)
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
             unsigned long long m[ST / 8];
 #pragma unroll
             for (int j = 0; j < ST / 8; ++j) {
@@ -203,6 +204,32 @@ oz_exp_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ desc
                 const int r = warp + 8 * j;
                 if (lane == 0 && r < rn && v) atomicMax(mwork + d.e_off + r0 + r, v);
             }
+        } else {
+            // k contiguous: thread (row t/4, quarter q = t%4) reads k = 2q + 8i, +1
+            // (i = 0..7), so the four threads of a row cover 64 contiguous bytes
+            // per load; the quarters combine with two shuffles
+            const int r = threadIdx.x >> 2, q = threadIdx.x & 3;
+            unsigned long long m = 0;
+            if (r < rn) {
+                const double *row = base + (long long) r * d.rs;
+#pragma unroll
+                for (int i = 0; i < ST / 8; ++i) {
+                    const int l = 2 * q + 8 * i;
+                    const unsigned long long v0 =
+                        l < ln ? (unsigned long long) __double_as_longlong(__ldg(row + (long long) l * d.ls)) : 0ull;
+                    const unsigned long long v1 =
+                        l + 1 < ln ? (unsigned long long) __double_as_longlong(__ldg(row + (long long) (l + 1) * d.ls)) : 0ull;
+                    const unsigned long long a = v0 & 0x7fffffffffffffffull, b = v1 & 0x7fffffffffffffffull;
+                    m = a > m ? a : m;
+                    m = b > m ? b : m;
+                }
+            }
+#pragma unroll
+            for (int o = 1; o < 4; o <<= 1) {
+                const unsigned long long w = __shfl_xor_sync(0xffffffffu, m, o);
+                m = w > m ? w : m;
+            }
+            if (q == 0 && r < rn && m) atomicMax(mwork + d.e_off + r0 + r, m);
         }
     }
 }
@@ -230,12 +257,22 @@ oz_slice_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ de
         const int r0 = (local % tx) * ST, l0 = (local / tx) * ST;
         const double *base = slice_src(src, d.src_off);
         const bool rfast = d.rs == 1;
-        __syncthreads();
-        for (int e = threadIdx.x; e < ST * ST; e += blockDim.x) {
+        // all 16 loads of a thread in flight at once (compile-time trip count)
+        double x[ST * ST / 256];
+#pragma unroll
+        for (int i = 0; i < ST * ST / 256; ++i) {
+            const int e = threadIdx.x + 256 * i;
             const int a = e % ST, b = e / ST;
             const int r = rfast ? a : b, l = rfast ? b : a;
             const int gr = r0 + r, gl = l0 + l;
-            tile[r][l] = (gr < d.rows && gl < d.kz) ? __ldg(base + gr * d.rs + gl * d.ls) : 0.0;
+            x[i] = (gr < d.rows && gl < d.kz) ? __ldg(base + gr * d.rs + gl * d.ls) : 0.0;
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < ST * ST / 256; ++i) {
+            const int e = threadIdx.x + 256 * i;
+            const int a = e % ST, b = e / ST;
+            tile[rfast ? a : b][rfast ? b : a] = x[i];
         }
         __syncthreads();
         // thread -> (row r, 16 consecutive k); a warp covers 32 rows of one chunk
@@ -379,16 +416,6 @@ __device__ __forceinline__ double pow2(int e)
     return ldexp(1.0, e);
 }
 
-__device__ __forceinline__ int find_group(const OzGroup *g, int n, int tile)
-{
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (g[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
-    }
-    return lo;
-}
-
 __device__ __forceinline__ int find_unit(const OzUnit *u, int n, int tile)
 {
     int lo = 0, hi = n - 1;
@@ -400,17 +427,6 @@ __device__ __forceinline__ int find_unit(const OzUnit *u, int n, int tile)
 }
 
 __device__ __forceinline__ void unit_tile(const OzUnit &p, int tile, int &tm, int &tn)
-{
-    int t = tile - p.tile_begin;
-    int gs = p.raster * p.tiles_n;
-    int first = (t / gs) * p.raster;
-    int gm = min(p.tiles_m - first, p.raster);
-    int r = t % gs;
-    tm = first + r % gm;
-    tn = r / gm;
-}
-
-__device__ __forceinline__ void group_tile(const OzGroup &p, int tile, int &tm, int &tn)
 {
     int t = tile - p.tile_begin;
     int gs = p.raster * p.tiles_n;

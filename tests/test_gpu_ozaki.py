@@ -121,6 +121,7 @@ def test_ozaki_k_chunks_bitexact(cuda, s):
     (50, 2000, 4, (1, 1, 4), 6),      # fewer rows than one B tile
     (200, 1500, 8, None, 7),          # the reference's default B^T B grid (fold)
     (130, 1000, 16, (2, 2, 4), 5),
+    (64, 70000, 4, (1, 1, 4), 7),     # columns of B more than 512 KB apart
 ])
 def test_ozaki_btb(cuda, n, k, p, grid, s):
     """B^T B: the op(A) = B^T blocks reuse the slices of the B blocks."""
