@@ -40,6 +40,8 @@ typedef struct {
     int rows, cols, r0, c0;   /* block of op(X): rows x cols starting at (r0, c0) */
     long long ld;             /* leading dimension of the packed copy */
     size_t off;               /* byte offset of the packed copy in the work buffer */
+    const double *direct;     /* plain mode: the caller's block used in place (NULL: packed) */
+    long long direct_ld;
 } blk_t;
 
 typedef struct {
@@ -628,6 +630,9 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
 {
     plan_t *pl = (plan_t *) e->impl;
     char *w = (char *) e->workbuf_d, *h = (char *) pl->stage;
+    /* An untransposed operand block whose address and leading dimension suit
+     * the GEMM's tensor maps (16-byte aligned start, even ld) is read in place;
+     * the others are packed (and transposed) into the work buffer. */
     ca3dmm_pack_desc_t *pa = (ca3dmm_pack_desc_t *) (h + pl->off_packA);
     for (int i = 0; i < pl->nA; i++) {
         blk_t *b = &pl->A[i];
@@ -638,6 +643,13 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
                                 : (long long) b->r0 + (long long) b->c0 * ldA;
         d->dst_off = (long long) ((b->off) / sizeof(double));
         d->ldd = b->ld;
+        b->direct = NULL;
+        if (!e->trans_A && (ldA & 1) == 0 &&
+            (((uintptr_t) A + sizeof(double) * (uintptr_t) d->src_off) & 15) == 0) {
+            b->direct = (const double *) A + d->src_off;
+            b->direct_ld = ldA;
+            d->rows = 0;
+        }
     }
     pl->pack_tiles_A = ca3dmm_pack_tiles(pa, pl->nA);
     ca3dmm_pack_desc_t *pb = (ca3dmm_pack_desc_t *) (h + pl->off_packB);
@@ -650,6 +662,13 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
                                 : (long long) b->r0 + (long long) b->c0 * ldB;
         d->dst_off = (long long) ((b->off) / sizeof(double));
         d->ldd = b->ld;
+        b->direct = NULL;
+        if (!e->trans_B && (ldB & 1) == 0 &&
+            (((uintptr_t) B + sizeof(double) * (uintptr_t) d->src_off) & 15) == 0) {
+            b->direct = (const double *) B + d->src_off;
+            b->direct_ld = ldB;
+            d->rows = 0;
+        }
     }
     pl->pack_tiles_B = ca3dmm_pack_tiles(pb, pl->nB);
     /* output target of the GEMM (kp == 1) or of the reduction (kp > 1) */
@@ -668,10 +687,11 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
     for (int i = 0; i < pl->ngroup; i++) {
         group_t *g = &pl->groups[i];
         ca3dmm_dgemm_desc_t *q = &gd[i];
-        q->A = (const double *) (w + pl->A[g->a_blk].off);
-        q->lda = pl->A[g->a_blk].ld;
-        q->B = (const double *) (w + pl->B[g->b_blk].off);
-        q->ldb = pl->B[g->b_blk].ld;
+        const blk_t *ba = &pl->A[g->a_blk], *bb = &pl->B[g->b_blk];
+        q->A = ba->direct ? ba->direct : (const double *) (w + ba->off);
+        q->lda = ba->direct ? ba->direct_ld : ba->ld;
+        q->B = bb->direct ? bb->direct : (const double *) (w + bb->off);
+        q->ldb = bb->direct ? bb->direct_ld : bb->ld;
         if (e->kp > 1) {
             q->C = (double *) (w + pl->off_slab) + (size_t) g->tk * pl->slab_stride + g->m0 +
                    (size_t) g->n0 * pl->slab_ld;
@@ -776,8 +796,8 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
         return CA3DMM_EINVAL;
     }
     int rc;
-    if (!pl->plan_valid || pl->c_ldA != ldA || pl->c_ldB != ldB || pl->c_dst != dst_C ||
-        pl->c_ldC != ldC) {
+    if (!pl->plan_valid || pl->c_A != src_A || pl->c_B != src_B || pl->c_ldA != ldA ||
+        pl->c_ldB != ldB || pl->c_dst != dst_C || pl->c_ldC != ldC) {
         rc = plan_upload(e, src_A, ldA, src_B, ldB, dst_C, ldC, st);
         if (rc) return rc;
     } else if (cudaMemsetAsync(w + pl->off_status, 0, 64, st) != cudaSuccess) {
@@ -1004,6 +1024,7 @@ static int hx_build_bands(ca3dmm_engine_p e, struct host_exec *x, cudaStream_t s
                     const blk_t *b = &pl->A[blocks[tk]];
                     ca3dmm_pack_desc_t *d = &pd[tk];
                     memset(d, 0, sizeof(*d));
+                    if (b->direct) continue;         /* read in place by the GEMM */
                     d->rows = rend - r; d->cols = b->cols; d->trans = e->trans_A; d->lds = x->lda;
                     d->src_off = e->trans_A ? (long long) b->c0 + (long long) (b->r0 + r) * x->lda
                                             : (long long) (b->r0 + r) + (long long) b->c0 * x->lda;
@@ -1073,8 +1094,8 @@ static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_
     const double *dAsrc = e->is_BTB ? x->dB : x->dA;
     const long long ldAsrc = e->is_BTB ? x->ldb : x->lda;
     /* device plan for the staging buffers (rebuilt only when they change) */
-    if (!pl->plan_valid || pl->c_ldA != ldAsrc || pl->c_ldB != x->ldb || pl->c_dst != x->dC ||
-        pl->c_ldC != x->ldc) {
+    if (!pl->plan_valid || pl->c_A != dAsrc || pl->c_B != x->dB || pl->c_ldA != ldAsrc ||
+        pl->c_ldB != x->ldb || pl->c_dst != x->dC || pl->c_ldC != x->ldc) {
         rc = plan_upload(e, dAsrc, (int) ldAsrc, x->dB, (int) x->ldb, x->dC, (int) x->ldc, st);
         if (rc) return rc;
         x->built_mode = -1;
