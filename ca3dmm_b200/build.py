@@ -21,6 +21,7 @@ C_SOURCES = ["vcomm.c", "partition.c", "dev_type.c", "mat_redist.c", "cannon.c",
              "grouped.c", "autotune.c"]
 CU_SOURCES = ["k_dgemm.cu", "k_pack.cu", "k_ozaki.cu", "k_noalloc.cu", "k_mlp.cu"]
 HEADERS = ["ca3dmm_kernels.h", "ca3dmm_ozaki.h", "ca3dmm_util.h", "k_common.cuh"]
+EXAMPLES = ["example_cholesky_qr"]
 
 
 def _newer(target, deps):
@@ -59,6 +60,14 @@ def build(verbose=False):
                                   "-I", INC, "-I", CSRC, "-c", s, "-o", o])
     if _newer(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs + ["-lm"])
+    # example callers (C programs linking the library like the reference's examples)
+    for ex in EXAMPLES:
+        s = os.path.join(HERE, "examples", ex + ".c")
+        b = os.path.join(HERE, "examples", ex)
+        if _newer(b, [s, LIB] + hdrs):
+            _run(["gcc", "-O2", "-std=gnu11", "-I", INC, "-I", os.path.join(CUDA, "include"), s,
+                  "-o", b, "-L", HERE, "-lca3dmm_b200", "-Wl,-rpath,$ORIGIN/..",
+                  "-L", os.path.join(CUDA, "lib64"), "-lcudart", "-lm"])
     if verbose:
         print("built", LIB)
     return LIB
