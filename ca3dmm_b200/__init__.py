@@ -267,6 +267,10 @@ class Ca3dmmEngine:
     def set_stream(self, stream, sync=1):
         lib().ca3dmm_engine_set_stream(self.e, C.c_void_p(stream), int(sync))
 
+    def set_raster(self, raster):
+        """Tile rows per raster band of the GEMM tile order (L2 reuse)."""
+        return lib().ca3dmm_engine_set_raster(self.e, int(raster))
+
     def required_workbuf_bytes(self):
         return lib().ca3dmm_engine_workbuf_bytes(self.e)
 
