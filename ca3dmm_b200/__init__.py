@@ -21,6 +21,8 @@ DEFAULT_COST_MODEL = os.path.join(HERE, "data", "costmodel_b200.txt")
 
 DEV_TYPE_HOST, DEV_TYPE_CUDA, DEV_TYPE_CUDA_MPI_DIRECT = 0, 1, 2
 GEMM_PLAIN, GEMM_OZAKI = 0, 1
+# return codes of the C ABI (ca3dmm_kernels.h)
+OK, EINVAL, ECUDA, ETIMEOUT, ENOMEM, ENODEV = 0, 1, 2, 3, 4, 5
 ERRORS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "device wait timed out",
           4: "out of memory", 5: "no device"}
 
@@ -151,6 +153,7 @@ def lib():
         "ca3dmm_mlp_load": (i, [C.c_char_p, C.POINTER(p)]),
         "ca3dmm_kernel_launches": (C.c_ulonglong, []),
         "ca3dmm_engine_exec_host": (i, [EP, p, i, p, i, p, i]),
+        "ca3dmm_device_wait_check": (i, [d, i]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -175,6 +178,11 @@ class VComm:
                 lib().ca3dmm_vcomm_free(C.byref(self.h))
         except Exception:
             pass
+
+
+def device_wait_check(timeout_s, arrive):
+    """ca3dmm_device_wait_check: 0, or ETIMEOUT when the bounded wait ran out."""
+    return int(lib().ca3dmm_device_wait_check(float(timeout_s), int(arrive)))
 
 
 def kernel_launches():

@@ -154,3 +154,43 @@ extern "C" int ca3dmm_reduce_slabs_launch(const double *slab, long long slab_str
     ca3dmm_note_launch(1);
     return CA3DMM_OK;
 }
+
+// Diagnostic of the bounded device wait every kernel of the library uses:
+// thread 0 waits on an mbarrier that is completed (arrive != 0) or that
+// nothing ever completes; the wait returns by itself after limit_ns.
+__global__ void wait_check_kernel(int *status, unsigned long long limit_ns, int arrive)
+{
+    __shared__ uint64_t bar;
+    __shared__ volatile int abort_flag;
+    if (threadIdx.x == 0) {
+        mbar_init(&bar, 1);
+        abort_flag = 0;
+        fence_barrier_init();
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        if (arrive) mbar_arrive(&bar);
+        if (mbar_wait_bounded(&bar, 0, &abort_flag, status, CA3DMM_DEV_TIMEOUT_QUEUE, limit_ns))
+            status[1] = 1;
+    }
+}
+
+extern "C" int ca3dmm_device_wait_check(double timeout_s, int arrive)
+{
+    if (!(timeout_s >= 0.0) || timeout_s > 60.0) return CA3DMM_EINVAL;
+    int *d = nullptr, h[2] = {0, 0};
+    CA3DMM_CUDA_TRY(cudaMalloc(&d, 2 * sizeof(int)));
+    int rc = CA3DMM_OK;
+    if (cudaMemset(d, 0, 2 * sizeof(int)) != cudaSuccess) rc = CA3DMM_ECUDA;
+    if (!rc) {
+        wait_check_kernel<<<1, 32>>>(d, (unsigned long long) (timeout_s * 1e9), arrive ? 1 : 0);
+        ca3dmm_note_launch(1);
+        if (cudaGetLastError() != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess ||
+            cudaMemcpy(h, d, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess)
+            rc = CA3DMM_ECUDA;
+    }
+    cudaFree(d);
+    if (rc) return rc;
+    if (h[0] != 0) return CA3DMM_ETIMEOUT;
+    return h[1] ? CA3DMM_OK : CA3DMM_ECUDA;
+}

@@ -170,6 +170,13 @@ void ca3dmm_engine_print_stat(ca3dmm_engine_p engine);
 int ca3dmm_engine_exec_host(ca3dmm_engine_p engine, const void *A_h, int ldA, const void *B_h,
                             int ldB, void *C_h, int ldC);
 
+/* Diagnostic of the bounded device waits used by every kernel of the library
+ * (each returns an error status instead of hanging when its partner never
+ * arrives): one thread waits on a device barrier that is completed
+ * (arrive != 0) or never completed (arrive == 0).  Returns CA3DMM_OK, or
+ * CA3DMM_ETIMEOUT after about timeout_s (<= 60 s); the device stays usable. */
+int ca3dmm_device_wait_check(double timeout_s, int arrive);
+
 /* Kernels this library has launched since it was loaded, counted on the
  * host at each launch (a launch recorded into a CUDA graph counts once, at
  * capture; its replays do not). */
