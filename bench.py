@@ -263,7 +263,7 @@ def grouped_problems(nprob, seed=2024):
 
 
 def run_grouped(args, world, rank, local):
-    """Configuration 4: one persistent grouped launch (captured in a CUDA graph)
+    """256 uneven GEMMs: one persistent grouped launch (captured in a CUDA graph)
     against one plain DMMA launch per GEMM."""
     import torch
     import ca3dmm_b200 as cb

@@ -106,7 +106,7 @@ def main():
     ap.add_argument("--lo", type=int, default=128)
     ap.add_argument("--hi", type=int, default=16384)
     ap.add_argument("--epochs", type=int, default=300)
-    ap.add_argument("--out", default="gpurun_out")
+    ap.add_argument("--out", default="costmodel_out")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     tr = shapes(a.train, 11, a.lo, a.hi)

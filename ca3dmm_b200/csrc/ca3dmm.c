@@ -46,6 +46,7 @@ typedef struct {
 
 typedef struct {
     int ngroup, nA, nB;
+    int tmn, tnn;             /* row / column blocks of the internal grouping (1: merged) */
     group_t *groups;
     blk_t *A, *B;
     /* work buffer layout (byte offsets) */
@@ -205,8 +206,14 @@ static int plan_build(ca3dmm_engine_p e)
     plan_t *pl = (plan_t *) calloc(1, sizeof(plan_t));
     if (!pl) return CA3DMM_ENOMEM;
     e->impl = pl;
-    const int tmn = e->mp > e->np && !e->is_BTB ? e->mp / e->np : 1;
-    const int tnn = e->np > e->mp && !e->is_BTB ? e->np / e->mp : 1;
+    /* One GEMM per k-slab over the whole C: the reference's task_m / task_n
+     * replication groups (src/ca3dmm.c:155-169) compute disjoint blocks of the
+     * same slab product, and every C entry is the same k-ordered dot product
+     * whichever block holds it, so on one GPU the blocks merge; fewer, larger
+     * GEMMs leave fewer partial edge tiles. */
+    const int tmn = 1, tnn = 1;
+    pl->tmn = tmn;
+    pl->tnn = tnn;
     const int kp = e->kp;
     pl->nA = tmn * kp;
     pl->nB = tnn * kp;
@@ -737,8 +744,7 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
          * reduction launch) -- when the chained units still give every SM
          * several output tiles; otherwise (e.g. B^T B with a small C) each
          * slab is its own unit and the slab reduction runs after the GEMM. */
-        const int tmn = e->mp > e->np && !e->is_BTB ? e->mp / e->np : 1;
-        const int tnn = e->np > e->mp && !e->is_BTB ? e->np / e->mp : 1;
+        const int tmn = pl->tmn, tnn = pl->tnn;
         long long unit_tiles = 0;
         for (int u = 0; u < tmn * tnn; u++) {
             const group_t *g = &pl->groups[u];
@@ -946,8 +952,7 @@ static int hx_create(ca3dmm_engine_p e, struct host_exec **out)
 static int hx_build_bands(ca3dmm_engine_p e, struct host_exec *x, cudaStream_t st)
 {
     plan_t *pl = (plan_t *) e->impl;
-    const int tmn = e->mp > e->np && !e->is_BTB ? e->mp / e->np : 1;
-    const int tnn = e->np > e->mp && !e->is_BTB ? e->np / e->mp : 1;
+    const int tmn = pl->tmn, tnn = pl->tnn;
     const int whole = pl->has_dst && pl->dst_srow == 0 && pl->dst_scol == 0 &&
                       pl->dst_nrow == e->m && pl->dst_ncol == e->n;
     const int ozaki = e->gemm_mode == CA3DMM_GEMM_OZAKI;

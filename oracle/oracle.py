@@ -81,13 +81,13 @@ def uniform01(h):
 
 
 def gen_uniform(seed, nrow, ncol):
-    """Entries uniform in [-1, 1) (configuration 1)."""
+    """Entries uniform in [-1, 1) (the 2048^3 example workload)."""
     return np.asfortranarray(2.0 * uniform01(hash_grid(seed, nrow, ncol)) - 1.0)
 
 
 def gen_signed_exp(seed, nrow, ncol, emin=-8, emax=8, unit=False):
-    """sign * (1 + u) * 2^e with integer e uniform in [emin, emax] (configuration 2);
-    unit=True gives u' * 2^e with u' uniform in [-1, 1) (configuration 4)."""
+    """sign * (1 + u) * 2^e with integer e uniform in [emin, emax] (the 8000^3 workload);
+    unit=True gives u' * 2^e with u' uniform in [-1, 1) (the uneven batched GEMMs)."""
     u = uniform01(hash_grid(seed, nrow, ncol))
     h2 = hash_grid(seed, nrow, ncol, salt=0xD6E8FEB86659FD93)
     e = ((h2 >> np.uint64(32)) % np.uint64(emax - emin + 1)).astype(np.int64) + emin
@@ -98,7 +98,7 @@ def gen_signed_exp(seed, nrow, ncol, emin=-8, emax=8, unit=False):
 
 
 def gen_btb(seed, nrow, ncol):
-    """Column j ~ N(0, 1) * 10^{u_j}, u_j uniform in [-3, 3] (configuration 3)."""
+    """Column j ~ N(0, 1) * 10^{u_j}, u_j uniform in [-3, 3] (the tall-skinny B^T B workload)."""
     u1 = uniform01(hash_grid(seed, nrow, ncol))
     u2 = uniform01(hash_grid(seed, nrow, ncol, salt=0x5851F42D4C957F2D))
     z = np.sqrt(-2.0 * np.log1p(-u1)) * np.cos(2.0 * np.pi * u2)

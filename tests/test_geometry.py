@@ -47,17 +47,17 @@ def test_vrank_geometry_matches_oracle(m, n, k, p, ta, tb, grid):
     e.free()
 
 
-def test_config2_matches_readme():
+def test_8000cube_24_ranks_matches_readme():
     e = cb.Ca3dmmEngine(8000, 8000, 8000, 0, 0, p=24, caller_workbuf=True)
     s = e.s
-    # README.md:66-67 and SURVEY a4: task_m_num = 2, Cannon 2 x 2, per-rank blocks
+    # README.md:66-67: task_m_num = 2, Cannon 2 x 2, per-rank blocks
     assert (s.mp, s.np, s.kp) == (4, 2, 3)
     assert (s.task_m_num, s.task_n_num, s.task_k_num) == (2, 1, 3)
     assert (s.A_2dmm_nrow, s.A_2dmm_ncol) == (2000, 1334)
     assert (s.B_rd_nrow, s.B_rd_ncol) == (1334, 2000)
     assert (s.B_2dmm_nrow, s.B_2dmm_ncol) == (1334, 4000)
     assert (s.C_2dmm_nrow, s.C_2dmm_ncol) == (2000, 4000)
-    assert s.n_group == 6
+    assert s.n_group == 3          # one grouped GEMM per k-slab (task_m blocks merged on one GPU)
 
 
 def test_btb_grid_default_fold_and_forced():
