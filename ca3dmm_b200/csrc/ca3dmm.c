@@ -50,7 +50,7 @@ typedef struct {
     group_t *groups;
     blk_t *A, *B;
     /* work buffer layout (byte offsets) */
-    size_t off_status, off_packA, off_packB, off_copy, off_gemm, off_ozplan;
+    size_t off_status, off_packA, off_packB, off_copy, off_tmapA, off_tmapB, off_gemm, off_ozplan;
     size_t off_A, off_B, off_slab, off_cout, off_oz, total;
     size_t gemm_plan_bytes, oz_plan_bytes, oz_bytes;
     long long slab_ld;        /* leading dimension of each C slab */
@@ -65,6 +65,7 @@ typedef struct {
     void *c_dst;
     int gemm_tiles;
     int pack_tiles_A, pack_tiles_B, pack_tiles_C;
+    int packA_tma, packB_tma;     /* transposing packs staged by TMA (tensor maps in the plan) */
     /* dst_C block */
     int has_dst, dst_srow, dst_nrow, dst_scol, dst_ncol;
     cudaEvent_t ev[5];
@@ -161,6 +162,8 @@ static void plan_layout(ca3dmm_engine_p e, plan_t *pl)
     pl->off_packA = off; off = align_up(off + sizeof(ca3dmm_pack_desc_t) * pl->nA);
     pl->off_packB = off; off = align_up(off + sizeof(ca3dmm_pack_desc_t) * pl->nB);
     pl->off_copy = off; off = align_up(off + sizeof(ca3dmm_pack_desc_t));
+    pl->off_tmapA = off; off = align_up(off + 128 * (size_t) pl->nA);
+    pl->off_tmapB = off; off = align_up(off + 128 * (size_t) pl->nB);
     pl->gemm_plan_bytes = ca3dmm_dgemm_plan_bytes(pl->ngroup);
     pl->off_gemm = off; off = align_up(off + pl->gemm_plan_bytes);
     pl->oz_plan_bytes = ca3dmm_oz_plan_bytes(pl->ngroup);
@@ -658,7 +661,12 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
             d->rows = 0;
         }
     }
-    pl->pack_tiles_A = ca3dmm_pack_tiles(pa, pl->nA);
+    pl->packA_tma = 0;
+    if (e->trans_A && ca3dmm_pack_tma_prepare(pa, pl->nA, (const double *) A, h + pl->off_tmapA,
+                                              &pl->pack_tiles_A) == CA3DMM_OK)
+        pl->packA_tma = 1;
+    else
+        pl->pack_tiles_A = ca3dmm_pack_tiles(pa, pl->nA);
     ca3dmm_pack_desc_t *pb = (ca3dmm_pack_desc_t *) (h + pl->off_packB);
     for (int i = 0; i < pl->nB; i++) {
         blk_t *b = &pl->B[i];
@@ -677,7 +685,12 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
             d->rows = 0;
         }
     }
-    pl->pack_tiles_B = ca3dmm_pack_tiles(pb, pl->nB);
+    pl->packB_tma = 0;
+    if (e->trans_B && ca3dmm_pack_tma_prepare(pb, pl->nB, (const double *) B, h + pl->off_tmapB,
+                                              &pl->pack_tiles_B) == CA3DMM_OK)
+        pl->packB_tma = 1;
+    else
+        pl->pack_tiles_B = ca3dmm_pack_tiles(pb, pl->nB);
     /* output target of the GEMM (kp == 1) or of the reduction (kp > 1) */
     int whole = pl->has_dst && pl->dst_srow == 0 && pl->dst_scol == 0 && pl->dst_nrow == e->m &&
                 pl->dst_ncol == e->n;
@@ -785,6 +798,23 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
     return CA3DMM_OK;
 }
 
+/* Pack the op(A) (which = 0) or op(B) (which = 1) blocks that are not read in
+ * place: TMA-staged transposes when the plan prepared them, else the plain
+ * pack kernel. */
+static int launch_pack_side(ca3dmm_engine_p e, int which, const void *src, cudaStream_t st)
+{
+    plan_t *pl = (plan_t *) e->impl;
+    char *w = (char *) e->workbuf_d;
+    const size_t off_desc = which ? pl->off_packB : pl->off_packA;
+    const int nd = which ? pl->nB : pl->nA, tiles = which ? pl->pack_tiles_B : pl->pack_tiles_A;
+    if (which ? pl->packB_tma : pl->packA_tma)
+        return ca3dmm_pack_tma_launch(w + (which ? pl->off_tmapB : pl->off_tmapA),
+                                      (const ca3dmm_pack_desc_t *) (w + off_desc), nd, tiles,
+                                      (double *) w, (int *) (w + pl->off_status), 5.0, st);
+    return ca3dmm_pack_launch((const double *) src, (double *) w,
+                              (const ca3dmm_pack_desc_t *) (w + off_desc), nd, tiles, st);
+}
+
 static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void *src_B, int ldB,
                        void *dst_C, int ldC, cudaStream_t st)
 {
@@ -815,13 +845,9 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
         rc = ca3dmm_oz_run_pack(&pl->oz, src_A, src_B, st);
         if (rc) return rc;
     } else {
-        rc = ca3dmm_pack_launch((const double *) src_A, (double *) w,
-                                (const ca3dmm_pack_desc_t *) (w + pl->off_packA), pl->nA,
-                                pl->pack_tiles_A, st);
+        rc = launch_pack_side(e, 0, src_A, st);
         if (rc) return rc;
-        rc = ca3dmm_pack_launch((const double *) src_B, (double *) w,
-                                (const ca3dmm_pack_desc_t *) (w + pl->off_packB), pl->nB,
-                                pl->pack_tiles_B, st);
+        rc = launch_pack_side(e, 1, src_B, st);
         if (rc) return rc;
     }
     if (timing) cudaEventRecord(pl->ev[1], st);
@@ -1148,8 +1174,7 @@ static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_
         rc = ca3dmm_oz_clear(&pl->oz, st);
         if (!rc) rc = ca3dmm_oz_slice_side(&pl->oz, 1, x->dB, st);
     } else {
-        rc = ca3dmm_pack_launch(x->dB, (double *) w, (const ca3dmm_pack_desc_t *) (w + pl->off_packB),
-                                pl->nB, pl->pack_tiles_B, st);
+        rc = launch_pack_side(e, 1, x->dB, st);
     }
     if (rc) return rc;
     for (int c = 0; c < x->nband; c++) {

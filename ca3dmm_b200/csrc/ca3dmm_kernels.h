@@ -70,6 +70,19 @@ typedef struct {
     int tile_begin;          /* first 64 x 64 tile of this block (set by ca3dmm_pack_tiles) */
 } ca3dmm_pack_desc_t;
 
+/* Transposing packs whose source blocks are 16-byte aligned with an even
+ * leading dimension run staged through shared memory by TMA:
+ * ca3dmm_pack_tma_prepare encodes one tensor map per descriptor into
+ * host_tmaps (128 B each; the caller uploads them 64-byte aligned) and sets
+ * the descriptors' tile_begin for that kernel's 64 x 16 tiles; it returns
+ * CA3DMM_EINVAL when a descriptor is not eligible (then use
+ * ca3dmm_pack_tiles + ca3dmm_pack_launch). */
+int ca3dmm_pack_tma_prepare(ca3dmm_pack_desc_t *descs, int ndesc, const double *src_base,
+                            void *host_tmaps, int *total_tiles);
+int ca3dmm_pack_tma_launch(const void *dev_tmaps, const ca3dmm_pack_desc_t *dev_descs, int ndesc,
+                           int total_tiles, double *dst_base, int *dev_status, double timeout_s,
+                           cudaStream_t stream);
+
 /* Assign each descriptor its range of 64 x 64 tiles; returns the total. */
 int ca3dmm_pack_tiles(ca3dmm_pack_desc_t *descs, int ndesc);
 /* One launch over the flat tile list of all descriptors (any mix of sizes and

@@ -7,6 +7,8 @@
 //     reduce-scatter with mpi_op_omp_sum (src/ca3dmm.c:1287-1343,
 //     src/mpi_op_omp.c:6-23), summing slabs in rank order.
 #include <atomic>
+#include <cstring>
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include "k_common.cuh"
 #include "ca3dmm_kernels.h"
@@ -29,7 +31,7 @@ __device__ __forceinline__ int find_desc(const ca3dmm_pack_desc_t *d, int n, int
 // Copy: thread -> (row, 16 columns), reads and writes run down the columns.
 // Transpose: through a padded shared tile; reads run along the source's
 // contiguous index, writes along the destination's.
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, 3)
 pack_kernel(const double *__restrict__ src_base, double *__restrict__ dst_base,
             const ca3dmm_pack_desc_t *__restrict__ descs, int ndesc, int total_tiles)
 {
@@ -56,16 +58,119 @@ pack_kernel(const double *__restrict__ src_base, double *__restrict__ dst_base,
             }
             continue;
         }
-        // dst (rows x cols) = transpose of the source block (cols x rows)
-        __syncthreads();
-        for (int e = threadIdx.x; e < PT * PT; e += blockDim.x) {
+        // dst (rows x cols) = transpose of the source block (cols x rows); the
+        // 16 loads of a thread are all in flight before the shared stores
+        double v[PT * PT / 256];
+#pragma unroll
+        for (int i = 0; i < PT * PT / 256; ++i) {
+            const int e = threadIdx.x + 256 * i;
             const int c = c0 + (e & 63), r = r0 + (e >> 6);
-            if (c < d.cols && r < d.rows) tile[e >> 6][e & 63] = __ldg(src + c + (long long) r * d.lds);
+            v[i] = (c < d.cols && r < d.rows) ? __ldg(src + c + (long long) r * d.lds) : 0.0;
         }
         __syncthreads();
-        for (int e = threadIdx.x; e < PT * PT; e += blockDim.x) {
+#pragma unroll
+        for (int i = 0; i < PT * PT / 256; ++i) {
+            const int e = threadIdx.x + 256 * i;
+            tile[e >> 6][e & 63] = v[i];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < PT * PT / 256; ++i) {
+            const int e = threadIdx.x + 256 * i;
             const int r = r0 + (e & 63), c = c0 + (e >> 6);
             if (r < d.rows && c < d.cols) dst[r + (long long) c * d.ldd] = tile[e & 63][e >> 6];
+        }
+    }
+}
+
+// Transposing pack staged through shared memory by TMA: tiles of 64
+// destination rows x 64 destination columns arrive as four 16 x 64 boxes of
+// the source (16 contiguous doubles = one 128-byte box row, so 512
+// contiguous source bytes per row and tile) with the 128-byte swizzle,
+// TT_STAGES tiles ahead of the threads that write them out.  A thread reads
+// 16-byte chunks (two destination columns of one row): 32 threads of
+// consecutive rows hit eight distinct swizzled chunks, the minimum four
+// wavefronts; the writes run down the destination columns.
+constexpr int TT_R = 64, TT_BOX = 16, TT_NBOX = 4, TT_C = TT_BOX * TT_NBOX, TT_STAGES = 4;
+constexpr int TT_BOX_BYTES = TT_R * TT_BOX * (int) sizeof(double);   // 8 KB
+constexpr int TT_BYTES = TT_BOX_BYTES * TT_NBOX;                       // 32 KB
+constexpr int TT_SMEM = TT_STAGES * TT_BYTES + 1024;
+
+__device__ __forceinline__ void tt_tile(const ca3dmm_pack_desc_t &d, int t, int &r0, int &c0)
+{
+    const int local = t - d.tile_begin, tr = (d.rows + TT_R - 1) / TT_R;
+    r0 = (local % tr) * TT_R;
+    c0 = (local / tr) * TT_C;
+}
+
+__global__ void __launch_bounds__(256)
+pack_transpose_tma_kernel(const CUtensorMap *__restrict__ tmaps,
+                          const ca3dmm_pack_desc_t *__restrict__ descs, int ndesc, int total_tiles,
+                          double *__restrict__ dst_base, int *status, unsigned long long limit_ns)
+{
+    extern __shared__ unsigned char tt_raw[];
+    unsigned char *sm = reinterpret_cast<unsigned char *>(
+        (reinterpret_cast<uintptr_t>(tt_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ uint64_t full[TT_STAGES];
+    __shared__ volatile int abort_flag;
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TT_STAGES; ++s) mbar_init(&full[s], 1);
+        abort_flag = 0;
+        fence_barrier_init();
+    }
+    __syncthreads();
+    const int mine = blockIdx.x < total_tiles ? (total_tiles - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+    int issued = 0;
+    auto issue = [&](int i) {
+        const int t = blockIdx.x + i * gridDim.x;
+        const int j = find_desc(descs, ndesc, t);
+        int r0, c0;
+        tt_tile(descs[j], t, r0, c0);
+        tmap_acquire(tmaps + j);
+        const int s = i % TT_STAGES;
+        mbar_arrive_expect_tx(&full[s], TT_BYTES);
+#pragma unroll
+        for (int b = 0; b < TT_NBOX; ++b)
+            tma_load_2d(sm + s * TT_BYTES + b * TT_BOX_BYTES, tmaps + j, c0 + b * TT_BOX, r0, &full[s]);
+    };
+    if (threadIdx.x == 0)
+        for (; issued < mine && issued < TT_STAGES; ++issued) issue(issued);
+    const int r = threadIdx.x & (TT_R - 1), q0 = threadIdx.x >> 6;
+    bool ok = true;
+    for (int i = 0; i < mine && ok; ++i) {
+        const int s = i % TT_STAGES;
+        if (!mbar_wait_bounded(&full[s], (uint32_t) (i / TT_STAGES) & 1u, &abort_flag, status,
+                               CA3DMM_DEV_TIMEOUT_CONSUME, limit_ns)) {
+            ok = false;
+            break;
+        }
+        const int t = blockIdx.x + i * gridDim.x;
+        const ca3dmm_pack_desc_t d = descs[find_desc(descs, ndesc, t)];
+        int r0, c0;
+        tt_tile(d, t, r0, c0);
+        double *dst = reinterpret_cast<double *>(reinterpret_cast<uintptr_t>(dst_base) +
+                                                 (uintptr_t) d.dst_off * sizeof(double));
+        const unsigned char *row = sm + s * TT_BYTES + r * 128;
+#pragma unroll
+        for (int h = 0; h < TT_C / 8; ++h) {
+            const int q = q0 + 4 * h;                       // chunk: columns 2q, 2q + 1
+            const double2 v = *reinterpret_cast<const double2 *>(
+                row + (q >> 3) * TT_BOX_BYTES + (((q & 7) ^ (r & 7)) << 4));
+            const int gr = r0 + r, gc = c0 + 2 * q;
+            if (gr < d.rows) {
+                if (gc < d.cols) dst[gr + (long long) gc * d.ldd] = v.x;
+                if (gc + 1 < d.cols) dst[gr + (long long) (gc + 1) * d.ldd] = v.y;
+            }
+        }
+        __syncthreads();                                     // stage s read by every thread
+        if (threadIdx.x == 0 && issued < mine) issue(issued++);
+    }
+    if (threadIdx.x == 0 && !ok) {
+        // let the copies this CTA issued land before its shared memory is released
+        for (int i = 0; i < issued; ++i) {
+            const uint64_t t0 = global_timer_ns();
+            while (!mbar_try_wait(&full[i % TT_STAGES], (uint32_t) (i / TT_STAGES) & 1u))
+                if (global_timer_ns() - t0 > limit_ns) break;
         }
     }
 }
@@ -132,6 +237,55 @@ extern "C" int ca3dmm_pack_launch(const double *src_base, double *dst_base,
     int grid = ca3dmm_device_sm_count() * 8;
     if (grid > total_tiles) grid = total_tiles;
     pack_kernel<<<grid, 256, 0, stream>>>(src_base, dst_base, dev_descs, ndesc, total_tiles);
+    CA3DMM_CUDA_TRY(cudaGetLastError());
+    ca3dmm_note_launch(1);
+    return CA3DMM_OK;
+}
+
+extern "C" int ca3dmm_encode_tmap_2d(void *tmap, int dtype_bytes, const void *base,
+                                     unsigned long long dim0, unsigned long long dim1,
+                                     unsigned long long stride1_bytes, unsigned box0,
+                                     unsigned box1, int swizzle128);
+
+extern "C" int ca3dmm_pack_tma_prepare(ca3dmm_pack_desc_t *descs, int ndesc, const double *src_base,
+                                       void *host_tmaps, int *total_tiles)
+{
+    CUtensorMap *tm = static_cast<CUtensorMap *>(host_tmaps);
+    int tiles = 0;
+    for (int j = 0; j < ndesc; ++j) {
+        ca3dmm_pack_desc_t &d = descs[j];
+        memset(&tm[j], 0, sizeof(CUtensorMap));
+        d.tile_begin = tiles;
+        if (d.rows <= 0 || d.cols <= 0) continue;
+        const double *b = src_base + d.src_off;
+        if (!d.trans || (d.lds & 1) || (reinterpret_cast<uintptr_t>(b) & 15)) return CA3DMM_EINVAL;
+        // source block: cols contiguous doubles per row, rows rows lds apart
+        const int rc = ca3dmm_encode_tmap_2d(&tm[j], 8, b, (unsigned long long) d.cols,
+                                             (unsigned long long) d.rows,
+                                             (unsigned long long) d.lds * 8, TT_BOX, TT_R, 1);
+        if (rc) return rc;
+        tiles += ((d.rows + TT_R - 1) / TT_R) * ((d.cols + TT_C - 1) / TT_C);
+    }
+    *total_tiles = tiles;
+    return CA3DMM_OK;
+}
+
+extern "C" int ca3dmm_pack_tma_launch(const void *dev_tmaps, const ca3dmm_pack_desc_t *dev_descs,
+                                      int ndesc, int total_tiles, double *dst_base,
+                                      int *dev_status, double timeout_s, cudaStream_t stream)
+{
+    if (ndesc <= 0 || total_tiles <= 0) return CA3DMM_OK;
+    static bool attr_done = false;
+    if (!attr_done) {
+        CA3DMM_CUDA_TRY(cudaFuncSetAttribute(pack_transpose_tma_kernel,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, TT_SMEM));
+        attr_done = true;
+    }
+    int grid = ca3dmm_device_sm_count();
+    if (grid > total_tiles) grid = total_tiles;
+    pack_transpose_tma_kernel<<<grid, 256, TT_SMEM, stream>>>(
+        static_cast<const CUtensorMap *>(dev_tmaps), dev_descs, ndesc, total_tiles, dst_base,
+        dev_status, (unsigned long long) (timeout_s * 1e9));
     CA3DMM_CUDA_TRY(cudaGetLastError());
     ca3dmm_note_launch(1);
     return CA3DMM_OK;
