@@ -96,7 +96,7 @@ struct host_exec {
     ca3dmm_tile_ranges_t rng[HX_MAX_BANDS];
     void *desc_h, *desc_d;        /* per-band A descriptors (pack or slicing) */
     size_t desc_stride;
-    int ndesc, ntile[HX_MAX_BANDS];
+    int ndesc, ntile[HX_MAX_BANDS][2];  /* per band: Ozaki exponent items + slicing tiles, or pack tiles */
     int built_mode, built_slices, built_raster;
     int ok;                       /* streams and events created */
 };
@@ -1048,7 +1048,7 @@ static int hx_build_bands(ca3dmm_engine_p e, struct host_exec *x, cudaStream_t s
             for (int tk = 0; tk < e->kp; tk++) blocks[tk] = tk * tmn + tm;
             if (ozaki) {
                 bad = ca3dmm_oz_encode_rows((char *) pl->stage + pl->off_ozplan, pl->ngroup, blocks,
-                                            e->kp, r, rend, dh, &x->ntile[c]);
+                                            e->kp, r, rend, dh, x->ntile[c]);
             } else {
                 ca3dmm_pack_desc_t *pd = (ca3dmm_pack_desc_t *) dh;
                 for (int tk = 0; tk < e->kp; tk++) {
@@ -1062,7 +1062,7 @@ static int hx_build_bands(ca3dmm_engine_p e, struct host_exec *x, cudaStream_t s
                     d->dst_off = (long long) (b->off / sizeof(double)) + r;
                     d->ldd = b->ld;
                 }
-                x->ntile[c] = ca3dmm_pack_tiles(pd, e->kp);
+                x->ntile[c][0] = ca3dmm_pack_tiles(pd, e->kp);
             }
         }
     }
@@ -1185,7 +1185,7 @@ static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_
             if (!rc) rc = ca3dmm_oz_run_gemm_ranges(&pl->oz, &x->rng[c], status_d, 5.0, st);
         } else {
             rc = ca3dmm_pack_launch(x->dA, (double *) w, (const ca3dmm_pack_desc_t *) dd, x->ndesc,
-                                    x->ntile[c], st);
+                                    x->ntile[c][0], st);
             if (!rc)
                 rc = ca3dmm_dgemm_launch_ranges(w + pl->off_gemm, pl->ngroup, &x->rng[c], status_d,
                                                 5.0, st);

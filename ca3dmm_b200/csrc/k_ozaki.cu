@@ -11,8 +11,9 @@
 //                         32-byte k-block, the s slices are contiguous, each a
 //                         K-major rows x 32-byte tile with the 32-byte swizzle
 //                         (16-byte chunk ^= (row >> 2) & 1) already applied.
-//                         HBM-bound; transposes through shared memory when the
-//                         source is k-strided.
+//                         HBM-bound; reads k-contiguous sources with 16-byte
+//                         loads per thread, transposes rows-contiguous ones
+//                         through shared memory.
 //  3. oz_gemm_kernel   -- tcgen05.mma kind::i8 (signed x signed), M=128 x K=32,
 //                         N = 64 per slice pair, up to four pairs of one A slice
 //                         fused into one N <= 256 MMA.  All s diagonal accumulators
@@ -62,14 +63,18 @@ constexpr int GROUP_M = 8;
 constexpr int EXP_BIAS = 2048;                   // stored exponent = E + bias, 0 = all-zero row
 
 // Slicing descriptor: block rows r in [0,rows), k index l in [0,kz);
-// element (r,l) at src[src_off + r*rs + l*ls].
+// element (r,l) at src[src_off + r*rs + l*ls].  Exactly one of rs, ls is 1
+// for a column-major source (both when ld = 1): shape KC reads along k, RC
+// along rows.
 struct SliceDesc {
     long long src_off, rs, ls;
     long long q_off;        // byte offset of the block's tiled slices in the work region
     long long e_off;        // int offset of the exponents in the work region
     int rows, kz, kpad;     // kpad = kz rounded up to OKB
     int rows_pad, tile_rows, nkb;   // rows rounded up to tile_rows (128 for A, 64 for B)
-    int tile_begin;         // first 64 x 64 slicing tile of this block (per operand)
+    int tile_begin;         // first slicing tile of this block (per operand)
+    int xbegin;             // first exponent work item of this block (per operand)
+    int shape;              // SHAPE_KC or SHAPE_RC
     int pad;
 };
 
@@ -101,14 +106,40 @@ struct PlanHeader {
 };
 
 // ------------------------------------------------------------------ slicing
-constexpr int ST = 64;   // slicing tile edge (rows x k)
+constexpr int ST = 64;   // exponent tile edge of the RC shape (rows x k)
+constexpr int SHAPE_KC = 1, SHAPE_RC = 2;
+// KC (k contiguous): exponent items of 8 rows x 512 k (a warp reads 4 KB of one
+// row), slicing tiles of 16 rows x 256 k (a thread reads its own 16 k).
+// RC (rows contiguous): exponent tiles of 64 rows x 64 k, slicing tiles of
+// 128 rows x 32 k (one k-block) transposed through shared memory.
+// Long contiguous runs per warp matter on B200: 512-byte row pieces 8 MB apart
+// read at half the rate of 4 KB runs.
+constexpr int KC_XR = 8, KC_XK = 512, KC_SR = 16, KC_SK = 256;
+constexpr int RC_SR = 128, RC_SK = 32;
 
-__device__ __forceinline__ int find_slice_desc(const SliceDesc *d, int n, int tile)
+__host__ __device__ inline int exp_items_of(const SliceDesc &d)
+{
+    if (d.rows <= 0 || d.kz <= 0) return 0;
+    if (d.shape == SHAPE_KC) return ((d.rows + KC_XR - 1) / KC_XR) * ((d.kz + KC_XK - 1) / KC_XK);
+    return ((d.rows + ST - 1) / ST) * ((d.kz + ST - 1) / ST);
+}
+
+__host__ __device__ inline int slice_tiles_of(const SliceDesc &d)
+{
+    if (d.rows <= 0 || d.kz <= 0) return 0;
+    if (d.shape == SHAPE_KC) return ((d.rows_pad + KC_SR - 1) / KC_SR) * ((d.kpad + KC_SK - 1) / KC_SK);
+    return ((d.rows_pad + RC_SR - 1) / RC_SR) * ((d.kpad + RC_SK - 1) / RC_SK);
+}
+
+// The descriptor holding flat item t: the last one whose first item is <= t
+// (blocks without items share their first item with the next block).
+template <bool EXP>
+__device__ __forceinline__ int find_slice_desc(const SliceDesc *d, int n, int t)
 {
     int lo = 0, hi = n - 1;
     while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;
-        if (d[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
+        if ((EXP ? d[mid].xbegin : d[mid].tile_begin) <= t) lo = mid; else hi = mid - 1;
     }
     return lo;
 }
@@ -131,112 +162,96 @@ __host__ __device__ inline size_t maxbits_bytes(long long n_exp)
     return ((size_t) n_exp * sizeof(unsigned long long) + 255) / 256 * 256;
 }
 
-// Pass 1, persistent over the flat list of 64 x 64 (rows x k) tiles of every
-// block: per row, the largest |x| as its bit pattern (for non-negative doubles
-// the bit pattern orders like the value).  The effective exponent
+__device__ __forceinline__ unsigned long long abs_bits(double x)
+{
+    return (unsigned long long) __double_as_longlong(x) & 0x7fffffffffffffffull;
+}
+
+// Pass 1, persistent over the flat list of exponent items of every block: per
+// row, the largest |x| as its bit pattern (for non-negative doubles the bit
+// pattern orders like the value).  The effective exponent
 // E(x) = min{E : |x| <= 2^E 127/128} is non-decreasing in |x|, so the row's
 // exponent max_l E(x_l) is E(max_l |x_l|), formed once per row in pass 2.
 __global__ void __launch_bounds__(256)
 oz_exp_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ descs, int ndesc,
-              int total_tiles, unsigned long long *__restrict__ mwork)
+              int total_items, unsigned long long *__restrict__ mwork)
 {
     __shared__ unsigned long long part[4][ST];
-    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
-        const SliceDesc d = descs[find_slice_desc(descs, ndesc, tile)];
-        const int local = tile - d.tile_begin, tx = (d.rows_pad + ST - 1) / ST;
-        const int r0 = (local % tx) * ST, l0 = (local / tx) * ST;
-        const int rn = min(ST, d.rows - r0), ln = min(ST, d.kz - l0);
-        if (rn <= 0 || ln <= 0) continue;               // padding tile (uniform)
-        const double *base = slice_src(src, d.src_off) + (long long) r0 * d.rs + (long long) l0 * d.ls;
-        if (d.rs == 1) {
-            // rows contiguous: thread (row r, k phase g) walks k = g, g + 4, ...
-            const int r = threadIdx.x & (ST - 1), g = threadIdx.x >> 6;
+    for (int item = blockIdx.x; item < total_items; item += gridDim.x) {
+        const SliceDesc &d = descs[find_slice_desc<true>(descs, ndesc, item)];
+        const int local = item - d.xbegin;
+        if (d.shape == SHAPE_KC) {
+            // warp w: row r0 + w, k [l0, l0 + 512) as 16-byte loads (scalar when unaligned)
+            const int nkr = (d.kz + KC_XK - 1) / KC_XK, lane = threadIdx.x & 31;
+            const int r = (local / nkr) * KC_XR + (threadIdx.x >> 5), l0 = (local % nkr) * KC_XK;
             unsigned long long m = 0;
-            if (r < rn) {
+            if (r < d.rows) {
+                const double *row = slice_src(src, d.src_off) + (long long) r * d.rs + l0;
+                const int ln = d.kz - l0;
+                if (!(reinterpret_cast<uintptr_t>(row) & 15) && ln >= KC_XK) {
+                    double2 v[KC_XK / 64];
 #pragma unroll
-                for (int j = 0; j < ST / 4; ++j) {
-                    const int l = g + 4 * j;
-                    if (l < ln) {
-                        const unsigned long long v =
-                            (unsigned long long) __double_as_longlong(__ldg(base + r + (long long) l * d.ls)) &
-                            0x7fffffffffffffffull;
-                        m = v > m ? v : m;
+                    for (int i = 0; i < KC_XK / 64; ++i)
+                        v[i] = __ldg(reinterpret_cast<const double2 *>(row) + lane + 32 * i);
+#pragma unroll
+                    for (int i = 0; i < KC_XK / 64; ++i) {
+                        const unsigned long long a = abs_bits(v[i].x), b = abs_bits(v[i].y);
+                        m = a > m ? a : m;
+                        m = b > m ? b : m;
+                    }
+                } else {
+                    double v[KC_XK / 32];
+#pragma unroll
+                    for (int i = 0; i < KC_XK / 32; ++i) {
+                        const int l = lane + 32 * i;
+                        v[i] = l < ln ? __ldg(row + l) : 0.0;
+                    }
+#pragma unroll
+                    for (int i = 0; i < KC_XK / 32; ++i) {
+                        const unsigned long long a = abs_bits(v[i]);
+                        m = a > m ? a : m;
                     }
                 }
             }
-            __syncthreads();                             // part[] of the previous tile is read
-            part[g][r] = m;
-            __syncthreads();
-            if (threadIdx.x < rn) {
-                unsigned long long v = part[0][threadIdx.x];
 #pragma unroll
-                for (int q = 1; q < 4; ++q) v = part[q][threadIdx.x] > v ? part[q][threadIdx.x] : v;
-                if (v) atomicMax(mwork + d.e_off + r0 + threadIdx.x, v);
-            }
-        } else if (d.rs >= 65536) {
-            // k contiguous, rows at least 512 KB apart: warp w reads whole rows w,
-            // w + 8, ... (64 consecutive k; one row, so one page, per load)
-            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-            unsigned long long m[ST / 8];
-#pragma unroll
-            for (int j = 0; j < ST / 8; ++j) {
-                const int r = warp + 8 * j;
-                unsigned long long v0 = 0, v1 = 0;
-                if (r < rn) {
-                    const double *row = base + (long long) r * d.rs;
-                    if (lane < ln)
-                        v0 = (unsigned long long) __double_as_longlong(__ldg(row + (long long) lane * d.ls));
-                    if (lane + 32 < ln)
-                        v1 = (unsigned long long) __double_as_longlong(__ldg(row + (long long) (lane + 32) * d.ls));
-                }
-                v0 &= 0x7fffffffffffffffull;
-                v1 &= 0x7fffffffffffffffull;
-                m[j] = v1 > v0 ? v1 : v0;
-            }
-#pragma unroll
-            for (int j = 0; j < ST / 8; ++j) {
-                unsigned long long v = m[j];
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    const unsigned long long w = __shfl_xor_sync(0xffffffffu, v, o);
-                    v = w > v ? w : v;
-                }
-                const int r = warp + 8 * j;
-                if (lane == 0 && r < rn && v) atomicMax(mwork + d.e_off + r0 + r, v);
-            }
-        } else {
-            // k contiguous: thread (row t/4, quarter q = t%4) reads k = 2q + 8i, +1
-            // (i = 0..7), so the four threads of a row cover 64 contiguous bytes
-            // per load; the quarters combine with two shuffles
-            const int r = threadIdx.x >> 2, q = threadIdx.x & 3;
-            unsigned long long m = 0;
-            if (r < rn) {
-                const double *row = base + (long long) r * d.rs;
-#pragma unroll
-                for (int i = 0; i < ST / 8; ++i) {
-                    const int l = 2 * q + 8 * i;
-                    const unsigned long long v0 =
-                        l < ln ? (unsigned long long) __double_as_longlong(__ldg(row + (long long) l * d.ls)) : 0ull;
-                    const unsigned long long v1 =
-                        l + 1 < ln ? (unsigned long long) __double_as_longlong(__ldg(row + (long long) (l + 1) * d.ls)) : 0ull;
-                    const unsigned long long a = v0 & 0x7fffffffffffffffull, b = v1 & 0x7fffffffffffffffull;
-                    m = a > m ? a : m;
-                    m = b > m ? b : m;
-                }
-            }
-#pragma unroll
-            for (int o = 1; o < 4; o <<= 1) {
+            for (int o = 16; o > 0; o >>= 1) {
                 const unsigned long long w = __shfl_xor_sync(0xffffffffu, m, o);
                 m = w > m ? w : m;
             }
-            if (q == 0 && r < rn && m) atomicMax(mwork + d.e_off + r0 + r, m);
+            if (lane == 0 && r < d.rows && m) atomicMax(mwork + d.e_off + r, m);
+            continue;
+        }
+        // RC: 64 x 64 tile, thread (row r, k phase g) walks k = g, g + 4, ...
+        const int tx = (d.rows + ST - 1) / ST;
+        const int r0 = (local % tx) * ST, l0 = (local / tx) * ST;
+        const int rn = min(ST, d.rows - r0), ln = min(ST, d.kz - l0);
+        const double *base = slice_src(src, d.src_off) + r0 + (long long) l0 * d.ls;
+        const int r = threadIdx.x & (ST - 1), g = threadIdx.x >> 6;
+        unsigned long long m = 0;
+        if (r < rn) {
+#pragma unroll
+            for (int j = 0; j < ST / 4; ++j) {
+                const int l = g + 4 * j;
+                if (l < ln) {
+                    const unsigned long long v = abs_bits(__ldg(base + r + (long long) l * d.ls));
+                    m = v > m ? v : m;
+                }
+            }
+        }
+        __syncthreads();                             // part[] of the previous tile is read
+        part[g][r] = m;
+        __syncthreads();
+        if (threadIdx.x < rn) {
+            unsigned long long v = part[0][threadIdx.x];
+#pragma unroll
+            for (int q = 1; q < 4; ++q) v = part[q][threadIdx.x] > v ? part[q][threadIdx.x] : v;
+            if (v) atomicMax(mwork + d.e_off + r0 + threadIdx.x, v);
         }
     }
 }
 
-// Pass 2: slices of one 64 x 64 tile through shared memory.  Thread (row r,
-// 16-byte k chunk c) forms N = rint(x 2^(8S-1-E)) for its 16 elements; the
-// balanced digits q_t in [-128, 127] of N (least significant first:
+// Pass 2 for one (row, 16 consecutive k): N = rint(x 2^(8S-1-E)) per element;
+// the balanced digits q_t in [-128, 127] of N (least significant first:
 // q = ((N + 128) mod 256) - 128, N = (N - q) / 256) are exactly the bytes of
 // N + 0x80..80 (S bytes of 0x80) with the top bit flipped, because adding 128
 // to every digit of a balanced representation gives the unsigned base-256
@@ -244,80 +259,121 @@ oz_exp_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ desc
 // Slice t holds digit S-1-t.  The 16 bytes of each slice are gathered with
 // byte permutes and stored with the 32-byte swizzle of the GEMM's operand tile.
 template <int S>
+__device__ __forceinline__ void slice16(const SliceDesc &d, unsigned char *__restrict__ work,
+                                        const unsigned long long *__restrict__ mwork, int gr,
+                                        int gl, const double (&x)[16])
+{
+    const unsigned long long mb = gr < d.rows ? mwork[d.e_off + gr] : 0ull;
+    int E = 0;
+    if (mb) {
+        int ex;
+        const double mant = frexp(__longlong_as_double((long long) mb), &ex);
+        E = ex + (mant > 0.9921875 ? 1 : 0);
+    }
+    if (gl == 0 && gr < d.rows) reinterpret_cast<int *>(work)[d.e_off + gr] = mb ? E + EXP_BIAS : 0;
+    // x 2^(8S-1-E) as two exact power-of-two factors (each inside the normal range)
+    const int sh = 8 * S - 1 - E;
+    const double up1 = ldexp(1.0, sh / 2), up2 = ldexp(1.0, sh - sh / 2);
+    constexpr unsigned long long BIAS = 0x8080808080808080ull >> (64 - 8 * S);
+    uint32_t lo[16], hi[16];
+#pragma unroll
+    for (int j = 0; j < 16; ++j) {
+        const long long N = __double2ll_rn(x[j] * up1 * up2);
+        const unsigned long long U = (unsigned long long) N + BIAS;
+        lo[j] = (uint32_t) U;
+        hi[j] = (uint32_t) (U >> 32);
+    }
+    const int rt = gr / d.tile_rows, rr = gr % d.tile_rows;
+    const int kb = gl / OKB, chunk = (gl % OKB) >> 4;
+    const long long tile_bytes = (long long) d.tile_rows * OKB;
+    unsigned char *dst = work + d.q_off + ((long long) rt * d.nkb + kb) * S * tile_bytes +
+                         rr * OKB + ((chunk ^ ((rr >> 2) & 1)) << 4);
+#pragma unroll
+    for (int t = 0; t < S; ++t) {
+        const int b = S - 1 - t, bb = b & 3;
+        const uint32_t *w = b < 4 ? lo : hi;
+        const uint32_t sel = (uint32_t) bb | ((uint32_t) (bb + 4) << 4);
+        uint32_t out[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint32_t p01 = __byte_perm(w[4 * q], w[4 * q + 1], sel);
+            const uint32_t p23 = __byte_perm(w[4 * q + 2], w[4 * q + 3], sel);
+            out[q] = __byte_perm(p01, p23, 0x5410) ^ 0x80808080u;
+        }
+        *reinterpret_cast<uint4 *>(dst + t * tile_bytes) = make_uint4(out[0], out[1], out[2], out[3]);
+    }
+}
+
+// Pass 2 over the flat list of slicing tiles (padding rows and k included:
+// they hold zero digits).
+template <int S>
 __global__ void __launch_bounds__(256)
 oz_slice_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ descs, int ndesc,
                 int total_tiles, unsigned char *__restrict__ work,
                 const unsigned long long *__restrict__ mwork)
 {
-    __shared__ double tile[ST][ST + 1];
-    int *ework = reinterpret_cast<int *>(work);
-    for (int gtile = blockIdx.x; gtile < total_tiles; gtile += gridDim.x) {
-        const SliceDesc d = descs[find_slice_desc(descs, ndesc, gtile)];
-        const int local = gtile - d.tile_begin, tx = (d.rows_pad + ST - 1) / ST;
-        const int r0 = (local % tx) * ST, l0 = (local / tx) * ST;
-        const double *base = slice_src(src, d.src_off);
-        const bool rfast = d.rs == 1;
-        // all 16 loads of a thread in flight at once (compile-time trip count)
-        double x[ST * ST / 256];
+    __shared__ __align__(16) double tl[RC_SK][RC_SR];
+    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+        const SliceDesc &d = descs[find_slice_desc<false>(descs, ndesc, tile)];
+        const int local = tile - d.tile_begin;
+        double x[16];
+        if (d.shape == SHAPE_KC) {
+            // thread (row tid / 16, 16-k chunk tid % 16) reads its 128 contiguous bytes
+            const int nkt = (d.kpad + KC_SK - 1) / KC_SK;
+            const int gr = (local / nkt) * KC_SR + (threadIdx.x >> 4);
+            const int gl = (local % nkt) * KC_SK + (threadIdx.x & 15) * 16;
+            if (gr >= d.rows_pad || gl >= d.kpad) continue;
+            if (gr < d.rows) {
+                const double *p = slice_src(src, d.src_off) + (long long) gr * d.rs + gl;
+                if (!(reinterpret_cast<uintptr_t>(p) & 15) && gl + 16 <= d.kz) {
 #pragma unroll
-        for (int i = 0; i < ST * ST / 256; ++i) {
-            const int e = threadIdx.x + 256 * i;
-            const int a = e % ST, b = e / ST;
-            const int r = rfast ? a : b, l = rfast ? b : a;
-            const int gr = r0 + r, gl = l0 + l;
-            x[i] = (gr < d.rows && gl < d.kz) ? __ldg(base + gr * d.rs + gl * d.ls) : 0.0;
-        }
-        __syncthreads();
+                    for (int i = 0; i < 8; ++i) {
+                        const double2 v = __ldg(reinterpret_cast<const double2 *>(p) + i);
+                        x[2 * i] = v.x;
+                        x[2 * i + 1] = v.y;
+                    }
+                } else {
 #pragma unroll
-        for (int i = 0; i < ST * ST / 256; ++i) {
-            const int e = threadIdx.x + 256 * i;
-            const int a = e % ST, b = e / ST;
-            tile[rfast ? a : b][rfast ? b : a] = x[i];
+                    for (int i = 0; i < 16; ++i) x[i] = gl + i < d.kz ? __ldg(p + i) : 0.0;
+                }
+            } else {
+#pragma unroll
+                for (int i = 0; i < 16; ++i) x[i] = 0.0;
+            }
+            slice16<S>(d, work, mwork, gr, gl, x);
+            continue;
         }
+        // RC: 128 rows x 32 k; thread (row pair tid % 64, k column tid / 64 + 4 i)
+        // loads 16 bytes of a column, the tile is transposed through shared memory
+        const int ntr = (d.rows_pad + RC_SR - 1) / RC_SR;
+        const int r0 = (local % ntr) * RC_SR, l0 = (local / ntr) * RC_SK;
+        const int rp = threadIdx.x & 63, cg = threadIdx.x >> 6;
+        const double *base = slice_src(src, d.src_off) + r0 + (long long) l0 * d.ls;
+        const int rn = d.rows - r0, ln = d.kz - l0;
+        double2 v[8];
+        if (!(reinterpret_cast<uintptr_t>(base) & 15) && !(d.ls & 1) && rn >= RC_SR && ln >= RC_SK) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i)
+                v[i] = __ldg(reinterpret_cast<const double2 *>(base + (long long) (cg + 4 * i) * d.ls) + rp);
+        } else {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                const int l = cg + 4 * i;
+                const double *c = base + (long long) l * d.ls + 2 * rp;
+                v[i].x = (l < ln && 2 * rp < rn) ? __ldg(c) : 0.0;
+                v[i].y = (l < ln && 2 * rp + 1 < rn) ? __ldg(c + 1) : 0.0;
+            }
+        }
+        __syncthreads();                             // tl of the previous tile is read
+#pragma unroll
+        for (int i = 0; i < 8; ++i) reinterpret_cast<double2 *>(&tl[cg + 4 * i][0])[rp] = v[i];
         __syncthreads();
-        // thread -> (row r, 16 consecutive k); a warp covers 32 rows of one chunk
-        const int r = threadIdx.x & (ST - 1), c = (threadIdx.x >> 6) * 16;
+        const int r = threadIdx.x & (RC_SR - 1), c = (threadIdx.x >> 7) * 16;
         const int gr = r0 + r, gl = l0 + c;
         if (gr >= d.rows_pad || gl >= d.kpad) continue;
-        const unsigned long long mb = gr < d.rows ? mwork[d.e_off + gr] : 0ull;
-        int E = 0;
-        if (mb) {
-            int ex;
-            const double mant = frexp(__longlong_as_double((long long) mb), &ex);
-            E = ex + (mant > 0.9921875 ? 1 : 0);
-        }
-        if (l0 == 0 && c == 0 && gr < d.rows) ework[d.e_off + gr] = mb ? E + EXP_BIAS : 0;
-        // x 2^(8S-1-E) as two exact power-of-two factors (each inside the normal range)
-        const int sh = 8 * S - 1 - E;
-        const double up1 = ldexp(1.0, sh / 2), up2 = ldexp(1.0, sh - sh / 2);
-        constexpr unsigned long long BIAS = 0x8080808080808080ull >> (64 - 8 * S);
-        uint32_t lo[16], hi[16];
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const long long N = __double2ll_rn(tile[r][c + j] * up1 * up2);
-            const unsigned long long U = (unsigned long long) N + BIAS;
-            lo[j] = (uint32_t) U;
-            hi[j] = (uint32_t) (U >> 32);
-        }
-        const int rt = gr / d.tile_rows, rr = gr % d.tile_rows;
-        const int kb = gl / OKB, chunk = (gl % OKB) >> 4;
-        const long long tile_bytes = (long long) d.tile_rows * OKB;
-        unsigned char *dst = work + d.q_off + ((long long) rt * d.nkb + kb) * S * tile_bytes +
-                             rr * OKB + ((chunk ^ ((rr >> 2) & 1)) << 4);
-#pragma unroll
-        for (int t = 0; t < S; ++t) {
-            const int b = S - 1 - t, bb = b & 3;
-            const uint32_t *w = b < 4 ? lo : hi;
-            const uint32_t sel = (uint32_t) bb | ((uint32_t) (bb + 4) << 4);
-            uint32_t out[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                const uint32_t p01 = __byte_perm(w[4 * q], w[4 * q + 1], sel);
-                const uint32_t p23 = __byte_perm(w[4 * q + 2], w[4 * q + 3], sel);
-                out[q] = __byte_perm(p01, p23, 0x5410) ^ 0x80808080u;
-            }
-            *reinterpret_cast<uint4 *>(dst + t * tile_bytes) = make_uint4(out[0], out[1], out[2], out[3]);
-        }
+        for (int j = 0; j < 16; ++j) x[j] = tl[c + j][r];
+        slice16<S>(d, work, mwork, gr, gl, x);
     }
 }
 
@@ -828,7 +884,7 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
         if (A[i].alias >= nB) return CA3DMM_EINVAL;
     long long eoff = 0;
     int max_rows = 1, max_kpad = 1;
-    int tiles_op[2] = {0, 0};
+    int tiles_op[2] = {0, 0}, items_op[2] = {0, 0};
     for (int i = 0; i < nA + nB; ++i) {
         const bool isA = i < nA;
         const ca3dmm_oz_blk_t &b = isA ? A[i] : B[i - nA];
@@ -859,9 +915,12 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
             d.src_off = (long long) b.c0 * d.rs + (long long) b.r0 * d.ls;
         }
         if (src.base) d.src_off += (long long) (reinterpret_cast<uintptr_t>(src.base) / sizeof(double));
+        if (d.ls != 1 && d.rs != 1) return CA3DMM_EINVAL;
+        d.shape = d.ls == 1 ? SHAPE_KC : SHAPE_RC;
         d.tile_begin = tiles_op[isA ? 0 : 1];
-        if (rows > 0 && kz > 0)
-            tiles_op[isA ? 0 : 1] += ((d.rows_pad + ST - 1) / ST) * ((d.kpad + ST - 1) / ST);
+        d.xbegin = items_op[isA ? 0 : 1];
+        tiles_op[isA ? 0 : 1] += slice_tiles_of(d);
+        items_op[isA ? 0 : 1] += exp_items_of(d);
         qoff += align256((size_t) slices * d.rows_pad * d.kpad);
         eoff += rows;
         if (d.rows_pad > max_rows) max_rows = d.rows_pad;
@@ -917,6 +976,8 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
     oz->max_rows = max_rows; oz->max_kpad = max_kpad;
     oz->slice_tiles_a = tiles_op[0];
     oz->slice_tiles_b = tiles_op[1];
+    oz->exp_items_a = items_op[0];
+    oz->exp_items_b = items_op[1];
     oz->n_exp = (long long) ne;
     oz->dev_plan = dev_plan;
     oz->dev_work = dev_work;
@@ -931,14 +992,14 @@ extern "C" int ca3dmm_oz_clear(const ca3dmm_oz_plan_t *oz, cudaStream_t stream)
 }
 
 static int launch_exp(const ca3dmm_oz_plan_t *oz, const void *src, const SliceDesc *descs,
-                      int ndesc, int ntiles, cudaStream_t stream)
+                      int ndesc, int nitems, cudaStream_t stream)
 {
-    if (ndesc <= 0 || ntiles <= 0) return CA3DMM_OK;
+    if (ndesc <= 0 || nitems <= 0) return CA3DMM_OK;
     unsigned char *w = static_cast<unsigned char *>(oz->dev_work);
     unsigned long long *mwork = reinterpret_cast<unsigned long long *>(w + exp_bytes(oz->n_exp));
     const int cap = ca3dmm_device_sm_count() * 8;
-    oz_exp_kernel<<<ntiles < cap ? ntiles : cap, 256, 0, stream>>>(
-        static_cast<const double *>(src), descs, ndesc, ntiles, mwork);
+    oz_exp_kernel<<<nitems < cap ? nitems : cap, 256, 0, stream>>>(
+        static_cast<const double *>(src), descs, ndesc, nitems, mwork);
     CA3DMM_CUDA_TRY(cudaGetLastError());
     ca3dmm_note_launch(1);
     return CA3DMM_OK;
@@ -951,7 +1012,7 @@ static int launch_slice(const ca3dmm_oz_plan_t *oz, const void *src, const Slice
     unsigned char *w = static_cast<unsigned char *>(oz->dev_work);
     const unsigned long long *mwork =
         reinterpret_cast<const unsigned long long *>(w + exp_bytes(oz->n_exp));
-    const int cap = ca3dmm_device_sm_count() * 8;
+    const int cap = ca3dmm_device_sm_count() * 4;
     const unsigned grid = ntiles < cap ? ntiles : cap;
     const double *x = static_cast<const double *>(src);
     switch (oz->slices) {
@@ -976,8 +1037,8 @@ extern "C" int ca3dmm_oz_run_pack(const ca3dmm_oz_plan_t *oz, const void *A, con
     const SliceDesc *sd =
         reinterpret_cast<const SliceDesc *>(static_cast<const unsigned char *>(oz->dev_plan) + L.sd);
     int rc = ca3dmm_oz_clear(oz, stream);
-    if (!rc) rc = launch_exp(oz, A, sd, oz->nA, oz->slice_tiles_a, stream);
-    if (!rc) rc = launch_exp(oz, B, sd + oz->nA, oz->nB, oz->slice_tiles_b, stream);
+    if (!rc) rc = launch_exp(oz, A, sd, oz->nA, oz->exp_items_a, stream);
+    if (!rc) rc = launch_exp(oz, B, sd + oz->nA, oz->nB, oz->exp_items_b, stream);
     if (!rc) rc = launch_slice(oz, A, sd, oz->nA, oz->slice_tiles_a, stream);
     if (!rc) rc = launch_slice(oz, B, sd + oz->nA, oz->nB, oz->slice_tiles_b, stream);
     return rc;
@@ -992,7 +1053,7 @@ extern "C" int ca3dmm_oz_slice_side(const ca3dmm_oz_plan_t *oz, int which, const
     const SliceDesc *d = which ? sd + oz->nA : sd;
     const int nd = which ? oz->nB : oz->nA;
     const int nt = which ? oz->slice_tiles_b : oz->slice_tiles_a;
-    int rc = launch_exp(oz, src, d, nd, nt, stream);
+    int rc = launch_exp(oz, src, d, nd, which ? oz->exp_items_b : oz->exp_items_a, stream);
     if (!rc) rc = launch_slice(oz, src, d, nd, nt, stream);
     return rc;
 }
@@ -1000,7 +1061,7 @@ extern "C" int ca3dmm_oz_slice_side(const ca3dmm_oz_plan_t *oz, int which, const
 extern "C" size_t ca3dmm_oz_desc_bytes(void) { return sizeof(SliceDesc); }
 
 extern "C" int ca3dmm_oz_encode_rows(const void *host_plan, int ngroup, const int *blocks,
-                                     int count, int r0, int r1, void *out_descs, int *ntiles)
+                                     int count, int r0, int r1, void *out_descs, int ntiles[2])
 {
     const PlanLayout L(ngroup);
     const unsigned char *h = static_cast<const unsigned char *>(host_plan);
@@ -1008,7 +1069,7 @@ extern "C" int ca3dmm_oz_encode_rows(const void *host_plan, int ngroup, const in
     const SliceDesc *sd = reinterpret_cast<const SliceDesc *>(h + L.sd);
     SliceDesc *out = static_cast<SliceDesc *>(out_descs);
     if (!blocks || count < 0 || r0 < 0 || r1 < r0) return CA3DMM_EINVAL;
-    int tiles = 0;
+    int tiles = 0, items = 0;
     for (int i = 0; i < count; ++i) {
         if (blocks[i] < 0 || blocks[i] >= hd->nA) return CA3DMM_EINVAL;
         const SliceDesc &d = sd[blocks[i]];
@@ -1021,20 +1082,23 @@ extern "C" int ca3dmm_oz_encode_rows(const void *host_plan, int ngroup, const in
         c.q_off = d.q_off + (long long) (r0 / d.tile_rows) * d.nkb * hd->slices * d.tile_rows * OKB;
         c.e_off = d.e_off + r0;
         c.tile_begin = tiles;
-        if (c.rows > 0 && c.kz > 0) tiles += ((c.rows_pad + ST - 1) / ST) * ((c.kpad + ST - 1) / ST);
+        c.xbegin = items;
+        tiles += slice_tiles_of(c);
+        items += exp_items_of(c);
         out[i] = c;
     }
-    *ntiles = tiles;
+    ntiles[0] = items;
+    ntiles[1] = tiles;
     return CA3DMM_OK;
 }
 
 extern "C" int ca3dmm_oz_slice_descs(const ca3dmm_oz_plan_t *oz, const void *src,
-                                     const void *dev_descs, int ndesc, int ntiles,
+                                     const void *dev_descs, int ndesc, const int ntiles[2],
                                      cudaStream_t stream)
 {
     const SliceDesc *d = static_cast<const SliceDesc *>(dev_descs);
-    int rc = launch_exp(oz, src, d, ndesc, ntiles, stream);
-    if (!rc) rc = launch_slice(oz, src, d, ndesc, ntiles, stream);
+    int rc = launch_exp(oz, src, d, ndesc, ntiles[0], stream);
+    if (!rc) rc = launch_slice(oz, src, d, ndesc, ntiles[1], stream);
     return rc;
 }
 
