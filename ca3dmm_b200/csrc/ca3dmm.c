@@ -96,7 +96,7 @@ struct host_exec {
     ca3dmm_tile_ranges_t rng[HX_MAX_BANDS];
     void *desc_h, *desc_d;        /* per-band A descriptors (pack or slicing) */
     size_t desc_stride;
-    int ndesc, ntile[HX_MAX_BANDS][2];  /* per band: Ozaki exponent items + slicing tiles, or pack tiles */
+    int ndesc, ntile[HX_MAX_BANDS][3];  /* per band: Ozaki exponent items + KC + RC slicing tiles, or pack tiles */
     int built_mode, built_slices, built_raster;
     int ok;                       /* streams and events created */
 };

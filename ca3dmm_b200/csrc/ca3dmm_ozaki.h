@@ -56,8 +56,8 @@ typedef struct {
     int slices, nA, nB, ngroup, nunit, max_nsub;
     int tiles;            /* output tiles of the grouped INT8 launch (numbered per unit) */
     int max_rows, max_kpad;
-    int slice_tiles_a, slice_tiles_b;   /* slicing tiles of the A / B blocks */
-    int exp_items_a, exp_items_b;       /* exponent work items of the A / B blocks */
+    int exp_items[2];     /* exponent work items of the A / B blocks */
+    int kc_tiles[2], rc_tiles[2];       /* slicing tiles of the A / B blocks: k-contiguous / rows-contiguous sources */
     long long n_exp;      /* rows with an exponent: E (int) then max bits (u64) arrays open the work region */
     void *dev_plan;       /* device copy of the plan (slice descriptors, tensor maps, groups) */
     void *dev_work;       /* slices and exponents */
@@ -89,15 +89,15 @@ int ca3dmm_oz_run_gemm(const ca3dmm_oz_plan_t *oz, int *dev_status, double timeo
  * memory, e.g. the A blocks restricted to a band of rows built by
  * ca3dmm_oz_encode_rows from the host copy of the plan (r0 a multiple of the
  * 128-row A tile, rows counted inside each listed A block; ntiles receives
- * the exponent item and slicing tile counts). */
+ * the exponent item count and the KC and RC slicing tile counts). */
 int ca3dmm_oz_clear(const ca3dmm_oz_plan_t *oz, cudaStream_t stream);
 int ca3dmm_oz_slice_side(const ca3dmm_oz_plan_t *oz, int which, const void *src,
                          cudaStream_t stream);
 size_t ca3dmm_oz_desc_bytes(void);
 int ca3dmm_oz_encode_rows(const void *host_plan, int ngroup, const int *blocks, int count, int r0,
-                          int r1, void *out_descs, int ntiles[2]);
+                          int r1, void *out_descs, int ntiles[3]);
 int ca3dmm_oz_slice_descs(const ca3dmm_oz_plan_t *oz, const void *src, const void *dev_descs,
-                          int ndesc, const int ntiles[2], cudaStream_t stream);
+                          int ndesc, const int ntiles[3], cudaStream_t stream);
 /* The GEMM over the tiles of `ranges` only (ca3dmm_kernels.h). */
 int ca3dmm_oz_run_gemm_ranges(const ca3dmm_oz_plan_t *oz, const ca3dmm_tile_ranges_t *ranges,
                               int *dev_status, double timeout_s, cudaStream_t stream);

@@ -2,7 +2,7 @@
 //
 //  1. oz_exp_kernel    -- per row of op(A) / column of op(B) over the block's k
 //                         range: E = frexp exponent of max|x| (max|x| < 2^E).
-//  2. oz_slice_kernel  -- x = sum_t q_t 2^(E-7-8t) + r with |r| <= 2^(E-8s): the
+//  2. oz_slice_kc/rc  -- x = sum_t q_t 2^(E-7-8t) + r with |r| <= 2^(E-8s): the
 //                         integer N = rint(x 2^(8s-1-E)) written in balanced
 //                         base-256 digits q_t in [-128, 127] (E chosen so that
 //                         max|x| <= 2^E 127/128, which keeps the top digit in range).
@@ -72,10 +72,9 @@ struct SliceDesc {
     long long e_off;        // int offset of the exponents in the work region
     int rows, kz, kpad;     // kpad = kz rounded up to OKB
     int rows_pad, tile_rows, nkb;   // rows rounded up to tile_rows (128 for A, 64 for B)
-    int tile_begin;         // first slicing tile of this block (per operand)
+    int kc_begin, rc_begin; // first slicing tile of this block among the KC / RC tiles of its operand
     int xbegin;             // first exponent work item of this block (per operand)
     int shape;              // SHAPE_KC or SHAPE_RC
-    int pad;
 };
 
 struct OzGroup {
@@ -131,15 +130,23 @@ __host__ __device__ inline int slice_tiles_of(const SliceDesc &d)
     return ((d.rows_pad + RC_SR - 1) / RC_SR) * ((d.kpad + RC_SK - 1) / RC_SK);
 }
 
+// Which numbering a search runs over: exponent items, KC or RC slicing tiles.
+constexpr int FIND_EXP = 0;
+
+__device__ __forceinline__ int desc_begin(const SliceDesc &d, int which)
+{
+    return which == SHAPE_KC ? d.kc_begin : which == SHAPE_RC ? d.rc_begin : d.xbegin;
+}
+
 // The descriptor holding flat item t: the last one whose first item is <= t
-// (blocks without items share their first item with the next block).
-template <bool EXP>
+// (blocks without items in this numbering share their first item with the next).
+template <int WHICH>
 __device__ __forceinline__ int find_slice_desc(const SliceDesc *d, int n, int t)
 {
     int lo = 0, hi = n - 1;
     while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;
-        if ((EXP ? d[mid].xbegin : d[mid].tile_begin) <= t) lo = mid; else hi = mid - 1;
+        if (desc_begin(d[mid], WHICH) <= t) lo = mid; else hi = mid - 1;
     }
     return lo;
 }
@@ -178,7 +185,7 @@ oz_exp_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ desc
 {
     __shared__ unsigned long long part[4][ST];
     for (int item = blockIdx.x; item < total_items; item += gridDim.x) {
-        const SliceDesc &d = descs[find_slice_desc<true>(descs, ndesc, item)];
+        const SliceDesc &d = descs[find_slice_desc<FIND_EXP>(descs, ndesc, item)];
         const int local = item - d.xbegin;
         if (d.shape == SHAPE_KC) {
             // warp w: row r0 + w, k [l0, l0 + 512) as 16-byte loads (scalar when unaligned)
@@ -304,46 +311,56 @@ __device__ __forceinline__ void slice16(const SliceDesc &d, unsigned char *__res
     }
 }
 
-// Pass 2 over the flat list of slicing tiles (padding rows and k included:
-// they hold zero digits).
+// Pass 2 over the flat list of slicing tiles of one shape (padding rows and k
+// included: they hold zero digits).  The KC kernel keeps no shared memory, so
+// the whole L1 caches its per-thread 128-byte runs.
 template <int S>
 __global__ void __launch_bounds__(256)
-oz_slice_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ descs, int ndesc,
-                int total_tiles, unsigned char *__restrict__ work,
-                const unsigned long long *__restrict__ mwork)
+oz_slice_kc_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ descs, int ndesc,
+                   int total_tiles, unsigned char *__restrict__ work,
+                   const unsigned long long *__restrict__ mwork)
 {
-    __shared__ __align__(16) double tl[RC_SK][RC_SR];
     for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
-        const SliceDesc &d = descs[find_slice_desc<false>(descs, ndesc, tile)];
-        const int local = tile - d.tile_begin;
+        const SliceDesc &d = descs[find_slice_desc<SHAPE_KC>(descs, ndesc, tile)];
+        const int local = tile - d.kc_begin;
+        // thread (row tid / 16, 16-k chunk tid % 16) reads its 128 contiguous bytes
+        const int nkt = (d.kpad + KC_SK - 1) / KC_SK;
+        const int gr = (local / nkt) * KC_SR + (threadIdx.x >> 4);
+        const int gl = (local % nkt) * KC_SK + (threadIdx.x & 15) * 16;
+        if (gr >= d.rows_pad || gl >= d.kpad) continue;
         double x[16];
-        if (d.shape == SHAPE_KC) {
-            // thread (row tid / 16, 16-k chunk tid % 16) reads its 128 contiguous bytes
-            const int nkt = (d.kpad + KC_SK - 1) / KC_SK;
-            const int gr = (local / nkt) * KC_SR + (threadIdx.x >> 4);
-            const int gl = (local % nkt) * KC_SK + (threadIdx.x & 15) * 16;
-            if (gr >= d.rows_pad || gl >= d.kpad) continue;
-            if (gr < d.rows) {
-                const double *p = slice_src(src, d.src_off) + (long long) gr * d.rs + gl;
-                if (!(reinterpret_cast<uintptr_t>(p) & 15) && gl + 16 <= d.kz) {
+        if (gr < d.rows) {
+            const double *p = slice_src(src, d.src_off) + (long long) gr * d.rs + gl;
+            if (!(reinterpret_cast<uintptr_t>(p) & 15) && gl + 16 <= d.kz) {
 #pragma unroll
-                    for (int i = 0; i < 8; ++i) {
-                        const double2 v = __ldg(reinterpret_cast<const double2 *>(p) + i);
-                        x[2 * i] = v.x;
-                        x[2 * i + 1] = v.y;
-                    }
-                } else {
-#pragma unroll
-                    for (int i = 0; i < 16; ++i) x[i] = gl + i < d.kz ? __ldg(p + i) : 0.0;
+                for (int i = 0; i < 8; ++i) {
+                    const double2 v = __ldg(reinterpret_cast<const double2 *>(p) + i);
+                    x[2 * i] = v.x;
+                    x[2 * i + 1] = v.y;
                 }
             } else {
 #pragma unroll
-                for (int i = 0; i < 16; ++i) x[i] = 0.0;
+                for (int i = 0; i < 16; ++i) x[i] = gl + i < d.kz ? __ldg(p + i) : 0.0;
             }
-            slice16<S>(d, work, mwork, gr, gl, x);
-            continue;
+        } else {
+#pragma unroll
+            for (int i = 0; i < 16; ++i) x[i] = 0.0;
         }
-        // RC: 128 rows x 32 k; thread (row pair tid % 64, k column tid / 64 + 4 i)
+        slice16<S>(d, work, mwork, gr, gl, x);
+    }
+}
+
+template <int S>
+__global__ void __launch_bounds__(256)
+oz_slice_rc_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ descs, int ndesc,
+                   int total_tiles, unsigned char *__restrict__ work,
+                   const unsigned long long *__restrict__ mwork)
+{
+    __shared__ __align__(16) double tl[RC_SK][RC_SR];
+    for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
+        const SliceDesc &d = descs[find_slice_desc<SHAPE_RC>(descs, ndesc, tile)];
+        const int local = tile - d.rc_begin;
+        // 128 rows x 32 k; thread (row pair tid % 64, k column tid / 64 + 4 i)
         // loads 16 bytes of a column, the tile is transposed through shared memory
         const int ntr = (d.rows_pad + RC_SR - 1) / RC_SR;
         const int r0 = (local % ntr) * RC_SR, l0 = (local / ntr) * RC_SK;
@@ -371,6 +388,7 @@ oz_slice_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ de
         const int r = threadIdx.x & (RC_SR - 1), c = (threadIdx.x >> 7) * 16;
         const int gr = r0 + r, gl = l0 + c;
         if (gr >= d.rows_pad || gl >= d.kpad) continue;
+        double x[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) x[j] = tl[c + j][r];
         slice16<S>(d, work, mwork, gr, gl, x);
@@ -884,7 +902,7 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
         if (A[i].alias >= nB) return CA3DMM_EINVAL;
     long long eoff = 0;
     int max_rows = 1, max_kpad = 1;
-    int tiles_op[2] = {0, 0}, items_op[2] = {0, 0};
+    for (int side = 0; side < 2; ++side) oz->kc_tiles[side] = oz->rc_tiles[side] = oz->exp_items[side] = 0;
     for (int i = 0; i < nA + nB; ++i) {
         const bool isA = i < nA;
         const ca3dmm_oz_blk_t &b = isA ? A[i] : B[i - nA];
@@ -917,10 +935,12 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
         if (src.base) d.src_off += (long long) (reinterpret_cast<uintptr_t>(src.base) / sizeof(double));
         if (d.ls != 1 && d.rs != 1) return CA3DMM_EINVAL;
         d.shape = d.ls == 1 ? SHAPE_KC : SHAPE_RC;
-        d.tile_begin = tiles_op[isA ? 0 : 1];
-        d.xbegin = items_op[isA ? 0 : 1];
-        tiles_op[isA ? 0 : 1] += slice_tiles_of(d);
-        items_op[isA ? 0 : 1] += exp_items_of(d);
+        const int side = isA ? 0 : 1;
+        d.kc_begin = oz->kc_tiles[side];
+        d.rc_begin = oz->rc_tiles[side];
+        d.xbegin = oz->exp_items[side];
+        (d.shape == SHAPE_KC ? oz->kc_tiles : oz->rc_tiles)[side] += slice_tiles_of(d);
+        oz->exp_items[side] += exp_items_of(d);
         qoff += align256((size_t) slices * d.rows_pad * d.kpad);
         eoff += rows;
         if (d.rows_pad > max_rows) max_rows = d.rows_pad;
@@ -974,10 +994,6 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
     oz->max_nsub = 1;
     for (int u = 0; u < nu; ++u) oz->max_nsub = un[u].nsub > oz->max_nsub ? un[u].nsub : oz->max_nsub;
     oz->max_rows = max_rows; oz->max_kpad = max_kpad;
-    oz->slice_tiles_a = tiles_op[0];
-    oz->slice_tiles_b = tiles_op[1];
-    oz->exp_items_a = items_op[0];
-    oz->exp_items_b = items_op[1];
     oz->n_exp = (long long) ne;
     oz->dev_plan = dev_plan;
     oz->dev_work = dev_work;
@@ -1006,27 +1022,34 @@ static int launch_exp(const ca3dmm_oz_plan_t *oz, const void *src, const SliceDe
 }
 
 static int launch_slice(const ca3dmm_oz_plan_t *oz, const void *src, const SliceDesc *descs,
-                        int ndesc, int ntiles, cudaStream_t stream)
+                        int ndesc, int nkc, int nrc, cudaStream_t stream)
 {
-    if (ndesc <= 0 || ntiles <= 0) return CA3DMM_OK;
+    if (ndesc <= 0) return CA3DMM_OK;
     unsigned char *w = static_cast<unsigned char *>(oz->dev_work);
     const unsigned long long *mwork =
         reinterpret_cast<const unsigned long long *>(w + exp_bytes(oz->n_exp));
     const int cap = ca3dmm_device_sm_count() * 4;
-    const unsigned grid = ntiles < cap ? ntiles : cap;
     const double *x = static_cast<const double *>(src);
-    switch (oz->slices) {
+    for (int shape = SHAPE_KC; shape <= SHAPE_RC; ++shape) {
+        const int nt = shape == SHAPE_KC ? nkc : nrc;
+        if (nt <= 0) continue;
+        const unsigned grid = nt < cap ? nt : cap;
+        switch (oz->slices) {
 #define CA3DMM_SLICE_CASE(S)                                                                       \
     case S:                                                                                        \
-        oz_slice_kernel<S><<<grid, 256, 0, stream>>>(x, descs, ndesc, ntiles, w, mwork);          \
+        if (shape == SHAPE_KC)                                                                     \
+            oz_slice_kc_kernel<S><<<grid, 256, 0, stream>>>(x, descs, ndesc, nt, w, mwork);       \
+        else                                                                                       \
+            oz_slice_rc_kernel<S><<<grid, 256, 0, stream>>>(x, descs, ndesc, nt, w, mwork);       \
         break;
-        CA3DMM_SLICE_CASE(2) CA3DMM_SLICE_CASE(3) CA3DMM_SLICE_CASE(4) CA3DMM_SLICE_CASE(5)
-        CA3DMM_SLICE_CASE(6) CA3DMM_SLICE_CASE(7) CA3DMM_SLICE_CASE(8)
+            CA3DMM_SLICE_CASE(2) CA3DMM_SLICE_CASE(3) CA3DMM_SLICE_CASE(4) CA3DMM_SLICE_CASE(5)
+            CA3DMM_SLICE_CASE(6) CA3DMM_SLICE_CASE(7) CA3DMM_SLICE_CASE(8)
 #undef CA3DMM_SLICE_CASE
-        default: return CA3DMM_EINVAL;
+            default: return CA3DMM_EINVAL;
+        }
+        CA3DMM_CUDA_TRY(cudaGetLastError());
+        ca3dmm_note_launch(1);
     }
-    CA3DMM_CUDA_TRY(cudaGetLastError());
-    ca3dmm_note_launch(1);
     return CA3DMM_OK;
 }
 
@@ -1037,10 +1060,10 @@ extern "C" int ca3dmm_oz_run_pack(const ca3dmm_oz_plan_t *oz, const void *A, con
     const SliceDesc *sd =
         reinterpret_cast<const SliceDesc *>(static_cast<const unsigned char *>(oz->dev_plan) + L.sd);
     int rc = ca3dmm_oz_clear(oz, stream);
-    if (!rc) rc = launch_exp(oz, A, sd, oz->nA, oz->exp_items_a, stream);
-    if (!rc) rc = launch_exp(oz, B, sd + oz->nA, oz->nB, oz->exp_items_b, stream);
-    if (!rc) rc = launch_slice(oz, A, sd, oz->nA, oz->slice_tiles_a, stream);
-    if (!rc) rc = launch_slice(oz, B, sd + oz->nA, oz->nB, oz->slice_tiles_b, stream);
+    if (!rc) rc = launch_exp(oz, A, sd, oz->nA, oz->exp_items[0], stream);
+    if (!rc) rc = launch_exp(oz, B, sd + oz->nA, oz->nB, oz->exp_items[1], stream);
+    if (!rc) rc = launch_slice(oz, A, sd, oz->nA, oz->kc_tiles[0], oz->rc_tiles[0], stream);
+    if (!rc) rc = launch_slice(oz, B, sd + oz->nA, oz->nB, oz->kc_tiles[1], oz->rc_tiles[1], stream);
     return rc;
 }
 
@@ -1052,16 +1075,16 @@ extern "C" int ca3dmm_oz_slice_side(const ca3dmm_oz_plan_t *oz, int which, const
         reinterpret_cast<const SliceDesc *>(static_cast<const unsigned char *>(oz->dev_plan) + L.sd);
     const SliceDesc *d = which ? sd + oz->nA : sd;
     const int nd = which ? oz->nB : oz->nA;
-    const int nt = which ? oz->slice_tiles_b : oz->slice_tiles_a;
-    int rc = launch_exp(oz, src, d, nd, which ? oz->exp_items_b : oz->exp_items_a, stream);
-    if (!rc) rc = launch_slice(oz, src, d, nd, nt, stream);
+    const int side = which ? 1 : 0;
+    int rc = launch_exp(oz, src, d, nd, oz->exp_items[side], stream);
+    if (!rc) rc = launch_slice(oz, src, d, nd, oz->kc_tiles[side], oz->rc_tiles[side], stream);
     return rc;
 }
 
 extern "C" size_t ca3dmm_oz_desc_bytes(void) { return sizeof(SliceDesc); }
 
 extern "C" int ca3dmm_oz_encode_rows(const void *host_plan, int ngroup, const int *blocks,
-                                     int count, int r0, int r1, void *out_descs, int ntiles[2])
+                                     int count, int r0, int r1, void *out_descs, int ntiles[3])
 {
     const PlanLayout L(ngroup);
     const unsigned char *h = static_cast<const unsigned char *>(host_plan);
@@ -1069,7 +1092,7 @@ extern "C" int ca3dmm_oz_encode_rows(const void *host_plan, int ngroup, const in
     const SliceDesc *sd = reinterpret_cast<const SliceDesc *>(h + L.sd);
     SliceDesc *out = static_cast<SliceDesc *>(out_descs);
     if (!blocks || count < 0 || r0 < 0 || r1 < r0) return CA3DMM_EINVAL;
-    int tiles = 0, items = 0;
+    int kc = 0, rct = 0, items = 0;
     for (int i = 0; i < count; ++i) {
         if (blocks[i] < 0 || blocks[i] >= hd->nA) return CA3DMM_EINVAL;
         const SliceDesc &d = sd[blocks[i]];
@@ -1081,24 +1104,26 @@ extern "C" int ca3dmm_oz_encode_rows(const void *host_plan, int ngroup, const in
         c.src_off = d.src_off + (long long) r0 * d.rs;
         c.q_off = d.q_off + (long long) (r0 / d.tile_rows) * d.nkb * hd->slices * d.tile_rows * OKB;
         c.e_off = d.e_off + r0;
-        c.tile_begin = tiles;
+        c.kc_begin = kc;
+        c.rc_begin = rct;
         c.xbegin = items;
-        tiles += slice_tiles_of(c);
+        (c.shape == SHAPE_KC ? kc : rct) += slice_tiles_of(c);
         items += exp_items_of(c);
         out[i] = c;
     }
     ntiles[0] = items;
-    ntiles[1] = tiles;
+    ntiles[1] = kc;
+    ntiles[2] = rct;
     return CA3DMM_OK;
 }
 
 extern "C" int ca3dmm_oz_slice_descs(const ca3dmm_oz_plan_t *oz, const void *src,
-                                     const void *dev_descs, int ndesc, const int ntiles[2],
+                                     const void *dev_descs, int ndesc, const int ntiles[3],
                                      cudaStream_t stream)
 {
     const SliceDesc *d = static_cast<const SliceDesc *>(dev_descs);
     int rc = launch_exp(oz, src, d, ndesc, ntiles[0], stream);
-    if (!rc) rc = launch_slice(oz, src, d, ndesc, ntiles[1], stream);
+    if (!rc) rc = launch_slice(oz, src, d, ndesc, ntiles[1], ntiles[2], stream);
     return rc;
 }
 
