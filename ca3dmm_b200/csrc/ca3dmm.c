@@ -47,6 +47,7 @@ typedef struct {
 typedef struct {
     int ngroup, nA, nB;
     int tmn, tnn;             /* row / column blocks of the internal grouping (1: merged) */
+    int ksplit;               /* plain mode: each slab's k range runs as ksplit sub-slabs */
     group_t *groups;
     blk_t *A, *B;
     /* work buffer layout (byte offsets) */
@@ -66,6 +67,7 @@ typedef struct {
     int gemm_tiles;
     int pack_tiles_A, pack_tiles_B, pack_tiles_C;
     int packA_tma, packB_tma;     /* transposing packs staged by TMA (tensor maps in the plan) */
+    int a_kmajor;                 /* plain mode: transposed A blocks read in place, K-major */
     /* dst_C block */
     int has_dst, dst_srow, dst_nrow, dst_scol, dst_ncol;
     cudaEvent_t ev[5];
@@ -164,7 +166,7 @@ static void plan_layout(ca3dmm_engine_p e, plan_t *pl)
     pl->off_copy = off; off = align_up(off + sizeof(ca3dmm_pack_desc_t));
     pl->off_tmapA = off; off = align_up(off + 128 * (size_t) pl->nA);
     pl->off_tmapB = off; off = align_up(off + 128 * (size_t) pl->nB);
-    pl->gemm_plan_bytes = ca3dmm_dgemm_plan_bytes(pl->ngroup);
+    pl->gemm_plan_bytes = ca3dmm_dgemm_plan_bytes(pl->ngroup * pl->ksplit);
     pl->off_gemm = off; off = align_up(off + pl->gemm_plan_bytes);
     pl->oz_plan_bytes = ca3dmm_oz_plan_bytes(pl->ngroup);
     pl->off_ozplan = off; off = align_up(off + pl->oz_plan_bytes);
@@ -185,7 +187,8 @@ static void plan_layout(ca3dmm_engine_p e, plan_t *pl)
     pl->slab_ld = ca3dmm_round_up(e->m, 2);
     pl->slab_stride = (size_t) pl->slab_ld * (size_t) e->n;
     pl->off_slab = off;
-    if (e->kp > 1) off = align_up(off + sizeof(double) * pl->slab_stride * (size_t) e->kp);
+    const int nslab = e->kp * pl->ksplit;    /* plain mode's sub-slabs; split mode uses kp of them */
+    if (nslab > 1) off = align_up(off + sizeof(double) * pl->slab_stride * (size_t) nslab);
     pl->off_cout = off;
     off = align_up(off + sizeof(double) * (size_t) e->m * (size_t) e->n);
     pl->off_oz = off;
@@ -202,6 +205,32 @@ static void plan_layout(ca3dmm_engine_p e, plan_t *pl)
         off = align_up(off + pl->oz_bytes);
     }
     pl->total = off;
+}
+
+/* Plain-mode k split of every slab against the tail wave: the DMMA launch
+ * runs one 128 x 128 tile per SM at a time, so T tiles take ceil(T / SMs)
+ * rounds; with each slab's k range cut into s sub-slabs (their own C slab
+ * buffers, summed in order by the slab reduction) the rounds are s times
+ * shorter and ceil(s T / SMs) / s can come closer to T / SMs.  Only for few
+ * rounds, sub-slabs of at least 512 k, and slab buffers of at most 1 GiB.
+ * (The reference runs one DGEMM per Cannon step, src/cannon.c:410-418.) */
+#define CA3DMM_KSPLIT_MAX 8
+#define CA3DMM_SMS_B200 148
+static int choose_ksplit(const ca3dmm_engine_p e)
+{
+    const long long tiles = (long long) ((e->m + 127) / 128) * ((e->n + 127) / 128) * e->kp;
+    const int kz = e->k / e->kp;
+    const double slab_bytes = 8.0 * (double) ca3dmm_round_up(e->m, 2) * (double) e->n;
+    if (tiles <= 0 || tiles >= 4LL * CA3DMM_SMS_B200) return 1;
+    int best = 1;
+    double best_cost = (double) ((tiles + CA3DMM_SMS_B200 - 1) / CA3DMM_SMS_B200);
+    for (int s = 2; s <= CA3DMM_KSPLIT_MAX; s++) {
+        if (kz / s < 512 || slab_bytes * e->kp * s > 1073741824.0) break;
+        const double cost =
+            (double) ((tiles * s + CA3DMM_SMS_B200 - 1) / CA3DMM_SMS_B200) / (double) s;
+        if (cost < 0.99 * best_cost) { best = s; best_cost = cost; }
+    }
+    return best;
 }
 
 static int plan_build(ca3dmm_engine_p e)
@@ -224,7 +253,9 @@ static int plan_build(ca3dmm_engine_p e)
     pl->groups = (group_t *) calloc((size_t) pl->ngroup, sizeof(group_t));
     pl->A = (blk_t *) calloc((size_t) pl->nA, sizeof(blk_t));
     pl->B = (blk_t *) calloc((size_t) pl->nB, sizeof(blk_t));
-    pl->gd = (ca3dmm_dgemm_desc_t *) calloc((size_t) pl->ngroup, sizeof(ca3dmm_dgemm_desc_t));
+    pl->ksplit = choose_ksplit(e);
+    pl->gd = (ca3dmm_dgemm_desc_t *) calloc((size_t) pl->ngroup * (size_t) pl->ksplit,
+                                            sizeof(ca3dmm_dgemm_desc_t));
     pl->ob = (ca3dmm_oz_blk_t *) calloc((size_t) (pl->nA + pl->nB), sizeof(ca3dmm_oz_blk_t));
     pl->os = (ca3dmm_oz_src_t *) calloc((size_t) (pl->nA + pl->nB), sizeof(ca3dmm_oz_src_t));
     pl->og = (ca3dmm_oz_group_t *) calloc((size_t) pl->ngroup, sizeof(ca3dmm_oz_group_t));
@@ -640,10 +671,18 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
 {
     plan_t *pl = (plan_t *) e->impl;
     char *w = (char *) e->workbuf_d, *h = (char *) pl->stage;
-    /* An untransposed operand block whose address and leading dimension suit
-     * the GEMM's tensor maps (16-byte aligned start, even ld) is read in place;
-     * the others are packed (and transposed) into the work buffer. */
+    /* An operand block whose address and leading dimension suit the GEMM's
+     * tensor maps (16-byte aligned start, even ld) is read in place: op(B)
+     * untransposed (K-major), op(A) untransposed (M-major) or transposed
+     * (K-major, when every A block qualifies: one A layout per launch).  The
+     * others are packed (and transposed) into the work buffer. */
     ca3dmm_pack_desc_t *pa = (ca3dmm_pack_desc_t *) (h + pl->off_packA);
+    pl->a_kmajor = e->trans_A && (ldA & 1) == 0;
+    for (int i = 0; i < pl->nA && pl->a_kmajor; i++) {
+        const blk_t *b = &pl->A[i];
+        const long long off = (long long) b->c0 + (long long) b->r0 * ldA;
+        if ((((uintptr_t) A + sizeof(double) * (uintptr_t) off) & 15) != 0) pl->a_kmajor = 0;
+    }
     for (int i = 0; i < pl->nA; i++) {
         blk_t *b = &pl->A[i];
         ca3dmm_pack_desc_t *d = &pa[i];
@@ -654,8 +693,9 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
         d->dst_off = (long long) ((b->off) / sizeof(double));
         d->ldd = b->ld;
         b->direct = NULL;
-        if (!e->trans_A && (ldA & 1) == 0 &&
-            (((uintptr_t) A + sizeof(double) * (uintptr_t) d->src_off) & 15) == 0) {
+        if ((!e->trans_A && (ldA & 1) == 0 &&
+             (((uintptr_t) A + sizeof(double) * (uintptr_t) d->src_off) & 15) == 0) ||
+            pl->a_kmajor) {
             b->direct = (const double *) A + d->src_off;
             b->direct_ld = ldA;
             d->rows = 0;
@@ -704,27 +744,38 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
     }
     pl->pack_tiles_C = ca3dmm_pack_tiles(pc, 1);
     ca3dmm_dgemm_desc_t *gd = pl->gd;
+    const int ks = pl->ksplit, nslab = e->kp * ks;
     for (int i = 0; i < pl->ngroup; i++) {
         group_t *g = &pl->groups[i];
-        ca3dmm_dgemm_desc_t *q = &gd[i];
         const blk_t *ba = &pl->A[g->a_blk], *bb = &pl->B[g->b_blk];
-        q->A = ba->direct ? ba->direct : (const double *) (w + ba->off);
-        q->lda = ba->direct ? ba->direct_ld : ba->ld;
-        q->B = bb->direct ? bb->direct : (const double *) (w + bb->off);
-        q->ldb = bb->direct ? bb->direct_ld : bb->ld;
-        if (e->kp > 1) {
-            q->C = (double *) (w + pl->off_slab) + (size_t) g->tk * pl->slab_stride + g->m0 +
-                   (size_t) g->n0 * pl->slab_ld;
-            q->ldc = pl->slab_ld;
-        } else {
-            q->C = out + g->m0 + (size_t) g->n0 * ldo;
-            q->ldc = ldo;
+        const double *a = ba->direct ? ba->direct : (const double *) (w + ba->off);
+        const long long lda = ba->direct ? ba->direct_ld : ba->ld;
+        const double *b = bb->direct ? bb->direct : (const double *) (w + bb->off);
+        const long long ldb = bb->direct ? bb->direct_ld : bb->ld;
+        for (int sub = 0; sub < ks; sub++) {
+            /* sub-slab k range: a multiple of 16 (whole k-tiles, 16-byte aligned starts) */
+            const int k0 = (int) ((long long) g->kz * sub / ks) / 16 * 16;
+            const int k1 = sub + 1 < ks ? (int) ((long long) g->kz * (sub + 1) / ks) / 16 * 16 : g->kz;
+            ca3dmm_dgemm_desc_t *q = &gd[i * ks + sub];
+            q->A = a + (pl->a_kmajor ? (long long) k0 : (long long) k0 * lda);
+            q->lda = lda;
+            q->B = b + k0;
+            q->ldb = ldb;
+            if (nslab > 1) {
+                q->C = (double *) (w + pl->off_slab) + (size_t) (g->tk * ks + sub) * pl->slab_stride +
+                       g->m0 + (size_t) g->n0 * pl->slab_ld;
+                q->ldc = pl->slab_ld;
+            } else {
+                q->C = out + g->m0 + (size_t) g->n0 * ldo;
+                q->ldc = ldo;
+            }
+            q->m = g->mz; q->n = g->nz; q->k = k1 - k0;
+            q->alpha = 1.0; q->beta = 0.0;
+            q->raster = e->raster;
+            q->a_kmajor = pl->a_kmajor;
         }
-        q->m = g->mz; q->n = g->nz; q->k = g->kz;
-        q->alpha = 1.0; q->beta = 0.0;
-        q->raster = e->raster;
     }
-    int rc = ca3dmm_dgemm_plan_encode(gd, pl->ngroup, h + pl->off_gemm, &pl->gemm_tiles);
+    int rc = ca3dmm_dgemm_plan_encode(gd, pl->ngroup * ks, h + pl->off_gemm, &pl->gemm_tiles);
     if (rc) return rc;
     if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
         ca3dmm_oz_blk_t *ob = pl->ob;
@@ -767,14 +818,15 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
         for (int i = 0; i < pl->ngroup; i++) {
             const group_t *g = &pl->groups[i];
             og[i].a_blk = g->a_blk; og[i].b_blk = g->b_blk;
-            if (pl->oz_fused) {
+            if (pl->oz_fused || e->kp == 1) {
                 og[i].C = out + g->m0 + (size_t) g->n0 * ldo;
                 og[i].ldc = ldo;
             } else {
-                og[i].C = gd[i].C;
-                og[i].ldc = gd[i].ldc;
+                og[i].C = (double *) (w + pl->off_slab) + (size_t) g->tk * pl->slab_stride + g->m0 +
+                          (size_t) g->n0 * pl->slab_ld;
+                og[i].ldc = pl->slab_ld;
             }
-            og[i].m = gd[i].m; og[i].n = gd[i].n; og[i].k = gd[i].k;
+            og[i].m = g->mz; og[i].n = g->nz; og[i].k = g->kz;
             og[i].raster = e->raster;
         }
         ca3dmm_oz_unit_t *un = pl->ou;
@@ -855,16 +907,19 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
     if (e->gemm_mode == CA3DMM_GEMM_OZAKI)
         rc = ca3dmm_oz_run_gemm(&pl->oz, status_d, 5.0, st);
     else
-        rc = ca3dmm_dgemm_launch(w + pl->off_gemm, pl->ngroup, pl->gemm_tiles, status_d, 5.0, st);
+        rc = ca3dmm_dgemm_launch(w + pl->off_gemm, pl->ngroup * pl->ksplit, pl->gemm_tiles,
+                                 pl->a_kmajor, status_d, 5.0, st);
     if (rc) return rc;
     if (timing) cudaEventRecord(pl->ev[2], st);
     int whole = pl->has_dst && pl->dst_srow == 0 && pl->dst_scol == 0 && pl->dst_nrow == e->m &&
                 pl->dst_ncol == e->n;
     double *out = whole ? (double *) dst_C : (double *) (w + pl->off_cout);
     long long ldo = whole ? ldC : e->m;
-    if (e->kp > 1 && !(e->gemm_mode == CA3DMM_GEMM_OZAKI && pl->oz_fused)) {
+    const int nred = e->gemm_mode == CA3DMM_GEMM_OZAKI ? (pl->oz_fused ? 1 : e->kp)
+                                                      : e->kp * pl->ksplit;
+    if (nred > 1) {
         rc = ca3dmm_reduce_slabs_launch((const double *) (w + pl->off_slab),
-                                        (long long) pl->slab_stride, pl->slab_ld, e->kp, e->m,
+                                        (long long) pl->slab_stride, pl->slab_ld, nred, e->m,
                                         e->n, out, ldo, st);
         if (rc) return rc;
     }
@@ -986,7 +1041,8 @@ static int hx_build_bands(ca3dmm_engine_p e, struct host_exec *x, cudaStream_t s
     x->built_mode = e->gemm_mode;
     x->built_slices = e->ozaki_slices;
     x->built_raster = e->raster;
-    if (e->is_BTB || !whole || ((ozaki && pl->oz_fused) ? 1 : e->kp) * tnn > CA3DMM_MAX_RANGES)
+    if (e->is_BTB || !whole || ((ozaki && pl->oz_fused) ? 1 : e->kp) * tnn > CA3DMM_MAX_RANGES ||
+        (!ozaki && pl->ksplit > 1))
         return 0;
     const int raster = e->raster > 0 ? e->raster : 8;
     const int bn = ozaki ? 64 : 128;
@@ -1187,8 +1243,8 @@ static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_
             rc = ca3dmm_pack_launch(x->dA, (double *) w, (const ca3dmm_pack_desc_t *) dd, x->ndesc,
                                     x->ntile[c][0], st);
             if (!rc)
-                rc = ca3dmm_dgemm_launch_ranges(w + pl->off_gemm, pl->ngroup, &x->rng[c], status_d,
-                                                5.0, st);
+                rc = ca3dmm_dgemm_launch_ranges(w + pl->off_gemm, pl->ngroup, &x->rng[c],
+                                                pl->a_kmajor, status_d, 5.0, st);
         }
         if (!rc && e->kp > 1 && !(ozaki && pl->oz_fused))
             rc = ca3dmm_reduce_slabs_launch((const double *) (w + pl->off_slab) + x->r0[c],

@@ -23,8 +23,10 @@ enum {
 
 /* ---- plain FP64 DMMA GEMM, grouped ---------------------------------------
  * One problem: C = alpha * op(A) op(B) + beta * C, where the operands are
- * already packed by the pack kernels:
+ * packed by the pack kernels or read in place:
  *   A: op(A) stored M-major, element (i,l) at A[i + l*lda]   (lda even, A 16B-aligned)
+ *      or, with a_kmajor, K-major: element (i,l) at A[l + i*lda] (the caller's
+ *      transposed A read as it lies)
  *   B: op(B) stored K-major, element (l,j) at B[l + j*ldb]   (ldb even, B 16B-aligned)
  *   C: column-major, element (i,j) at C[i + j*ldc]           (any ldc >= m)      */
 typedef struct {
@@ -34,13 +36,16 @@ typedef struct {
     int m, n, k;
     double alpha, beta;
     int raster;          /* tile rows per raster band (0 = default 8) */
+    int a_kmajor;        /* 1: A is K-major (see above) */
 } ca3dmm_dgemm_desc_t;
 
 /* Bytes of the device plan for nprob problems (tensor maps + problem records). */
 size_t ca3dmm_dgemm_plan_bytes(int nprob);
 /* Encode the plan into host memory `host_plan` (size plan_bytes); the caller
  * copies it to device memory `dev_plan` before launching.  Tensor maps embed
- * the device addresses of A and B.  Returns the total tile count. */
+ * the device addresses of A and B.  Returns the total tile count.  Every
+ * problem of one plan has the same A layout (a_kmajor), which the launch
+ * repeats. */
 int ca3dmm_dgemm_plan_encode(const ca3dmm_dgemm_desc_t *probs, int nprob, void *host_plan,
                              int *total_tiles);
 /* Up to CA3DMM_MAX_RANGES contiguous ranges [begin, begin + len) of a grouped
@@ -53,11 +58,12 @@ typedef struct {
 } ca3dmm_tile_ranges_t;
 
 /* Persistent grouped launch over every tile of every problem. */
-int ca3dmm_dgemm_launch(const void *dev_plan, int nprob, int total_tiles, int *dev_status,
-                        double timeout_s, cudaStream_t stream);
+int ca3dmm_dgemm_launch(const void *dev_plan, int nprob, int total_tiles, int a_kmajor,
+                        int *dev_status, double timeout_s, cudaStream_t stream);
 /* The same over the tiles of `ranges` only. */
 int ca3dmm_dgemm_launch_ranges(const void *dev_plan, int nprob, const ca3dmm_tile_ranges_t *ranges,
-                               int *dev_status, double timeout_s, cudaStream_t stream);
+                               int a_kmajor, int *dev_status, double timeout_s,
+                               cudaStream_t stream);
 
 /* ---- pack / transpose ----------------------------------------------------
  * Batched block copies between column-major matrices.  Descriptor j copies a

@@ -188,7 +188,7 @@ static int cannon_exec_device(cannon_engine_p e, double alpha, double beta, cons
     memset(h, 0, 256);
     CA3DMM_CUDA_TRY(cudaMemcpy(w + cp->off_plan, h, 256 + ca3dmm_dgemm_plan_bytes(1), cudaMemcpyHostToDevice));
     cudaEventRecord(cp->ev[0], 0);
-    rc = ca3dmm_dgemm_launch(w + cp->off_plan + 256, 1, tiles, (int *) (w + cp->off_plan), 5.0, 0);
+    rc = ca3dmm_dgemm_launch(w + cp->off_plan + 256, 1, tiles, 0, (int *) (w + cp->off_plan), 5.0, 0);
     if (rc) return rc;
     cudaEventRecord(cp->ev[1], 0);
     CA3DMM_CUDA_TRY(cudaMemcpy(cp->status_h, w + cp->off_plan, sizeof(int), cudaMemcpyDeviceToHost));

@@ -276,7 +276,7 @@ int ca3dmm_grouped_exec(ca3dmm_grouped_p g, const double *const *A, const int *l
         rc = ca3dmm_pack_launch(NULL, (double *) w, (const ca3dmm_pack_desc_t *) (w + g->off_packB),
                                 g->nprob, g->tiles_B, st);
         if (rc) return rc;
-        rc = ca3dmm_dgemm_launch(w + g->off_gemm, g->nprob, g->gemm_tiles, status, 5.0, st);
+        rc = ca3dmm_dgemm_launch(w + g->off_gemm, g->nprob, g->gemm_tiles, 0, status, 5.0, st);
         if (rc) return rc;
     } else {
         rc = ca3dmm_oz_run_pack(&g->oz, NULL, NULL, st);

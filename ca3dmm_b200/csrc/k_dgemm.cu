@@ -8,7 +8,9 @@
 //
 // Layout (per stage, 32 KiB, 1024-byte aligned):
 //   A tile: 128 (m) x 16 (k) doubles as 8 TMA boxes of 16 m x 16 k, each box
-//           16 rows (k) of 128 B (m), SWIZZLE_128B.
+//           16 rows (k) of 128 B (m), SWIZZLE_128B -- or, for a K-major A
+//           (a transposed operand read in place), 1 box of 128 rows (m) of
+//           128 B (k), like B.
 //   B tile: 128 (n) x 16 (k) doubles as 1 TMA box, 128 rows (n) of 128 B (k),
 //           SWIZZLE_128B.
 // Fragment ownership is permuted so every fragment load is one conflict-free
@@ -20,6 +22,11 @@
 //     chunk of a B row holds the b0 fragments of two consecutive k-steps.
 // With the 128B swizzle (16-byte chunk index XOR row % 8) these choices put
 // every quarter-warp of a 128-bit load on 8 distinct chunks.
+// K-major A: a 16-byte chunk of a tile row holds that row's a0 (or a1) of two
+// consecutive k-steps, as for B.  MMA rows g and g + 8 of m16 tile i are tile
+// rows 16i + 2 sigma(g) and 16i + 2 sigma(g) + 1, sigma swapping the two low
+// bits of g, so the two rows of a quarter-warp differ by 4 (mod 8) and hit
+// disjoint chunk sets, and the C pairs (m, m+1) stay adjacent.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdio>
@@ -134,11 +141,87 @@ struct LoadCursor {
     }
 };
 
+// sigma: swap the two low bits of g (0..7)
+__device__ __forceinline__ int sigma_row(int g) { return (g & 4) | ((g & 1) << 1) | ((g >> 1) & 1); }
+
+// The k loop of one output tile: wait for each stage, run the 16-k block's
+// DMMAs, release the stage and (thread 0) refill it.  AK: A tile K-major.
+template <bool AK, class Issue>
+__device__ __forceinline__ bool k_loop(const uint8_t *smem, uint64_t *full, uint64_t *empty,
+                                       int ktiles, uint32_t &it, double (&acc)[4][4][4],
+                                       volatile int *abort_flag, int *status,
+                                       unsigned long long limit_ns, bool producer,
+                                       Issue &issue_one, int wm, int wn, int g, int t, int lane)
+{
+    for (int kt = 0; kt < ktiles; ++kt, ++it) {
+        const uint32_t stage = it % STAGES, phase = (it / STAGES) & 1u;
+        if (!mbar_wait_bounded(&full[stage], phase, abort_flag, status,
+                               CA3DMM_DEV_TIMEOUT_CONSUME, limit_ns))
+            return false;
+        const uint8_t *sA = smem + stage * STAGE_BYTES;
+        const uint8_t *sB = sA + A_BYTES;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            double2 bf[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                const int nl = wn * 32 + 4 * g + j;
+                bf[j] = *reinterpret_cast<const double2 *>(
+                    sB + nl * 128 + (((4 * q + t) ^ (nl & 7)) << 4));
+            }
+            if (AK) {
+#pragma unroll
+                for (int ip = 0; ip < 2; ++ip) {
+                    double2 alo[2], ahi[2];
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        // K-major A: tile row of MMA row g of m16 tile i
+                        const int ra = wm * 64 + 2 * sigma_row(g) + 16 * (2 * ip + h);
+                        alo[h] = *reinterpret_cast<const double2 *>(
+                            sA + ra * 128 + (((4 * q + t) ^ (ra & 7)) << 4));
+                        ahi[h] = *reinterpret_cast<const double2 *>(
+                            sA + (ra + 1) * 128 + (((4 * q + t) ^ ((ra + 1) & 7)) << 4));
+                    }
+#pragma unroll
+                    for (int b = 0; b < 2; ++b)
+#pragma unroll
+                        for (int h = 0; h < 2; ++h)
+#pragma unroll
+                            for (int j = 0; j < 4; ++j)
+                                dmma(acc[2 * ip + h][j], b ? alo[h].y : alo[h].x,
+                                     b ? ahi[h].y : ahi[h].x, b ? bf[j].y : bf[j].x);
+                    
+                }
+            } else {
+#pragma unroll
+                for (int b = 0; b < 2; ++b) {
+                    const int kr = 8 * q + 2 * t + b;
+                    double2 af[4];
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+                        af[i] = *reinterpret_cast<const double2 *>(
+                            sA + (wm * 4 + i) * 2048 + kr * 128 + ((g ^ (kr & 7)) << 4));
+#pragma unroll
+                    for (int i = 0; i < 4; ++i)
+#pragma unroll
+                        for (int j = 0; j < 4; ++j)
+                            dmma(acc[i][j], af[i].x, af[i].y, b ? bf[j].y : bf[j].x);
+                }
+            }
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[stage]);
+        if (producer && !issue_one()) return false;
+    }
+    return true;
+}
+
 // All 8 warps compute; thread 0 also drives the TMA pipeline.  Load L lands
 // in stage L % STAGES; before issuing it the producer waits for the release
 // of load L - STAGES.  Loads are issued STAGES-1 ahead of consumption, and the
 // refill after consuming load `it` waits on the release of load it - 1, which
 // every warp has usually finished, so the producer thread rarely stalls.
+template <bool AK>
 __global__ void __launch_bounds__(THREADS, 1)
 dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restrict__ probs,
                    int nprob, const ca3dmm_tile_ranges_t rg, int total_tiles, int *status,
@@ -182,9 +265,13 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
         uint8_t *sA = smem + s * STAGE_BYTES;
         uint8_t *sB = sA + A_BYTES;
         mbar_arrive_expect_tx(&full[s], STAGE_BYTES);
+        if (AK) {
+            tma_load_2d(sA, ta, lc.kt * BK, lc.m0, &full[s]);
+        } else {
 #pragma unroll
-        for (int j = 0; j < BM / 16; ++j)
-            tma_load_2d(sA + j * 2048, ta, lc.m0 + 16 * j, lc.kt * BK, &full[s]);
+            for (int j = 0; j < BM / 16; ++j)
+                tma_load_2d(sA + j * 2048, ta, lc.m0 + 16 * j, lc.kt * BK, &full[s]);
+        }
         tma_load_2d(sB, tb, lc.kt * BK, lc.n0, &full[s]);
         ++issued;
         lc.advance(probs, nprob, rg, total_tiles, gridDim.x);
@@ -218,49 +305,11 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
 #pragma unroll
                 for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
 
-        for (int kt = 0; kt < ktiles; ++kt, ++it) {
-            const uint32_t stage = it % STAGES, phase = (it / STAGES) & 1u;
-            if (!mbar_wait_bounded(&full[stage], phase, &abort_flag, status,
-                                   CA3DMM_DEV_TIMEOUT_CONSUME, limit_ns)) {
-                ok = false;
-                break;
-            }
-            const uint8_t *sA = smem + stage * STAGE_BYTES;
-            const uint8_t *sB = sA + A_BYTES;
-#pragma unroll
-            for (int q = 0; q < 2; ++q) {
-                double2 bf[4];
-#pragma unroll
-                for (int j = 0; j < 4; ++j) {
-                    const int nl = wn * 32 + 4 * g + j;
-                    bf[j] = *reinterpret_cast<const double2 *>(
-                        sB + nl * 128 + (((4 * q + t) ^ (nl & 7)) << 4));
-                }
-#pragma unroll
-                for (int b = 0; b < 2; ++b) {
-                    const int kr = 8 * q + 2 * t + b;
-                    double2 af[4];
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-                        af[i] = *reinterpret_cast<const double2 *>(
-                            sA + (wm * 4 + i) * 2048 + kr * 128 + ((g ^ (kr & 7)) << 4));
-#pragma unroll
-                    for (int i = 0; i < 4; ++i)
-#pragma unroll
-                        for (int j = 0; j < 4; ++j)
-                            dmma(acc[i][j], af[i].x, af[i].y, b ? bf[j].y : bf[j].x);
-                }
-            }
-            __syncwarp();
-            if (lane == 0) mbar_arrive(&empty[stage]);
-            if (producer && !issue_one()) {
-                ok = false;
-                break;
-            }
-        }
+        ok = k_loop<AK>(smem, full, empty, ktiles, it, acc, &abort_flag, status, limit_ns,
+                        producer, issue_one, wm, wn, g, t, lane);
         if (!ok) break;
 
-        const int mb = tm * BM + wm * 64 + 2 * g;
+        const int mb = tm * BM + wm * 64 + 2 * (AK ? sigma_row(g) : g);
         const int nb = tn * BN + wn * 32 + 8 * t;
 #pragma unroll
         for (int i = 0; i < 4; ++i)
@@ -345,12 +394,18 @@ extern "C" int ca3dmm_dgemm_plan_encode(const ca3dmm_dgemm_desc_t *probs, int np
     for (int i = 0; i < nprob; ++i) {
         const ca3dmm_dgemm_desc_t &q = probs[i];
         if (q.m < 0 || q.n < 0 || q.k < 0) return CA3DMM_EINVAL;
-        if ((q.lda & 1) || (q.ldb & 1) || q.lda < q.m || q.ldb < q.k) return CA3DMM_EINVAL;
+        if ((q.a_kmajor != 0) != (probs[0].a_kmajor != 0)) return CA3DMM_EINVAL;
+        if ((q.lda & 1) || (q.ldb & 1) || q.lda < (q.a_kmajor ? q.k : q.m) || q.ldb < q.k)
+            return CA3DMM_EINVAL;
         memset(&tm[2 * i], 0, 2 * sizeof(CUtensorMap));
         if (q.m > 0 && q.n > 0 && q.k > 0) {
-            int r = ca3dmm_encode_tmap_2d(&tm[2 * i], 8, q.A, (unsigned long long) q.m,
-                                          (unsigned long long) q.k,
-                                          (unsigned long long) q.lda * 8, 16, 16, 1);
+            int r = q.a_kmajor
+                        ? ca3dmm_encode_tmap_2d(&tm[2 * i], 8, q.A, (unsigned long long) q.k,
+                                                (unsigned long long) q.m,
+                                                (unsigned long long) q.lda * 8, 16, BM, 1)
+                        : ca3dmm_encode_tmap_2d(&tm[2 * i], 8, q.A, (unsigned long long) q.m,
+                                                (unsigned long long) q.k,
+                                                (unsigned long long) q.lda * 8, 16, 16, 1);
             if (r) return r;
             r = ca3dmm_encode_tmap_2d(&tm[2 * i + 1], 8, q.B, (unsigned long long) q.k,
                                       (unsigned long long) q.n, (unsigned long long) q.ldb * 8,
@@ -376,27 +431,32 @@ extern "C" int ca3dmm_dgemm_plan_encode(const ca3dmm_dgemm_desc_t *probs, int np
     return CA3DMM_OK;
 }
 
-extern "C" int ca3dmm_dgemm_launch(const void *dev_plan, int nprob, int total_tiles,
+extern "C" int ca3dmm_dgemm_launch(const void *dev_plan, int nprob, int total_tiles, int a_kmajor,
                                    int *dev_status, double timeout_s, cudaStream_t stream)
 {
     ca3dmm_tile_ranges_t rg;
     memset(&rg, 0, sizeof(rg));
     rg.n = 1;
     rg.len[0] = total_tiles;
-    return ca3dmm_dgemm_launch_ranges(dev_plan, nprob, &rg, dev_status, timeout_s, stream);
+    return ca3dmm_dgemm_launch_ranges(dev_plan, nprob, &rg, a_kmajor, dev_status, timeout_s,
+                                      stream);
 }
 
 extern "C" int ca3dmm_dgemm_launch_ranges(const void *dev_plan, int nprob,
-                                          const ca3dmm_tile_ranges_t *ranges, int *dev_status,
-                                          double timeout_s, cudaStream_t stream)
+                                          const ca3dmm_tile_ranges_t *ranges, int a_kmajor,
+                                          int *dev_status, double timeout_s, cudaStream_t stream)
 {
     if (!ranges || ranges->n < 0 || ranges->n > CA3DMM_MAX_RANGES) return CA3DMM_EINVAL;
     const int total_tiles = range_total(*ranges);
     if (total_tiles <= 0) return CA3DMM_OK;
     static bool attr_done = false;
     if (!attr_done) {
-        CA3DMM_CUDA_TRY(cudaFuncSetAttribute(
-            dgemm_dmma_grouped, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) SMEM_BYTES));
+        CA3DMM_CUDA_TRY(cudaFuncSetAttribute(dgemm_dmma_grouped<false>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int) SMEM_BYTES));
+        CA3DMM_CUDA_TRY(cudaFuncSetAttribute(dgemm_dmma_grouped<true>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int) SMEM_BYTES));
         attr_done = true;
     }
     const CUtensorMap *tm = reinterpret_cast<const CUtensorMap *>(dev_plan);
@@ -404,8 +464,12 @@ extern "C" int ca3dmm_dgemm_launch_ranges(const void *dev_plan, int nprob,
     int grid = ca3dmm_device_sm_count();
     if (grid > total_tiles) grid = total_tiles;
     unsigned long long limit = (unsigned long long) (timeout_s * 1e9);
-    dgemm_dmma_grouped<<<grid, THREADS, SMEM_BYTES, stream>>>(tm, dp, nprob, *ranges, total_tiles,
-                                                               dev_status, limit);
+    if (a_kmajor)
+        dgemm_dmma_grouped<true><<<grid, THREADS, SMEM_BYTES, stream>>>(
+            tm, dp, nprob, *ranges, total_tiles, dev_status, limit);
+    else
+        dgemm_dmma_grouped<false><<<grid, THREADS, SMEM_BYTES, stream>>>(
+            tm, dp, nprob, *ranges, total_tiles, dev_status, limit);
     CA3DMM_CUDA_TRY(cudaGetLastError());
     ca3dmm_note_launch(1);
     return CA3DMM_OK;

@@ -147,7 +147,7 @@ extern "C" int ca3dmm_dgemm_kslab_noalloc(int m, int n, int k, int kp, const dou
     CA3DMM_CUDA_TRY(cudaMemsetAsync(status, 0, sizeof(int), st));
     CA3DMM_CUDA_TRY(cudaMemcpyAsync(scratch + off_plan, host_plan, plan_bytes,
                                     cudaMemcpyHostToDevice, st));
-    rc = ca3dmm_dgemm_launch(scratch + off_plan, kp, tiles, status, 5.0, st);
+    rc = ca3dmm_dgemm_launch(scratch + off_plan, kp, tiles, 0, status, 5.0, st);
     if (rc) return rc;
     if (kp > 1) {
         rc = ca3dmm_reduce_slabs_launch(slabs, (long long) slab_elems, ldp, kp, m, n, C, ldC, st);

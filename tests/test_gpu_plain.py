@@ -161,3 +161,34 @@ def test_caller_workbuf_and_bad_ld(cuda):
     assert e.exec(dA, lda, dB, ldb, dC, m) == 0
     assert np.max(np.abs(from_dev(dC, m, n) - A @ B)) <= 1e-12 * np.max(np.abs(A @ B))
     assert e.exec(dA, m - 1, dB, ldb, dC, m) == 1     # ldA < m is rejected, nothing runs
+
+
+def test_transposed_a_in_place_matches_packed(cuda):
+    """op(A) = A^T read in place as a K-major operand (even ldA, aligned slab
+    starts) gives the same bits as the transposing pack (odd ldA): the DMMA
+    sequence per output element is the same."""
+    m, n, k = 700, 600, 1600
+    A = orc.gen_uniform(41, k, m)
+    B = orc.gen_uniform(42, k, n)
+    dB, ldb = to_dev(B)
+    outs = []
+    for pad in (2, 3):                       # ldA = k + 2 (in place), k + 3 (packed)
+        dA, lda = to_dev(A, pad_ld=k + pad)
+        dC = dev_zeros(m * n)
+        e = cb.Ca3dmmEngine(m, n, k, 1, 0, p=8, proc_grid=(2, 2, 2))
+        assert e.ok and e.exec(dA, lda, dB, ldb, dC, m) == 0
+        outs.append(from_dev(dC, m, n))
+    assert np.array_equal(outs[0], outs[1])
+    _dd_check(outs[0], A, B, 1, 0, m, n, k)
+
+
+@pytest.mark.parametrize("n,k,grid", [(200, 40000, (1, 1, 4)), (130, 9000, (1, 1, 2))])
+def test_btb_k_split_sub_slabs(cuda, n, k, grid):
+    """Few output tiles and long slabs: each slab's k range runs as several
+    sub-slabs with their own C buffers, summed by the slab reduction."""
+    Bm = orc.gen_btb(7, k, n)
+    dB, ldb = to_dev(Bm)
+    dC = dev_zeros(n * n)
+    e = cb.Ca3dmmEngine(n, n, k, p=grid[2], btb=True, proc_grid=grid)
+    assert e.ok and e.exec(None, 0, dB, ldb, dC, n) == 0
+    _dd_check(from_dev(dC, n, n), Bm, Bm, 1, 0, n, n, k)
