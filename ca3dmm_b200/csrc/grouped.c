@@ -14,6 +14,8 @@
 struct ca3dmm_grouped {
     int nprob, mode, slices;
     int *m, *n, *k, *ta, *tb;
+    int *order;                   /* launch order of the problems: longest k first */
+    int a_kmajor;                 /* plain mode: A layout of the launch (the majority's) */
     long long *lda_p, *ldb_p;     /* leading dimensions of the packed copies */
     size_t *offA, *offB;          /* byte offsets of the packed copies */
     /* work buffer layout */
@@ -43,11 +45,34 @@ struct ca3dmm_grouped {
 
 static size_t galign(size_t x) { return (x + GALIGN - 1) / GALIGN * GALIGN; }
 
+/* The persistent GEMM kernels hand out tiles round-robin in launch order, and
+ * a tile's time grows with its problem's k.  Ordering the problems by k,
+ * longest first, makes each round of tiles nearly uniform, so no SM is left
+ * with a long tile while the others idle (longest-processing-time first). */
+static int by_key(const void *a, const void *b)
+{
+    const unsigned long long x = *(const unsigned long long *) a, y = *(const unsigned long long *) b;
+    return x < y ? -1 : (x > y);
+}
+
+/* order[] = problem indices by k descending, ties in index order */
+static int order_by_k(int nprob, const int *k, int *order)
+{
+    unsigned long long *key = (unsigned long long *) malloc(sizeof(unsigned long long) * nprob);
+    if (!key) return CA3DMM_ENOMEM;
+    for (int i = 0; i < nprob; i++)
+        key[i] = ((unsigned long long) (0x7fffffff - k[i]) << 32) | (unsigned) i;
+    qsort(key, (size_t) nprob, sizeof(*key), by_key);
+    for (int i = 0; i < nprob; i++) order[i] = (int) (key[i] & 0xffffffffu);
+    free(key);
+    return CA3DMM_OK;
+}
+
 void ca3dmm_grouped_free(ca3dmm_grouped_p *gp)
 {
     if (!gp || !*gp) return;
     ca3dmm_grouped_p g = *gp;
-    free(g->m); free(g->n); free(g->k); free(g->ta); free(g->tb);
+    free(g->m); free(g->n); free(g->k); free(g->ta); free(g->tb); free(g->order);
     free(g->lda_p); free(g->ldb_p); free(g->offA); free(g->offB);
     free(g->cA); free(g->cB); free(g->cC); free(g->cldA); free(g->cldB); free(g->cldC);
     free(g->gd); free(g->ob); free(g->os); free(g->og);
@@ -81,6 +106,7 @@ int ca3dmm_grouped_init(int nprob, const int *m, const int *n, const int *k, con
     g->sync = 1;
     size_t ni = sizeof(int) * nprob;
     g->m = malloc(ni); g->n = malloc(ni); g->k = malloc(ni); g->ta = malloc(ni); g->tb = malloc(ni);
+    g->order = malloc(ni);
     g->lda_p = malloc(sizeof(long long) * nprob); g->ldb_p = malloc(sizeof(long long) * nprob);
     g->offA = malloc(sizeof(size_t) * nprob); g->offB = malloc(sizeof(size_t) * nprob);
     g->cA = calloc(nprob, sizeof(void *)); g->cB = calloc(nprob, sizeof(void *));
@@ -91,7 +117,7 @@ int ca3dmm_grouped_init(int nprob, const int *m, const int *n, const int *k, con
     g->ob = calloc(2 * (size_t) nprob, sizeof(ca3dmm_oz_blk_t));
     g->os = calloc(2 * (size_t) nprob, sizeof(ca3dmm_oz_src_t));
     g->og = calloc(nprob, sizeof(ca3dmm_oz_group_t));
-    if (!g->m || !g->n || !g->k || !g->ta || !g->tb || !g->lda_p || !g->ldb_p || !g->offA ||
+    if (!g->m || !g->n || !g->k || !g->ta || !g->tb || !g->order || !g->lda_p || !g->ldb_p || !g->offA ||
         !g->offB || !g->cA || !g->cB || !g->cC || !g->cldA || !g->cldB || !g->cldC || !g->gd ||
         !g->ob || !g->os || !g->og) {
         ca3dmm_grouped_free(&g);
@@ -102,6 +128,10 @@ int ca3dmm_grouped_init(int nprob, const int *m, const int *n, const int *k, con
         g->ta[i] = trans_A ? (trans_A[i] != 0) : 0;
         g->tb[i] = trans_B ? (trans_B[i] != 0) : 0;
     }
+    if (order_by_k(nprob, g->k, g->order)) {
+        ca3dmm_grouped_free(&g);
+        return CA3DMM_ENOMEM;
+    }
     size_t off = 0;
     g->off_status = off; off = galign(off + 64);
     g->off_packA = off; off = galign(off + sizeof(ca3dmm_pack_desc_t) * nprob);
@@ -111,10 +141,16 @@ int ca3dmm_grouped_init(int nprob, const int *m, const int *n, const int *k, con
     g->stage_bytes = off;
     g->off_A = off;
     if (gemm_mode == 0) {
+        /* One A layout per DMMA launch: K-major when most A bytes are
+         * transposed (those are then read in place), else M-major. */
+        double bytes_t = 0.0, bytes_n = 0.0;
+        for (int i = 0; i < nprob; i++) *(g->ta[i] ? &bytes_t : &bytes_n) += (double) m[i] * k[i];
+        g->a_kmajor = bytes_t > bytes_n;
         for (int i = 0; i < nprob; i++) {
-            g->lda_p[i] = ca3dmm_round_up(m[i], 2);
+            g->lda_p[i] = ca3dmm_round_up(g->a_kmajor ? k[i] : m[i], 2);
             g->offA[i] = off;
-            off = galign(off + sizeof(double) * (size_t) g->lda_p[i] * (size_t) k[i]);
+            off = galign(off + sizeof(double) * (size_t) g->lda_p[i] *
+                                   (size_t) (g->a_kmajor ? m[i] : k[i]));
         }
         g->off_B = off;
         for (int i = 0; i < nprob; i++) {
@@ -193,26 +229,45 @@ static int build_plan(ca3dmm_grouped_p g, const double *const *A, const int *ldA
     if (g->mode == 0) {
         ca3dmm_pack_desc_t *pa = (ca3dmm_pack_desc_t *) (h + g->off_packA);
         ca3dmm_pack_desc_t *pb = (ca3dmm_pack_desc_t *) (h + g->off_packB);
+        /* An operand in the launch's layout with an even leading dimension and a
+         * 16-byte aligned start is read in place; the others are packed (A into
+         * the launch's layout, B K-major). */
+        const int ak = g->a_kmajor;
         for (int i = 0; i < np; i++) {
             /* sources by absolute address (NULL base), packed copies relative to w */
+            const int a_direct = g->ta[i] == ak && !(ldA[i] & 1) && !((uintptr_t) A[i] & 15);
+            const int b_direct = !g->tb[i] && !(ldB[i] & 1) && !((uintptr_t) B[i] & 15);
             memset(&pa[i], 0, sizeof(pa[i]));
-            pa[i].rows = g->m[i]; pa[i].cols = g->k[i]; pa[i].trans = g->ta[i];
-            pa[i].lds = ldA[i];
-            pa[i].src_off = (long long) ((uintptr_t) A[i] / sizeof(double));
-            pa[i].dst_off = (long long) (g->offA[i] / sizeof(double));
-            pa[i].ldd = g->lda_p[i];
+            if (!a_direct) {
+                /* K-major copy of op(A) = the k x m matrix op(A)^T */
+                pa[i].rows = ak ? g->k[i] : g->m[i];
+                pa[i].cols = ak ? g->m[i] : g->k[i];
+                pa[i].trans = ak ? !g->ta[i] : g->ta[i];
+                pa[i].lds = ldA[i];
+                pa[i].src_off = (long long) ((uintptr_t) A[i] / sizeof(double));
+                pa[i].dst_off = (long long) (g->offA[i] / sizeof(double));
+                pa[i].ldd = g->lda_p[i];
+            }
             memset(&pb[i], 0, sizeof(pb[i]));
-            pb[i].rows = g->k[i]; pb[i].cols = g->n[i]; pb[i].trans = g->tb[i];
-            pb[i].lds = ldB[i];
-            pb[i].src_off = (long long) ((uintptr_t) B[i] / sizeof(double));
-            pb[i].dst_off = (long long) (g->offB[i] / sizeof(double));
-            pb[i].ldd = g->ldb_p[i];
-            ca3dmm_dgemm_desc_t *q = &g->gd[i];
-            q->A = (const double *) (w + g->offA[i]); q->lda = g->lda_p[i];
-            q->B = (const double *) (w + g->offB[i]); q->ldb = g->ldb_p[i];
+            if (!b_direct) {
+                pb[i].rows = g->k[i]; pb[i].cols = g->n[i]; pb[i].trans = g->tb[i];
+                pb[i].lds = ldB[i];
+                pb[i].src_off = (long long) ((uintptr_t) B[i] / sizeof(double));
+                pb[i].dst_off = (long long) (g->offB[i] / sizeof(double));
+                pb[i].ldd = g->ldb_p[i];
+            }
+        }
+        for (int j = 0; j < np; j++) {
+            const int i = g->order[j];
+            ca3dmm_dgemm_desc_t *q = &g->gd[j];
+            if (pa[i].rows) { q->A = (const double *) (w + g->offA[i]); q->lda = g->lda_p[i]; }
+            else { q->A = A[i]; q->lda = ldA[i]; }
+            if (pb[i].rows) { q->B = (const double *) (w + g->offB[i]); q->ldb = g->ldb_p[i]; }
+            else { q->B = B[i]; q->ldb = ldB[i]; }
             q->C = C[i]; q->ldc = ldC[i];
             q->m = g->m[i]; q->n = g->n[i]; q->k = g->k[i];
             q->alpha = 1.0; q->beta = 0.0;
+            q->a_kmajor = ak;
         }
         g->tiles_A = ca3dmm_pack_tiles(pa, np);
         g->tiles_B = ca3dmm_pack_tiles(pb, np);
@@ -227,9 +282,12 @@ static int build_plan(ca3dmm_grouped_p g, const double *const *A, const int *ldA
             g->ob[np + i].rows = g->k[i]; g->ob[np + i].cols = g->n[i];
             g->ob[np + i].alias = -1;
             g->os[np + i].base = B[i]; g->os[np + i].ld = ldB[i]; g->os[np + i].trans = g->tb[i];
-            g->og[i].a_blk = i; g->og[i].b_blk = i;
-            g->og[i].C = C[i]; g->og[i].ldc = ldC[i];
-            g->og[i].m = g->m[i]; g->og[i].n = g->n[i]; g->og[i].k = g->k[i];
+        }
+        for (int j = 0; j < np; j++) {
+            const int i = g->order[j];
+            g->og[j].a_blk = i; g->og[j].b_blk = i;
+            g->og[j].C = C[i]; g->og[j].ldc = ldC[i];
+            g->og[j].m = g->m[i]; g->og[j].n = g->n[i]; g->og[j].k = g->k[i];
         }
         int rc = ca3dmm_oz_plan_encode(&g->oz, g->slices, np, g->ob, g->os, np, g->ob + np,
                                        g->os + np, np, g->og, 0, NULL, w + g->off_oz, g->oz_bytes,
@@ -276,7 +334,8 @@ int ca3dmm_grouped_exec(ca3dmm_grouped_p g, const double *const *A, const int *l
         rc = ca3dmm_pack_launch(NULL, (double *) w, (const ca3dmm_pack_desc_t *) (w + g->off_packB),
                                 g->nprob, g->tiles_B, st);
         if (rc) return rc;
-        rc = ca3dmm_dgemm_launch(w + g->off_gemm, g->nprob, g->gemm_tiles, 0, status, 5.0, st);
+        rc = ca3dmm_dgemm_launch(w + g->off_gemm, g->nprob, g->gemm_tiles, g->a_kmajor, status,
+                                 5.0, st);
         if (rc) return rc;
     } else {
         rc = ca3dmm_oz_run_pack(&g->oz, NULL, NULL, st);

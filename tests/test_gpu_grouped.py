@@ -24,23 +24,28 @@ def _batch(seed, nprob, lo=16, hi=700):
     return probs
 
 
-def _upload(probs):
+def _upload(probs, even=False):
     dA, dB, dC, lda, ldb, ldc = [], [], [], [], [], []
     for m, n, k, ta, tb, A, B in probs:
-        a, la = to_dev(A, pad_ld=A.shape[0] + 1)     # odd pads exercise the pack path
-        b, lb = to_dev(B)
+        if even:     # even leading dimensions: operands in the launch's layout are read in place
+            a, la = to_dev(A, pad_ld=A.shape[0] + (2 if A.shape[0] % 2 == 0 else 1))
+            b, lb = to_dev(B, pad_ld=B.shape[0] + (2 if B.shape[0] % 2 == 0 else 1))
+        else:        # odd pads exercise the pack path
+            a, la = to_dev(A, pad_ld=A.shape[0] + 1)
+            b, lb = to_dev(B)
         dA.append(a); lda.append(la); dB.append(b); ldb.append(lb)
         dC.append(dev_zeros(m * n)); ldc.append(m)
     return dA, dB, dC, lda, ldb, ldc
 
 
-@pytest.mark.parametrize("mode,slices", [(cb.GEMM_PLAIN, 0), (cb.GEMM_OZAKI, 7)])
-def test_grouped_batch(cuda, mode, slices):
+@pytest.mark.parametrize("mode,slices,even", [(cb.GEMM_PLAIN, 0, False), (cb.GEMM_PLAIN, 0, True),
+                                              (cb.GEMM_OZAKI, 7, False)])
+def test_grouped_batch(cuda, mode, slices, even):
     probs = _batch(5, 40)
     g = cb.GroupedGemm([p[0] for p in probs], [p[1] for p in probs], [p[2] for p in probs],
                        [p[3] for p in probs], [p[4] for p in probs], mode=mode, slices=slices)
     assert g.ok
-    dA, dB, dC, lda, ldb, ldc = _upload(probs)
+    dA, dB, dC, lda, ldb, ldc = _upload(probs, even)
     assert g.exec(dA, lda, dB, ldb, dC, ldc) == 0
     for i, (m, n, k, ta, tb, A, B) in enumerate(probs):
         got = from_dev(dC[i], m, n)
