@@ -42,6 +42,7 @@ def parse():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--trans-a", type=int, default=0)
+    ap.add_argument("--trans-b", type=int, default=0)
     ap.add_argument("--size", type=int, default=M)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="square", choices=["square", "grouped", "btb"],
@@ -49,6 +50,8 @@ def parse():
                          "independent GEMMs in one graph-captured launch; btb: B^T B of a "
                          "1048576 x 512 B on a 1x1x32 grid")
     ap.add_argument("--nprob", type=int, default=256)
+    ap.add_argument("--btb-rows", type=int, default=1048576,
+                    help="rows of B for --workload btb (smaller values: profiling captures)")
     ap.add_argument("--no-slice-sweep", action="store_true",
                     help="skip timing the other split-precision slice counts")
     return ap.parse_args()
@@ -161,7 +164,7 @@ def cpu_cores():
         return os.cpu_count() or 1
 
 
-def ref_cpu_run(A, B, ta, n, ntest):
+def ref_cpu_run(A, B, ta, n, ntest, tb=0):
     """The reference's own CPU path (src/ca3dmm.c, DEV_TYPE_HOST, OpenBLAS),
     compiled unmodified under the thread-backed MPI subset: P rank threads
     with one BLAS thread each, driven as examples/example_AB.c drives it (one
@@ -170,17 +173,17 @@ def ref_cpu_run(A, B, ta, n, ntest):
     from oracle import oracle as orc
     if orc.ref_lib() is None:
         return None
-    _, times, _, _ = orc.ref_ca3dmm(P, n, n, n, ta, 0, A, B, grid=GRID, ntest=ntest, timeout=600.0)
+    _, times, _, _ = orc.ref_ca3dmm(P, n, n, n, ta, tb, A, B, grid=GRID, ntest=ntest, timeout=600.0)
     return list(times[:, 0])
 
 
-def cpu_baseline(A, B, ta, n, budget_s=20.0):
+def cpu_baseline(A, B, ta, n, budget_s=20.0, tb=0):
     """CPU baseline on this host: the reference's own CPU path when it was
     built (kind "reference"), else the oracle's numpy restatement of the
     virtual-rank algorithm on k-slab 0 (kind "port")."""
     from oracle import oracle as orc
     flops = 2.0 * n * n * n
-    ms = ref_cpu_run(A, B, ta, n, 1)
+    ms = ref_cpu_run(A, B, ta, n, 1, tb)
     if ms is not None:
         return {"value": flops / (ms[0] * 1e-3) / 1e12, "unit": "TFLOP/s",
                 "cores": min(P, cpu_cores()), "kind": "reference",
@@ -194,7 +197,7 @@ def cpu_baseline(A, B, ta, n, budget_s=20.0):
         pass
     k0, kz = orc.block_spos_size(n, 3, 0)
     Ask = np.asfortranarray((A.T if ta else A)[:, k0:k0 + kz])
-    Bsk = np.asfortranarray(B[k0:k0 + kz, :])
+    Bsk = np.asfortranarray((B.T if tb else B)[k0:k0 + kz, :])
     reps, t = 0, 0.0
     while True:
         t0 = time.perf_counter()
@@ -219,7 +222,7 @@ def reference_arm(args, world, rank):
     A, B = make_inputs(n, args.trans_a)
     steps, warm = max(args.steps, 1), max(args.warmup, 0)
     flops = 2.0 * n * n * n
-    ms = ref_cpu_run(A, B, args.trans_a, n, warm + steps)
+    ms = ref_cpu_run(A, B, args.trans_a, n, warm + steps, args.trans_b)
     if ms is not None:
         t = float(np.mean(ms[warm:]))
         v = flops / (t * 1e-3) / 1e12
@@ -231,9 +234,9 @@ def reference_arm(args, world, rank):
     else:
         vals = []
         for _ in range(warm):
-            cpu_baseline(A, B, args.trans_a, n, budget_s=4.0)
+            cpu_baseline(A, B, args.trans_a, n, budget_s=4.0, tb=args.trans_b)
         for _ in range(steps):
-            base = cpu_baseline(A, B, args.trans_a, n, budget_s=4.0)
+            base = cpu_baseline(A, B, args.trans_a, n, budget_s=4.0, tb=args.trans_b)
             vals.append(base["value"])
         v = float(np.median(vals))
         base["value"] = v
@@ -243,8 +246,9 @@ def reference_arm(args, world, rank):
             "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": t,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": "ca3dmm_exec M=N=K=%d transA=%d grid 4x2x3 (24 virtual ranks)"
-                                   % (n, args.trans_a), "l2": "inputs larger than L2"},
+            "config": {"workload": "ca3dmm_exec M=N=K=%d transA=%d transB=%d grid 4x2x3 (24 "
+                                   "virtual ranks)" % (n, args.trans_a, args.trans_b),
+                       "l2": "inputs larger than L2"},
             "cpu_baseline": base,
             "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
@@ -328,7 +332,7 @@ def run_grouped(args, world, rank, local):
     print(json.dumps(out), flush=True)
 
 
-BTB_K, BTB_N, BTB_P, BTB_GRID = 1048576, 512, 32, (1, 1, 32)
+BTB_N, BTB_P, BTB_GRID = 512, 32, (1, 1, 32)
 
 
 def make_btb(k, n, seed=303):
@@ -344,20 +348,24 @@ def make_btb(k, n, seed=303):
 
 def workload(args):
     if args.workload == "btb":
-        B = make_btb(BTB_K, BTB_N)
-        return {"m": BTB_N, "n": BTB_N, "k": BTB_K, "ta": 0, "btb": True, "p": BTB_P,
+        rows = args.btb_rows
+        B = make_btb(rows, BTB_N)
+        return {"m": BTB_N, "n": BTB_N, "k": rows, "ta": 0, "tb": 0, "btb": True, "p": BTB_P,
                 "grid": BTB_GRID, "A": None, "B": B,
-                "label": "btb %dx%d grid 1x1x32" % (BTB_K, BTB_N),
+                "label": "btb %dx%d grid 1x1x32" % (rows, BTB_N),
                 "desc": "ca3dmm_exec B^T B, B %dx%d, columns N(0,1)*10^u, u in [-3,3], 32 virtual "
-                        "ranks on grid 1x1x32 (kp-slab reduction on device)" % (BTB_K, BTB_N),
-                "l2": "B is 4.3 GB, larger than L2, no flush"}
+                        "ranks on grid 1x1x32 (kp-slab reduction on device)" % (rows, BTB_N),
+                "l2": "B is %.1f GB%s, no flush" % (rows * BTB_N * 8 / 1e9,
+                                                    ", larger than L2" if rows * BTB_N * 8 > 126e6
+                                                    else "")}
     n = args.size
     A, B = make_inputs(n, args.trans_a)
-    return {"m": n, "n": n, "k": n, "ta": args.trans_a, "btb": False, "p": P, "grid": GRID,
+    return {"m": n, "n": n, "k": n, "ta": args.trans_a, "tb": args.trans_b, "btb": False, "p": P,
+            "grid": GRID,
             "A": A, "B": B, "label": "square %d^3 grid 4x2x3" % n,
-            "desc": "ca3dmm_exec M=N=K=%d transA=%d transB=0, 24 virtual ranks, grid 4x2x3 "
+            "desc": "ca3dmm_exec M=N=K=%d transA=%d transB=%d, 24 virtual ranks, grid 4x2x3 "
                     "(cuboid 2000x4000x2667), entries sign*(1+u)*2^e, e in [-8,8]"
-                    % (n, args.trans_a),
+                    % (n, args.trans_a, args.trans_b),
             "l2": "inputs larger than L2 (512 MB per operand), no flush"}
 
 
@@ -371,7 +379,7 @@ def sampled_error(Cdev, wl, nsample=2048):
         hi, lo, ab = orc.dd_entries(wl["B"], wl["B"], 1, 0, k, ii, jj)
     else:
         ii, jj = orc.sample_indices(m, n, nrand=nsample, nlines=1)
-        hi, lo, ab = orc.dd_entries(wl["A"], wl["B"], wl["ta"], 0, k, ii, jj)
+        hi, lo, ab = orc.dd_entries(wl["A"], wl["B"], wl["ta"], wl["tb"], k, ii, jj)
     idx = torch.from_numpy(ii + jj * m).cuda()
     return orc.errors(Cdev[idx].cpu().numpy(), hi, lo, ab)
 
@@ -421,7 +429,7 @@ def main():
     flops = 2.0 * m * n * k
 
     def engine():
-        return cb.Ca3dmmEngine(m, n, k, ta, 0, p=wl["p"], proc_grid=wl["grid"], btb=btb)
+        return cb.Ca3dmmEngine(m, n, k, ta, wl["tb"], p=wl["p"], proc_grid=wl["grid"], btb=btb)
 
     def leg(eng, steps, warmup):
         for _ in range(warmup):
@@ -551,7 +559,7 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = btb_cpu_baseline(wl) if btb else \
-            cpu_baseline(wl["A"], wl["B"], ta, n)
+            cpu_baseline(wl["A"], wl["B"], ta, n, tb=wl["tb"])
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:

@@ -38,7 +38,8 @@ typedef struct {
 
 typedef struct {
     int rows, cols, r0, c0;   /* block of op(X): rows x cols starting at (r0, c0) */
-    long long ld;             /* leading dimension of the packed copy */
+    long long ld;             /* leading dimension of the packed copy (M-major op(A), K-major op(B)) */
+    long long kld;            /* op(A) blocks: leading dimension of a K-major packed copy */
     size_t off;               /* byte offset of the packed copy in the work buffer */
     const double *direct;     /* plain mode: the caller's block used in place (NULL: packed) */
     long long direct_ld;
@@ -174,7 +175,10 @@ static void plan_layout(ca3dmm_engine_p e, plan_t *pl)
     pl->off_A = off;
     for (int i = 0; i < pl->nA; i++) {
         pl->A[i].off = off + packs;
-        packs += align_up(sizeof(double) * (size_t) pl->A[i].ld * (size_t) pl->A[i].cols);
+        /* room for either packed layout: M-major (ld x cols) or K-major (kld x rows) */
+        const size_t mm = (size_t) pl->A[i].ld * (size_t) pl->A[i].cols;
+        const size_t km = (size_t) pl->A[i].kld * (size_t) pl->A[i].rows;
+        packs += align_up(sizeof(double) * (mm > km ? mm : km));
     }
     off += packs;
     packs = 0;
@@ -271,6 +275,7 @@ static int plan_build(ca3dmm_engine_p e)
             blk_t *a = &pl->A[tk * tmn + tm];
             a->rows = mz; a->cols = kz; a->r0 = ms; a->c0 = ks;
             a->ld = ca3dmm_round_up(mz > 0 ? mz : 1, 2);
+            a->kld = ca3dmm_round_up(kz > 0 ? kz : 1, 2);
         }
         for (int tn = 0; tn < tnn; tn++) {
             int ns, nz;
@@ -665,6 +670,29 @@ void ca3dmm_engine_free(ca3dmm_engine_p *engine_)
     *engine_ = NULL;
 }
 
+/* Pack descriptor of op(A) rows [r, rend) of block b from a source with
+ * leading dimension lds: an M-major (transposing when trans_A) copy, or, when
+ * the launch reads A K-major, a plain copy of the transposed source's columns
+ * into the K-major layout. */
+static void a_pack_desc(const ca3dmm_engine_p e, const plan_t *pl, const blk_t *b, int r, int rend,
+                        long long lds, ca3dmm_pack_desc_t *d)
+{
+    memset(d, 0, sizeof(*d));
+    d->lds = lds;
+    if (pl->a_kmajor) {
+        d->rows = b->cols; d->cols = rend - r; d->trans = 0;
+        d->src_off = (long long) b->c0 + (long long) (b->r0 + r) * lds;
+        d->dst_off = (long long) (b->off / sizeof(double)) + (long long) r * b->kld;
+        d->ldd = b->kld;
+    } else {
+        d->rows = rend - r; d->cols = b->cols; d->trans = e->trans_A;
+        d->src_off = e->trans_A ? (long long) b->c0 + (long long) (b->r0 + r) * lds
+                                : (long long) (b->r0 + r) + (long long) b->c0 * lds;
+        d->dst_off = (long long) (b->off / sizeof(double)) + r;
+        d->ldd = b->ld;
+    }
+}
+
 /* Build the per-call device plan into pinned staging and upload it. */
 static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B, int ldB,
                        void *dst, int ldC, cudaStream_t st)
@@ -677,33 +705,26 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
      * (K-major, when every A block qualifies: one A layout per launch).  The
      * others are packed (and transposed) into the work buffer. */
     ca3dmm_pack_desc_t *pa = (ca3dmm_pack_desc_t *) (h + pl->off_packA);
+    /* A transposed op(A) with an even ldA is read K-major: blocks with an
+     * aligned start in place, the others (an odd first k index) copied, not
+     * transposed, into the K-major layout. */
     pl->a_kmajor = e->trans_A && (ldA & 1) == 0;
-    for (int i = 0; i < pl->nA && pl->a_kmajor; i++) {
-        const blk_t *b = &pl->A[i];
-        const long long off = (long long) b->c0 + (long long) b->r0 * ldA;
-        if ((((uintptr_t) A + sizeof(double) * (uintptr_t) off) & 15) != 0) pl->a_kmajor = 0;
-    }
     for (int i = 0; i < pl->nA; i++) {
         blk_t *b = &pl->A[i];
         ca3dmm_pack_desc_t *d = &pa[i];
-        memset(d, 0, sizeof(*d));
-        d->rows = b->rows; d->cols = b->cols; d->trans = e->trans_A; d->lds = ldA;
-        d->src_off = e->trans_A ? (long long) b->c0 + (long long) b->r0 * ldA
-                                : (long long) b->r0 + (long long) b->c0 * ldA;
-        d->dst_off = (long long) ((b->off) / sizeof(double));
-        d->ldd = b->ld;
+        a_pack_desc(e, pl, b, 0, b->rows, ldA, d);
         b->direct = NULL;
-        if ((!e->trans_A && (ldA & 1) == 0 &&
-             (((uintptr_t) A + sizeof(double) * (uintptr_t) d->src_off) & 15) == 0) ||
-            pl->a_kmajor) {
+        if ((!e->trans_A || pl->a_kmajor) && (ldA & 1) == 0 &&
+            (((uintptr_t) A + sizeof(double) * (uintptr_t) d->src_off) & 15) == 0) {
             b->direct = (const double *) A + d->src_off;
             b->direct_ld = ldA;
             d->rows = 0;
         }
     }
     pl->packA_tma = 0;
-    if (e->trans_A && ca3dmm_pack_tma_prepare(pa, pl->nA, (const double *) A, h + pl->off_tmapA,
-                                              &pl->pack_tiles_A) == CA3DMM_OK)
+    if (e->trans_A && !pl->a_kmajor &&
+        ca3dmm_pack_tma_prepare(pa, pl->nA, (const double *) A, h + pl->off_tmapA,
+                                &pl->pack_tiles_A) == CA3DMM_OK)
         pl->packA_tma = 1;
     else
         pl->pack_tiles_A = ca3dmm_pack_tiles(pa, pl->nA);
@@ -749,7 +770,7 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
         group_t *g = &pl->groups[i];
         const blk_t *ba = &pl->A[g->a_blk], *bb = &pl->B[g->b_blk];
         const double *a = ba->direct ? ba->direct : (const double *) (w + ba->off);
-        const long long lda = ba->direct ? ba->direct_ld : ba->ld;
+        const long long lda = ba->direct ? ba->direct_ld : (pl->a_kmajor ? ba->kld : ba->ld);
         const double *b = bb->direct ? bb->direct : (const double *) (w + bb->off);
         const long long ldb = bb->direct ? bb->direct_ld : bb->ld;
         for (int sub = 0; sub < ks; sub++) {
@@ -1112,11 +1133,7 @@ static int hx_build_bands(ca3dmm_engine_p e, struct host_exec *x, cudaStream_t s
                     ca3dmm_pack_desc_t *d = &pd[tk];
                     memset(d, 0, sizeof(*d));
                     if (b->direct) continue;         /* read in place by the GEMM */
-                    d->rows = rend - r; d->cols = b->cols; d->trans = e->trans_A; d->lds = x->lda;
-                    d->src_off = e->trans_A ? (long long) b->c0 + (long long) (b->r0 + r) * x->lda
-                                            : (long long) (b->r0 + r) + (long long) b->c0 * x->lda;
-                    d->dst_off = (long long) (b->off / sizeof(double)) + r;
-                    d->ldd = b->ld;
+                    a_pack_desc(e, pl, b, r, rend, x->lda, d);
                 }
                 x->ntile[c][0] = ca3dmm_pack_tiles(pd, e->kp);
             }

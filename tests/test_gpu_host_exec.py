@@ -23,6 +23,7 @@ def _pinned(x):
     (3000, 257, 700, 1, 0, 6, None),
     (2600, 300, 500, 0, 1, 4, (2, 1, 2)),
     (1500, 1500, 64, 1, 1, 1, None),
+    (2600, 300, 901, 1, 0, 8, (2, 2, 2)),       # odd ldA on the device, even in staging; odd slab start
     (4100, 2600, 300, 0, 0, 24, (4, 2, 3)),    # split mode chains the 3 slabs per tile
 ])
 @pytest.mark.parametrize("mode,slices", [(cb.GEMM_PLAIN, 0), (cb.GEMM_OZAKI, 7)])

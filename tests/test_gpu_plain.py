@@ -163,17 +163,20 @@ def test_caller_workbuf_and_bad_ld(cuda):
     assert e.exec(dA, m - 1, dB, ldb, dC, m) == 1     # ldA < m is rejected, nothing runs
 
 
-def test_transposed_a_in_place_matches_packed(cuda):
-    """op(A) = A^T read in place as a K-major operand (even ldA, aligned slab
-    starts) gives the same bits as the transposing pack (odd ldA): the DMMA
-    sequence per output element is the same."""
-    m, n, k = 700, 600, 1600
+@pytest.mark.parametrize("k", [1600, 1601])
+def test_transposed_a_in_place_matches_packed(cuda, k):
+    """op(A) = A^T read K-major (even ldA: slabs with an aligned start in place,
+    k = 1601's second slab, starting at the odd k index 801, copied into the
+    K-major layout) gives the same bits as the transposing pack into the
+    M-major layout (odd ldA): the DMMA sequence per output element is the same."""
+    m, n = 700, 600
     A = orc.gen_uniform(41, k, m)
     B = orc.gen_uniform(42, k, n)
     dB, ldb = to_dev(B)
     outs = []
-    for pad in (2, 3):                       # ldA = k + 2 (in place), k + 3 (packed)
-        dA, lda = to_dev(A, pad_ld=k + pad)
+    even_ld = k + 2 - k % 2
+    for ld in (even_ld, even_ld + 1):        # K-major (in place / copied), M-major (packed)
+        dA, lda = to_dev(A, pad_ld=ld)
         dC = dev_zeros(m * n)
         e = cb.Ca3dmmEngine(m, n, k, 1, 0, p=8, proc_grid=(2, 2, 2))
         assert e.ok and e.exec(dA, lda, dB, ldb, dC, m) == 0
