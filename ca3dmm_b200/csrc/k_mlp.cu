@@ -59,24 +59,32 @@ __global__ void mse_grad(const float *__restrict__ out, const float *__restrict_
     if (threadIdx.x == 0) *loss = part[0] / (float) B;
 }
 
-// dW[o][i] = sum_r dY[r][o] X[r][i], db[o] = sum_r dY[r][o]  (thread per (o, i))
-__global__ void dense_wgrad(const float *__restrict__ dY, const float *__restrict__ X,
-                            float *__restrict__ dW, float *__restrict__ db, int B, int nin,
-                            int nout)
+// dW[o][i] = sum_r dY[r][o] X[r][i], db[o] = sum_r dY[r][o].  Block (o, group of
+// 32 columns; column nin is the bias, X = 1): warp w sums the rows r = w, w + 8,
+// ... of its lane's column, then the 8 partial sums are added in warp order --
+// a fixed order, so the gradient does not depend on scheduling.
+constexpr int WG_WARPS = 8;
+__global__ void __launch_bounds__(WG_WARPS * 32)
+dense_wgrad(const float *__restrict__ dY, const float *__restrict__ X, float *__restrict__ dW,
+            float *__restrict__ db, int B, int nin, int nout)
 {
-    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx < nout * nin) {
-        const int o = idx / nin, i = idx % nin;
-        float s = 0.f;
-        for (int r = 0; r < B; ++r) s += dY[r * nout + o] * X[r * nin + i];
-        dW[idx] = s;
-    } else if (idx < nout * nin + nout) {
-        const int o = idx - nout * nin;
-        float s = 0.f;
-        for (int r = 0; r < B; ++r) s += dY[r * nout + o];
-        db[o] = s;
+    __shared__ float part[WG_WARPS][32];
+    const int o = blockIdx.x, lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int i = blockIdx.y * 32 + lane;
+    float s = 0.f;
+    if (i <= nin)
+        for (int r = w; r < B; r += WG_WARPS) s += dY[r * nout + o] * (i < nin ? X[r * nin + i] : 1.f);
+    part[w][lane] = s;
+    __syncthreads();
+    if (w == 0 && i <= nin) {
+        float t = 0.f;
+#pragma unroll
+        for (int q = 0; q < WG_WARPS; ++q) t += part[q][lane];
+        if (i < nin) dW[o * nin + i] = t; else db[o] = t;
     }
 }
+
+inline dim3 wgrad_grid(int nin, int nout) { return dim3(nout, (nin + 1 + 31) / 32); }
 
 // dX[r][i] = (sum_o dY[r][o] W[o][i]) * (A[r][i] > 0)   (ReLU of the layer below)
 __global__ void dense_xgrad(const float *__restrict__ dY, const float *__restrict__ W,
@@ -149,11 +157,13 @@ int fwd_bwd(ca3dmm_mlp *m, int B)
     float *gW1 = m->grads, *gb1 = gW1 + m->h1 * m->nin, *gW2 = gb1 + m->h1,
           *gb2 = gW2 + m->h2 * m->h1, *gW3 = gb2 + m->h2, *gb3 = gW3 + m->h2;
     mse_grad<<<1, 256>>>(m->out, m->y, m->dout, m->loss, B);
-    dense_wgrad<<<blocks(m->h2 + 1), 256>>>(m->dout, m->a2, gW3, gb3, B, m->h2, 1);
+    dense_wgrad<<<wgrad_grid(m->h2, 1), WG_WARPS * 32>>>(m->dout, m->a2, gW3, gb3, B, m->h2, 1);
     dense_xgrad<<<blocks((long long) B * m->h2), 256>>>(m->dout, W3, m->a2, m->d2, B, m->h2, 1);
-    dense_wgrad<<<blocks(m->h2 * m->h1 + m->h2), 256>>>(m->d2, m->a1, gW2, gb2, B, m->h1, m->h2);
+    dense_wgrad<<<wgrad_grid(m->h1, m->h2), WG_WARPS * 32>>>(m->d2, m->a1, gW2, gb2, B, m->h1,
+                                                             m->h2);
     dense_xgrad<<<blocks((long long) B * m->h1), 256>>>(m->d2, W2, m->a1, m->d1, B, m->h1, m->h2);
-    dense_wgrad<<<blocks(m->h1 * m->nin + m->h1), 256>>>(m->d1, m->X, gW1, gb1, B, m->nin, m->h1);
+    dense_wgrad<<<wgrad_grid(m->nin, m->h1), WG_WARPS * 32>>>(m->d1, m->X, gW1, gb1, B, m->nin,
+                                                              m->h1);
     (void) W1;
     CA3DMM_CUDA_TRY(cudaGetLastError());
     ca3dmm_note_launch(6);
