@@ -54,12 +54,16 @@ struct alignas(16) DProb {
     int vec_ok, raster;
 };
 
-__device__ __forceinline__ int find_problem(const DProb *probs, int nprob, int tile)
+// The problem holding tile `tile`.  sb: a shared-memory copy of the problems'
+// first tiles (nullptr when there are more than PROB_CACHE problems), so that a
+// batch of small GEMMs does not pay a chain of dependent global loads per tile.
+constexpr int PROB_CACHE = 1024;
+__device__ __forceinline__ int find_problem(const int *sb, const DProb *probs, int nprob, int tile)
 {
     int lo = 0, hi = nprob - 1;
     while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;
-        if (probs[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
+        if ((sb ? sb[mid] : probs[mid].tile_begin) <= tile) lo = mid; else hi = mid - 1;
     }
     return lo;
 }
@@ -111,12 +115,12 @@ __device__ __forceinline__ void store_pair(const DProb &p, int m, int n, double 
 struct LoadCursor {
     int tile, kt, ktiles, pi, m0, n0;   // tile: virtual index into the launch's ranges
     bool valid;
-    __device__ void seek(const DProb *probs, int nprob, const ca3dmm_tile_ranges_t &rg,
-                         int total_tiles, int stride)
+    __device__ void seek(const int *sb, const DProb *probs, int nprob,
+                         const ca3dmm_tile_ranges_t &rg, int total_tiles, int stride)
     {
         while (tile < total_tiles) {
             const int t = range_tile(rg, tile);
-            pi = find_problem(probs, nprob, t);
+            pi = find_problem(sb, probs, nprob, t);
             const DProb &p = probs[pi];
             ktiles = (p.k + BK - 1) / BK;
             if (ktiles > 0) {
@@ -131,13 +135,14 @@ struct LoadCursor {
         }
         valid = false;
     }
-    __device__ void advance(const DProb *probs, int nprob, const ca3dmm_tile_ranges_t &rg,
+    __device__ void advance(const int *sb, const DProb *probs, int nprob,
+                            const ca3dmm_tile_ranges_t &rg,
                             int total_tiles, int stride)
     {
         if (++kt < ktiles) return;
         kt = 0;
         tile += stride;
-        seek(probs, nprob, rg, total_tiles, stride);
+        seek(sb, probs, nprob, rg, total_tiles, stride);
     }
 };
 
@@ -233,6 +238,12 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
     uint64_t *empty = full + STAGES;
     __shared__ volatile int abort_flag;
+    __shared__ int s_pbeg[PROB_CACHE];
+    // the search table: rematerialised at each use (a kernel parameter and a
+    // shared address), not held in a register across the main loop
+#define CA3DMM_PB (nprob <= PROB_CACHE ? s_pbeg : nullptr)
+    if (nprob <= PROB_CACHE)
+        for (int i = threadIdx.x; i < nprob; i += blockDim.x) s_pbeg[i] = probs[i].tile_begin;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const bool producer = threadIdx.x == 0;
@@ -274,13 +285,13 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
         }
         tma_load_2d(sB, tb, lc.kt * BK, lc.n0, &full[s]);
         ++issued;
-        lc.advance(probs, nprob, rg, total_tiles, gridDim.x);
+        lc.advance(CA3DMM_PB, probs, nprob, rg, total_tiles, gridDim.x);
         return true;
     };
     if (producer) {
         lc.tile = blockIdx.x;
         lc.kt = 0;
-        lc.seek(probs, nprob, rg, total_tiles, gridDim.x);
+        lc.seek(CA3DMM_PB, probs, nprob, rg, total_tiles, gridDim.x);
         for (int s = 0; s < STAGES - 1; ++s)
             if (!issue_one()) break;
     }
@@ -293,7 +304,7 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
 
     for (int v = blockIdx.x; v < total_tiles && ok; v += gridDim.x) {
         const int tile = range_tile(rg, v);
-        int pi = find_problem(probs, nprob, tile);
+        int pi = find_problem(CA3DMM_PB, probs, nprob, tile);
         const DProb &p = probs[pi];
         int tm, tn;
         tile_coords(p, tile, tm, tn);
@@ -336,6 +347,7 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
         }
     }
 }
+#undef CA3DMM_PB
 
 typedef CUresult (*encode_tiled_fn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *,
                                     const cuuint64_t *, const cuuint64_t *, const cuuint32_t *,

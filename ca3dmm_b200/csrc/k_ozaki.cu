@@ -140,15 +140,33 @@ __device__ __forceinline__ int desc_begin(const SliceDesc &d, int which)
 
 // The descriptor holding flat item t: the last one whose first item is <= t
 // (blocks without items in this numbering share their first item with the next).
-template <int WHICH>
-__device__ __forceinline__ int find_slice_desc(const SliceDesc *d, int n, int t)
-{
-    int lo = 0, hi = n - 1;
-    while (lo < hi) {
-        int mid = (lo + hi + 1) >> 1;
-        if (desc_begin(d[mid], WHICH) <= t) lo = mid; else hi = mid - 1;
+// The slicing kernels copy the first items of up to DESC_CACHE descriptors
+// into shared memory once, so that the search per tile is not a chain of
+// dependent global loads (a batch of 256 GEMMs has 256 descriptors per side).
+constexpr int DESC_CACHE = 1024;
+
+struct DescFinder {
+    int *begin;      // shared copy, or nullptr when there are more descriptors than DESC_CACHE
+    __device__ __forceinline__ int operator()(const SliceDesc *d, int n, int t, int which) const
+    {
+        int lo = 0, hi = n - 1;
+        while (lo < hi) {
+            int mid = (lo + hi + 1) >> 1;
+            if ((begin ? begin[mid] : desc_begin(d[mid], which)) <= t) lo = mid; else hi = mid - 1;
+        }
+        return lo;
     }
-    return lo;
+};
+
+// Fill the shared copy (every thread of the block calls this once, before its loop).
+__device__ __forceinline__ DescFinder make_finder(int *sbeg, const SliceDesc *d, int n, int which)
+{
+    DescFinder f;
+    f.begin = n <= DESC_CACHE ? sbeg : nullptr;
+    if (f.begin)
+        for (int i = threadIdx.x; i < n; i += blockDim.x) sbeg[i] = desc_begin(d[i], which);
+    __syncthreads();
+    return f;
 }
 
 __device__ __forceinline__ const double *slice_src(const double *base, long long off)
@@ -184,8 +202,10 @@ oz_exp_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ desc
               int total_items, unsigned long long *__restrict__ mwork)
 {
     __shared__ unsigned long long part[4][ST];
+    __shared__ int sbeg[DESC_CACHE];
+    const DescFinder find = make_finder(sbeg, descs, ndesc, FIND_EXP);
     for (int item = blockIdx.x; item < total_items; item += gridDim.x) {
-        const SliceDesc &d = descs[find_slice_desc<FIND_EXP>(descs, ndesc, item)];
+        const SliceDesc &d = descs[find(descs, ndesc, item, FIND_EXP)];
         const int local = item - d.xbegin;
         if (d.shape == SHAPE_KC) {
             // warp w: row r0 + w, k [l0, l0 + 512) as 16-byte loads (scalar when unaligned)
@@ -328,9 +348,11 @@ oz_slice_kc_kernel(const double *__restrict__ src, const SliceDesc *__restrict__
                    const unsigned long long *__restrict__ mwork)
 {
     __shared__ __align__(16) double sm[KC_SR * (KC_SK / 16) * KC_SLOT];
+    __shared__ int sbeg[DESC_CACHE];
+    const DescFinder find = make_finder(sbeg, descs, ndesc, SHAPE_KC);
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
-        const SliceDesc &d = descs[find_slice_desc<SHAPE_KC>(descs, ndesc, tile)];
+        const SliceDesc &d = descs[find(descs, ndesc, tile, SHAPE_KC)];
         const int local = tile - d.kc_begin;
         const int nkt = (d.kpad + KC_SK - 1) / KC_SK;
         const int r0 = (local / nkt) * KC_SR, l0 = (local % nkt) * KC_SK;
@@ -384,8 +406,10 @@ oz_slice_rc_kernel(const double *__restrict__ src, const SliceDesc *__restrict__
                    const unsigned long long *__restrict__ mwork)
 {
     __shared__ __align__(16) double tl[RC_SK][RC_SR];
+    __shared__ int sbeg[DESC_CACHE];
+    const DescFinder find = make_finder(sbeg, descs, ndesc, SHAPE_RC);
     for (int tile = blockIdx.x; tile < total_tiles; tile += gridDim.x) {
-        const SliceDesc &d = descs[find_slice_desc<SHAPE_RC>(descs, ndesc, tile)];
+        const SliceDesc &d = descs[find(descs, ndesc, tile, SHAPE_RC)];
         const int local = tile - d.rc_begin;
         // 128 rows x 32 k; thread (row pair tid % 64, k column tid / 64 + 4 i)
         // loads 16 bytes of a column, the tile is transposed through shared memory
@@ -517,12 +541,16 @@ __device__ __forceinline__ double pow2(int e)
     return ldexp(1.0, e);
 }
 
-__device__ __forceinline__ int find_unit(const OzUnit *u, int n, int tile)
+// The unit holding tile `tile`.  sb: a shared-memory copy of the units' first
+// tiles (nullptr when there are more than UNIT_CACHE units), so that a batch of
+// small GEMMs does not pay a chain of dependent global loads per tile.
+constexpr int UNIT_CACHE = 1024;
+__device__ __forceinline__ int find_unit(const int *sb, const OzUnit *u, int n, int tile)
 {
     int lo = 0, hi = n - 1;
     while (lo < hi) {
         int mid = (lo + hi + 1) >> 1;
-        if (u[mid].tile_begin <= tile) lo = mid; else hi = mid - 1;
+        if ((sb ? sb[mid] : u[mid].tile_begin) <= tile) lo = mid; else hi = mid - 1;
     }
     return lo;
 }
@@ -569,7 +597,11 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
     __shared__ double col_scale_all[4][OBN];   // 2^F_j per epilogue warp (no cross-warp barrier)
+    __shared__ int s_ubeg[UNIT_CACHE];
     const int *ework = reinterpret_cast<const int *>(work);
+    const int *ub = nunit <= UNIT_CACHE ? s_ubeg : nullptr;
+    if (ub)
+        for (int i = threadIdx.x; i < nunit; i += blockDim.x) s_ubeg[i] = units[i].tile_begin;
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const uint32_t tmem_cols = slices * OBN <= 256 ? 256u : 512u;
@@ -613,7 +645,7 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
           for (int sub = 0; sub < nsub_max && ok; ++sub)
             for (int v = blockIdx.x; v < total_tiles && ok && !abort_flag; v += gridDim.x) {
                 const int tile = range_tile(rg, v);
-                const OzUnit &U = units[find_unit(units, nunit, tile)];
+                const OzUnit &U = units[find_unit(ub, units, nunit, tile)];
                 int tm, tn;
                 unit_tile(U, tile, tm, tn);
               if (sub < U.nsub) {
@@ -669,7 +701,7 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
             bool ok = true;
           for (int sub = 0; sub < nsub_max && ok; ++sub)
             for (int v = blockIdx.x; v < total_tiles && ok; v += gridDim.x) {
-                const OzUnit &U = units[find_unit(units, nunit, range_tile(rg, v))];
+                const OzUnit &U = units[find_unit(ub, units, nunit, range_tile(rg, v))];
               if (sub < U.nsub) {
                 const OzGroup &p = groups[U.group + sub * U.sub_stride];
                 const int nch = nchunks(p.nkb, kb_per_chunk);
@@ -737,7 +769,7 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
       for (int sub = 0; sub < nsub_max && ok; ++sub)
         for (int v = blockIdx.x; v < total_tiles && ok; v += gridDim.x) {
             const int tile = range_tile(rg, v);
-            const OzUnit &U = units[find_unit(units, nunit, tile)];
+            const OzUnit &U = units[find_unit(ub, units, nunit, tile)];
             int tm, tn;
             unit_tile(U, tile, tm, tn);
           if (sub < U.nsub) {
