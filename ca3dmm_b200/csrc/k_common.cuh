@@ -132,6 +132,17 @@ CA3DMM_DEV void tma_load_2d(void *smem_dst, const void *tmap, int x, int y, uint
         : "memory");
 }
 
+// 5D tiled TMA load (coordinates innermost first), completing on `bar`.
+CA3DMM_DEV void tma_load_5d(void *smem_dst, const void *tmap, int c0, int c1, int c2, int c3,
+                            int c4, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4, %5, %6}], [%7];" ::"r"(smem_u32(smem_dst)),
+        "l"(tmap), "r"(c0), "r"(c1), "r"(c2), "r"(c3), "r"(c4), "r"(smem_u32(bar))
+        : "memory");
+}
+
 CA3DMM_DEV void tmap_prefetch(const void *tmap)
 {
     asm volatile("prefetch.tensormap [%0];" ::"l"(tmap) : "memory");

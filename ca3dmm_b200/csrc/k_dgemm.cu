@@ -392,6 +392,32 @@ extern "C" int ca3dmm_encode_tmap_2d(void *tmap, int dtype_bytes, const void *ba
     return r == CUDA_SUCCESS ? CA3DMM_OK : CA3DMM_EINVAL;
 }
 
+extern "C" int ca3dmm_encode_tmap_u8(void *tmap, int rank, const void *base,
+                                     const unsigned long long *dims,
+                                     const unsigned long long *strides_bytes,
+                                     const unsigned *box)
+{
+    encode_tiled_fn enc = get_encode();
+    if (!enc) return CA3DMM_ENODEV;
+    if (rank < 1 || rank > 5 || (reinterpret_cast<uintptr_t>(base) & 15)) return CA3DMM_EINVAL;
+    cuuint64_t d[5], st[4];
+    cuuint32_t bx[5], es[5];
+    for (int i = 0; i < rank; ++i) {
+        d[i] = dims[i];
+        bx[i] = box[i];
+        es[i] = 1;
+        if (i > 0) {
+            if (strides_bytes[i - 1] & 15) return CA3DMM_EINVAL;
+            st[i - 1] = strides_bytes[i - 1];
+        }
+    }
+    CUresult r = enc(reinterpret_cast<CUtensorMap *>(tmap), CU_TENSOR_MAP_DATA_TYPE_UINT8,
+                     (cuuint32_t) rank, const_cast<void *>(base), d, st, bx, es,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    return r == CUDA_SUCCESS ? CA3DMM_OK : CA3DMM_EINVAL;
+}
+
 extern "C" size_t ca3dmm_dgemm_plan_bytes(int nprob)
 {
     return (size_t) nprob * 2 * sizeof(CUtensorMap) + (size_t) nprob * sizeof(DProb);

@@ -48,6 +48,10 @@ extern "C" int ca3dmm_encode_tmap_2d(void *tmap, int dtype_bytes, const void *ba
                                      unsigned long long dim0, unsigned long long dim1,
                                      unsigned long long stride1_bytes, unsigned box0,
                                      unsigned box1, int swizzle128);
+extern "C" int ca3dmm_encode_tmap_u8(void *tmap, int rank, const void *base,
+                                     const unsigned long long *dims,
+                                     const unsigned long long *strides_bytes,
+                                     const unsigned *box);
 
 namespace {
 
@@ -83,7 +87,8 @@ struct OzGroup {
     int m, n, k;
     int nkb;                    // 32-byte k-blocks
     int tiles_m, tiles_n, tile_begin, raster;
-    int a_from_b, pad;          // A slices stored in the B layout (64-row tiles): B^T B
+    int a_from_b;               // A slices stored in the B layout (64-row tiles): B^T B
+    int a_tmap;                 // a_from_b: the group's 5D tensor map gathers a whole A stage
     long long ea_off, eb_off;   // exponent offsets (ints) of the A rows / B columns
     long long qa_off, qb_off;   // byte offsets of the tiled slices
 };
@@ -577,7 +582,8 @@ __device__ __forceinline__ int nchunks(int nkb, int kb_per_chunk)
 // measured 1.45x faster than the same loops over a runtime count.
 template <int S>
 __global__ void __launch_bounds__(OTHREADS, 1)
-oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ units, int nunit,
+oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ units,
+               const unsigned char *__restrict__ tmaps, int nunit,
                int nsub_max, const ca3dmm_tile_ranges_t rg,
                int total_tiles, int nstage,
                int kb_per_chunk, int4 tsplit, const unsigned char *__restrict__ work,
@@ -642,6 +648,7 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
         if (lane == 0) {
             uint32_t it = 0;
             bool ok = true;
+            int last_g = -1;
           for (int sub = 0; sub < nsub_max && ok; ++sub)
             for (int v = blockIdx.x; v < total_tiles && ok && !abort_flag; v += gridDim.x) {
                 const int tile = range_tile(rg, v);
@@ -649,7 +656,13 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
                 int tm, tn;
                 unit_tile(U, tile, tm, tn);
               if (sub < U.nsub) {
-                const OzGroup &p = groups[U.group + sub * U.sub_stride];
+                const int gi = U.group + sub * U.sub_stride;
+                const OzGroup &p = groups[gi];
+                const unsigned char *tm5 = tmaps + (size_t) gi * 128;
+                if (p.a_tmap && gi != last_g) {
+                    tmap_acquire(tm5);
+                    last_g = gi;
+                }
                 const unsigned char *qa =
                     p.a_from_b ? work + p.qa_off + (long long) (2 * tm) * p.nkb * b_bytes
                                : work + p.qa_off + (long long) tm * p.nkb * a_bytes;
@@ -664,7 +677,9 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
                     }
                     uint8_t *sA = smem + s * stage_bytes;
                     mbar_arrive_expect_tx(&full[s], stage_bytes);
-                    if (p.a_from_b) {
+                    if (p.a_tmap) {
+                        tma_load_5d(sA, tm5, 0, 0, 2 * tm, 0, kb, &full[s]);
+                    } else if (p.a_from_b) {
                         // rows 0-63 / 64-127 of each A slice: the same slice of the
                         // 64-row tiles 2 tm and 2 tm + 1 of the B layout
                         const unsigned char *h0 = qa + (long long) kb * b_bytes;
@@ -903,13 +918,14 @@ int4 slice_split(int s)
 // Device plan layout for g groups (at most 2g operand blocks, g units):
 // [header 256 B][2g slice descriptors][g groups][g units]
 struct PlanLayout {
-    size_t sd, gr, un, total;
+    size_t sd, gr, un, tm, total;
     explicit PlanLayout(int g)
     {
         sd = 256;
         gr = (sd + (size_t) 2 * g * sizeof(SliceDesc) + 127) / 128 * 128;
         un = (gr + (size_t) g * sizeof(OzGroup) + 127) / 128 * 128;
-        total = un + (size_t) g * sizeof(OzUnit);
+        tm = (un + (size_t) g * sizeof(OzUnit) + 127) / 128 * 128;
+        total = tm + (size_t) g * 128;          // one 128-byte tensor map per group
     }
 };
 
@@ -1012,7 +1028,23 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
         const int al = A[G[g].a_blk].alias;
         const SliceDesc &da = al >= 0 ? sd[nA + al] : sd[G[g].a_blk], &db = sd[nA + G[g].b_blk];
         o.a_from_b = al >= 0 ? 1 : 0;
-        o.pad = 0;
+        o.a_tmap = 0;
+        if (o.a_from_b && da.rows_pad % OBM == 0 && da.nkb > 0) {
+            // One 5D box gathers an A stage from the B layout: (32 k bytes, 64 rows,
+            // 64-row tile 2 tm and 2 tm + 1, slice, k-block); in shared memory the
+            // box lands as [slice][tile][row][32 B], the 128-row A slices in turn.
+            const unsigned long long dims[5] = {(unsigned long long) OKB, (unsigned long long) OBN,
+                                                (unsigned long long) (da.rows_pad / OBN),
+                                                (unsigned long long) slices,
+                                                (unsigned long long) da.nkb};
+            const unsigned long long strides[4] = {
+                (unsigned long long) OKB, (unsigned long long) da.nkb * slices * B_SLICE_BYTES,
+                (unsigned long long) B_SLICE_BYTES, (unsigned long long) slices * B_SLICE_BYTES};
+            const unsigned box[5] = {(unsigned) OKB, (unsigned) OBN, 2u, (unsigned) slices, 1u};
+            o.a_tmap = ca3dmm_encode_tmap_u8(h + L.tm + (size_t) g * 128, 5,
+                                             static_cast<unsigned char *>(dev_work) + da.q_off,
+                                             dims, strides, box) == CA3DMM_OK ? 1 : 0;
+        }
         o.C = G[g].C; o.ldc = G[g].ldc;
         o.m = G[g].m; o.n = G[g].n; o.k = G[g].k;
         o.nkb = G[g].k > 0 ? da.nkb : 0;
@@ -1223,7 +1255,7 @@ extern "C" int ca3dmm_oz_run_gemm_ranges(const ca3dmm_oz_plan_t *oz, const ca3dm
         CA3DMM_CUDA_TRY(cudaFuncSetAttribute(oz_gemm_kernel<S>,                                    \
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,          \
                                              (int) smem));                                         \
-        oz_gemm_kernel<S><<<grid, OTHREADS, smem, stream>>>(groups, units, oz->nunit,             \
+        oz_gemm_kernel<S><<<grid, OTHREADS, smem, stream>>>(groups, units, pl + L.tm, oz->nunit,  \
                                                            oz->max_nsub, *rg, vtiles,              \
                                                            nstage,                                 \
                                                            kb_per_chunk, split, work, dev_status,  \
