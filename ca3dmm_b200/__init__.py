@@ -55,7 +55,7 @@ class Ca3dmmEngineS(C.Structure):
         ("n_exec", C.c_int), ("n_group", C.c_int), ("gemm_mode", C.c_int),
         ("ozaki_slices", C.c_int), ("last_error", C.c_int), ("stream", C.c_void_p),
         ("sync_exec", C.c_int), ("workbuf_bytes", C.c_size_t), ("impl", C.c_void_p),
-        ("raster", C.c_int)]
+        ("raster", C.c_int), ("btb_symmetric", C.c_int)]
 
 
 class TuneCfg(C.Structure):

@@ -49,6 +49,8 @@ typedef struct {
     int ngroup, nA, nB;
     int tmn, tnn;             /* row / column blocks of the internal grouping (1: merged) */
     int ksplit;               /* plain mode: each slab's k range runs as ksplit sub-slabs */
+    int sym;                  /* B^T B upper block triangle only: one group per 128-row block
+                                 row and slab, the lower triangle mirrored after the sum */
     group_t *groups;
     blk_t *A, *B;
     /* work buffer layout (byte offsets) */
@@ -220,9 +222,10 @@ static void plan_layout(ca3dmm_engine_p e, plan_t *pl)
  * (The reference runs one DGEMM per Cannon step, src/cannon.c:410-418.) */
 #define CA3DMM_KSPLIT_MAX 8
 #define CA3DMM_SMS_B200 148
-static int choose_ksplit(const ca3dmm_engine_p e)
+static int choose_ksplit(const ca3dmm_engine_p e, int sym)
 {
-    const long long tiles = (long long) ((e->m + 127) / 128) * ((e->n + 127) / 128) * e->kp;
+    const long long tb = (e->m + 127) / 128;
+    const long long tiles = (sym ? tb * (tb + 1) / 2 : tb * ((e->n + 127) / 128)) * e->kp;
     const int kz = e->k / e->kp;
     const double slab_bytes = 8.0 * (double) ca3dmm_round_up(e->m, 2) * (double) e->n;
     if (tiles <= 0 || tiles >= 4LL * CA3DMM_SMS_B200) return 1;
@@ -251,13 +254,18 @@ static int plan_build(ca3dmm_engine_p e)
     pl->tmn = tmn;
     pl->tnn = tnn;
     const int kp = e->kp;
+    /* symmetric B^T B: per slab one group for each 128-row block row bi, over
+     * rows [128 bi, 128 bi + 128) and columns [128 bi, n) -- the upper block
+     * triangle (C = B^T B is symmetric; the reference computes all of it) */
+    pl->sym = e->is_BTB && e->btb_symmetric;
+    const int nbr = pl->sym ? (e->m + 127) / 128 : 1;
     pl->nA = tmn * kp;
     pl->nB = tnn * kp;
-    pl->ngroup = kp * tmn * tnn;
+    pl->ngroup = kp * (pl->sym ? nbr : tmn * tnn);
     pl->groups = (group_t *) calloc((size_t) pl->ngroup, sizeof(group_t));
     pl->A = (blk_t *) calloc((size_t) pl->nA, sizeof(blk_t));
     pl->B = (blk_t *) calloc((size_t) pl->nB, sizeof(blk_t));
-    pl->ksplit = choose_ksplit(e);
+    pl->ksplit = choose_ksplit(e, pl->sym);
     pl->gd = (ca3dmm_dgemm_desc_t *) calloc((size_t) pl->ngroup * (size_t) pl->ksplit,
                                             sizeof(ca3dmm_dgemm_desc_t));
     pl->ob = (ca3dmm_oz_blk_t *) calloc((size_t) (pl->nA + pl->nB), sizeof(ca3dmm_oz_blk_t));
@@ -284,7 +292,15 @@ static int plan_build(ca3dmm_engine_p e)
             b->rows = kz; b->cols = nz; b->r0 = ks; b->c0 = ns;
             b->ld = ca3dmm_round_up(kz > 0 ? kz : 1, 2);
         }
-        for (int tm = 0; tm < tmn; tm++)
+        for (int bi = 0; pl->sym && bi < nbr; bi++) {
+            group_t *g = &pl->groups[tk * nbr + bi];
+            g->tk = tk; g->tm = 0; g->tn = 0;
+            g->a_blk = tk; g->b_blk = tk;
+            g->m0 = 128 * bi; g->mz = e->m - g->m0 < 128 ? e->m - g->m0 : 128;
+            g->n0 = 128 * bi; g->nz = e->n - g->n0;
+            g->k0 = ks; g->kz = kz;
+        }
+        for (int tm = 0; !pl->sym && tm < tmn; tm++)
             for (int tn = 0; tn < tnn; tn++) {
                 group_t *g = &pl->groups[(tk * tmn + tm) * tnn + tn];
                 g->tk = tk; g->tm = tm; g->tn = tn;
@@ -480,6 +496,11 @@ static void finish_init(ca3dmm_engine_p e, int dst_srow, int dst_nrow, int dst_s
     e->ozaki_slices = sl;
     e->sync_exec = 1;
     e->raster = 8;
+    if (e->is_BTB) {
+        int sym;
+        GET_ENV_INT_VAR(sym, "CA3DMM_BTB_SYMMETRIC", "btb_symmetric", 0, 0, 1);
+        e->btb_symmetric = sym;
+    }
     int rc = plan_build(e);
     if (rc) {
         ERROR_PRINTF("Failed to build the device plan (error %d)\n", rc);
@@ -773,6 +794,10 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
         const long long lda = ba->direct ? ba->direct_ld : (pl->a_kmajor ? ba->kld : ba->ld);
         const double *b = bb->direct ? bb->direct : (const double *) (w + bb->off);
         const long long ldb = bb->direct ? bb->direct_ld : bb->ld;
+        /* the group's first row inside its A block and first column inside its B block */
+        const long long dr = g->m0 - ba->r0, dc = g->n0 - bb->c0;
+        a += pl->a_kmajor ? dr * lda : dr;
+        b += dc * ldb;
         for (int sub = 0; sub < ks; sub++) {
             /* sub-slab k range: a multiple of 16 (whole k-tiles, 16-byte aligned starts) */
             const int k0 = (int) ((long long) g->kz * sub / ks) / 16 * 16;
@@ -835,10 +860,12 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
             const group_t *g = &pl->groups[u];
             unit_tiles += (long long) ((g->mz + 127) / 128) * ((g->nz + 63) / 64);
         }
-        pl->oz_fused = e->kp > 1 && unit_tiles >= 8LL * ca3dmm_device_sm_count();
+        pl->oz_fused = e->kp > 1 && !pl->sym && unit_tiles >= 8LL * ca3dmm_device_sm_count();
         for (int i = 0; i < pl->ngroup; i++) {
             const group_t *g = &pl->groups[i];
             og[i].a_blk = g->a_blk; og[i].b_blk = g->b_blk;
+            og[i].row0 = g->m0 - pl->A[g->a_blk].r0;
+            og[i].col0 = g->n0 - pl->B[g->b_blk].c0;
             if (pl->oz_fused || e->kp == 1) {
                 og[i].C = out + g->m0 + (size_t) g->n0 * ldo;
                 og[i].ldc = ldo;
@@ -942,6 +969,10 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
         rc = ca3dmm_reduce_slabs_launch((const double *) (w + pl->off_slab),
                                         (long long) pl->slab_stride, pl->slab_ld, nred, e->m,
                                         e->n, out, ldo, st);
+        if (rc) return rc;
+    }
+    if (pl->sym) {
+        rc = ca3dmm_mirror_upper_launch(out, ldo, e->m, st);
         if (rc) return rc;
     }
     if (timing) cudaEventRecord(pl->ev[3], st);

@@ -102,6 +102,8 @@ int ca3dmm_pack_launch(const double *src_base, double *dst_base,
 /* ---- kp-slab reduction ---------------------------------------------------
  * out[i + j*ldo] = sum_{s=0}^{nslab-1} slab[s*slab_stride + i + j*lds]
  * (summed in slab order 0,1,...). */
+/* C(i, j) = C(j, i) for i > j (n x n C, column-major). */
+int ca3dmm_mirror_upper_launch(double *C, long long ldc, int n, cudaStream_t stream);
 int ca3dmm_reduce_slabs_launch(const double *slab, long long slab_stride, long long lds,
                                int nslab, int m, int n, double *out, long long ldo,
                                cudaStream_t stream);

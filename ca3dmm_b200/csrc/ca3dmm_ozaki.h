@@ -41,6 +41,8 @@ typedef struct {
     long long ldc;
     int m, n, k;
     int raster;           /* tile rows per raster band (0 = default) */
+    int row0, col0;       /* first row of the group inside its A block (a multiple of 128) and
+                             first column inside its B block (a multiple of 64) */
 } ca3dmm_oz_group_t;
 
 /* Work unit: nsub groups (group, group + sub_stride, ...) of equal m x n that

@@ -286,6 +286,7 @@ static int build_plan(ca3dmm_grouped_p g, const double *const *A, const int *ldA
         for (int j = 0; j < np; j++) {
             const int i = g->order[j];
             g->og[j].a_blk = i; g->og[j].b_blk = i;
+            g->og[j].row0 = 0; g->og[j].col0 = 0;
             g->og[j].C = C[i]; g->og[j].ldc = ldC[i];
             g->og[j].m = g->m[i]; g->og[j].n = g->n[i]; g->og[j].k = g->k[i];
         }

@@ -1027,14 +1027,25 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
         OzGroup &o = gr[g];
         const int al = A[G[g].a_blk].alias;
         const SliceDesc &da = al >= 0 ? sd[nA + al] : sd[G[g].a_blk], &db = sd[nA + G[g].b_blk];
+        const int row0 = G[g].row0, col0 = G[g].col0;
+        if (row0 < 0 || col0 < 0 || row0 % OBM || col0 % OBN) return CA3DMM_EINVAL;
         o.a_from_b = al >= 0 ? 1 : 0;
+        o.C = G[g].C; o.ldc = G[g].ldc;
+        o.m = G[g].m; o.n = G[g].n; o.k = G[g].k;
+        o.nkb = G[g].k > 0 ? da.nkb : 0;
+        // a group may start inside its blocks: 128-row A tiles (aliased: two
+        // 64-row B tiles, the same bytes) and 64-column B tiles further on
+        o.ea_off = da.e_off + row0;
+        o.eb_off = db.e_off + col0;
+        o.qa_off = da.q_off + (long long) (row0 / OBM) * da.nkb * slices * A_SLICE_BYTES;
+        o.qb_off = db.q_off + (long long) (col0 / OBN) * db.nkb * slices * B_SLICE_BYTES;
         o.a_tmap = 0;
-        if (o.a_from_b && da.rows_pad % OBM == 0 && da.nkb > 0) {
+        if (o.a_from_b && da.rows_pad % OBM == 0 && da.nkb > 0 && da.rows_pad > row0) {
             // One 5D box gathers an A stage from the B layout: (32 k bytes, 64 rows,
             // 64-row tile 2 tm and 2 tm + 1, slice, k-block); in shared memory the
             // box lands as [slice][tile][row][32 B], the 128-row A slices in turn.
             const unsigned long long dims[5] = {(unsigned long long) OKB, (unsigned long long) OBN,
-                                                (unsigned long long) (da.rows_pad / OBN),
+                                                (unsigned long long) ((da.rows_pad - row0) / OBN),
                                                 (unsigned long long) slices,
                                                 (unsigned long long) da.nkb};
             const unsigned long long strides[4] = {
@@ -1042,16 +1053,9 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
                 (unsigned long long) B_SLICE_BYTES, (unsigned long long) slices * B_SLICE_BYTES};
             const unsigned box[5] = {(unsigned) OKB, (unsigned) OBN, 2u, (unsigned) slices, 1u};
             o.a_tmap = ca3dmm_encode_tmap_u8(h + L.tm + (size_t) g * 128, 5,
-                                             static_cast<unsigned char *>(dev_work) + da.q_off,
+                                             static_cast<unsigned char *>(dev_work) + o.qa_off,
                                              dims, strides, box) == CA3DMM_OK ? 1 : 0;
         }
-        o.C = G[g].C; o.ldc = G[g].ldc;
-        o.m = G[g].m; o.n = G[g].n; o.k = G[g].k;
-        o.nkb = G[g].k > 0 ? da.nkb : 0;
-        o.ea_off = da.e_off;
-        o.eb_off = db.e_off;
-        o.qa_off = da.q_off;
-        o.qb_off = db.q_off;
         o.tiles_m = (o.m > 0 && o.n > 0) ? (o.m + OBM - 1) / OBM : 0;
         o.tiles_n = (o.m > 0 && o.n > 0) ? (o.n + OBN - 1) / OBN : 0;
         o.tile_begin = tiles;

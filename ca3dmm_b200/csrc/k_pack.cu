@@ -309,6 +309,49 @@ extern "C" int ca3dmm_reduce_slabs_launch(const double *slab, long long slab_str
     return CA3DMM_OK;
 }
 
+// C(i, j) = C(j, i) for i > j: the strictly lower triangle of an n x n C
+// rewritten from the upper one, through 32 x 32 shared-memory tiles (block
+// (bi, bj), bi > bj, reads the upper tile (bj, bi) transposed).
+__global__ void __launch_bounds__(256)
+mirror_upper_kernel(double *__restrict__ C, long long ldc, int n)
+{
+    __shared__ double t[32][33];
+    const int nb = (n + 31) / 32;
+    const long long ntile = (long long) nb * (nb + 1) / 2;       // blocks with bi >= bj
+    for (long long idx = blockIdx.x; idx < ntile; idx += gridDim.x) {
+        // idx -> (bi, bj), bj <= bi, row-major over the lower block triangle
+        int bi = (int) ((sqrt(8.0 * (double) idx + 1.0) - 1.0) * 0.5);
+        while ((long long) (bi + 1) * (bi + 2) / 2 <= idx) ++bi;
+        while ((long long) bi * (bi + 1) / 2 > idx) --bi;
+        const int bj = (int) (idx - (long long) bi * (bi + 1) / 2);
+        const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5;
+        __syncthreads();                             // t of the previous tile is read
+        // read the upper tile: rows 32 bj.., columns 32 bi.. (element (r, c) at r + c ldc)
+        for (int y = ty; y < 32; y += 8) {
+            const int r = 32 * bj + tx, c = 32 * bi + y;
+            t[y][tx] = (r < n && c < n) ? C[r + (long long) c * ldc] : 0.0;
+        }
+        __syncthreads();
+        // write the lower tile: rows 32 bi + tx, columns 32 bj + y, only strictly below the diagonal
+        for (int y = ty; y < 32; y += 8) {
+            const int r = 32 * bi + tx, c = 32 * bj + y;
+            if (r < n && c < n && r > c) C[r + (long long) c * ldc] = t[tx][y];
+        }
+    }
+}
+
+extern "C" int ca3dmm_mirror_upper_launch(double *C, long long ldc, int n, cudaStream_t stream)
+{
+    if (n <= 1) return CA3DMM_OK;
+    const int nb = (n + 31) / 32;
+    long long tiles = (long long) nb * (nb + 1) / 2;
+    const long long cap = (long long) ca3dmm_device_sm_count() * 8;
+    mirror_upper_kernel<<<(unsigned) (tiles < cap ? tiles : cap), 256, 0, stream>>>(C, ldc, n);
+    CA3DMM_CUDA_TRY(cudaGetLastError());
+    ca3dmm_note_launch(1);
+    return CA3DMM_OK;
+}
+
 // Diagnostic of the bounded device wait every kernel of the library uses:
 // thread 0 waits on an mbarrier that is completed (arrive != 0) or that
 // nothing ever completes; the wait returns by itself after limit_ns.

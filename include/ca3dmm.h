@@ -118,6 +118,8 @@ struct ca3dmm_engine {
     size_t workbuf_bytes;           /* device work buffer size */
     void *impl;                     /* opaque device plan */
     int raster;                     /* GEMM tile rows per raster band (tuning knob) */
+    int btb_symmetric;              /* B^T B: compute the upper block triangle only, mirror it
+                                       (env CA3DMM_BTB_SYMMETRIC=1 at init_BTB) */
 };
 typedef struct ca3dmm_engine ca3dmm_engine_s;
 typedef struct ca3dmm_engine *ca3dmm_engine_p;
