@@ -246,9 +246,8 @@ def reference_arm(args, world, rank):
             "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": t,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": "ca3dmm_exec M=N=K=%d transA=%d transB=%d grid 4x2x3 (24 "
-                                   "virtual ranks)" % (n, args.trans_a, args.trans_b),
-                       "l2": "inputs larger than L2"},
+            "config": {"workload": square_desc(n, args.trans_a, args.trans_b),
+                       "l2": "inputs larger than L2 (512 MB per operand at 8000^3)"},
             "cpu_baseline": base,
             "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
@@ -346,6 +345,12 @@ def make_btb(k, n, seed=303):
     return z.numpy().T          # Fortran-ordered view of the (n, k) row-major buffer
 
 
+def square_desc(n, ta, tb):
+    """The square workload's name, the same in both arms' JSON lines."""
+    return ("ca3dmm_exec M=N=K=%d transA=%d transB=%d, 24 virtual ranks, grid 4x2x3 (cuboid "
+            "2000x4000x2667 at 8000^3), entries sign*(1+u)*2^e, e in [-8,8]" % (n, ta, tb))
+
+
 def workload(args):
     if args.workload == "btb":
         rows = args.btb_rows
@@ -363,9 +368,7 @@ def workload(args):
     return {"m": n, "n": n, "k": n, "ta": args.trans_a, "tb": args.trans_b, "btb": False, "p": P,
             "grid": GRID,
             "A": A, "B": B, "label": "square %d^3 grid 4x2x3" % n,
-            "desc": "ca3dmm_exec M=N=K=%d transA=%d transB=%d, 24 virtual ranks, grid 4x2x3 "
-                    "(cuboid 2000x4000x2667), entries sign*(1+u)*2^e, e in [-8,8]"
-                    % (n, args.trans_a, args.trans_b),
+            "desc": square_desc(n, args.trans_a, args.trans_b),
             "l2": "inputs larger than L2 (512 MB per operand), no flush"}
 
 

@@ -11,8 +11,9 @@ ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 EXE = os.path.join(ROOT, "ca3dmm_b200", "examples", "example_cholesky_qr")
 
 
-def run(*args):
-    r = subprocess.run([EXE] + [str(a) for a in args], capture_output=True, text=True, timeout=300)
+def run(*args, env=None):
+    r = subprocess.run([EXE] + [str(a) for a in args], capture_output=True, text=True, timeout=300,
+                       env=dict(os.environ, **(env or {})))
     return r.returncode, r.stdout + r.stderr
 
 
@@ -42,3 +43,19 @@ def test_cholesky_qr_orthogonality(cuda, cond_exp):
     # with columns scaled over 10^+-1.5 a row of B spans three decades, and the
     # per-row exponent of the slicing leaves the small columns fewer bits: the
     # split result stays within 1e-11 but is not held to the plain error here
+
+
+@pytest.mark.gpu
+def test_cholesky_qr_symmetric_gram(cuda):
+    """The Gram matrix through the symmetric B^T B (upper block triangle + mirror): the
+    split-precision run gives the same error as the full product (same bits), the plain
+    run stays as accurate."""
+    for mode, sl in ((0, 0), (1, 7)):
+        rc, full = run(60000, 256, mode, sl, 32, 0.0)
+        assert rc == 0, full
+        rc, sym = run(60000, 256, mode, sl, 32, 0.0, env={"CA3DMM_BTB_SYMMETRIC": "1"})
+        assert rc == 0, sym
+        if mode == 1:
+            assert _err(sym) == _err(full), (full, sym)
+        else:
+            assert _err(sym) < 1e-12, sym
