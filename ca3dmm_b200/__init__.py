@@ -154,6 +154,10 @@ def lib():
         "ca3dmm_kernel_launches": (C.c_ulonglong, []),
         "ca3dmm_engine_exec_host": (i, [EP, p, i, p, i, p, i]),
         "ca3dmm_device_wait_check": (i, [d, i]),
+        "mat_redist_layouts_init": (i, [i, pi, i, pi, C.POINTER(p)]),
+        "mat_redist_layouts_pieces": (i, [p]),
+        "mat_redist_layouts_exec": (i, [p, C.POINTER(p), pi, C.POINTER(p), pi, p]),
+        "mat_redist_layouts_free": (None, [C.POINTER(p)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(L, name)
@@ -385,6 +389,45 @@ class GroupedGemm:
     def free(self):
         if self.h:
             lib().ca3dmm_grouped_free(C.byref(self.h))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class RedistLayouts:
+    """Python mirror of mat_redist_layouts_{init,exec,free}: redistribution of
+    a row-major matrix between two layouts of rectangles {srow, scol, nrow,
+    ncol} (the reference's mat_redist with every rank's call folded into one)."""
+
+    def __init__(self, src_rects, req_rects):
+        L = lib()
+        sr = [int(x) for r in src_rects for x in r]
+        rr = [int(x) for r in req_rects for x in r]
+        self.nsrc, self.nreq = len(src_rects), len(req_rects)
+        self.h = C.c_void_p()
+        self.rc = L.mat_redist_layouts_init(self.nsrc, (C.c_int * len(sr))(*sr), self.nreq,
+                                            (C.c_int * len(rr))(*rr), C.byref(self.h))
+
+    @property
+    def ok(self):
+        return self.rc == 0 and bool(self.h)
+
+    def pieces(self):
+        return lib().mat_redist_layouts_pieces(self.h)
+
+    def exec(self, src_blks, src_lds, dst_blks, dst_lds, stream=None):
+        P1, P2 = C.c_void_p * self.nsrc, C.c_void_p * self.nreq
+        return lib().mat_redist_layouts_exec(
+            self.h, P1(*[_ptr(x) for x in src_blks]), (C.c_int * self.nsrc)(*src_lds),
+            P2(*[_ptr(x) for x in dst_blks]), (C.c_int * self.nreq)(*dst_lds),
+            C.c_void_p(stream) if stream is not None else None)
+
+    def free(self):
+        if self.h:
+            lib().mat_redist_layouts_free(C.byref(self.h))
 
     def __del__(self):
         try:

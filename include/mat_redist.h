@@ -73,6 +73,30 @@ void mat_redist_engine_free(mat_redist_engine_p *engine_);
 void mat_redist_engine_exec(mat_redist_engine_p engine, const void *src_blk, const int src_ld,
                             void *dst_blk, const int dst_ld);
 
+/* ---- arbitrary layouts (appended by this build) ----------------------------
+ * The reference redistributes between two distributed layouts with every rank
+ * calling mat_redist_engine_init/exec on its own source rectangle and the
+ * rectangle it requires (src/mat_redist.c:44-419: intersections of each
+ * rank's source block with every rank's required block, packed, exchanged by
+ * Neighbor_alltoallv, unpacked).  Folded onto one GPU: the caller gives all
+ * nsrc source rectangles and all nreq required rectangles at once (row-major
+ * view as in the reference; rect k = {srow, scol, nrow, ncol} at 4k), and exec
+ * copies, for every pair (i, j), the intersection of source block i and
+ * required block j from src_blks[i] (row-major, ld src_lds[i]) into
+ * dst_blks[j] (ld dst_lds[j]) in one batched device launch.  Required
+ * elements that no source block holds are left untouched; source blocks
+ * should not overlap (an element held twice is copied from either).
+ * 8-byte elements; device pointers.  exec on stream NULL is synchronous,
+ * otherwise enqueued on the given cudaStream_t. */
+typedef struct mat_redist_layouts *mat_redist_layouts_p;
+int mat_redist_layouts_init(int nsrc, const int *src_rects, int nreq, const int *req_rects,
+                            mat_redist_layouts_p *layouts);
+int mat_redist_layouts_pieces(mat_redist_layouts_p layouts);   /* non-empty intersections */
+int mat_redist_layouts_exec(mat_redist_layouts_p layouts, const void *const *src_blks,
+                            const int *src_lds, void *const *dst_blks, const int *dst_lds,
+                            void *stream);
+void mat_redist_layouts_free(mat_redist_layouts_p *layouts);
+
 #ifdef __cplusplus
 }
 #endif

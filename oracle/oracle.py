@@ -288,6 +288,8 @@ def ref_lib():
         dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
         L.ref_ca3dmm.argtypes = [C.c_int] * 7 + [ip, dp, dp, dp, C.c_int, dp, ip, ip, C.c_double]
         L.ref_fault_run.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double]
+        L.ref_redist.argtypes = [C.c_int, ip, ip, dp, C.c_int, dp, C.POINTER(C.c_longlong),
+                                 C.c_double]
         _ref = L
     return _ref
 
@@ -313,6 +315,30 @@ def ref_ca3dmm(p, m, n, k, ta, tb, A, B, grid=None, ntest=1, btb=False, timeout=
     if rc:
         raise RuntimeError("reference run failed")
     return Cm, times, geom, tuple(int(x) for x in gout)
+
+
+def ref_redist(src_rects, req_rects, G, timeout=60.0):
+    """The reference's own mat_redist on p = len(src_rects) vmpi rank threads
+    (rank r: source rectangle src_rects[r], required rectangle req_rects[r],
+    row-major {srow, scol, nrow, ncol} of the row-major matrix G).  Returns the
+    p required blocks as row-major arrays."""
+    L = ref_lib()
+    if L is None:
+        raise RuntimeError("reference CPU path not built (oracle/_ref)")
+    p = len(src_rects)
+    assert len(req_rects) == p
+    G = np.ascontiguousarray(G, dtype=np.float64)
+    sizes = [int(r[2]) * int(r[3]) for r in req_rects]
+    offs = np.concatenate([[0], np.cumsum(sizes)[:-1]]).astype(np.int64)
+    out = np.zeros(max(sum(sizes), 1))
+    ip = C.POINTER(C.c_int)
+    sr = np.ascontiguousarray(np.array(src_rects, dtype=np.int32).ravel())
+    rr = np.ascontiguousarray(np.array(req_rects, dtype=np.int32).ravel())
+    rc = L.ref_redist(p, sr.ctypes.data_as(ip), rr.ctypes.data_as(ip), _d(G), G.shape[1], _d(out),
+                      offs.ctypes.data_as(C.POINTER(C.c_longlong)), float(timeout))
+    if rc:
+        raise RuntimeError("reference redistribution failed")
+    return [out[o:o + z].reshape(int(r[2]), int(r[3])) for o, z, r in zip(offs, sizes, req_rects)]
 
 
 def ref_fault_run(p, dead_rank, m=64, timeout=1.0):

@@ -13,6 +13,7 @@
 #include "mpi.h"
 #include "cblas.h"
 #include "ca3dmm.h"
+#include "mat_redist.h"
 
 typedef struct {
     int m, n, k, ta, tb, btb, ntest;
@@ -136,4 +137,51 @@ int ref_fault_run(int p, int dead_rank, int m, double timeout_s)
 {
     fault_t f = {dead_rank, m};
     return vmpi_run(p, fault_main, &f, timeout_s);
+}
+
+/* The reference's mat_redist (src/mat_redist.c) on p rank threads: rank r owns
+ * source rectangle src_rects[4r..] and requires req_rects[4r..] (row-major
+ * view, {srow, scol, nrow, ncol}) of a row-major matrix G (ldg columns).  Each
+ * rank fills its source block from G, runs mat_redist_engine_init/exec with
+ * DEV_TYPE_HOST, and writes its required block to out at out_offs[r] (row-major,
+ * ld = its ncol).  Returns 0, or nonzero when a rank failed or timed out. */
+typedef struct {
+    const int *src, *req;
+    const double *G;
+    int ldg;
+    double *out;
+    const long long *offs;
+    int fail;
+} redist_t;
+
+static void redist_main(int rank, void *arg)
+{
+    redist_t *j = (redist_t *) arg;
+    omp_set_num_threads(1);
+    const int *s = j->src + 4 * rank, *r = j->req + 4 * rank;
+    double *sb = (double *) malloc(sizeof(double) * ((size_t) s[2] * s[3] + 1));
+    double *db = (double *) calloc((size_t) r[2] * r[3] + 1, sizeof(double));
+    for (int i = 0; i < s[2]; i++)
+        for (int c = 0; c < s[3]; c++)
+            sb[(size_t) i * s[3] + c] = j->G[(size_t) (s[0] + i) * j->ldg + s[1] + c];
+    mat_redist_engine_p e = NULL;
+    mat_redist_engine_init(s[0], s[1], s[2], s[3], r[0], r[1], r[2], r[3], MPI_COMM_WORLD,
+                           MPI_DOUBLE, sizeof(double), DEV_TYPE_HOST, &e, NULL);
+    if (e == NULL) {
+        j->fail = 1;
+    } else {
+        mat_redist_engine_exec(e, sb, s[3] > 0 ? s[3] : 1, db, r[3] > 0 ? r[3] : 1);
+        memcpy(j->out + j->offs[rank], db, sizeof(double) * (size_t) r[2] * r[3]);
+        mat_redist_engine_free(&e);
+    }
+    free(sb);
+    free(db);
+}
+
+int ref_redist(int p, const int *src_rects, const int *req_rects, const double *G, int ldg,
+               double *out, const long long *out_offs, double timeout_s)
+{
+    redist_t j = {src_rects, req_rects, G, ldg, out, out_offs, 0};
+    int rc = vmpi_run(p, redist_main, &j, timeout_s);
+    return rc || j.fail;
 }

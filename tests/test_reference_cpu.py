@@ -53,3 +53,28 @@ def test_dead_rank_is_reported_not_hung():
     t0 = time.time()
     assert orc.ref_fault_run(4, 2, 64, 1.0) != 0
     assert time.time() - t0 < 30
+
+
+def _grid_rects(R, Cc, pr, pc):
+    rs = [R * i // pr for i in range(pr + 1)]
+    cs = [Cc * j // pc for j in range(pc + 1)]
+    return [(rs[i], cs[j], rs[i + 1] - rs[i], cs[j + 1] - cs[j]) for i in range(pr) for j in range(pc)]
+
+
+@pytest.mark.parametrize("R,Cc,src,req", [
+    (37, 53, (2, 3), (3, 2)),
+    (64, 40, (1, 6), (6, 1)),        # 1D column blocks -> 1D row blocks
+    (50, 50, (4, 1), (2, 2)),
+])
+def test_reference_mat_redist_between_layouts(R, Cc, src, req):
+    """The reference's own mat_redist (src/mat_redist.c, vmpi rank threads) moves
+    every required block out of the source layout: the pin for the GPU's
+    folded layout redistribution."""
+    if orc.ref_lib() is None:
+        pytest.skip("reference CPU path not built")
+    G = orc.gen_uniform(77, R, Cc)
+    sr = _grid_rects(R, Cc, *src)
+    rr = _grid_rects(R, Cc, *req)
+    out = orc.ref_redist(sr, rr, G)
+    for o, r in zip(out, rr):
+        assert np.array_equal(o, G[r[0]:r[0] + r[2], r[1]:r[1] + r[3]])
