@@ -28,7 +28,9 @@
 //                         last chunk.
 // Warp roles of the GEMM: warp 0 copy producer, warps 1, 6, 7 MMA issuers, each
 // owning a set of A slices (warp 1 also owns the TMEM allocation), warps 2..5
-// epilogue (warp w reads TMEM lanes 32*(w%4)..+31).  Each issuing thread needs
+// and 8..11 epilogue (warp w reads TMEM lanes 32*(w%4)..+31, columns 0-31 of
+// each 64-column accumulator for w <= 5, 32-63 for w >= 8: two warps per lane
+// quarter halve the time the MMAs wait for the accumulators to drain).  Each issuing thread needs
 // ~150-190 cycles per tcgen05.mma, so one issuer cannot keep the tensor core
 // busy; the A slices are dealt out so that no issuer has more than four MMAs
 // per k-block (s <= 8).  Issuers of different slices add into
@@ -56,7 +58,8 @@ extern "C" int ca3dmm_encode_tmap_u8(void *tmap, int rank, const void *base,
 namespace {
 
 constexpr int OBM = 128, OBN = 64, OKB = 32;    // tile rows, tile cols, k bytes per stage
-constexpr int OTHREADS = 256;                    // 8 warps
+constexpr int OTHREADS = 384;                    // 12 warps
+constexpr int EPI_WARPS = 8;                     // two per TMEM lane quarter
 constexpr int MAX_ISSUERS = 3;                   // MMA issuer warps 1, 6, 7
 constexpr int MAX_SLICES = 8;
 constexpr int MAX_STAGES = 8;
@@ -608,7 +611,7 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
     uint64_t *acc_empty = acc_full + 1;
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
-    __shared__ double col_scale_all[4][OBN];   // 2^F_j per epilogue warp (no cross-warp barrier)
+    __shared__ double col_scale_all[OTHREADS / 32][32];   // 2^F_j per epilogue warp (no cross-warp barrier)
     __shared__ int s_ubeg[UNIT_CACHE];
     const int *ework = reinterpret_cast<const int *>(work);
     const int *ub = nunit <= UNIT_CACHE ? s_ubeg : nullptr;
@@ -623,7 +626,7 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
             mbar_init(&empty[s], MAX_ISSUERS);     // one commit per MMA issuer
         }
         mbar_init(acc_full, MAX_ISSUERS);
-        mbar_init(acc_empty, 4);
+        mbar_init(acc_empty, EPI_WARPS);
         abort_flag = 0;
         fence_barrier_init();
     }
@@ -711,7 +714,7 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
                     if (global_timer_ns() - t0 > limit_ns) break;
             }
         }
-    } else if (warp == 1 || warp >= 6) {
+    } else if (warp == 1 || warp == 6 || warp == 7) {
         // ---------------------------------------------------------- MMA issuers
         if (lane == 0) {
             // this issuer's A slices (bit t of the mask; possibly none: an idle
@@ -783,8 +786,9 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
     } else {
         // ---------------------------------------------------------- epilogue
         const int q = warp & 3;                       // TMEM lane quarter of this warp
+        const int c0 = warp >= 8 ? 32 : 0;            // its 32 columns of each accumulator
         const int row = q * 32 + lane;
-        double *col_scale = col_scale_all[q];
+        double *col_scale = col_scale_all[warp];
         uint32_t ci = 0;
         bool ok = true;
       for (int sub = 0; sub < nsub_max && ok; ++sub)
@@ -803,15 +807,15 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
             const int Ei = eb ? eb - EXP_BIAS : 0;
             // column scales 2^F_j of this tile into this warp's shared slots
             __syncwarp();
-            for (int j = lane; j < OBN; j += 32) {
-                const int gc = tn * OBN + j;
+            {
+                const int gc = tn * OBN + c0 + lane;
                 const int fb = gc < gn ? ework[p.eb_off + gc] : 0;
-                col_scale[j] = pow2(fb ? fb - EXP_BIAS : 0);
+                col_scale[lane] = pow2(fb ? fb - EXP_BIAS : 0);
             }
             __syncwarp();
-            double acc[OBN];
+            double acc[32];
 #pragma unroll
-            for (int j = 0; j < OBN; ++j) acc[j] = 0.0;
+            for (int j = 0; j < 32; ++j) acc[j] = 0.0;
             const int nch = nchunks(p.nkb, kb_per_chunk);
             for (int ch = 0; ch < nch; ++ch, ++ci) {
                 if (!mbar_wait_bounded(acc_full, ci & 1u, &abort_flag, status,
@@ -828,17 +832,13 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
                         // sum by a power of two is exact, so in the normal range this
                         // equals the oracle's sum of ldexp(D_d, E_i + F_j - 14 - 8d).
                         const double rs = pow2(Ei - 14 - 8 * d);
+                        uint32_t v[32];
+                        const uint32_t ta = tmem_base + ((uint32_t) (q * 32) << 16) +
+                                            (uint32_t) (d * OBN + c0);
+                        tmem_ld32(ta, v);
+                        tmem_zero32(ta);
 #pragma unroll
-                        for (int h = 0; h < OBN / 32; ++h) {
-                            uint32_t v[32];
-                            const uint32_t ta = tmem_base + ((uint32_t) (q * 32) << 16) +
-                                                (uint32_t) (d * OBN + h * 32);
-                            tmem_ld32(ta, v);
-                            tmem_zero32(ta);
-#pragma unroll
-                            for (int j = 0; j < 32; ++j)
-                                acc[h * 32 + j] = fma(i32_to_f64(v[j]), rs, acc[h * 32 + j]);
-                        }
+                        for (int j = 0; j < 32; ++j) acc[j] = fma(i32_to_f64(v[j]), rs, acc[j]);
                     }
                     tmem_wait_st();
                 }
@@ -850,15 +850,15 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
             if (gr < gm) {
                 // slab 0 stores; later slabs of the chain add in slab order (this
                 // thread wrote the value it reads)
-                double *crow = Cg + gr + (long long) (tn * OBN) * ldc;
-                const int nj = min(OBN, gn - tn * OBN);
+                double *crow = Cg + gr + (long long) (tn * OBN + c0) * ldc;
+                const int nj = min(32, gn - tn * OBN - c0);
                 if (sub == 0) {
 #pragma unroll
-                    for (int j = 0; j < OBN; ++j)
+                    for (int j = 0; j < 32; ++j)
                         if (j < nj) crow[(long long) j * ldc] = acc[j] * col_scale[j];
                 } else {
 #pragma unroll
-                    for (int j0 = 0; j0 < OBN; j0 += 8) {
+                    for (int j0 = 0; j0 < 32; j0 += 8) {
                         double c[8];
 #pragma unroll
                         for (int j = 0; j < 8; ++j)
