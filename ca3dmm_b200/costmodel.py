@@ -107,6 +107,8 @@ def main():
     ap.add_argument("--hi", type=int, default=16384)
     ap.add_argument("--epochs", type=int, default=300)
     ap.add_argument("--out", default="costmodel_out")
+    ap.add_argument("--shipped", action="store_true",
+                    help="also evaluate the shipped model (ca3dmm_b200/data) on the held-out shapes")
     a = ap.parse_args()
     os.makedirs(a.out, exist_ok=True)
     tr = shapes(a.train, 11, a.lo, a.hi)
@@ -129,6 +131,8 @@ def main():
            "candidates": CANDS, "collect_s": t_collect, "train_s": t_train,
            "train_loss_log2ms": loss, "test": evaluate(model, Fte, Tte),
            "train": evaluate(model, Ftr, Ttr)}
+    if a.shipped:
+        res["shipped_test"] = evaluate(cb.CostModel.default(), Fte, Tte)
     with open(os.path.join(a.out, "costmodel_eval.json"), "w") as f:
         json.dump(res, f, indent=1)
     print(json.dumps(res), flush=True)
