@@ -164,16 +164,19 @@ def cpu_cores():
         return os.cpu_count() or 1
 
 
-def ref_cpu_run(A, B, ta, n, ntest, tb=0):
+def ref_cpu_run(A, B, ta, n, ntest, tb=0, p=P, grid=GRID, matmul=False):
     """The reference's own CPU path (src/ca3dmm.c, DEV_TYPE_HOST, OpenBLAS),
-    compiled unmodified under the thread-backed MPI subset: P rank threads
+    compiled unmodified under the thread-backed MPI subset: p rank threads
     with one BLAS thread each, driven as examples/example_AB.c drives it (one
     warm-up exec, then `ntest` timed execs).  Returns exec ms per timed exec
-    of rank 0, or None when the reference build is absent."""
+    of rank 0 (with matmul: also its "matmul only" ms, examples/example_AB.c:190),
+    or None when the reference build is absent."""
     from oracle import oracle as orc
     if orc.ref_lib() is None:
         return None
-    _, times, _, _ = orc.ref_ca3dmm(P, n, n, n, ta, tb, A, B, grid=GRID, ntest=ntest, timeout=600.0)
+    _, times, _, g = orc.ref_ca3dmm(p, n, n, n, ta, tb, A, B, grid=grid, ntest=ntest, timeout=600.0)
+    if matmul:
+        return list(times[:, 0]), list(times[:, 1]), g
     return list(times[:, 0])
 
 
@@ -183,12 +186,26 @@ def cpu_baseline(A, B, ta, n, budget_s=20.0, tb=0):
     virtual-rank algorithm on k-slab 0 (kind "port")."""
     from oracle import oracle as orc
     flops = 2.0 * n * n * n
-    ms = ref_cpu_run(A, B, ta, n, 1, tb)
-    if ms is not None:
-        return {"value": flops / (ms[0] * 1e-3) / 1e12, "unit": "TFLOP/s",
-                "cores": min(P, cpu_cores()), "kind": "reference",
-                "sample": "one full %d^3 exec (after one warm-up) of the reference's CPU path, "
-                          "24 rank threads on grid 4x2x3, 1 OpenBLAS thread per rank" % n}
+    r = ref_cpu_run(A, B, ta, n, 1, tb, matmul=True)
+    if r is not None:
+        ms, mm, _ = r
+        out = {"value": flops / (ms[0] * 1e-3) / 1e12, "unit": "TFLOP/s",
+               "cores": min(P, cpu_cores()), "kind": "reference",
+               "sample": "one full %d^3 exec (after one warm-up) of the reference's CPU path, "
+                         "24 rank threads on grid 4x2x3, 1 OpenBLAS thread per rank" % n,
+               "matmul_only_value": flops / (mm[0] * 1e-3) / 1e12}
+        # the second protocol of the study: one rank per host core, the
+        # reference's own grid choice for that many ranks
+        pc = cpu_cores()
+        if pc != P:
+            r2 = ref_cpu_run(A, B, ta, n, 1, tb, p=pc, grid=None, matmul=True)
+            if r2 is not None:
+                ms2, mm2, g2 = r2
+                out["p_equals_cores"] = {
+                    "p": pc, "grid": "%dx%dx%d" % g2[:3],
+                    "value": flops / (ms2[0] * 1e-3) / 1e12,
+                    "matmul_only_value": flops / (mm2[0] * 1e-3) / 1e12}
+        return out
     cores = os.cpu_count()
     try:
         from threadpoolctl import threadpool_info
