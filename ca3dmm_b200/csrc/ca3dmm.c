@@ -103,6 +103,7 @@ struct host_exec {
     size_t desc_stride;
     int ndesc, ntile[HX_MAX_BANDS][3];  /* per band: Ozaki exponent items + KC + RC slicing tiles, or pack tiles */
     int built_mode, built_slices, built_raster;
+    int slab_built;               /* B^T B: per-slab slicing descriptors uploaded (split mode) */
     int ok;                       /* streams and events created */
 };
 
@@ -1208,6 +1209,107 @@ static int hx_copy_in_A_rows(ca3dmm_engine_p e, struct host_exec *x, const doubl
     return CA3DMM_OK;
 }
 
+/* B^T B from host memory, pipelined over the kp k-slabs: slab j of B (its
+ * rows [k0_j, k0_j + kz_j)) is copied in while slab j - 1 is sliced (split
+ * precision) and multiplied into its C slab buffer; the slab sum (and the
+ * mirror of the symmetric option) and the copy out of C follow.  Used when
+ * kp > 1, the whole C is the destination and every operand block is read in
+ * place (plain) -- returns 1 to ask for the serial path otherwise. */
+static int hx_btb_slabs(ca3dmm_engine_p e, struct host_exec *x, const void *B_h, int ldB,
+                        void *C_h, int ldC, cudaStream_t st)
+{
+    plan_t *pl = (plan_t *) e->impl;
+    const int ozaki = e->gemm_mode == CA3DMM_GEMM_OZAKI;
+    const int kp = e->kp, n = e->n, ks = ozaki ? 1 : pl->ksplit;
+    const int whole = pl->has_dst && pl->dst_srow == 0 && pl->dst_scol == 0 &&
+                      pl->dst_nrow == e->m && pl->dst_ncol == e->n;
+    if (!e->is_BTB || kp < 2 || kp > HX_MAX_BANDS || !whole || (ozaki && pl->oz_fused)) return 1;
+    for (int i = 0; !ozaki && i < pl->nA; i++)
+        if (!pl->A[i].direct) return 1;
+    for (int i = 0; !ozaki && i < pl->nB; i++)
+        if (!pl->B[i].direct) return 1;
+    const int gps = pl->ngroup / kp;        /* groups of one slab (consecutive) */
+    if (ozaki && !x->slab_built) {
+        /* one slicing descriptor per slab: its B block (op(A) reuses its slices) */
+        const size_t one = ca3dmm_oz_desc_bytes();
+        x->desc_stride = align_up(one);
+        if (!x->desc_h) {
+            const size_t p1 = align_up(sizeof(ca3dmm_pack_desc_t) * (size_t) kp);
+            const size_t p2 = align_up(one * (size_t) kp);
+            const size_t cap = (p1 > p2 ? p1 : p2) * HX_MAX_BANDS;
+            if (cudaMallocHost(&x->desc_h, cap) != cudaSuccess) { x->desc_h = NULL; return 1; }
+            if (cudaMalloc(&x->desc_d, cap) != cudaSuccess) { x->desc_d = NULL; return 1; }
+        }
+        for (int j = 0; j < kp; j++) {
+            const int idx = pl->nA + j;
+            if (ca3dmm_oz_encode_blocks((char *) pl->stage + pl->off_ozplan, pl->ngroup, &idx, 1,
+                                        (char *) x->desc_h + (size_t) j * x->desc_stride,
+                                        x->ntile[j]))
+                return 1;
+        }
+        CA3DMM_CUDA_TRY(cudaMemcpyAsync(x->desc_d, x->desc_h, x->desc_stride * (size_t) kp,
+                                        cudaMemcpyHostToDevice, st));
+        x->slab_built = 1;
+    }
+    char *w = (char *) e->workbuf_d;
+    int *status_d = (int *) (w + pl->off_status);
+    CA3DMM_CUDA_TRY(cudaMemsetAsync(status_d, 0, 64, st));
+    /* copies in: B slab by slab */
+    for (int j = 0; j < kp; j++) {
+        int k0, kz;
+        calc_block_spos_size(e->k, kp, j, &k0, &kz);
+        if (kz > 0 && n > 0)
+            CA3DMM_CUDA_TRY(cudaMemcpy2DAsync(x->dB + k0, sizeof(double) * (size_t) x->ldb,
+                                              (const double *) B_h + k0, sizeof(double) * (size_t) ldB,
+                                              sizeof(double) * (size_t) kz, (size_t) n,
+                                              cudaMemcpyHostToDevice, x->s_in));
+        CA3DMM_CUDA_TRY(cudaEventRecord(x->ev_a[j], x->s_in));
+    }
+    int rc = ozaki ? ca3dmm_oz_clear(&pl->oz, st) : CA3DMM_OK;
+    if (rc) return rc;
+    int tile0 = 0;
+    for (int j = 0; j < kp; j++) {
+        /* the tiles of slab j's groups (and k sub-slabs): consecutive in both GEMM plans */
+        int count = 0;
+        for (int g = j * gps; g < (j + 1) * gps; g++) {
+            const group_t *gg = &pl->groups[g];
+            if (gg->mz <= 0 || gg->nz <= 0) continue;
+            count += ks * ((gg->mz + 127) / 128) * (ozaki ? (gg->nz + 63) / 64 : (gg->nz + 127) / 128);
+        }
+        ca3dmm_tile_ranges_t rg;
+        memset(&rg, 0, sizeof(rg));
+        rg.n = 1;
+        rg.begin[0] = tile0;
+        rg.len[0] = count;
+        tile0 += count;
+        CA3DMM_CUDA_TRY(cudaStreamWaitEvent(st, x->ev_a[j], 0));
+        if (ozaki) {
+            const void *dd = (const char *) x->desc_d + (size_t) j * x->desc_stride;
+            rc = ca3dmm_oz_slice_descs(&pl->oz, x->dB, dd, 1, x->ntile[j], st);
+            if (!rc) rc = ca3dmm_oz_run_gemm_ranges(&pl->oz, &rg, status_d, 5.0, st);
+        } else {
+            rc = ca3dmm_dgemm_launch_ranges(w + pl->off_gemm, pl->ngroup * pl->ksplit, &rg,
+                                            pl->a_kmajor, status_d, 5.0, st);
+        }
+        if (rc) return rc;
+    }
+    const int nred = kp * ks;
+    rc = ca3dmm_reduce_slabs_launch((const double *) (w + pl->off_slab), (long long) pl->slab_stride,
+                                    pl->slab_ld, nred, e->m, e->n, x->dC, x->ldc, st);
+    if (!rc && pl->sym) rc = ca3dmm_mirror_upper_launch(x->dC, x->ldc, e->m, st);
+    if (rc) return rc;
+    CA3DMM_CUDA_TRY(cudaMemcpy2DAsync(C_h, sizeof(double) * (size_t) ldC, x->dC,
+                                      sizeof(double) * (size_t) x->ldc, sizeof(double) * (size_t) e->m,
+                                      (size_t) e->n, cudaMemcpyDeviceToHost, st));
+    CA3DMM_CUDA_TRY(cudaMemcpyAsync(pl->status_h, status_d, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CA3DMM_CUDA_TRY(cudaStreamSynchronize(st));
+    if (pl->status_h[0] != 0) {
+        ERROR_PRINTF("Device status %d: a bounded wait ran out\n", pl->status_h[0]);
+        return CA3DMM_ETIMEOUT;
+    }
+    return CA3DMM_OK;
+}
+
 static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_h, int ldB,
                      void *C_h, int ldC)
 {
@@ -1234,12 +1336,17 @@ static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_
         rc = plan_upload(e, dAsrc, (int) ldAsrc, x->dB, (int) x->ldb, x->dC, (int) x->ldc, st);
         if (rc) return rc;
         x->built_mode = -1;
+        x->slab_built = 0;
     }
     if (x->built_mode != e->gemm_mode || x->built_slices != e->ozaki_slices ||
         x->built_raster != e->raster)
         hx_build_bands(e, x, st);
     /* the inputs may not be overwritten before the previous exec's reads are done */
     CA3DMM_CUDA_TRY(cudaStreamSynchronize(st));
+    if (e->is_BTB) {
+        const int r = hx_btb_slabs(e, x, B_h, ldB, C_h, ldC, st);
+        if (r != 1) return r;
+    }
     const int dn = pl->dst_nrow, dc = pl->dst_ncol;
     if (x->nband < 2) {
         /* serial: copy in, the device exec, copy out */

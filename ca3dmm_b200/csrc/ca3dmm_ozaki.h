@@ -98,6 +98,10 @@ int ca3dmm_oz_slice_side(const ca3dmm_oz_plan_t *oz, int which, const void *src,
 size_t ca3dmm_oz_desc_bytes(void);
 int ca3dmm_oz_encode_rows(const void *host_plan, int ngroup, const int *blocks, int count, int r0,
                           int r1, void *out_descs, int ntiles[3]);
+/* Descriptors of whole blocks (indices into the plan's A then B blocks), with
+ * their tile numbering restarted, for slicing those blocks alone. */
+int ca3dmm_oz_encode_blocks(const void *host_plan, int ngroup, const int *descs, int count,
+                            void *out_descs, int ntiles[3]);
 int ca3dmm_oz_slice_descs(const ca3dmm_oz_plan_t *oz, const void *src, const void *dev_descs,
                           int ndesc, const int ntiles[3], cudaStream_t stream);
 /* The GEMM over the tiles of `ranges` only (ca3dmm_kernels.h). */

@@ -1218,6 +1218,32 @@ extern "C" int ca3dmm_oz_encode_rows(const void *host_plan, int ngroup, const in
     return CA3DMM_OK;
 }
 
+extern "C" int ca3dmm_oz_encode_blocks(const void *host_plan, int ngroup, const int *descs,
+                                       int count, void *out_descs, int ntiles[3])
+{
+    const PlanLayout L(ngroup);
+    const unsigned char *h = static_cast<const unsigned char *>(host_plan);
+    const PlanHeader *hd = reinterpret_cast<const PlanHeader *>(h);
+    const SliceDesc *sd = reinterpret_cast<const SliceDesc *>(h + L.sd);
+    SliceDesc *out = static_cast<SliceDesc *>(out_descs);
+    if (!descs || count < 0) return CA3DMM_EINVAL;
+    int kc = 0, rct = 0, items = 0;
+    for (int i = 0; i < count; ++i) {
+        if (descs[i] < 0 || descs[i] >= hd->nA + hd->nB) return CA3DMM_EINVAL;
+        SliceDesc c = sd[descs[i]];
+        c.kc_begin = kc;
+        c.rc_begin = rct;
+        c.xbegin = items;
+        (c.shape == SHAPE_KC ? kc : rct) += slice_tiles_of(c);
+        items += exp_items_of(c);
+        out[i] = c;
+    }
+    ntiles[0] = items;
+    ntiles[1] = kc;
+    ntiles[2] = rct;
+    return CA3DMM_OK;
+}
+
 extern "C" int ca3dmm_oz_slice_descs(const ca3dmm_oz_plan_t *oz, const void *src,
                                      const void *dev_descs, int ndesc, const int ntiles[3],
                                      cudaStream_t stream)

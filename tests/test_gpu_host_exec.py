@@ -67,15 +67,29 @@ def test_exec_host_pageable_and_padded_leading_dims(cuda):
     assert np.all(hC[m:] == 0.0)
 
 
-def test_exec_host_btb(cuda):
-    n, k = 96, 5000
+@pytest.mark.parametrize("n,k,grid,mode,sym", [
+    (96, 5000, (1, 1, 8), cb.GEMM_OZAKI, 0),      # slab pipeline, split precision
+    (96, 5000, (1, 1, 8), cb.GEMM_PLAIN, 0),      # slab pipeline, plain (k sub-slabs too)
+    (300, 20000, (1, 1, 4), cb.GEMM_OZAKI, 1),    # symmetric option through the pipeline
+    (300, 20000, (1, 1, 4), cb.GEMM_PLAIN, 1),
+    (130, 3000, (1, 1, 1), cb.GEMM_OZAKI, 0),     # kp = 1: serial path
+])
+def test_exec_host_btb(cuda, monkeypatch, n, k, grid, mode, sym):
+    """B^T B from host buffers: B arrives slab by slab while earlier slabs are
+    sliced and multiplied; the result equals the device exec bit for bit."""
+    monkeypatch.setenv("CA3DMM_BTB_SYMMETRIC", str(sym))
     Bm = orc.gen_btb(7, k, n)
-    e = cb.Ca3dmmEngine(n, n, k, p=8, btb=True, proc_grid=(1, 1, 8))
-    assert e.ok and e.set_gemm_mode(cb.GEMM_OZAKI, 7) == 0
+    e = cb.Ca3dmmEngine(n, n, k, p=grid[2], btb=True, proc_grid=grid)
+    assert e.ok
+    if mode == cb.GEMM_OZAKI:
+        assert e.set_gemm_mode(cb.GEMM_OZAKI, 7) == 0
     hB, ldb = _pinned(Bm)
     hC = torch.zeros(n * n, dtype=torch.float64).pin_memory()
-    assert e.exec_host(None, 0, hB, ldb, hC, n) == 0
     dB, _ = to_dev(Bm)
     dC = dev_zeros(n * n)
     assert e.exec(None, 0, dB, ldb, dC, n) == 0
-    assert np.array_equal(hC.numpy().reshape((n, n), order="F"), from_dev(dC, n, n))
+    want = from_dev(dC, n, n)
+    for _ in range(2):                       # the second call reuses the staging and descriptors
+        hC.zero_()
+        assert e.exec_host(None, 0, hB, ldb, hC, n) == 0
+        assert np.array_equal(hC.numpy().reshape((n, n), order="F"), want)
