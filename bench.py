@@ -44,6 +44,13 @@ def parse():
     ap.add_argument("--trans-a", type=int, default=0)
     ap.add_argument("--trans-b", type=int, default=0)
     ap.add_argument("--size", type=int, default=M)
+    ap.add_argument("--p", type=int, default=P, help="virtual ranks of the square workload")
+    ap.add_argument("--grid", default="%dx%dx%d" % GRID,
+                    help="virtual grid mp x np x kp of the square workload, or auto (the "
+                         "reference's own choice for --p ranks)")
+    ap.add_argument("--dist", default="signed_exp", choices=["signed_exp", "uniform"],
+                    help="square workload entries: sign*(1+u)*2^e, e in [-8,8] (8000^3), or "
+                         "uniform in [-1,1) (the 2048^3 example workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--workload", default="square", choices=["square", "grouped", "btb"],
                     help="square: the headline 8000^3 engine exec; grouped: 256 uneven "
@@ -150,8 +157,10 @@ def ncu_traffic():
         return {}
 
 
-def make_inputs(n, trans_a):
+def make_inputs(n, trans_a, dist="signed_exp"):
     from oracle import oracle as orc
+    if dist == "uniform":
+        return orc.gen_uniform(1, n, n), orc.gen_uniform(2, n, n)
     A = orc.gen_signed_exp(101, n, n)
     B = orc.gen_signed_exp(202, n, n)
     return A, B
@@ -162,6 +171,20 @@ def cpu_cores():
         return len(os.sched_getaffinity(0))
     except Exception:
         return os.cpu_count() or 1
+
+
+def grid_of(args):
+    """The square workload's virtual grid: a tuple, or None for the planner's choice."""
+    if args.grid == "auto":
+        return None
+    g = tuple(int(x) for x in args.grid.lower().split("x"))
+    if len(g) != 3:
+        raise SystemExit("--grid wants mp x np x kp, e.g. 4x2x3, or auto")
+    return g
+
+
+def grid_str(grid):
+    return "auto" if grid is None else "%dx%dx%d" % tuple(grid)
 
 
 def ref_cpu_run(A, B, ta, n, ntest, tb=0, p=P, grid=GRID, matmul=False):
@@ -180,24 +203,25 @@ def ref_cpu_run(A, B, ta, n, ntest, tb=0, p=P, grid=GRID, matmul=False):
     return list(times[:, 0])
 
 
-def cpu_baseline(A, B, ta, n, budget_s=20.0, tb=0):
+def cpu_baseline(A, B, ta, n, budget_s=20.0, tb=0, p=P, grid=GRID):
     """CPU baseline on this host: the reference's own CPU path when it was
     built (kind "reference"), else the oracle's numpy restatement of the
     virtual-rank algorithm on k-slab 0 (kind "port")."""
     from oracle import oracle as orc
     flops = 2.0 * n * n * n
-    r = ref_cpu_run(A, B, ta, n, 1, tb, matmul=True)
+    r = ref_cpu_run(A, B, ta, n, 1, tb, p=p, grid=grid, matmul=True)
     if r is not None:
         ms, mm, _ = r
         out = {"value": flops / (ms[0] * 1e-3) / 1e12, "unit": "TFLOP/s",
-               "cores": min(P, cpu_cores()), "kind": "reference",
+               "cores": min(p, cpu_cores()), "kind": "reference",
                "sample": "one full %d^3 exec (after one warm-up) of the reference's CPU path, "
-                         "24 rank threads on grid 4x2x3, 1 OpenBLAS thread per rank" % n,
+                         "%d rank threads on grid %s, 1 OpenBLAS thread per rank"
+                         % (n, p, grid_str(grid)),
                "matmul_only_value": flops / (mm[0] * 1e-3) / 1e12}
         # the second protocol of the study: one rank per host core, the
         # reference's own grid choice for that many ranks
         pc = cpu_cores()
-        if pc != P:
+        if pc != p:
             r2 = ref_cpu_run(A, B, ta, n, 1, tb, p=pc, grid=None, matmul=True)
             if r2 is not None:
                 ms2, mm2, g2 = r2
@@ -236,24 +260,28 @@ def reference_arm(args, world, rank):
     if rank != 0:
         return
     n = args.size
-    A, B = make_inputs(n, args.trans_a)
+    A, B = make_inputs(n, args.trans_a, args.dist)
     steps, warm = max(args.steps, 1), max(args.warmup, 0)
     flops = 2.0 * n * n * n
-    ms = ref_cpu_run(A, B, args.trans_a, n, warm + steps, args.trans_b)
+    grid = grid_of(args)
+    ms = ref_cpu_run(A, B, args.trans_a, n, warm + steps, args.trans_b, p=args.p, grid=grid)
     if ms is not None:
         t = float(np.mean(ms[warm:]))
         v = flops / (t * 1e-3) / 1e12
-        base = {"value": v, "unit": "TFLOP/s", "cores": min(P, cpu_cores()), "kind": "reference",
-                "sample": "%d full %d^3 execs of the reference's CPU path (24 rank threads, grid "
-                          "4x2x3, 1 OpenBLAS thread per rank) after %d warm-up" % (steps, n, warm + 1)}
+        base = {"value": v, "unit": "TFLOP/s", "cores": min(args.p, cpu_cores()),
+                "kind": "reference",
+                "sample": "%d full %d^3 execs of the reference's CPU path (%d rank threads, grid "
+                          "%s, 1 OpenBLAS thread per rank) after %d warm-up"
+                          % (steps, n, args.p, grid_str(grid), warm + 1)}
         note = ("reference src/ca3dmm.c CPU path (DEV_TYPE_HOST, OpenBLAS 0.3.31) compiled "
                 "unmodified; MPI ranks are threads of one process")
     else:
         vals = []
         for _ in range(warm):
-            cpu_baseline(A, B, args.trans_a, n, budget_s=4.0, tb=args.trans_b)
+            cpu_baseline(A, B, args.trans_a, n, budget_s=4.0, tb=args.trans_b, p=args.p, grid=grid)
         for _ in range(steps):
-            base = cpu_baseline(A, B, args.trans_a, n, budget_s=4.0, tb=args.trans_b)
+            base = cpu_baseline(A, B, args.trans_a, n, budget_s=4.0, tb=args.trans_b, p=args.p,
+                                grid=grid)
             vals.append(base["value"])
         v = float(np.median(vals))
         base["value"] = v
@@ -263,7 +291,8 @@ def reference_arm(args, world, rank):
             "n_gpus": args.gpus, "steps": steps, "warmup": warm, "ms_per_step": t,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic",
-            "config": {"workload": square_desc(n, args.trans_a, args.trans_b),
+            "config": {"workload": square_desc(n, args.trans_a, args.trans_b, args.p, grid,
+                                               args.dist),
                        "l2": "inputs larger than L2 (512 MB per operand at 8000^3)"},
             "cpu_baseline": base,
             "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
@@ -362,10 +391,12 @@ def make_btb(k, n, seed=303):
     return z.numpy().T          # Fortran-ordered view of the (n, k) row-major buffer
 
 
-def square_desc(n, ta, tb):
+def square_desc(n, ta, tb, p=P, grid=GRID, dist="signed_exp"):
     """The square workload's name, the same in both arms' JSON lines."""
-    return ("ca3dmm_exec M=N=K=%d transA=%d transB=%d, 24 virtual ranks, grid 4x2x3 (cuboid "
-            "2000x4000x2667 at 8000^3), entries sign*(1+u)*2^e, e in [-8,8]" % (n, ta, tb))
+    cub = " (cuboid 2000x4000x2667 at 8000^3)" if (p, grid) == (P, GRID) else ""
+    ent = "uniform in [-1,1)" if dist == "uniform" else "sign*(1+u)*2^e, e in [-8,8]"
+    return ("ca3dmm_exec M=N=K=%d transA=%d transB=%d, %d virtual ranks, grid %s%s, entries %s"
+            % (n, ta, tb, p, grid_str(grid), cub, ent))
 
 
 def workload(args):
@@ -381,11 +412,12 @@ def workload(args):
                                                     ", larger than L2" if rows * BTB_N * 8 > 126e6
                                                     else "")}
     n = args.size
-    A, B = make_inputs(n, args.trans_a)
-    return {"m": n, "n": n, "k": n, "ta": args.trans_a, "tb": args.trans_b, "btb": False, "p": P,
-            "grid": GRID,
-            "A": A, "B": B, "label": "square %d^3 grid 4x2x3" % n,
-            "desc": square_desc(n, args.trans_a, args.trans_b),
+    A, B = make_inputs(n, args.trans_a, args.dist)
+    grid = grid_of(args)
+    return {"m": n, "n": n, "k": n, "ta": args.trans_a, "tb": args.trans_b, "btb": False,
+            "p": args.p, "grid": grid,
+            "A": A, "B": B, "label": "square %d^3 grid %s" % (n, grid_str(grid)),
+            "desc": square_desc(n, args.trans_a, args.trans_b, args.p, grid, args.dist),
             "l2": "inputs larger than L2 (512 MB per operand), no flush"}
 
 
@@ -596,7 +628,7 @@ def main():
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = btb_cpu_baseline(wl) if btb else \
-            cpu_baseline(wl["A"], wl["B"], ta, n, tb=wl["tb"])
+            cpu_baseline(wl["A"], wl["B"], ta, n, tb=wl["tb"], p=wl["p"], grid=wl["grid"])
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:
