@@ -61,6 +61,10 @@ def parse():
                     help="rows of B for --workload btb (smaller values: profiling captures)")
     ap.add_argument("--no-slice-sweep", action="store_true",
                     help="skip timing the other split-precision slice counts")
+    ap.add_argument("--ref-gpu", action="store_true",
+                    help="also time the reference's own GPU path (cuBLAS DGEMM, MPI steps staged "
+                         "through host memory) on this GPU, for context")
+    ap.add_argument("--ref-gpu-child", action="store_true", help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
@@ -452,8 +456,57 @@ def btb_cpu_baseline(wl, rows=131072):
                       "grid 1x1x32" % (rows, wl["k"])}
 
 
+def ref_gpu_child(args):
+    """Runs in a child process (its own CUDA runtime, and the reference's
+    exit-on-error paths stay out of the bench): the reference's GPU path over
+    the same workload, on the workload's grid and on one rank (where the
+    reference's "matmul only" time is one cuBLAS DGEMM of the whole product)."""
+    from oracle import oracle as orc
+    wl = workload(args)
+    m, n, k = wl["m"], wl["n"], wl["k"]
+    flops = 2.0 * m * n * k
+    out = {}
+    for name, p, grid in (("grid", wl["p"], wl["grid"]), ("one_rank", 1, None)):
+        if name == "one_rank" and wl["btb"]:
+            continue
+        t0 = time.perf_counter()
+        _, times, g = orc.ref_ca3dmm_cuda(p, m, n, k, wl["ta"], wl["tb"], wl["A"], wl["B"],
+                                          grid=grid, ntest=3, btb=wl["btb"], timeout=600.0)
+        ex, mm = float(np.median(times[:, 0])), float(np.median(times[:, 1]))
+        out[name] = {"p": p, "grid": "%dx%dx%d" % g[:3], "exec_ms": ex, "matmul_only_ms": mm,
+                     "value": flops / (ex * 1e-3) / 1e12,
+                     "matmul_only_value": flops / (mm * 1e-3) / 1e12,
+                     "wall_s": time.perf_counter() - t0}
+    print("REFGPU " + json.dumps(out), flush=True)
+
+
+def ref_gpu_leg(args):
+    """The reference's own GPU path on this GPU (context only): oracle/_ref's
+    build of src/*.c with USE_CUDA and src/cuda_proxy.cu for sm_100a, p rank
+    threads sharing the GPU, cuBLAS calls serialised.  None when not built."""
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libref_ca3dmm_cuda.so")):
+        return None
+    cmd = [sys.executable, os.path.join(ROOT, "bench.py"), "--ref-gpu-child"] + \
+        [a for a in sys.argv[1:] if a != "--ref-gpu"]
+    r = subprocess.run(cmd, capture_output=True, text=True, timeout=900)
+    for line in r.stdout.splitlines():
+        if line.startswith("REFGPU "):
+            res = json.loads(line[7:])
+            res["unit"] = "TFLOP/s"
+            res["note"] = ("the reference's GPU path (DEV_TYPE_CUDA: cuBLAS DGEMM per Cannon step, "
+                           "redistribution, allgather and kp reduction staged through pinned host "
+                           "memory) on this GPU, 3 timed execs after one warm-up, median; context, "
+                           "not the reference arm")
+            return res
+    return {"unavailable": "reference GPU run failed (rc %d): %s" %
+            (r.returncode, (r.stderr or r.stdout).strip().splitlines()[-1:])}
+
+
 def main():
     args = parse()
+    if args.ref_gpu_child:
+        ref_gpu_child(args)
+        return
     world, rank, local = dist_setup(args)
     if args.workload == "grouped" and args.impl == "ours":
         run_grouped(args, world, rank, local)
@@ -629,6 +682,8 @@ def main():
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         out["cpu_baseline"] = btb_cpu_baseline(wl) if btb else \
             cpu_baseline(wl["A"], wl["B"], ta, n, tb=wl["tb"], p=wl["p"], grid=wl["grid"])
+    if rank == 0 and world == 1 and args.ref_gpu:
+        out["reference_gpu"] = ref_gpu_leg(args)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:

@@ -64,7 +64,47 @@ def build():
                      ["-o", clib, "-L", d, "-l:" + f, "-Wl,--disable-new-dtags", "-Wl,-rpath," + d,
                       "-Wl,-Bsymbolic",
                       "-lpthread", "-lm"])
+            build_ref_cuda(refsrc, out, vdir, openblas)
     return lib
+
+
+# The reference's cuBLAS wrappers that touch its static handle; cuda_proxy.cu is
+# compiled with each renamed, and ref_cuda_serial.c puts a lock in front.
+_SERIALISED = ("cuda_cublas_dcopy", "cuda_cublas_dscal", "cuda_cublas_ddot", "cuda_cublas_dgemm",
+               "cuda_cublas_dgeam", "cuda_cublas_dtrsm", "cuda_cusolver_dpotrf",
+               "cuda_cusolver_dsyevd")
+
+
+def build_ref_cuda(refsrc, out, vdir, openblas):
+    """oracle/_ref/libref_ca3dmm_cuda.so: the reference's GPU path (USE_CUDA;
+    src/cuda_proxy.cu rebuilt for sm_100a, linked to this image's cuBLAS,
+    cuSOLVER and cuRAND) under vmpi, driven by ref_driver_cuda.c.  Context
+    figures only; skipped when nvcc or the CUDA libraries are missing."""
+    cuda = os.environ.get("CUDA_HOME", "/usr/local/cuda")
+    nvcc = os.path.join(cuda, "bin", "nvcc")
+    libdir = os.path.join(cuda, "lib64")
+    if not (os.path.exists(nvcc) and os.path.exists(os.path.join(libdir, "libcublas.so"))):
+        return None
+    srcs = [os.path.join(refsrc, f) for f in ("ca3dmm.c", "cannon.c", "mat_redist.c", "partition.c",
+                                                "utils.c", "dev_type.c", "mpi_op_omp.c")]
+    cu = os.path.join(refsrc, "cuda_proxy.cu")
+    mine = [os.path.join(vdir, f) for f in ("vmpi.c", "ref_driver_cuda.c", "ref_cuda_serial.c")]
+    hdrs = [os.path.join(vdir, f) for f in ("mpi.h", "cblas.h", "lapacke.h")]
+    clib = os.path.join(out, "libref_ca3dmm_cuda.so")
+    if not _newer(clib, srcs + [cu] + mine + hdrs + [os.path.abspath(__file__)]):
+        return clib
+    obj = os.path.join(out, "ref_cuda_proxy.o")
+    _run([nvcc, "-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-Xcompiler", "-fPIC",
+          "-I", refsrc] + ["-D%s=vgpu_raw_%s" % (f, f) for f in _SERIALISED] + ["-c", cu, "-o", obj])
+    d, f = os.path.split(openblas)
+    pre = ["-DVMPI_SCIPY_OPENBLAS"] if "scipy_openblas" in f else []
+    _run(["gcc", "-O2", "-fPIC", "-shared", "-fopenmp", "-DUSE_OPENBLAS", "-DUSE_CUDA"] + pre + [
+          "-Wno-implicit-function-declaration", "-I", vdir, "-I", refsrc,
+          "-I", os.path.join(cuda, "include")] + srcs + mine + [obj] +
+         ["-o", clib, "-L", d, "-l:" + f, "-L", libdir, "-lcublas", "-lcusolver", "-lcurand",
+          "-lcudart", "-Wl,--disable-new-dtags", "-Wl,-rpath," + d, "-Wl,-rpath," + libdir,
+          "-Wl,-Bsymbolic", "-lpthread", "-lm"])
+    return clib
 
 
 def find_openblas():

@@ -344,3 +344,43 @@ def ref_redist(src_rects, req_rects, G, timeout=60.0):
 def ref_fault_run(p, dead_rank, m=64, timeout=1.0):
     """One rank returns at once; the others must stop by timeout (nonzero)."""
     return ref_lib().ref_fault_run(p, dead_rank, m, float(timeout))
+
+
+# ---------------------------------------------------------------- reference GPU path
+_ref_cuda = None
+
+
+def ref_cuda_lib():
+    """The reference's own GPU path (USE_CUDA, cuda_proxy.cu rebuilt for sm_100a)
+    under vmpi (oracle/_ref/libref_ca3dmm_cuda.so), or None."""
+    global _ref_cuda
+    if _ref_cuda is None:
+        path = os.path.join(HERE, "_ref", "libref_ca3dmm_cuda.so")
+        if not os.path.exists(path):
+            return None
+        L = C.CDLL(path)
+        dp, ip = C.POINTER(C.c_double), C.POINTER(C.c_int)
+        L.ref_ca3dmm_cuda.argtypes = [C.c_int] * 7 + [ip, dp, dp, dp, C.c_int, dp, ip, C.c_double]
+        _ref_cuda = L
+    return _ref_cuda
+
+
+def ref_ca3dmm_cuda(p, m, n, k, ta, tb, A, B, grid=None, ntest=1, btb=False, timeout=300.0):
+    """Run the unmodified reference with DEV_TYPE_CUDA (cuBLAS DGEMM, host-staged
+    MPI steps) on p vmpi rank threads sharing one GPU, the way
+    examples/example_AB.c does.  Returns (C, times [ntest x 2] of rank 0: total
+    exec ms and matmul-only ms, (mp, np, kp, rp))."""
+    L = ref_cuda_lib()
+    if L is None:
+        raise RuntimeError("reference GPU path not built (oracle/_ref)")
+    A = np.asfortranarray(A if A is not None else np.zeros((1, 1)), dtype=np.float64)
+    B = np.asfortranarray(B, dtype=np.float64)
+    Cm = np.zeros((n if btb else m, n), order="F")
+    times = np.zeros((max(ntest, 1), 2))
+    gout = np.zeros(4, dtype=np.int32)
+    g = (C.c_int * 3)(*grid) if grid is not None else None
+    rc = L.ref_ca3dmm_cuda(p, m, n, k, int(ta), int(tb), int(btb), g, _d(A), _d(B), _d(Cm), ntest,
+                           _d(times), gout.ctypes.data_as(C.POINTER(C.c_int)), float(timeout))
+    if rc:
+        raise RuntimeError("reference GPU run failed")
+    return Cm, times, tuple(int(x) for x in gout)

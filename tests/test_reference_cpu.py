@@ -78,3 +78,17 @@ def test_reference_mat_redist_between_layouts(R, Cc, src, req):
     out = orc.ref_redist(sr, rr, G)
     for o, r in zip(out, rr):
         assert np.array_equal(o, G[r[0]:r[0] + r[2], r[1]:r[1] + r[3]])
+
+
+def test_reference_gpu_build_loads_and_serialises_cublas():
+    """The reference's GPU path build (context figures) loads without a GPU and
+    routes every wrapper that touches the reference's static cuBLAS handle
+    through the serialising shim (the originals renamed vgpu_raw_*)."""
+    import os
+    path = os.path.join(os.path.dirname(orc.HERE), "oracle", "_ref", "libref_ca3dmm_cuda.so")
+    if not os.path.exists(path):
+        pytest.skip("reference GPU path not built")
+    L = orc.ref_cuda_lib()
+    assert L is not None and hasattr(L, "ref_ca3dmm_cuda")
+    for f in ("cuda_cublas_dgemm", "cuda_cublas_dgeam", "cuda_cublas_dcopy"):
+        assert hasattr(L, f) and hasattr(L, "vgpu_raw_" + f), f
