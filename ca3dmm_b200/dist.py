@@ -4,8 +4,8 @@ Each process is one rank of the reference's process grid (the grid and the
 per-rank cuboids of ``ca3dmm_engine_init`` / ``_init_BTB``, src/ca3dmm.c:23-722,
 with p = the group's size).  It owns the blocks of A, B and C it passes, in any
 layout (examples/example_AB.c:85-98 uses 1D column blocks), and computes the
-C_2dmm block of its k-slab with the single-GPU engine.  The exchanges are three
-all-to-alls:
+C_2dmm block of its k-slab with the single-GPU engine.  An exec is two
+all-to-alls around the local GEMM:
 
 1. operands: each rank sends every peer the intersection of its A and B blocks
    with the peer's op(A) panel (C_2dmm rows x slab k) and op(B) panel (slab k x
