@@ -65,6 +65,10 @@ def parse():
                     help="also time the reference's own GPU path (cuBLAS DGEMM, MPI steps staged "
                          "through host memory) on this GPU, for context")
     ap.add_argument("--ref-gpu-child", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--sharded", action="store_true",
+                    help="square workload as one CA3DMM across the launched GPUs (one rank per "
+                         "GPU on the reference's grid for p = N, NCCL all-to-alls; strong "
+                         "scaling) instead of N independent replicas")
     return ap.parse_args()
 
 
@@ -502,8 +506,95 @@ def ref_gpu_leg(args):
             (r.returncode, (r.stderr or r.stdout).strip().splitlines()[-1:])}
 
 
+def run_sharded(args, world, rank, local):
+    """CA3DMM across the launched GPUs (ca3dmm_b200.dist over NCCL): A, B and C
+    of the square workload in examples/example_AB.c's 1D column blocks, one rank
+    per GPU on the reference's grid for p = N (or --grid when its product is at
+    most N).  Total work is fixed (strong scaling); time is the slowest rank's."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    import ca3dmm_b200 as cb
+    from ca3dmm_b200.dist import DistCa3dmmEngine
+    from oracle import oracle as orc
+    torch.cuda.set_device(local)
+    if world == 1:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        if "MASTER_PORT" not in os.environ:
+            import socket
+            with socket.socket() as sk:
+                sk.bind(("127.0.0.1", 0))
+                os.environ["MASTER_PORT"] = str(sk.getsockname()[1])
+        os.environ.setdefault("RANK", "0")
+        os.environ.setdefault("WORLD_SIZE", "1")
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    n, ta, tb = args.size, args.trans_a, args.trans_b
+    grid = grid_of(args)
+    if grid is not None and grid[0] * grid[1] * grid[2] > world:
+        grid = None
+    A, B = make_inputs(n, ta, args.dist)
+    s0, sz = cb.calc_block_spos_size(n, world, rank)
+    blk = (0, n, s0, sz)
+
+    def cols(X):
+        return torch.from_numpy(np.asfortranarray(X[:, s0:s0 + sz]).ravel(order="F").copy()
+                                if sz else np.zeros(1)).cuda()
+
+    dA, dB = cols(A), cols(B)
+    dC = torch.zeros(max(n * sz, 1), dtype=torch.float64, device="cuda")
+    oz_slices = int(os.environ.get("CA3DMM_BENCH_SLICES", "7"))
+    legs = {}
+    flops = 2.0 * n * n * n
+    for mode, key in ((cb.GEMM_PLAIN, "plain"), (cb.GEMM_OZAKI, "ozaki")):
+        e = DistCa3dmmEngine(n, n, n, ta, tb, blk, blk, blk, proc_grid=grid, gemm_mode=mode,
+                             slices=oz_slices)
+        for _ in range(args.warmup):
+            e.exec(dA, n, dB, n, dC, n)
+        e.reset_stat()
+        dist.barrier()
+        torch.cuda.synchronize()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ev0.record()
+        for _ in range(args.steps):
+            e.exec(dA, n, dB, n, dC, n)
+        ev1.record()
+        torch.cuda.synchronize()
+        ms = max_over_ranks(ev0.elapsed_time(ev1) / args.steps, world)
+        st = {kk: (v / max(e.stats["n_exec"], 1) if kk != "n_exec" else v)
+              for kk, v in e.stats.items()}
+        # this rank's C columns against the double-double truth (sampled)
+        err = None
+        if sz:
+            ii, jj = orc.sample_indices(n, sz, nrand=512, nlines=0)
+            hi, lo, ab = orc.dd_entries(A, B, ta, tb, n, ii, jj + s0)
+            err = orc.errors(dC[torch.from_numpy(ii + jj * n).cuda()].cpu().numpy(), hi, lo, ab)
+        legs[key] = {"ms_per_step": ms, "tflops": flops / (ms * 1e-3) / 1e12,
+                     "grid": "%dx%dx%d" % (e.mp, e.np_, e.kp), "idle_ranks": e.rp,
+                     "rank0_phases_ms": st, "rank0_err": err}
+        e.free()
+    head = "ozaki"
+    out = {"metric": METRIC, "value": legs[head]["tflops"], "unit": "TFLOP/s", "n_gpus": world,
+           "steps": args.steps, "warmup": args.warmup, "ms_per_step": legs[head]["ms_per_step"],
+           "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f64",
+           "data": "synthetic",
+           "config": {"workload": "sharded " + square_desc(n, ta, tb, world, None, args.dist)
+                      .replace("virtual ranks", "GPU ranks"),
+                      "layout": "A, B, C in 1D column blocks over the ranks",
+                      "exchange": "NCCL all_to_all_single: operand panels, C pieces",
+                      "l2": "inputs larger than L2 at 8000^3, no flush"},
+           "legs": legs}
+    if rank == 0:
+        print(json.dumps(out), flush=True)
+    dist.barrier()
+    dist.destroy_process_group()
+
+
 def main():
     args = parse()
+    if args.sharded and args.impl == "ours":
+        world, rank, local = dist_setup(args)
+        run_sharded(args, world, rank, local)
+        return
     if args.ref_gpu_child:
         ref_gpu_child(args)
         return
