@@ -13,6 +13,7 @@ CSRC = os.path.join(HERE, "csrc")
 INC = os.path.join(ROOT, "include")
 OBJ = os.path.join(HERE, "_obj")
 LIB = os.path.join(HERE, "libca3dmm_b200.so")
+ARCHIVE = os.path.join(HERE, "libca3dmm_b200.a")
 CUDA = os.environ.get("CUDA_HOME", "/usr/local/cuda")
 NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -60,6 +61,12 @@ def build(verbose=False):
                                   "-I", INC, "-I", CSRC, "-c", s, "-o", o])
     if _newer(LIB, objs):
         _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs + ["-lm"])
+    # the static archive beside the shared library, as the reference installs both
+    # (src/common.make:1-2, 56-66); link with -lcudart_static -lstdc++ -ldl -lpthread -lrt
+    if _newer(ARCHIVE, objs):
+        if os.path.exists(ARCHIVE):
+            os.remove(ARCHIVE)
+        _run(["ar", "rcs", ARCHIVE] + objs)
     # example callers (C programs linking the library like the reference's examples)
     for ex in EXAMPLES:
         s = os.path.join(HERE, "examples", ex + ".c")

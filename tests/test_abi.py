@@ -37,3 +37,30 @@ def test_library_exports_every_declared_symbol():
     L = ctypes.CDLL(cb.LIB_PATH)
     missing = [n for n in declared_functions() if not hasattr(L, n)]
     assert not missing, missing
+
+
+def test_static_archive_defines_every_symbol_and_links():
+    """libca3dmm_b200.a (installed beside the .so, as the reference installs
+    libca3dmm.a and .so) defines every declared function, and a C caller links
+    statically against it and runs a host-only entry point."""
+    import subprocess
+    from ca3dmm_b200 import build
+    arc = build.ARCHIVE
+    assert os.path.exists(arc)
+    nm = subprocess.run(["nm", "--defined-only", arc], capture_output=True, text=True).stdout
+    defined = {ln.split()[-1] for ln in nm.splitlines() if " T " in ln}
+    missing = [n for n in declared_functions() if n not in defined]
+    assert not missing, missing
+    src = os.path.join(build.OBJ, "static_caller.c")
+    exe = os.path.join(build.OBJ, "static_caller")
+    with open(src, "w") as f:
+        f.write('#include "ca3dmm.h"\n'
+                "int main(void) { int mp, np, kp, rp;\n"
+                "  calc_3d_decomposition_cannon(24, 8000, 8000, 8000, &mp, &np, &kp, &rp);\n"
+                "  return (mp == 4 && np == 2 && kp == 3 && rp == 0) ? 0 : 1; }\n")
+    cuda_lib = os.path.join(build.CUDA, "lib64")
+    r = subprocess.run(["gcc", "-O2", "-I", os.path.join(ROOT, "include"), src, arc, "-L", cuda_lib,
+                        "-lcudart_static", "-lstdc++", "-ldl", "-lpthread", "-lrt", "-lm", "-o", exe],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    assert subprocess.run([exe]).returncode == 0
