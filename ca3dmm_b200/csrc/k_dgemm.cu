@@ -31,6 +31,7 @@
 #include <cuda_runtime.h>
 #include <cstdio>
 #include <cstring>
+#include <atomic>
 #include "k_common.cuh"
 #include "ca3dmm_kernels.h"
 
@@ -356,17 +357,28 @@ typedef CUresult (*encode_tiled_fn)(CUtensorMap *, CUtensorMapDataType, cuuint32
 
 encode_tiled_fn get_encode()
 {
-    static encode_tiled_fn fn = nullptr;
-    if (!fn) {
+    // resolved once; the initialisation of a function-local static is thread-safe
+    static const encode_tiled_fn fn = []() -> encode_tiled_fn {
         cudaDriverEntryPointQueryResult q;
         void *p = nullptr;
         if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) !=
                 cudaSuccess ||
             q != cudaDriverEntryPointSuccess)
             return nullptr;
-        fn = reinterpret_cast<encode_tiled_fn>(p);
-    }
+        return reinterpret_cast<encode_tiled_fn>(p);
+    }();
     return fn;
+}
+
+// cuTensorMapEncodeTiled is a driver call: it fails in a host thread that has
+// no current context, which a thread that has made no runtime call yet lacks
+// (the runtime binds the primary context lazily).  cudaSetDevice binds the
+// current device's primary context to the calling thread without waiting on
+// any stream.
+void bind_device_context()
+{
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaSetDevice(dev);
 }
 
 }  // namespace
@@ -379,6 +391,7 @@ extern "C" int ca3dmm_encode_tmap_2d(void *tmap, int dtype_bytes, const void *ba
     encode_tiled_fn enc = get_encode();
     if (!enc) return CA3DMM_ENODEV;
     if ((reinterpret_cast<uintptr_t>(base) & 15) || (stride1_bytes & 15)) return CA3DMM_EINVAL;
+    bind_device_context();
     CUtensorMapDataType dt =
         dtype_bytes == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_UINT8;
     cuuint64_t dims[2] = {dim0, dim1};
@@ -400,6 +413,7 @@ extern "C" int ca3dmm_encode_tmap_u8(void *tmap, int rank, const void *base,
     encode_tiled_fn enc = get_encode();
     if (!enc) return CA3DMM_ENODEV;
     if (rank < 1 || rank > 5 || (reinterpret_cast<uintptr_t>(base) & 15)) return CA3DMM_EINVAL;
+    bind_device_context();
     cuuint64_t d[5], st[4];
     cuuint32_t bx[5], es[5];
     for (int i = 0; i < rank; ++i) {
@@ -487,15 +501,20 @@ extern "C" int ca3dmm_dgemm_launch_ranges(const void *dev_plan, int nprob,
     if (!ranges || ranges->n < 0 || ranges->n > CA3DMM_MAX_RANGES) return CA3DMM_EINVAL;
     const int total_tiles = range_total(*ranges);
     if (total_tiles <= 0) return CA3DMM_OK;
-    static bool attr_done = false;
-    if (!attr_done) {
+    // the shared-memory attribute is per device: one bit per device once set
+    // (two threads may both set it; that is harmless)
+    static std::atomic<unsigned long long> attr_done{0};
+    int dev = 0;
+    CA3DMM_CUDA_TRY(cudaGetDevice(&dev));
+    const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+    if (!(attr_done.load(std::memory_order_acquire) & bit) || !bit) {
         CA3DMM_CUDA_TRY(cudaFuncSetAttribute(dgemm_dmma_grouped<false>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int) SMEM_BYTES));
         CA3DMM_CUDA_TRY(cudaFuncSetAttribute(dgemm_dmma_grouped<true>,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int) SMEM_BYTES));
-        attr_done = true;
+        attr_done.fetch_or(bit, std::memory_order_release);
     }
     const CUtensorMap *tm = reinterpret_cast<const CUtensorMap *>(dev_plan);
     const DProb *dp = reinterpret_cast<const DProb *>(tm + 2 * nprob);
@@ -515,14 +534,14 @@ extern "C" int ca3dmm_dgemm_launch_ranges(const void *dev_plan, int nprob,
 
 extern "C" int ca3dmm_device_sm_count(void)
 {
-    static int sms[64] = {0};
+    static std::atomic<int> sms[64];        // zero-initialised (static storage)
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return 148;
-    if (!sms[dev]) {
-        int v = 0;
+    int v = sms[dev].load(std::memory_order_relaxed);
+    if (!v) {
         if (cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || v <= 0)
             v = 148;
-        sms[dev] = v;
+        sms[dev].store(v, std::memory_order_relaxed);
     }
-    return sms[dev];
+    return v;
 }

@@ -275,11 +275,14 @@ extern "C" int ca3dmm_pack_tma_launch(const void *dev_tmaps, const ca3dmm_pack_d
                                       int *dev_status, double timeout_s, cudaStream_t stream)
 {
     if (ndesc <= 0 || total_tiles <= 0) return CA3DMM_OK;
-    static bool attr_done = false;
-    if (!attr_done) {
+    static std::atomic<unsigned long long> attr_done{0};     // one bit per device
+    int dev = 0;
+    CA3DMM_CUDA_TRY(cudaGetDevice(&dev));
+    const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+    if (!(attr_done.load(std::memory_order_acquire) & bit) || !bit) {
         CA3DMM_CUDA_TRY(cudaFuncSetAttribute(pack_transpose_tma_kernel,
                                              cudaFuncAttributeMaxDynamicSharedMemorySize, TT_SMEM));
-        attr_done = true;
+        attr_done.fetch_or(bit, std::memory_order_release);
     }
     int grid = ca3dmm_device_sm_count();
     if (grid > total_tiles) grid = total_tiles;
