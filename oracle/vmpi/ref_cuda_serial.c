@@ -1,5 +1,5 @@
 /* Serialises the reference's cuBLAS wrappers across vmpi rank threads (TEST AND
- * BASELINE INFRASTRUCTURE ONLY).
+ * COMPARISON INFRASTRUCTURE ONLY).
  *
  * src/cuda_proxy.cu:151-174 keeps one static cuBLAS handle per process, which
  * is right for one MPI rank per process but not for ranks that are threads of

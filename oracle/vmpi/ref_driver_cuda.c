@@ -1,4 +1,4 @@
-/* Driver of the reference's own GPU path under vmpi (TEST AND BASELINE
+/* Driver of the reference's own GPU path under vmpi (TEST AND COMPARISON
  * INFRASTRUCTURE ONLY; context figures, never the product).
  *
  * Runs the unmodified reference (src/ca3dmm.c and friends compiled with
