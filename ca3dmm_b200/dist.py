@@ -146,11 +146,26 @@ class DistCa3dmmEngine:
         self.ops = ops if ops is not None else _CudaOps(device)
         self.comm_device = device if self.direct else torch.device("cpu")
         # every rank's rectangles
-        mine = list(src_A if not btb else (0, 0, 0, 0)) + list(src_B) + list(dst_C)
+        # every rank's rectangles and call arguments: each rank checks all of
+        # them, so an inconsistent call raises on every rank before any exchange
+        g3 = list(proc_grid) if proc_grid is not None else [-1, -1, -1]
+        mine = list(src_A if not btb else (0, 0, 0, 0)) + list(src_B) + list(dst_C) + \
+            [m, n, k, self.ta, self.tb, int(self.btb), int(gemm_mode), int(slices)] + g3
         allr = self._allgather_ints(mine)
+        if any(r[12:] != allr[0][12:] for r in allr):
+            raise ValueError("ranks disagree on m, n, k, transposes, mode or grid")
         self.srcA = [tuple(r[0:4]) for r in allr]
         self.srcB = [tuple(r[4:8]) for r in allr]
         self.dstC = [tuple(r[8:12]) for r in allr]
+        a_shape = (k, m) if self.ta else (m, k)
+        b_shape = (k, n) if btb else ((n, k) if self.tb else (k, n))
+        c_shape = (self.m, n)
+        for rects, shape, what in ((self.srcA if not btb else [], a_shape, "src_A"),
+                                   (self.srcB, b_shape, "src_B"), (self.dstC, c_shape, "dst_C")):
+            for r in rects:
+                if min(r) < 0 or r[0] + r[1] > shape[0] or r[2] + r[3] > shape[1]:
+                    raise ValueError("%s rectangle %s outside the %d x %d matrix" %
+                                     ((what, r) + shape))
         # the reference's grid and every rank's cuboid (no device call)
         geo = cb.Ca3dmmEngine(m, n, k, self.ta if not btb else 0, self.tb, p=self.world,
                               proc_grid=proc_grid, btb=btb, caller_workbuf=True)
@@ -168,6 +183,13 @@ class DistCa3dmmEngine:
                        for g in info]
         self._check_cover()
         self.panels = [self._panels(r) for r in range(self.world)]
+        # every panel must be covered by the ranks' source blocks
+        for r in range(self.world):
+            for mat, rect in self.panels[r]:
+                got = sum(_area(_inter(self._src(mat, q), rect)) for q in range(self.world))
+                if got < _area(rect):
+                    raise ValueError("the source blocks do not cover rank %d's %s panel %s" %
+                                     (r, "A" if mat == _A else "B", rect))
         self._plan_operands()
         self._plan_c()
         self.gemm_mode, self.slices = gemm_mode, slices

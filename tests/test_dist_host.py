@@ -251,3 +251,64 @@ CASES = {
 @pytest.mark.parametrize("world", sorted(CASES))
 def test_dist_engine_on_gloo_ranks(world):
     _run(world, CASES[world])
+
+
+def _bad_worker(rank, world, port, q):
+    import datetime
+    import torch.distributed as dist
+    sys.path.insert(0, ROOT)
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=60))
+    from ca3dmm_b200.dist import DistCa3dmmEngine
+    m, n, k = 40, 30, 50
+    cols = lambda nr, nc: _layout("cols", nr, nc, world, rank)
+    calls = {
+        # rank 1 passes another m
+        "sizes": lambda: DistCa3dmmEngine(m + rank, n, k, 0, 0, cols(m, k), cols(k, n),
+                                          cols(m, n), ops=NumpyOps()),
+        # rank 1 owns no part of A: rank panels are not covered
+        "cover": lambda: DistCa3dmmEngine(m, n, k, 0, 0, cols(m, k) if rank == 0 else (0, 0, 0, 0),
+                                          cols(k, n), cols(m, n), ops=NumpyOps()),
+        # a source rectangle beyond the matrix
+        "bounds": lambda: DistCa3dmmEngine(m, n, k, 0, 0, cols(m, k), (0, k + 1, 0, n),
+                                           cols(m, n), ops=NumpyOps()),
+    }
+    out = {}
+    for name, fn in calls.items():
+        try:
+            fn()
+            out[name] = None
+        except ValueError as exc:
+            out[name] = str(exc)
+    dist.barrier()
+    dist.destroy_process_group()
+    q.put((rank, out))
+
+
+def test_dist_engine_rejects_inconsistent_calls_on_every_rank():
+    """Inconsistent arguments, uncovered panels and out-of-range blocks raise
+    ValueError on every rank before any exchange (no rank is left waiting)."""
+    import queue
+    import time
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _free_port()
+    procs = [ctx.Process(target=_bad_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in procs:
+        p.start()
+    res, t0 = {}, time.time()
+    while len(res) < 2:
+        try:
+            r, o = q.get(timeout=2)
+            res[r] = o
+        except queue.Empty:
+            assert not any(p.exitcode not in (None, 0) for p in procs), "a rank failed"
+            assert time.time() - t0 < 120, "ranks timed out"
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    for r in range(2):
+        assert "disagree" in res[r]["sizes"]
+        assert "do not cover" in res[r]["cover"]
+        assert "outside" in res[r]["bounds"]
