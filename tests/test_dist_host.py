@@ -225,6 +225,8 @@ def _run(world, cases):
 
 
 CASES = {
+    1: [(70, 50, 90, 1, 0, None, "cols", 1, 7, False, 81),      # one rank: in place
+        (40, 40, 300, 0, 0, None, "cols", 1, 7, True, 82)],
     2: [(90, 70, 130, 0, 0, None, "cols", 1, 7, False, 1),
         (64, 96, 200, 1, 1, (1, 1, 2), "blocks", 1, 6, False, 2),
         (50, 40, 300, 0, 0, None, "rows", 0, 0, False, 3),
