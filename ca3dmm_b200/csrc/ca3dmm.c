@@ -71,6 +71,8 @@ typedef struct {
     int pack_tiles_A, pack_tiles_B, pack_tiles_C;
     int packA_tma, packB_tma;     /* transposing packs staged by TMA (tensor maps in the plan) */
     int a_kmajor;                 /* plain mode: transposed A blocks read in place, K-major */
+    int plain_merged;             /* plain mode: the kp slabs run as one GEMM over all of k */
+    int merge_allowed;            /* CA3DMM_PLAIN_MERGE_SLABS (default 1) */
     /* dst_C block */
     int has_dst, dst_srow, dst_nrow, dst_scol, dst_ncol;
     cudaEvent_t ev[5];
@@ -267,6 +269,9 @@ static int plan_build(ca3dmm_engine_p e)
     pl->A = (blk_t *) calloc((size_t) pl->nA, sizeof(blk_t));
     pl->B = (blk_t *) calloc((size_t) pl->nB, sizeof(blk_t));
     pl->ksplit = choose_ksplit(e, pl->sym);
+    int merge;
+    GET_ENV_INT_VAR(merge, "CA3DMM_PLAIN_MERGE_SLABS", "plain_merge_slabs", 1, 0, 1);
+    pl->merge_allowed = merge;
     pl->gd = (ca3dmm_dgemm_desc_t *) calloc((size_t) pl->ngroup * (size_t) pl->ksplit,
                                             sizeof(ca3dmm_dgemm_desc_t));
     pl->ob = (ca3dmm_oz_blk_t *) calloc((size_t) (pl->nA + pl->nB), sizeof(ca3dmm_oz_blk_t));
@@ -768,8 +773,27 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
             d->rows = 0;
         }
     }
+    /* Plain FP64 with slab 0's operand blocks read in place (a 16-byte aligned
+     * start and an even ld, so the same tensor maps reach every k): the kp
+     * slabs of the one (merged) group are consecutive k ranges of the same A
+     * and B, so when one slab alone has enough tiles for every SM they run as
+     * one GEMM over all of k that writes C directly -- no packs of the other
+     * slabs' blocks, no slab buffers, no slab sum.  The plain path's contract
+     * is k u |A||B| accuracy, not the slab sum's rounding order (split
+     * precision keeps the slabs: its exponents are per slab). */
+    pl->plain_merged = 0;
+    if (pl->merge_allowed && e->gemm_mode == CA3DMM_GEMM_PLAIN && !pl->sym && !e->is_BTB &&
+        pl->ksplit == 1 &&
+        e->kp > 1 && pl->tmn == 1 && pl->tnn == 1 && pl->A[0].direct && pl->B[0].direct &&
+        (long long) ((e->m + 127) / 128) * ((e->n + 127) / 128) >= 4LL * CA3DMM_SMS_B200) {
+        pl->plain_merged = 1;
+        for (int i = 1; i < pl->nA; i++) pa[i].rows = 0;
+        for (int i = 1; i < pl->nB; i++) pb[i].rows = 0;
+        pl->packA_tma = 0;
+        pl->pack_tiles_A = ca3dmm_pack_tiles(pa, pl->nA);
+    }
     pl->packB_tma = 0;
-    if (e->trans_B && ca3dmm_pack_tma_prepare(pb, pl->nB, (const double *) B, h + pl->off_tmapB,
+    if (e->trans_B && !pl->plain_merged && ca3dmm_pack_tma_prepare(pb, pl->nB, (const double *) B, h + pl->off_tmapB,
                                               &pl->pack_tiles_B) == CA3DMM_OK)
         pl->packB_tma = 1;
     else
@@ -788,6 +812,7 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
     pl->pack_tiles_C = ca3dmm_pack_tiles(pc, 1);
     ca3dmm_dgemm_desc_t *gd = pl->gd;
     const int ks = pl->ksplit, nslab = e->kp * ks;
+
     for (int i = 0; i < pl->ngroup; i++) {
         group_t *g = &pl->groups[i];
         const blk_t *ba = &pl->A[g->a_blk], *bb = &pl->B[g->b_blk];
@@ -808,6 +833,18 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
             q->lda = lda;
             q->B = b + k0;
             q->ldb = ldb;
+            if (pl->plain_merged) {
+                /* slab 0's group carries all of k (its blocks start at k = 0); the
+                 * other slabs' groups are empty */
+                const int first = g->tk == 0;
+                q->C = out + g->m0 + (size_t) g->n0 * ldo;
+                q->ldc = ldo;
+                q->m = first ? g->mz : 0; q->n = first ? g->nz : 0; q->k = first ? e->k : 0;
+                q->alpha = 1.0; q->beta = 0.0;
+                q->raster = e->raster;
+                q->a_kmajor = pl->a_kmajor;
+                continue;
+            }
             if (nslab > 1) {
                 q->C = (double *) (w + pl->off_slab) + (size_t) (g->tk * ks + sub) * pl->slab_stride +
                        g->m0 + (size_t) g->n0 * pl->slab_ld;
@@ -965,7 +1002,7 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
     double *out = whole ? (double *) dst_C : (double *) (w + pl->off_cout);
     long long ldo = whole ? ldC : e->m;
     const int nred = e->gemm_mode == CA3DMM_GEMM_OZAKI ? (pl->oz_fused ? 1 : e->kp)
-                                                      : e->kp * pl->ksplit;
+                                                      : (pl->plain_merged ? 1 : e->kp * pl->ksplit);
     if (nred > 1) {
         rc = ca3dmm_reduce_slabs_launch((const double *) (w + pl->off_slab),
                                         (long long) pl->slab_stride, pl->slab_ld, nred, e->m,
@@ -1141,7 +1178,7 @@ static int hx_build_bands(ca3dmm_engine_p e, struct host_exec *x, cudaStream_t s
             ca3dmm_tile_ranges_t *rg = &x->rng[c];
             memset(rg, 0, sizeof(*rg));
             const int row_lo = r / 128, nrow_t = band_rows / 128;
-            for (int tk = 0; tk < (chained ? 1 : e->kp); tk++)
+            for (int tk = 0; tk < ((chained || (!ozaki && pl->plain_merged)) ? 1 : e->kp); tk++)
                 for (int tn = 0; tn < tnn; tn++) {
                     const int g = (tk * tmn + tm) * tnn + tn;
                     const group_t *gg = &pl->groups[g];
@@ -1164,7 +1201,8 @@ static int hx_build_bands(ca3dmm_engine_p e, struct host_exec *x, cudaStream_t s
                     const blk_t *b = &pl->A[blocks[tk]];
                     ca3dmm_pack_desc_t *d = &pd[tk];
                     memset(d, 0, sizeof(*d));
-                    if (b->direct) continue;         /* read in place by the GEMM */
+                    /* read in place by the GEMM, or a slab the merged plain GEMM skips */
+                    if (b->direct || (pl->plain_merged && tk > 0)) continue;
                     a_pack_desc(e, pl, b, r, rend, x->lda, d);
                 }
                 x->ntile[c][0] = ca3dmm_pack_tiles(pd, e->kp);
@@ -1401,7 +1439,7 @@ static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_
                 rc = ca3dmm_dgemm_launch_ranges(w + pl->off_gemm, pl->ngroup, &x->rng[c],
                                                 pl->a_kmajor, status_d, 5.0, st);
         }
-        if (!rc && e->kp > 1 && !(ozaki && pl->oz_fused))
+        if (!rc && e->kp > 1 && !(ozaki && pl->oz_fused) && !(!ozaki && pl->plain_merged))
             rc = ca3dmm_reduce_slabs_launch((const double *) (w + pl->off_slab) + x->r0[c],
                                             (long long) pl->slab_stride, pl->slab_ld, e->kp,
                                             x->r1[c] - x->r0[c], e->n, x->dC + x->r0[c], x->ldc, st);

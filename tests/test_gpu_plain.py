@@ -195,3 +195,53 @@ def test_btb_k_split_sub_slabs(cuda, n, k, grid):
     e = cb.Ca3dmmEngine(n, n, k, p=grid[2], btb=True, proc_grid=grid)
     assert e.ok and e.exec(None, 0, dB, ldb, dC, n) == 0
     _dd_check(from_dev(dC, n, n), Bm, Bm, 1, 0, n, n, k)
+
+
+@pytest.mark.parametrize("ta,pad", [(0, 0), (0, 1), (1, 0)])
+def test_plain_slabs_merged_when_tiles_suffice(cuda, ta, pad):
+    """kp = 2 over a C of 25 x 25 = 625 tiles (>= 4 per SM): with every operand
+    block read in place (even ld, M-major or K-major A) the two slabs run as one
+    GEMM over all of k writing C directly; with an odd ldA (packed blocks) they
+    run per slab and are summed.  Both stay within k u |A||B| (sampled), and
+    the host-buffer exec gives the device exec's bits."""
+    import torch
+    m, n, k = 3200, 3100, 1500
+    A = orc.gen_signed_exp(51, *((k, m) if ta else (m, k)))
+    B = orc.gen_signed_exp(52, k, n)
+    dA, lda = to_dev(A, pad_ld=A.shape[0] + pad)
+    dB, ldb = to_dev(B)
+    dC = dev_zeros(m * n)
+    e = cb.Ca3dmmEngine(m, n, k, ta, 0, p=2, proc_grid=(1, 1, 2))
+    assert e.ok and e.s.kp == 2
+    assert e.exec(dA, lda, dB, ldb, dC, m) == 0
+    Cg = from_dev(dC, m, n)
+    _dd_check(Cg, A, B, ta, 0, m, n, k, full=False)
+    hA = np.zeros((lda, A.shape[1]), order="F")
+    hA[:A.shape[0], :] = A
+    hC = torch.zeros(m * n, dtype=torch.float64).pin_memory()
+    hAt = torch.from_numpy(hA.ravel(order="F").copy()).pin_memory()
+    hBt = torch.from_numpy(np.asfortranarray(B).ravel(order="F").copy()).pin_memory()
+    assert e.exec_host(hAt, lda, hBt, ldb, hC, m) == 0
+    if pad == 0:
+        assert np.array_equal(hC.numpy().reshape(n, m).T, Cg)
+
+
+def test_plain_slab_merge_can_be_switched_off(cuda, monkeypatch):
+    """CA3DMM_PLAIN_MERGE_SLABS=0 keeps the kp-slab decomposition (per-slab
+    GEMMs summed in slab order, the reference's rounding order) where the
+    merged GEMM would run; both within k u |A||B|, and the two orders differ."""
+    m, n, k = 3200, 3100, 1500
+    A = orc.gen_signed_exp(61, m, k)
+    B = orc.gen_signed_exp(62, k, n)
+    dA, lda = to_dev(A)
+    dB, ldb = to_dev(B)
+    outs = []
+    for merge in ("1", "0"):
+        monkeypatch.setenv("CA3DMM_PLAIN_MERGE_SLABS", merge)
+        e = cb.Ca3dmmEngine(m, n, k, 0, 0, p=3, proc_grid=(1, 1, 3))
+        dC = dev_zeros(m * n)
+        assert e.ok and e.exec(dA, lda, dB, ldb, dC, m) == 0
+        outs.append(from_dev(dC, m, n))
+        _dd_check(outs[-1], A, B, 0, 0, m, n, k, full=False)
+        e.free()
+    assert not np.array_equal(outs[0], outs[1])
