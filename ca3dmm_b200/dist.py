@@ -50,7 +50,11 @@ def _area(r):
 class _CudaOps:
     """The device side: batched rectangle copies (mat_redist_layouts, one launch
     per call), the single-GPU engine for the local GEMM and the ordered slab sum
-    (the engine's kp-slab reduction kernel)."""
+    (the engine's kp-slab reduction kernel).  Everything runs on the caller's
+    current torch stream, in order with the torch copies around it."""
+
+    def _stream(self):
+        return self.torch.cuda.current_stream(self.device).cuda_stream
 
     def __init__(self, device):
         import torch
@@ -79,7 +83,8 @@ class _CudaOps:
             return
         sp = [t.data_ptr() + 8 * off for t, off, _ in srcs]
         dp = [t.data_ptr() + 8 * off for t, off, _ in dsts]
-        rc = L.exec(sp, [max(ld, 1) for _, _, ld in srcs], dp, [max(ld, 1) for _, _, ld in dsts])
+        rc = L.exec(sp, [max(ld, 1) for _, _, ld in srcs], dp, [max(ld, 1) for _, _, ld in dsts],
+                    self._stream())
         if rc:
             raise RuntimeError("mat_redist_layouts_exec failed: %s" % cb.ERRORS.get(rc, rc))
 
@@ -92,6 +97,7 @@ class _CudaOps:
         return e
 
     def gemm(self, e, A, lda, B, ldb, C, ldc):
+        e.set_stream(self._stream(), 1)
         rc = e.exec(A, lda, B, ldb, C, ldc)
         if rc:
             raise RuntimeError("local exec failed: %s" % cb.ERRORS.get(rc, rc))
@@ -101,7 +107,8 @@ class _CudaOps:
         import ctypes as C
         rc = L.ca3dmm_reduce_slabs_launch(C.c_void_p(layers.data_ptr()), C.c_longlong(nr * nc),
                                           C.c_longlong(max(nr, 1)), kp, nr, nc,
-                                          C.c_void_p(out.data_ptr()), C.c_longlong(ldo), None)
+                                          C.c_void_p(out.data_ptr()), C.c_longlong(ldo),
+                                          C.c_void_p(self._stream()))
         if rc:
             raise RuntimeError("slab sum failed: %s" % cb.ERRORS.get(rc, rc))
 
