@@ -105,8 +105,29 @@ def _split(length, parts, i):
     return i * base + min(i, rem), base + (1 if i < rem else 0)
 
 
+def _random_layout(seed, nrow, ncol, world, rank):
+    """Irregular blocks: random row and column cuts into pr x pc blocks dealt to
+    a random permutation of the ranks (ranks beyond pr x pc own nothing)."""
+    rng = np.random.default_rng(seed)
+    pr = int(rng.integers(1, world + 1))
+    pc = int(rng.integers(1, world // pr + 1))
+    rc = np.sort(rng.choice(np.arange(1, max(nrow, 2)), size=min(pr - 1, max(nrow - 1, 0)),
+                            replace=False)) if pr > 1 else np.array([], dtype=int)
+    cc = np.sort(rng.choice(np.arange(1, max(ncol, 2)), size=min(pc - 1, max(ncol - 1, 0)),
+                            replace=False)) if pc > 1 else np.array([], dtype=int)
+    rs = [0] + [int(x) for x in rc] + [nrow]
+    cs = [0] + [int(x) for x in cc] + [ncol]
+    blocks = [(rs[i], rs[i + 1] - rs[i], cs[j], cs[j + 1] - cs[j])
+              for i in range(len(rs) - 1) for j in range(len(cs) - 1)]
+    order = rng.permutation(world)
+    slot = int(np.where(order == rank)[0][0])
+    return blocks[slot] if slot < len(blocks) else (0, 0, 0, 0)
+
+
 def _layout(kind, nrow, ncol, world, rank):
     """This rank's (srow, nrow, scol, ncol) of an nrow x ncol matrix."""
+    if isinstance(kind, int):                  # a seed: irregular blocks
+        return _random_layout(kind, nrow, ncol, world, rank)
     if kind == "cols":                         # examples/example_AB.c:85-98
         s, z = _split(ncol, world, rank)
         return (0, nrow, s, z)
@@ -253,6 +274,29 @@ CASES = {
 @pytest.mark.parametrize("world", sorted(CASES))
 def test_dist_engine_on_gloo_ranks(world):
     _run(world, CASES[world])
+
+
+def _random_cases(world, seed, count):
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(count):
+        btb = bool(rng.integers(0, 4) == 0)
+        m, n, k = (int(x) for x in rng.integers(5, 160, 3))
+        if btb:
+            m = n
+            k = int(rng.integers(50, 900))
+        out.append((m, n, k, 0 if btb else int(rng.integers(0, 2)),
+                    0 if btb else int(rng.integers(0, 2)), None, 1000 * seed + i,
+                    int(rng.integers(0, 2)), int(rng.integers(5, 9)), btb, 500 + 7 * i + seed))
+    return out
+
+
+@pytest.mark.parametrize("world,seed", [(3, 1), (5, 2), (7, 3)])
+def test_dist_engine_irregular_layouts(world, seed):
+    """Random shapes, grids chosen by the planner and irregular source and
+    destination blocks (random cuts dealt to a random permutation of ranks,
+    some ranks owning nothing)."""
+    _run(world, _random_cases(world, seed, 6))
 
 
 def _bad_worker(rank, world, port, q):
