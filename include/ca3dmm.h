@@ -33,7 +33,8 @@
 #include "dev_type.h"
 
 /* GEMM modes (CA3DMM_GEMM_MODE env var or ca3dmm_engine_set_gemm_mode) */
-#define CA3DMM_GEMM_PLAIN 0   /* FP64 DMMA tensor-core GEMM */
+#define CA3DMM_GEMM_PLAIN 0   /* FP64 DMMA tensor-core GEMM (env CA3DMM_PLAIN_MERGE_SLABS=0 at
+                                 init keeps the kp-slab sum order instead of one GEMM over k) */
 #define CA3DMM_GEMM_OZAKI 1   /* split precision: INT8 slices on tcgen05, FP64 recombination */
 
 struct ca3dmm_engine {
