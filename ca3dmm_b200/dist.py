@@ -410,6 +410,12 @@ class DistCa3dmmEngine:
             self.stats[key] = 0 if key == "n_exec" else 0.0
 
     def free(self):
-        if self.local is not None:
+        if getattr(self, "local", None) is not None:
             self.local.free()
             self.local = None
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
