@@ -410,9 +410,10 @@ class DistCa3dmmEngine:
             self.stats[key] = 0 if key == "n_exec" else 0.0
 
     def free(self):
-        if getattr(self, "local", None) is not None:
-            self.local.free()
-            self.local = None
+        local = getattr(self, "local", None)
+        if local is not None and hasattr(local, "free"):
+            local.free()
+        self.local = None
 
     def __del__(self):
         try:
