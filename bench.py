@@ -301,7 +301,7 @@ def reference_arm(args, world, rank):
             "data": "synthetic",
             "config": {"workload": square_desc(n, args.trans_a, args.trans_b, args.p, grid,
                                                args.dist),
-                       "l2": "inputs larger than L2 (512 MB per operand at 8000^3)"},
+                       "l2": square_l2(n)},
             "cpu_baseline": base,
             "e2e": {"value": v, "unit": "TFLOP/s", "h2d_bytes_per_step": 0,
                     "d2h_bytes_per_step": 0},
@@ -407,6 +407,13 @@ def square_desc(n, ta, tb, p=P, grid=GRID, dist="signed_exp"):
             % (n, ta, tb, p, grid_str(grid), cub, ent))
 
 
+def square_l2(n):
+    """The L2 note of the square workload, the same in both arms' JSON lines."""
+    mb = n * n * 8 / 1e6
+    return ("inputs larger than L2 (%.0f MB per operand), no flush" % mb if n * n * 8 > 126e6
+            else "inputs of %.1f MB per operand (smaller than L2), no flush" % mb)
+
+
 def workload(args):
     if args.workload == "btb":
         rows = args.btb_rows
@@ -426,7 +433,7 @@ def workload(args):
             "p": args.p, "grid": grid,
             "A": A, "B": B, "label": "square %d^3 grid %s" % (n, grid_str(grid)),
             "desc": square_desc(n, args.trans_a, args.trans_b, args.p, grid, args.dist),
-            "l2": "inputs larger than L2 (512 MB per operand), no flush"}
+            "l2": square_l2(n)}
 
 
 def sampled_error(Cdev, wl, nsample=2048):
@@ -757,15 +764,23 @@ def main():
                 "traffic": traffic.get("dgemm_dmma_grouped")}
     roof["frac"] = roof["achieved"] / roof["peak"]
     in_bytes = (0 if dA is None else dA.numel() * 8) + dB.numel() * 8
+    # the metric's comparison, split precision against plain FP64 at their
+    # errors against the double-double truth, as top-level keys
+    eo, ep = legs["ozaki"]["err"], legs["plain"]["err"]
+    plain_tf = flops / (legs["plain"]["ms_per_step"] * 1e-3) / 1e12
+    split_tf = flops / (legs["ozaki"]["ms_per_step"] * 1e-3) / 1e12
     out = {
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
-        "config": {"workload": wl["desc"], "gemm": head,
-                   "ozaki_slices": eng.s.ozaki_slices if head == "ozaki" else None,
-                   "l2": wl["l2"]},
-        "legs": legs, "roofline": roof, "clocks": clocks,
+        "config": {"workload": wl["desc"], "l2": wl["l2"]},
+        "gemm": head, "ozaki_slices": eng_oz.s.ozaki_slices,
+        "plain_tflops": plain_tf, "split_tflops": split_tf,
+        "split_over_plain": split_tf / plain_tf,
+        "err_normwise_split": eo["normwise"], "err_normwise_plain": ep["normwise"],
+        "err_vs_absprod_split": eo["vs_absprod"], "err_vs_absprod_plain": ep["vs_absprod"],
+        "roofline": roof, "clocks": clocks,
         "e2e": {"value": whole_job_tflops(flops, world, e2e_ms), "unit": "TFLOP/s",
                 "h2d_bytes_per_step": in_bytes, "d2h_bytes_per_step": m * n * 8},
         "gpu_launches": int(launches),
@@ -775,6 +790,7 @@ def main():
             cpu_baseline(wl["A"], wl["B"], ta, n, tb=wl["tb"], p=wl["p"], grid=wl["grid"])
     if rank == 0 and world == 1 and args.ref_gpu:
         out["reference_gpu"] = ref_gpu_leg(args)
+    out["legs"] = legs                    # detail last (slice sweep, phase times)
     if rank == 0:
         print(json.dumps(out), flush=True)
     if world > 1:

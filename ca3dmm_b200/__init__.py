@@ -123,6 +123,7 @@ def lib():
         "dev_type_malloc": (p, [sz, i]),
         "dev_type_free": (None, [p, i]),
         "dev_type_memcpy": (None, [p, p, sz, i, i]),
+        "dev_type_copy_mat_blk": (None, [sz, i, i, p, i, p, i, i]),
         "ca3dmm_dgemm_kslab_noalloc": (i, [i, i, i, i, p, i, p, i, p, i, p]),
         "ca3dmm_dgemm_kslab_noalloc_scratch_bytes": (sz, []),
         "ca3dmm_grouped_init": (i, [i, pi, pi, pi, pi, pi, i, i, C.POINTER(p), C.POINTER(sz)]),

@@ -99,6 +99,11 @@ int ca3dmm_pack_launch(const double *src_base, double *dst_base,
                        const ca3dmm_pack_desc_t *dev_descs, int ndesc, int total_tiles,
                        cudaStream_t stream);
 
+/* One column-major block copy dst[r + c*ldd] = src[r + c*lds] (rows x cols),
+ * stream-ordered, the geometry passed as kernel arguments. */
+int ca3dmm_copy_block_launch(const double *src, long long lds, double *dst, long long ldd,
+                             int rows, int cols, cudaStream_t stream);
+
 /* ---- kp-slab reduction ---------------------------------------------------
  * out[i + j*ldo] = sum_{s=0}^{nslab-1} slab[s*slab_stride + i + j*lds]
  * (summed in slab order 0,1,...). */

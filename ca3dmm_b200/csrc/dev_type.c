@@ -56,18 +56,9 @@ void dev_type_copy_mat_blk(size_t dt_size, const int nrow, const int ncol, const
             ERROR_PRINTF("dev_type_copy_mat_blk failed\n");
         return;
     }
-    ca3dmm_pack_desc_t d;
-    memset(&d, 0, sizeof(d));
-    d.lds = lds; d.ldd = ldd; d.rows = ncol; d.cols = nrow; d.trans = 0;
-    int tiles = ca3dmm_pack_tiles(&d, 1);
-    ca3dmm_pack_desc_t *dd = NULL;
-    if (cudaMalloc((void **) &dd, sizeof(d)) != cudaSuccess) {
-        ERROR_PRINTF("dev_type_copy_mat_blk: descriptor allocation failed\n");
-        return;
-    }
-    cudaMemcpy(dd, &d, sizeof(d), cudaMemcpyHostToDevice);
-    if (ca3dmm_pack_launch((const double *) src, (double *) dst, dd, 1, tiles, 0))
-        ERROR_PRINTF("dev_type_copy_mat_blk: pack launch failed\n");
-    cudaDeviceSynchronize();
-    cudaFree(dd);
+    /* the reference launches its copy kernel on the default stream and
+     * returns (src/cuda_proxy.cu:141-149); likewise here, with the block
+     * geometry passed by value so that nothing is allocated or synchronised */
+    if (ca3dmm_copy_block_launch((const double *) src, lds, (double *) dst, ldd, ncol, nrow, 0))
+        ERROR_PRINTF("dev_type_copy_mat_blk: copy launch failed\n");
 }

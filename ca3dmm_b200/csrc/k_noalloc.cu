@@ -3,11 +3,10 @@
 // Some callers cannot call cudaMalloc: code hosted inside a process whose
 // device memory is owned by another allocator (a serving framework's pool, a
 // memory-capped MPS client) and may not take memory behind that allocator's
-// back, and latency-critical paths where cudaMalloc / cudaFree would
-// synchronise the whole device.  ca3dmm_dgemm_kslab_noalloc serves them: the
-// caller passes A, B and C, and the partial k-slab results, the tensor maps
-// and the status word live in one fixed, file-scope device array instead of
-// an engine work buffer.
+// back, or code that must not let an allocation fail half-way through a job.
+// ca3dmm_dgemm_kslab_noalloc serves them: the caller passes A, B and C, and
+// the partial k-slab results, the tensor maps and the status word live in one
+// fixed, file-scope device array instead of an engine work buffer.
 //
 // The array is part of the library image, so every GPU that loads the library
 // holds CA3DMM_NOALLOC_SCRATCH_BYTES of it until the process exits.  All
@@ -15,12 +14,12 @@
 // host threads without ordering) race on it.  It keeps whatever the last call
 // left there; this entry point clears the one part that must start at zero
 // (the status word) itself, and every partial slab it reads back is fully
-// rewritten by the GEMM first.
+// rewritten by the GEMM first.  The call is synchronous: it copies its plan
+// from host memory and waits for the stream before returning the status.
 #include <cuda.h>
 #include <cuda_runtime.h>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 #include "k_common.cuh"
 #include "ca3dmm_kernels.h"
 
@@ -31,29 +30,21 @@ static __device__ __align__(256) unsigned char g_kslab_scratch[CA3DMM_NOALLOC_SC
 
 namespace {
 
-// Device address of g_kslab_scratch per device.  In host code the array's
-// name is only a host-side stand-in, so the address comes from
-// cudaGetSymbolAddress, taken once per device with that device current.
-void *g_scratch_addr[64];
-std::mutex g_scratch_mu;
-
+// Device address of g_kslab_scratch on the current device.  In host code the
+// array's name is only a host-side stand-in, so the address comes from
+// cudaGetSymbolAddress with that device current.  It is looked up on every
+// call (the lookup allocates nothing): a cached address would go stale after
+// a cudaDeviceReset or under another context.
 int scratch_address(void **out)
 {
-    int dev = -1;
-    CA3DMM_CUDA_TRY(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= 64) return CA3DMM_ENODEV;
-    std::lock_guard<std::mutex> lock(g_scratch_mu);
-    if (g_scratch_addr[dev] == nullptr) {
-        void *p = nullptr;
-        cudaError_t err = cudaGetSymbolAddress(&p, g_kslab_scratch);
-        if (err != cudaSuccess || p == nullptr) {
-            fprintf(stderr, "[ERROR] %s, %d: cudaGetSymbolAddress(g_kslab_scratch) failed: %s\n",
-                    __FILE__, __LINE__, cudaGetErrorString(err));
-            return CA3DMM_ECUDA;
-        }
-        g_scratch_addr[dev] = p;
+    void *p = nullptr;
+    cudaError_t err = cudaGetSymbolAddress(&p, g_kslab_scratch);
+    if (err != cudaSuccess || p == nullptr) {
+        fprintf(stderr, "[ERROR] %s, %d: cudaGetSymbolAddress(g_kslab_scratch) failed: %s\n",
+                __FILE__, __LINE__, cudaGetErrorString(err));
+        return CA3DMM_ECUDA;
     }
-    *out = g_scratch_addr[dev];
+    *out = p;
     return CA3DMM_OK;
 }
 
@@ -70,9 +61,9 @@ extern "C" size_t ca3dmm_dgemm_kslab_noalloc_scratch_bytes(void)
 // planes of the CA3DMM grid: slab s multiplies A[:, ks] by B[ks, :] (ks the
 // balanced split of k) with the FP64 DMMA kernel into a partial C held in the
 // fixed scratch array, then the partials are summed in slab order into C.
-// The first call on a device looks up the scratch address (no allocation);
-// make that first call before any stream capture begins.
-// Synchronous on `stream`; returns 0 or a CA3DMM_E* code.
+// Every call looks up the scratch address (no allocation).  Synchronous on
+// `stream` (it waits for the stream), so it must not be called while the
+// stream is being captured; returns 0 or a CA3DMM_E* code.
 extern "C" int ca3dmm_dgemm_kslab_noalloc(int m, int n, int k, int kp, const double *A, int ldA,
                                           const double *B, int ldB, double *C, int ldC,
                                           void *stream)

@@ -229,6 +229,38 @@ extern "C" int ca3dmm_pack_tiles(ca3dmm_pack_desc_t *descs, int ndesc)
     return tiles;
 }
 
+// One block copy with its geometry passed by value (no descriptor in device
+// memory): thread (row, 16 columns) of a 128 x 16 tile, the grid's y extent
+// walking further column tiles when there are more than 65535 of them.
+__global__ void __launch_bounds__(128)
+copy_block_kernel(const double *__restrict__ src, long long lds, double *__restrict__ dst,
+                  long long ldd, int rows, int cols)
+{
+    const int r = blockIdx.x * 128 + threadIdx.x;
+    if (r >= rows) return;
+    for (long long c0 = (long long) blockIdx.y * 16; c0 < cols; c0 += (long long) gridDim.y * 16) {
+        double v[16];
+#pragma unroll
+        for (int c = 0; c < 16; ++c)
+            if (c0 + c < cols) v[c] = __ldg(src + r + (c0 + c) * lds);
+#pragma unroll
+        for (int c = 0; c < 16; ++c)
+            if (c0 + c < cols) dst[r + (c0 + c) * ldd] = v[c];
+    }
+}
+
+extern "C" int ca3dmm_copy_block_launch(const double *src, long long lds, double *dst,
+                                        long long ldd, int rows, int cols, cudaStream_t stream)
+{
+    if (rows <= 0 || cols <= 0) return CA3DMM_OK;
+    const long long ty = ((long long) cols + 15) / 16;
+    dim3 grid((unsigned) ((rows + 127) / 128), (unsigned) (ty < 65535 ? ty : 65535));
+    copy_block_kernel<<<grid, 128, 0, stream>>>(src, lds, dst, ldd, rows, cols);
+    CA3DMM_CUDA_TRY(cudaGetLastError());
+    ca3dmm_note_launch(1);
+    return CA3DMM_OK;
+}
+
 extern "C" int ca3dmm_pack_launch(const double *src_base, double *dst_base,
                                   const ca3dmm_pack_desc_t *dev_descs, int ndesc, int total_tiles,
                                   cudaStream_t stream)

@@ -205,19 +205,20 @@ int ca3dmm_engine_vrank_info(ca3dmm_engine_p engine, int vrank, int *out34);
 
 /* No counterpart in the reference.  C = A * B (column-major, device pointers,
  * no transposes) as kp k-slabs summed in slab order, for callers that may not
- * allocate device memory themselves (code living in a process whose device
- * memory belongs to another allocator, or on a latency-critical path where
- * cudaMalloc / cudaFree would synchronise the device).  Allocates nothing: the
- * partial slabs, plan and status word live in one fixed device array of
+ * allocate device memory themselves: code living in a process whose device
+ * memory belongs to another allocator (a serving framework's pool, a
+ * memory-capped MPS client), or code that must not meet an allocation failure
+ * in the middle of a job.  Allocates nothing: the partial slabs, plan and
+ * status word live in one fixed device array of
  * ca3dmm_dgemm_kslab_noalloc_scratch_bytes() bytes (32 MiB) that every GPU
  * loading the library holds until exit; a problem needing more
  * (kp > 1: ~8 * m * n * kp bytes) is rejected with CA3DMM_EINVAL.  A, B must be
  * 16-byte aligned with even ldA >= m, ldB >= k; every slab start
  * k0 = calc_block_spos_size(k, kp, s) must be even; ldC >= m; 1 <= kp <= 64.
- * The first call on a device looks up the array's device address; make that
- * first call before any stream capture begins.  Calls that overlap on the GPU
- * race on the shared array.  Synchronous on `stream`
- * (cudaStream_t, NULL = legacy default stream); returns 0 or a CA3DMM_E* code. */
+ * Calls that overlap on the GPU race on the shared array.  The call is
+ * synchronous on `stream` (cudaStream_t, NULL = legacy default stream): it
+ * waits for the stream before returning, so it must not be made while that
+ * stream is being captured.  Returns 0 or a CA3DMM_E* code. */
 int ca3dmm_dgemm_kslab_noalloc(int m, int n, int k, int kp, const double *A, int ldA,
                                const double *B, int ldB, double *C, int ldC, void *stream);
 size_t ca3dmm_dgemm_kslab_noalloc_scratch_bytes(void);

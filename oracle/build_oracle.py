@@ -18,7 +18,9 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF = os.environ.get("CA3DMM_REFERENCE_DIR", "/root/reference")
+# The reference tree: CA3DMM_REFERENCE_DIR, else a checkout named "reference" beside the repo.
+REF = os.environ.get("CA3DMM_REFERENCE_DIR",
+                     os.path.join(os.path.dirname(os.path.dirname(HERE)), "reference"))
 
 
 def _newer(t, deps):

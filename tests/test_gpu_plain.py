@@ -245,3 +245,21 @@ def test_plain_slab_merge_can_be_switched_off(cuda, monkeypatch):
         _dd_check(outs[-1], A, B, 0, 0, m, n, k, full=False)
         e.free()
     assert not np.array_equal(outs[0], outs[1])
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("nrow,ncol,lds,ldd", [(37, 300, 310, 305), (1, 1, 1, 1), (2000, 17, 20, 40)])
+def test_dev_type_copy_mat_blk(cuda, nrow, ncol, lds, ldd):
+    """dev_type_copy_mat_blk (src/dev_type.c:133-156): row-major nrow x ncol
+    block copy, stream-ordered on the default stream; bit-exact."""
+    import torch
+    rng = np.random.default_rng(nrow + ncol)
+    src = torch.from_numpy(rng.standard_normal(nrow * lds)).cuda()
+    dst = torch.full((nrow * ldd,), -7.0, dtype=torch.float64, device="cuda")
+    cb.lib().dev_type_copy_mat_blk(8, nrow, ncol, src.data_ptr(), lds, dst.data_ptr(), ldd,
+                                   cb.DEV_TYPE_CUDA)
+    torch.cuda.synchronize()
+    s = src.cpu().numpy().reshape(nrow, lds)
+    d = dst.cpu().numpy().reshape(nrow, ldd)
+    assert np.array_equal(d[:, :ncol], s[:, :ncol])
+    assert np.all(d[:, ncol:] == -7.0)

@@ -1,13 +1,15 @@
 """The allocation-free k-slab GEMM entry point (ca3dmm_dgemm_kslab_noalloc).
 
 It exists for callers that may not allocate device memory themselves -- code
-inside a process whose device memory is owned by another allocator, or on a
-latency-critical path where cudaMalloc / cudaFree would synchronise the device
--- and keeps its partial slabs in a fixed device array of the library instead.
-This file is collected last on purpose.  It checks, through the C ABI, that
-two calls in a row give what the existing engine entry point
-(ca3dmm_engine_exec on a 1 x 1 x kp grid) gives, within the tolerance the
-other GPU tests use, and that oversized problems are refused.
+inside a process whose device memory is owned by another allocator (a serving
+framework's pool, a memory-capped MPS client), or code that must not meet an
+allocation failure half-way through a job -- and keeps its partial slabs in a
+fixed device array of the library instead.  This file is collected last on
+purpose.  It checks, through the C ABI, that two calls in a row agree with
+the double-double truth within k u |A||B| (the tolerance the other GPU tests
+use) and with the existing engine entry point (ca3dmm_engine_exec on a
+1 x 1 x kp grid), and that oversized problems and slab starts the TMA cannot
+reach are refused.
 """
 import numpy as np
 import pytest
@@ -38,7 +40,8 @@ def test_noalloc_matches_engine_two_calls(cuda, m, n, k, kp):
     A = orc.gen_signed_exp(41, m, k)
     B = orc.gen_signed_exp(42, k, n)
     want = _engine_result(A, B, m, n, k, kp)
-    _, _, ab = orc.dd_gemm(A, B, 0, 0, m, n, k)
+    hi, lo, ab = orc.dd_gemm(A, B, 0, 0, m, n, k)
+    assert np.max(np.abs((want - hi) - lo) / ab) <= k * U
     dA, lda = to_dev(A, pad_ld=m + (m % 2))
     dB, ldb = to_dev(B, pad_ld=k + (k % 2))
     for call in range(2):
@@ -47,7 +50,9 @@ def test_noalloc_matches_engine_two_calls(cuda, m, n, k, kp):
                                           dC.data_ptr(), m, None)
         assert rc == 0, (call, rc)
         got = from_dev(dC, m, n)
-        assert np.max(np.abs(got - want) / ab) <= k * U, call
+        # against the double-double truth hi + lo, and against the engine
+        assert np.max(np.abs((got - hi) - lo) / ab) <= k * U, call
+        assert np.max(np.abs(got - want) / ab) <= 2 * k * U, call
 
 
 def test_noalloc_rejects_oversized_and_misaligned(cuda):
@@ -63,3 +68,17 @@ def test_noalloc_rejects_oversized_and_misaligned(cuda):
     # odd leading dimension of B violates the TMA rule: refused, nothing runs
     assert L.ca3dmm_dgemm_kslab_noalloc(64, 64, 63, 1, dA.data_ptr(), 64, dB.data_ptr(), 63,
                                         dC.data_ptr(), 64, None) == 1
+
+
+def test_noalloc_rejects_odd_slab_start(cuda):
+    """k = 6 on kp = 2 slabs puts slab 1 at k0 = 3: the TMA base B + 3 is not
+    16-byte aligned, so the call is refused before anything runs."""
+    L = cb.lib()
+    dA = dev_zeros(64 * 8)            # room for k = 8 (the second call)
+    dB = dev_zeros(8 * 64)
+    dC = dev_zeros(64 * 64)
+    assert L.ca3dmm_dgemm_kslab_noalloc(64, 64, 6, 2, dA.data_ptr(), 64, dB.data_ptr(), 6,
+                                        dC.data_ptr(), 64, None) == 1
+    # k = 8 on the same two slabs (k0 = 4) runs
+    assert L.ca3dmm_dgemm_kslab_noalloc(64, 64, 8, 2, dA.data_ptr(), 64, dB.data_ptr(), 8,
+                                        dC.data_ptr(), 64, None) == 0
