@@ -990,9 +990,10 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
     }
     if (timing) cudaEventRecord(pl->ev[1], st);
     int *status_d = (int *) (w + pl->off_status);
-    if (e->gemm_mode == CA3DMM_GEMM_OZAKI)
+    if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
         rc = ca3dmm_oz_run_gemm(&pl->oz, status_d, 5.0, st);
-    else
+        if (!rc) rc = ca3dmm_oz_run_nonfinite(&pl->oz, NULL, src_A, src_B, st);
+    } else
         rc = ca3dmm_dgemm_launch(w + pl->off_gemm, pl->ngroup * pl->ksplit, pl->gemm_tiles,
                                  pl->a_kmajor, status_d, 5.0, st);
     if (rc) return rc;
@@ -1325,6 +1326,7 @@ static int hx_btb_slabs(ca3dmm_engine_p e, struct host_exec *x, const void *B_h,
             const void *dd = (const char *) x->desc_d + (size_t) j * x->desc_stride;
             rc = ca3dmm_oz_slice_descs(&pl->oz, x->dB, dd, 1, x->ntile[j], st);
             if (!rc) rc = ca3dmm_oz_run_gemm_ranges(&pl->oz, &rg, status_d, 5.0, st);
+            if (!rc) rc = ca3dmm_oz_run_nonfinite(&pl->oz, &rg, x->dB, x->dB, st);
         } else {
             rc = ca3dmm_dgemm_launch_ranges(w + pl->off_gemm, pl->ngroup * pl->ksplit, &rg,
                                             pl->a_kmajor, status_d, 5.0, st);
@@ -1432,6 +1434,7 @@ static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_
         if (ozaki) {
             rc = ca3dmm_oz_slice_descs(&pl->oz, x->dA, dd, x->ndesc, x->ntile[c], st);
             if (!rc) rc = ca3dmm_oz_run_gemm_ranges(&pl->oz, &x->rng[c], status_d, 5.0, st);
+            if (!rc) rc = ca3dmm_oz_run_nonfinite(&pl->oz, &x->rng[c], x->dA, x->dB, st);
         } else {
             rc = ca3dmm_pack_launch(x->dA, (double *) w, (const ca3dmm_pack_desc_t *) dd, x->ndesc,
                                     x->ntile[c][0], st);

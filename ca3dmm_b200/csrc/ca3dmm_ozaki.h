@@ -5,10 +5,12 @@
  *   rint(a_il 2^(8s-1-E_i)) = sum_{t<s} qa_t,il 256^(s-1-t), balanced digits
  *   qa_t in [-128, 127], so a_il = sum_t qa_t,il 2^(E_i-7-8t) + r, |r| <= 2^(E_i-8s),
  * likewise F_j for the columns of op(B).  Then
- *   C_ij ~= sum_{d=s-1..0} 2^(E_i + F_j - 14 - 8d) * sum_{t+u=d} (qa_t qb_u)_ij
+ *   C_ij ~= 2^(E_i + F_j) sum_{d=s-1..0} 2^(-14 - 8d) sum_{t+u=d} (qa_t qb_u)_ij
  * where every inner sum is an exact INT32 tensor-core accumulation over k
  * chunks with s kc 2^14 < 2^31, and only the recombination over d (most
- * significant product last) and over chunks is done in FP64. */
+ * significant product last) and over chunks is done in FP64; the power of two
+ * 2^(E_i + F_j) is applied once, at the store.  Rows and columns holding an
+ * Inf or a NaN are sliced as zero rows (ca3dmm_oz_run_nonfinite). */
 #ifndef CA3DMM_OZAKI_H
 #define CA3DMM_OZAKI_H
 
@@ -104,6 +106,15 @@ int ca3dmm_oz_encode_blocks(const void *host_plan, int ngroup, const int *descs,
                             void *out_descs, int ntiles[3]);
 int ca3dmm_oz_slice_descs(const ca3dmm_oz_plan_t *oz, const void *src, const void *dev_descs,
                           int ndesc, const int ntiles[3], cudaStream_t stream);
+/* Non-finite inputs: rows of op(A) and columns of op(B) holding an Inf or a
+ * NaN are sliced as zero rows; this pass then writes the IEEE value (NaN,
+ * +Inf or -Inf, independent of the summation order) of every C entry in those
+ * rows and columns, over the tiles of `ranges` (NULL: every tile).  Run it
+ * after the GEMM over the same tiles and before any slab reduction, with the
+ * operand pointers given to the slicing.  It returns at once on the device
+ * when no row or column was flagged. */
+int ca3dmm_oz_run_nonfinite(const ca3dmm_oz_plan_t *oz, const ca3dmm_tile_ranges_t *ranges,
+                            const void *A, const void *B, cudaStream_t stream);
 /* The GEMM over the tiles of `ranges` only (ca3dmm_kernels.h). */
 int ca3dmm_oz_run_gemm_ranges(const ca3dmm_oz_plan_t *oz, const ca3dmm_tile_ranges_t *ranges,
                               int *dev_status, double timeout_s, cudaStream_t stream);

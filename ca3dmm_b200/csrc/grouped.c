@@ -343,6 +343,8 @@ int ca3dmm_grouped_exec(ca3dmm_grouped_p g, const double *const *A, const int *l
         if (rc) return rc;
         rc = ca3dmm_oz_run_gemm(&g->oz, status, 5.0, st);
         if (rc) return rc;
+        rc = ca3dmm_oz_run_nonfinite(&g->oz, NULL, NULL, NULL, st);
+        if (rc) return rc;
     }
     if (timing) cudaEventRecord(g->ev[1], st);
     if (g->sync) {

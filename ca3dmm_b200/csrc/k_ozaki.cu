@@ -23,9 +23,11 @@
 //                         per stage -- and feeds all s(s+1)/2 slice products.
 //                         The k range is processed in chunks short enough for the
 //                         INT32 sums to stay exact (s kc 2^14 < 2^31); after each
-//                         chunk the epilogue adds 2^(E_i+F_j-14-8d) D_d, d = s-1
-//                         down to 0, into FP64 registers, and stores C after the
-//                         last chunk.
+//                         chunk the epilogue adds 2^(-14-8d) D_d, d = s-1 down
+//                         to 0, into FP64 registers, and stores 2^(E_i+F_j) times
+//                         that sum after the last chunk.
+//  4. oz_nonfinite_kernel -- rows / columns holding an Inf or a NaN were sliced as
+//                         zero rows; writes the IEEE value of their C entries.
 // Warp roles of the GEMM: warp 0 copy producer, warps 1, 6, 7 MMA issuers, each
 // owning a set of A slices (warp 1 also owns the TMEM allocation), warps 2..5
 // and 8..11 epilogue (warp w reads TMEM lanes 32*(w%4)..+31, columns 0-31 of
@@ -68,6 +70,8 @@ constexpr int B_SLICE_BYTES = OBN * OKB;        // 2 KiB
 constexpr int SMEM_BUDGET = 200 * 1024;
 constexpr int GROUP_M = 8;
 constexpr int EXP_BIAS = 2048;                   // stored exponent = E + bias, 0 = all-zero row
+// |x| bit patterns at or above this are Inf (equal) or NaN (above)
+constexpr unsigned long long INF_BITS = 0x7ff0000000000000ull;
 
 // Slicing descriptor: block rows r in [0,rows), k index l in [0,kz);
 // element (r,l) at src[src_off + r*rs + l*ls].  Exactly one of rs, ls is 1
@@ -94,6 +98,8 @@ struct OzGroup {
     int a_tmap;                 // a_from_b: the group's 5D tensor map gathers a whole A stage
     long long ea_off, eb_off;   // exponent offsets (ints) of the A rows / B columns
     long long qa_off, qb_off;   // byte offsets of the tiled slices
+    int a_desc, b_desc;         // slicing descriptors of the operand blocks (A: a B block when aliased)
+    int row0, col0;             // first row / column of the group inside those blocks
 };
 
 // A work unit is a chain of nsub groups (group, group + sub_stride, ...) that
@@ -185,7 +191,8 @@ __device__ __forceinline__ const double *slice_src(const double *base, long long
 }
 
 // Work region: [E + EXP_BIAS per row, int][max |x| per row as its IEEE bit
-// pattern, u64][tiled slices].  Both prefix arrays are cleared before a run.
+// pattern, u64; then one u64 set when any row holds an Inf or a NaN][tiled
+// slices].  Both prefix arrays are cleared before a run.
 __host__ __device__ inline size_t exp_bytes(long long n_exp)
 {
     return ((size_t) n_exp * sizeof(int) + 255) / 256 * 256;
@@ -207,7 +214,8 @@ __device__ __forceinline__ unsigned long long abs_bits(double x)
 // exponent max_l E(x_l) is E(max_l |x_l|), formed once per row in pass 2.
 __global__ void __launch_bounds__(256)
 oz_exp_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ descs, int ndesc,
-              int total_items, unsigned long long *__restrict__ mwork)
+              int total_items, unsigned long long *__restrict__ mwork,
+              unsigned long long *__restrict__ nonfinite)
 {
     __shared__ unsigned long long part[4][ST];
     __shared__ int sbeg[DESC_CACHE];
@@ -253,7 +261,10 @@ oz_exp_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ desc
                 const unsigned long long w = __shfl_xor_sync(0xffffffffu, m, o);
                 m = w > m ? w : m;
             }
-            if (lane == 0 && r < d.rows && m) atomicMax(mwork + d.e_off + r, m);
+            if (lane == 0 && r < d.rows && m) {
+                atomicMax(mwork + d.e_off + r, m);
+                if (m >= INF_BITS) *nonfinite = 1ull;
+            }
             continue;
         }
         // RC: 64 x 64 tile, thread (row r, k phase g) walks k = g, g + 4, ...
@@ -281,6 +292,7 @@ oz_exp_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ desc
 #pragma unroll
             for (int q = 1; q < 4; ++q) v = part[q][threadIdx.x] > v ? part[q][threadIdx.x] : v;
             if (v) atomicMax(mwork + d.e_off + r0 + threadIdx.x, v);
+            if (v >= INF_BITS) *nonfinite = 1ull;
         }
     }
 }
@@ -298,7 +310,11 @@ __device__ __forceinline__ void slice16(const SliceDesc &d, unsigned char *__res
                                         const unsigned long long *__restrict__ mwork, int gr,
                                         int gl, const double (&x)[16])
 {
-    const unsigned long long mb = gr < d.rows ? mwork[d.e_off + gr] : 0ull;
+    // a row holding an Inf or a NaN is sliced as a zero row; oz_nonfinite_kernel
+    // writes the IEEE result of its C entries after the GEMM
+    const unsigned long long mr = gr < d.rows ? mwork[d.e_off + gr] : 0ull;
+    const bool fin = mr < INF_BITS;
+    const unsigned long long mb = fin ? mr : 0ull;
     int E = 0;
     if (mb) {
         int ex;
@@ -313,7 +329,7 @@ __device__ __forceinline__ void slice16(const SliceDesc &d, unsigned char *__res
     uint32_t lo[16], hi[16];
 #pragma unroll
     for (int j = 0; j < 16; ++j) {
-        const long long N = __double2ll_rn(x[j] * up1 * up2);
+        const long long N = __double2ll_rn((fin ? x[j] : 0.0) * up1 * up2);
         const unsigned long long U = (unsigned long long) N + BIAS;
         lo[j] = (uint32_t) U;
         hi[j] = (uint32_t) (U >> 32);
@@ -555,6 +571,15 @@ __device__ __forceinline__ double pow2(int e)
     return ldexp(1.0, e);
 }
 
+// x 2^e with one rounding (exact unless the result leaves the normal range):
+// a multiplication by the exact power of two where 2^e is a normal double,
+// ldexp beyond that.
+__device__ __forceinline__ double scale2(double x, int e)
+{
+    if (e >= -1022 && e <= 1023) return x * __longlong_as_double((long long) (e + 1023) << 52);
+    return ldexp(x, e);
+}
+
 // The unit holding tile `tile`.  sb: a shared-memory copy of the units' first
 // tiles (nullptr when there are more than UNIT_CACHE units), so that a batch of
 // small GEMMs does not pay a chain of dependent global loads per tile.
@@ -611,7 +636,7 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
     uint64_t *acc_empty = acc_full + 1;
     __shared__ uint32_t tmem_slot;
     __shared__ volatile int abort_flag;
-    __shared__ double col_scale_all[OTHREADS / 32][32];   // 2^F_j per epilogue warp (no cross-warp barrier)
+    __shared__ int col_exp_all[OTHREADS / 32][32];      // F_j per epilogue warp (no cross-warp barrier)
     __shared__ int s_ubeg[UNIT_CACHE];
     const int *ework = reinterpret_cast<const int *>(work);
     const int *ub = nunit <= UNIT_CACHE ? s_ubeg : nullptr;
@@ -788,7 +813,7 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
         const int q = warp & 3;                       // TMEM lane quarter of this warp
         const int c0 = warp >= 8 ? 32 : 0;            // its 32 columns of each accumulator
         const int row = q * 32 + lane;
-        double *col_scale = col_scale_all[warp];
+        int *col_exp = col_exp_all[warp];
         uint32_t ci = 0;
         bool ok = true;
       for (int sub = 0; sub < nsub_max && ok; ++sub)
@@ -805,12 +830,12 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
             double *const Cg = p.C;
             const int eb = gr < gm ? ework[p.ea_off + gr] : 0;
             const int Ei = eb ? eb - EXP_BIAS : 0;
-            // column scales 2^F_j of this tile into this warp's shared slots
+            // column exponents F_j of this tile into this warp's shared slots
             __syncwarp();
             {
                 const int gc = tn * OBN + c0 + lane;
                 const int fb = gc < gn ? ework[p.eb_off + gc] : 0;
-                col_scale[lane] = pow2(fb ? fb - EXP_BIAS : 0);
+                col_exp[lane] = fb ? fb - EXP_BIAS : 0;
             }
             __syncwarp();
             double acc[32];
@@ -826,12 +851,12 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
                 tc_fence_after();
                 if (p.nkb > 0) {
                     for (int d = slices - 1; d >= 0; --d) {
-                        // acc_j += D_d 2^(E_i - 14 - 8d), the term exact (|D_d| < 2^31,
-                        // power-of-two scale), one rounding per addition; the column
-                        // factor 2^F_j is applied at the store.  Scaling a rounded
-                        // sum by a power of two is exact, so in the normal range this
-                        // equals the oracle's sum of ldexp(D_d, E_i + F_j - 14 - 8d).
-                        const double rs = pow2(Ei - 14 - 8 * d);
+                        // acc_j += D_d 2^(-14 - 8d), the term exact (|D_d| < 2^31,
+                        // power-of-two scale), one rounding per addition; the factor
+                        // 2^(E_i + F_j) is applied once at the store (one rounding,
+                        // only where the result leaves the normal range), as the
+                        // oracle's ldexp(sum_d ldexp(D_d, -14 - 8d), E_i + F_j).
+                        const double rs = pow2(-14 - 8 * d);
                         uint32_t v[32];
                         const uint32_t ta = tmem_base + ((uint32_t) (q * 32) << 16) +
                                             (uint32_t) (d * OBN + c0);
@@ -855,7 +880,7 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
                 if (sub == 0) {
 #pragma unroll
                     for (int j = 0; j < 32; ++j)
-                        if (j < nj) crow[(long long) j * ldc] = acc[j] * col_scale[j];
+                        if (j < nj) crow[(long long) j * ldc] = scale2(acc[j], Ei + col_exp[j]);
                 } else {
 #pragma unroll
                     for (int j0 = 0; j0 < 32; j0 += 8) {
@@ -866,7 +891,8 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
 #pragma unroll
                         for (int j = 0; j < 8; ++j)
                             if (j0 + j < nj)
-                                crow[(long long) (j0 + j) * ldc] = c[j] + acc[j0 + j] * col_scale[j0 + j];
+                                crow[(long long) (j0 + j) * ldc] =
+                                    c[j] + scale2(acc[j0 + j], Ei + col_exp[j0 + j]);
                     }
                 }
             }
@@ -880,6 +906,89 @@ oz_gemm_kernel(const OzGroup *__restrict__ groups, const OzUnit *__restrict__ un
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
                      "r"(tmem_cols)
                      : "memory");
+    }
+}
+
+// ------------------------------------------------------------------ non-finite inputs
+// A row of op(A) or a column of op(B) that holds an Inf or a NaN was sliced
+// as a zero row, so the GEMM wrote the finite entries of C exactly as without
+// it.  Every C entry in such a row or column is non-finite under IEEE
+// arithmetic -- each of its products with a non-finite factor is an Inf or a
+// NaN -- and which one does not depend on the summation order: NaN when some
+// product is NaN (a NaN factor, or Inf times 0) or products of both infinite
+// signs occur, else the infinity of the products' sign.  This pass writes that
+// value over the tiles of a launch, after the GEMM over the same tiles and
+// before any slab sum (which then carries it through IEEE additions).  It
+// returns at once when the exponent passes flagged nothing.
+constexpr int NF_THREADS = 256;
+
+__device__ __forceinline__ int product_class(double a, double b)
+{
+    if (isnan(a) || isnan(b)) return 1;
+    if (isinf(a) || isinf(b)) {
+        if (a == 0.0 || b == 0.0) return 1;
+        return signbit(a) != signbit(b) ? 4 : 2;
+    }
+    return 0;
+}
+
+__global__ void __launch_bounds__(NF_THREADS)
+oz_nonfinite_kernel(const double *__restrict__ srcA, const double *__restrict__ srcB,
+                    const SliceDesc *__restrict__ descs, int nA, const OzGroup *__restrict__ groups,
+                    const OzUnit *__restrict__ units, int nunit, const ca3dmm_tile_ranges_t rg,
+                    int total_tiles, const unsigned long long *__restrict__ mwork,
+                    const unsigned long long *__restrict__ nonfinite)
+{
+    if (*nonfinite == 0ull) return;
+    __shared__ unsigned char row_bad[OBM], col_bad[OBN];
+    for (int v = blockIdx.x; v < total_tiles; v += gridDim.x) {
+        const int tile = range_tile(rg, v);
+        const OzUnit &U = units[find_unit(nullptr, units, nunit, tile)];
+        int tm, tn;
+        unit_tile(U, tile, tm, tn);
+        const OzGroup &g0 = groups[U.group];
+        // rows and columns of this tile flagged in any k-slab of the unit
+        __syncthreads();                              // the previous tile's flags are read
+        if (threadIdx.x < OBM + OBN) {
+            const bool isrow = threadIdx.x < OBM;
+            const int idx = isrow ? tm * OBM + threadIdx.x : tn * OBN + threadIdx.x - OBM;
+            bool bad = false;
+            if (idx < (isrow ? g0.m : g0.n))
+                for (int sub = 0; sub < U.nsub; ++sub) {
+                    const OzGroup &g = groups[U.group + sub * U.sub_stride];
+                    bad = bad || mwork[(isrow ? g.ea_off : g.eb_off) + idx] >= INF_BITS;
+                }
+            (isrow ? row_bad[threadIdx.x] : col_bad[threadIdx.x - OBM]) = bad ? 1 : 0;
+        }
+        const int any = __syncthreads_or(threadIdx.x < OBM + OBN &&
+                                         (threadIdx.x < OBM ? row_bad[threadIdx.x]
+                                                            : col_bad[threadIdx.x - OBM]));
+        if (!any) continue;
+        for (int e = threadIdx.x; e < OBM * OBN; e += blockDim.x) {
+            const int r = e % OBM, c = e / OBM;
+            const int i = tm * OBM + r, j = tn * OBN + c;
+            if (i >= g0.m || j >= g0.n || !(row_bad[r] || col_bad[c])) continue;
+            int cls = 0;
+            for (int sub = 0; sub < U.nsub && !(cls & 1); ++sub) {
+                const OzGroup &g = groups[U.group + sub * U.sub_stride];
+                const unsigned long long ma = mwork[g.ea_off + i], mb = mwork[g.eb_off + j];
+                if (ma < INF_BITS && mb < INF_BITS) continue;      // all products finite
+                if (ma > INF_BITS || mb > INF_BITS) { cls |= 1; break; }   // a NaN factor
+                const SliceDesc &da = descs[g.a_desc], &db = descs[g.b_desc];
+                const double *pa = slice_src(g.a_desc < nA ? srcA : srcB, da.src_off) +
+                                   (long long) (g.row0 + i) * da.rs;
+                const double *pb = slice_src(srcB, db.src_off) + (long long) (g.col0 + j) * db.rs;
+                for (int l = 0; l < g.k; ++l)
+                    cls |= product_class(__ldg(pa + (long long) l * da.ls),
+                                         __ldg(pb + (long long) l * db.ls));
+            }
+            double out;
+            if ((cls & 1) || (cls & 6) == 6) out = __longlong_as_double(0x7ff8000000000000ll);
+            else if (cls & 2) out = __longlong_as_double(0x7ff0000000000000ll);
+            else if (cls & 4) out = __longlong_as_double((long long) 0xfff0000000000000ull);
+            else continue;
+            g0.C[i + (long long) j * g0.ldc] = out;
+        }
     }
 }
 
@@ -953,7 +1062,7 @@ extern "C" size_t ca3dmm_oz_work_bytes(int nA, const int *a_rows, const int *a_k
         q += align256((size_t) slices * rows_pad_of(b_cols[i], OBN) *
                       kpad_of(b_k[i] > 0 ? b_k[i] : 1));
     }
-    return exp_bytes((long long) e) + maxbits_bytes((long long) e) + q + 256;
+    return exp_bytes((long long) e) + maxbits_bytes((long long) e + 1) + q + 256;
 }
 
 extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
@@ -976,7 +1085,7 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
     size_t ne = 0;
     for (int i = 0; i < nA; ++i) ne += A[i].rows;
     for (int i = 0; i < nB; ++i) ne += B[i].cols;
-    size_t qoff = exp_bytes((long long) ne) + maxbits_bytes((long long) ne);
+    size_t qoff = exp_bytes((long long) ne) + maxbits_bytes((long long) ne + 1);
     // B blocks whose slices an A block reuses get 128-row padding, so that both
     // 64-row halves of every 128-row A tile exist
     for (int i = 0; i < nA; ++i)
@@ -1043,6 +1152,10 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
         // 64-row B tiles, the same bytes) and 64-column B tiles further on
         o.ea_off = da.e_off + row0;
         o.eb_off = db.e_off + col0;
+        o.a_desc = al >= 0 ? nA + al : G[g].a_blk;
+        o.b_desc = nA + G[g].b_blk;
+        o.row0 = row0;
+        o.col0 = col0;
         o.qa_off = da.q_off + (long long) (row0 / OBM) * da.nkb * slices * A_SLICE_BYTES;
         o.qb_off = db.q_off + (long long) (col0 / OBN) * db.nkb * slices * B_SLICE_BYTES;
         o.a_tmap = 0;
@@ -1103,8 +1216,8 @@ extern "C" int ca3dmm_oz_plan_encode(ca3dmm_oz_plan_t *oz, int slices, int nA,
 
 extern "C" int ca3dmm_oz_clear(const ca3dmm_oz_plan_t *oz, cudaStream_t stream)
 {
-    CA3DMM_CUDA_TRY(cudaMemsetAsync(oz->dev_work, 0, exp_bytes(oz->n_exp) + maxbits_bytes(oz->n_exp),
-                                    stream));
+    CA3DMM_CUDA_TRY(cudaMemsetAsync(oz->dev_work, 0,
+                                    exp_bytes(oz->n_exp) + maxbits_bytes(oz->n_exp + 1), stream));
     return CA3DMM_OK;
 }
 
@@ -1116,7 +1229,7 @@ static int launch_exp(const ca3dmm_oz_plan_t *oz, const void *src, const SliceDe
     unsigned long long *mwork = reinterpret_cast<unsigned long long *>(w + exp_bytes(oz->n_exp));
     const int cap = ca3dmm_device_sm_count() * 8;
     oz_exp_kernel<<<nitems < cap ? nitems : cap, 256, 0, stream>>>(
-        static_cast<const double *>(src), descs, ndesc, nitems, mwork);
+        static_cast<const double *>(src), descs, ndesc, nitems, mwork, mwork + oz->n_exp);
     CA3DMM_CUDA_TRY(cudaGetLastError());
     ca3dmm_note_launch(1);
     return CA3DMM_OK;
@@ -1302,6 +1415,35 @@ extern "C" int ca3dmm_oz_run_gemm_ranges(const ca3dmm_oz_plan_t *oz, const ca3dm
 #undef CA3DMM_GEMM_CASE
         default: return CA3DMM_EINVAL;
     }
+    CA3DMM_CUDA_TRY(cudaGetLastError());
+    ca3dmm_note_launch(1);
+    return CA3DMM_OK;
+}
+
+extern "C" int ca3dmm_oz_run_nonfinite(const ca3dmm_oz_plan_t *oz, const ca3dmm_tile_ranges_t *rg,
+                                       const void *A, const void *B, cudaStream_t stream)
+{
+    ca3dmm_tile_ranges_t all;
+    if (!rg) {
+        memset(&all, 0, sizeof(all));
+        all.n = 1;
+        all.len[0] = oz->tiles;
+        rg = &all;
+    }
+    if (rg->n < 0 || rg->n > CA3DMM_MAX_RANGES) return CA3DMM_EINVAL;
+    const int vtiles = range_total(*rg);
+    if (vtiles <= 0) return CA3DMM_OK;
+    const PlanLayout L(oz->ngroup);
+    const unsigned char *pl = static_cast<const unsigned char *>(oz->dev_plan);
+    const unsigned long long *mwork = reinterpret_cast<const unsigned long long *>(
+        static_cast<const unsigned char *>(oz->dev_work) + exp_bytes(oz->n_exp));
+    int grid = ca3dmm_device_sm_count() * 4;
+    if (grid > vtiles) grid = vtiles;
+    oz_nonfinite_kernel<<<grid, NF_THREADS, 0, stream>>>(
+        static_cast<const double *>(A), static_cast<const double *>(B),
+        reinterpret_cast<const SliceDesc *>(pl + L.sd), oz->nA,
+        reinterpret_cast<const OzGroup *>(pl + L.gr), reinterpret_cast<const OzUnit *>(pl + L.un),
+        oz->nunit, *rg, vtiles, mwork, mwork + oz->n_exp);
     CA3DMM_CUDA_TRY(cudaGetLastError());
     ca3dmm_note_launch(1);
     return CA3DMM_OK;

@@ -228,16 +228,24 @@ static int row_exponent(double mxe)
     return mxe == INT_MIN ? 0 : (int) mxe;
 }
 
+/*    A row (or column) holding an Inf or a NaN is sliced as a zero row       */
+/*    (E = 0, all digits 0); orc_nonfinite_fixup then gives its C entries     */
+/*    their IEEE value.                                                       */
 void orc_ozaki_slice_rows(const double *A, long lda, int tA, int m, int k, int s,
                           int8_t *out_q, int *out_e)
 {
     for (long i = 0; i < m; i++) {
-        int mx = INT_MIN;
-        for (long l = 0; l < k; l++) { int e = eff_exponent(opA(A, lda, tA, i, l)); if (e > mx) mx = e; }
-        int E = row_exponent(mx);
+        int mx = INT_MIN, fin = 1;
+        for (long l = 0; l < k; l++) {
+            double v = opA(A, lda, tA, i, l);
+            if (!isfinite(v)) { fin = 0; continue; }
+            int e = eff_exponent(v);
+            if (e > mx) mx = e;
+        }
+        int E = fin ? row_exponent(mx) : 0;
         out_e[i] = E;
         for (long l = 0; l < k; l++)
-            slice_one(opA(A, lda, tA, i, l), E, s, out_q + i * k + l, (long) m * k);
+            slice_one(fin ? opA(A, lda, tA, i, l) : 0.0, E, s, out_q + i * k + l, (long) m * k);
     }
 }
 
@@ -246,12 +254,17 @@ void orc_ozaki_slice_cols(const double *B, long ldb, int tB, int k, int n, int s
                           int8_t *out_q, int *out_e)
 {
     for (long j = 0; j < n; j++) {
-        int mx = INT_MIN;
-        for (long l = 0; l < k; l++) { int e = eff_exponent(opB(B, ldb, tB, l, j)); if (e > mx) mx = e; }
-        int E = row_exponent(mx);
+        int mx = INT_MIN, fin = 1;
+        for (long l = 0; l < k; l++) {
+            double v = opB(B, ldb, tB, l, j);
+            if (!isfinite(v)) { fin = 0; continue; }
+            int e = eff_exponent(v);
+            if (e > mx) mx = e;
+        }
+        int E = fin ? row_exponent(mx) : 0;
         out_e[j] = E;
         for (long l = 0; l < k; l++)
-            slice_one(opB(B, ldb, tB, l, j), E, s, out_q + j * k + l, (long) n * k);
+            slice_one(fin ? opB(B, ldb, tB, l, j) : 0.0, E, s, out_q + j * k + l, (long) n * k);
     }
 }
 
@@ -267,8 +280,8 @@ int orc_ozaki_kchunk(int s)
 /* Ozaki product from slices, for small sizes: per k chunk (orc_ozaki_kchunk),
  * diagonals d = t + u <= s - 1 as exact integer sums, recombined into one
  * running FP64 sum per entry: for each chunk in order, d = s-1 down to 0,
- * acc += 2^(E_i + F_j - 14 - 8d) * D_d (the product's order).  C is m x n
- * column-major. */
+ * acc += 2^(-14 - 8d) * D_d (the product's order); then C = 2^(E_i + F_j) acc
+ * with one rounding (ldexp).  C is m x n column-major. */
 void orc_ozaki_gemm(const int8_t *qa, const int *ea, const int8_t *qb, const int *eb,
                     int m, int n, int k, int s, double *C)
 {
@@ -288,12 +301,47 @@ void orc_ozaki_gemm(const int8_t *qa, const int *ea, const int8_t *qb, const int
                         for (long l = c0; l < c1; l++)
                             sum += (long long) a[l] * b[l];
                     }
-                    acc += ldexp((double) sum, ea[i] + eb[j] - 14 - 8 * d);
+                    acc += ldexp((double) sum, -14 - 8 * d);
                 }
                 if (k == 0) break;
             }
-            C[i + j * m] = acc;
+            C[i + j * m] = ldexp(acc, ea[i] + eb[j]);
         }
+}
+
+/* IEEE value of the C entries whose row of op(A) or column of op(B) holds an
+ * Inf or a NaN (every other entry is left as it is).  Each such entry is
+ * non-finite whatever the summation order: NaN when a product is NaN (a NaN
+ * factor, or Inf times 0) or products of both infinite signs occur, else the
+ * infinity of the products' sign.  C is m x n column-major. */
+void orc_nonfinite_fixup(const double *A, long lda, int tA, const double *B, long ldb, int tB,
+                         int m, int n, int k, double *C)
+{
+    char *rbad = (char *) calloc((size_t) (m > 0 ? m : 1), 1);
+    char *cbad = (char *) calloc((size_t) (n > 0 ? n : 1), 1);
+    for (long i = 0; i < m; i++)
+        for (long l = 0; l < k; l++) if (!isfinite(opA(A, lda, tA, i, l))) rbad[i] = 1;
+    for (long j = 0; j < n; j++)
+        for (long l = 0; l < k; l++) if (!isfinite(opB(B, ldb, tB, l, j))) cbad[j] = 1;
+    for (long j = 0; j < n; j++)
+        for (long i = 0; i < m; i++) {
+            if (!rbad[i] && !cbad[j]) continue;
+            int nan_ = 0, pinf = 0, ninf = 0;
+            for (long l = 0; l < k; l++) {
+                double a = opA(A, lda, tA, i, l), b = opB(B, ldb, tB, l, j);
+                if (isnan(a) || isnan(b)) nan_ = 1;
+                else if (isinf(a) || isinf(b)) {
+                    if (a == 0.0 || b == 0.0) nan_ = 1;
+                    else if (signbit(a) != signbit(b)) ninf = 1;
+                    else pinf = 1;
+                }
+            }
+            if (nan_ || (pinf && ninf)) C[i + j * m] = NAN;
+            else if (pinf) C[i + j * m] = INFINITY;
+            else if (ninf) C[i + j * m] = -INFINITY;
+        }
+    free(rbad);
+    free(cbad);
 }
 
 /* ---------------------------------------------------------------------- */

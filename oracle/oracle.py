@@ -42,6 +42,8 @@ def lib():
         L.orc_ozaki_slice_cols.argtypes = [dp, C.c_long, C.c_int, C.c_int, C.c_int, C.c_int, u8p,
                                            ip]
         L.orc_ozaki_gemm.argtypes = [u8p, ip, u8p, ip, C.c_int, C.c_int, C.c_int, C.c_int, dp]
+        L.orc_nonfinite_fixup.argtypes = [dp, C.c_long, C.c_int, dp, C.c_long, C.c_int, C.c_int,
+                                          C.c_int, C.c_int, dp]
         L.orc_ozaki_kchunk.argtypes = [C.c_int]
         L.orc_ozaki_kchunk.restype = C.c_int
         fp = C.POINTER(C.c_float)
@@ -203,6 +205,18 @@ def ozaki_gemm(qa, ea, qb, eb, m, n, k, s):
                          np.ascontiguousarray(qb).ctypes.data_as(u8),
                          np.ascontiguousarray(eb, dtype=np.int32).ctypes.data_as(ip),
                          m, n, k, s, _d(Cm))
+    return Cm
+
+
+def nonfinite_fixup(A, B, tA, tB, m, n, k, Cm):
+    """IEEE value of the C entries in rows of op(A) / columns of op(B) that
+    hold an Inf or a NaN (orc_nonfinite_fixup); Cm (m x n, Fortran order) is
+    updated in place and returned."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    B = np.asfortranarray(B, dtype=np.float64)
+    assert Cm.flags["F_CONTIGUOUS"] and Cm.dtype == np.float64
+    lib().orc_nonfinite_fixup(_d(A), A.shape[0], int(tA), _d(B), B.shape[0], int(tB), m, n, k,
+                              _d(Cm))
     return Cm
 
 
