@@ -20,7 +20,7 @@ LIB_PATH = os.path.join(HERE, "libca3dmm_b200.so")
 DEFAULT_COST_MODEL = os.path.join(HERE, "data", "costmodel_b200.txt")
 
 DEV_TYPE_HOST, DEV_TYPE_CUDA, DEV_TYPE_CUDA_MPI_DIRECT = 0, 1, 2
-GEMM_PLAIN, GEMM_OZAKI = 0, 1
+GEMM_PLAIN, GEMM_OZAKI, GEMM_CRT = 0, 1, 2
 # return codes of the C ABI (ca3dmm_kernels.h)
 OK, EINVAL, ECUDA, ETIMEOUT, ENOMEM, ENODEV = 0, 1, 2, 3, 4, 5
 ERRORS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "device wait timed out",
@@ -55,7 +55,8 @@ class Ca3dmmEngineS(C.Structure):
         ("n_exec", C.c_int), ("n_group", C.c_int), ("gemm_mode", C.c_int),
         ("ozaki_slices", C.c_int), ("last_error", C.c_int), ("stream", C.c_void_p),
         ("sync_exec", C.c_int), ("workbuf_bytes", C.c_size_t), ("impl", C.c_void_p),
-        ("raster", C.c_int), ("btb_symmetric", C.c_int)]
+        ("raster", C.c_int), ("btb_symmetric", C.c_int), ("crt_moduli", C.c_int),
+        ("crt_bits", C.c_int)]
 
 
 class TuneCfg(C.Structure):

@@ -25,6 +25,7 @@
 #include "ca3dmm_util.h"
 #include "ca3dmm_kernels.h"
 #include "ca3dmm_ozaki.h"
+#include "ca3dmm_crt.h"
 #include "ca3dmm.h"
 
 #define ALIGN_BYTES 256
@@ -84,6 +85,15 @@ typedef struct {
     ca3dmm_oz_group_t *og;
     ca3dmm_oz_unit_t *ou;
     int oz_fused;                 /* split mode adds its kp slabs into C itself */
+    /* modular split precision (CA3DMM_GEMM_CRT): crt_nsl k slabs of at most
+     * CA3DMM_CRT_MAX_K (B^T B: the kp slabs), each one group over all of C,
+     * summed by the slab reduction when there are several */
+    int crt_nsl;
+    ca3dmm_crt_plan_t crt;
+    ca3dmm_oz_blk_t *cb;          /* crt_nsl op(A) blocks, then crt_nsl op(B) blocks */
+    ca3dmm_oz_src_t *cs;
+    ca3dmm_crt_group_t *cg;
+    size_t off_crtplan, crt_plan_bytes, off_crt, crt_bytes;
     struct host_exec *hx;         /* state of ca3dmm_engine_exec_host (lazily created) */
 } plan_t;
 
@@ -176,6 +186,8 @@ static void plan_layout(ca3dmm_engine_p e, plan_t *pl)
     pl->off_gemm = off; off = align_up(off + pl->gemm_plan_bytes);
     pl->oz_plan_bytes = ca3dmm_oz_plan_bytes(pl->ngroup);
     pl->off_ozplan = off; off = align_up(off + pl->oz_plan_bytes);
+    pl->crt_plan_bytes = ca3dmm_crt_plan_bytes(2 * pl->crt_nsl, pl->crt_nsl);
+    pl->off_crtplan = off; off = align_up(off + pl->crt_plan_bytes);
     size_t packs = 0;
     pl->off_A = off;
     for (int i = 0; i < pl->nA; i++) {
@@ -196,7 +208,8 @@ static void plan_layout(ca3dmm_engine_p e, plan_t *pl)
     pl->slab_ld = ca3dmm_round_up(e->m, 2);
     pl->slab_stride = (size_t) pl->slab_ld * (size_t) e->n;
     pl->off_slab = off;
-    const int nslab = e->kp * pl->ksplit;    /* plain mode's sub-slabs; split mode uses kp of them */
+    int nslab = e->kp * pl->ksplit;          /* plain mode's sub-slabs; split mode uses kp of them */
+    if (pl->crt_nsl > nslab) nslab = pl->crt_nsl;
     if (nslab > 1) off = align_up(off + sizeof(double) * pl->slab_stride * (size_t) nslab);
     pl->off_cout = off;
     off = align_up(off + sizeof(double) * (size_t) e->m * (size_t) e->n);
@@ -212,6 +225,27 @@ static void plan_layout(ca3dmm_engine_p e, plan_t *pl)
             free(dims);
         }
         off = align_up(off + pl->oz_bytes);
+    }
+    pl->off_crt = off;
+    pl->crt_bytes = 0;
+    if (e->gemm_mode == CA3DMM_GEMM_CRT) {
+        const int ns = pl->crt_nsl;
+        int *d = (int *) malloc(sizeof(int) * 6 * (size_t) ns);
+        if (d) {
+            int *am = d, *ak = d + ns, *bk = d + 2 * ns, *bn = d + 3 * ns, *gm = d + 4 * ns,
+                *gn = d + 5 * ns;
+            for (int i = 0; i < ns; i++) {
+                /* an aliased op(A) block (B^T B) has no residues of its own */
+                am[i] = pl->cb[i].alias >= 0 ? 0 : pl->cb[i].rows;
+                ak[i] = pl->cb[i].cols;
+                bk[i] = pl->cb[ns + i].rows; bn[i] = pl->cb[ns + i].cols;
+                gm[i] = pl->cg[i].m; gn[i] = pl->cg[i].n;
+            }
+            pl->crt_bytes = ca3dmm_crt_work_bytes(ns, am, ak, ns, bk, bn, ns, gm, gn,
+                                                  e->crt_moduli > 0 ? e->crt_moduli : 1);
+            free(d);
+        }
+        off = align_up(off + pl->crt_bytes);
     }
     pl->total = off;
 }
@@ -241,6 +275,32 @@ static int choose_ksplit(const ca3dmm_engine_p e, int sym)
         if (cost < 0.99 * best_cost) { best = s; best_cost = cost; }
     }
     return best;
+}
+
+/* Modular split precision: k slabs of at most CA3DMM_CRT_MAX_K (the exact
+ * INT32 range of the residue products); B^T B keeps the reference's kp slabs. */
+static int crt_slabs(const ca3dmm_engine_p e)
+{
+    if (e->is_BTB) return e->kp > 0 ? e->kp : 1;
+    const int ns = (e->k + CA3DMM_CRT_MAX_K - 1) / CA3DMM_CRT_MAX_K;
+    return ns > 0 ? ns : 1;
+}
+
+/* Moduli for the modular mode: `want` (8..18), or 0 for the fewest whose
+ * product admits 51-bit operand integers for the deepest slab.  Returns 0 when
+ * no count works (a slab deeper than CA3DMM_CRT_MAX_K). */
+static int crt_resolve(const ca3dmm_engine_p e, int want)
+{
+    const int ns = crt_slabs(e);
+    const int kmax = (e->k + ns - 1) / ns;
+    if (kmax > CA3DMM_CRT_MAX_K) return 0;
+    if (want != 0) {
+        if (want < 8 || want > CA3DMM_CRT_MAX_MODULI) return 0;
+        return ca3dmm_crt_bits(want, kmax) >= 2 ? want : 0;
+    }
+    for (int nm = 8; nm <= CA3DMM_CRT_MAX_MODULI; nm++)
+        if (ca3dmm_crt_bits(nm, kmax) >= 51) return nm;
+    return CA3DMM_CRT_MAX_MODULI;
 }
 
 static int plan_build(ca3dmm_engine_p e)
@@ -317,8 +377,26 @@ static int plan_build(ca3dmm_engine_p e)
                 g->k0 = ks; g->kz = kz;
             }
     }
+    /* modular split precision: one group over all of C per k slab */
+    const int ns = crt_slabs(e);
+    pl->crt_nsl = ns;
+    pl->cb = (ca3dmm_oz_blk_t *) calloc(2 * (size_t) ns, sizeof(ca3dmm_oz_blk_t));
+    pl->cs = (ca3dmm_oz_src_t *) calloc(2 * (size_t) ns, sizeof(ca3dmm_oz_src_t));
+    pl->cg = (ca3dmm_crt_group_t *) calloc((size_t) ns, sizeof(ca3dmm_crt_group_t));
+    if (!pl->cb || !pl->cs || !pl->cg) return CA3DMM_ENOMEM;
+    for (int s2 = 0; s2 < ns; s2++) {
+        int ks, kz;
+        calc_block_spos_size(e->k, ns, s2, &ks, &kz);
+        ca3dmm_oz_blk_t *a = &pl->cb[s2], *b = &pl->cb[ns + s2];
+        a->r0 = 0; a->c0 = ks; a->rows = e->m; a->cols = kz;
+        a->alias = e->is_BTB ? s2 : -1;      /* op(A) = B^T: the B block's residues */
+        b->r0 = ks; b->c0 = 0; b->rows = kz; b->cols = e->n; b->alias = -1;
+        ca3dmm_crt_group_t *g = &pl->cg[s2];
+        g->a_blk = s2; g->b_blk = s2;
+        g->m = e->m; g->n = e->n; g->k = kz;
+    }
     plan_layout(e, pl);
-    pl->stage_bytes = pl->off_ozplan + pl->oz_plan_bytes;
+    pl->stage_bytes = pl->off_crtplan + pl->crt_plan_bytes;
     return CA3DMM_OK;
 }
 
@@ -353,6 +431,9 @@ static void plan_free(plan_t *pl)
     free(pl->os);
     free(pl->og);
     free(pl->ou);
+    free(pl->cb);
+    free(pl->cs);
+    free(pl->cg);
     if (pl->hx) {
         struct host_exec *x = pl->hx;
         cudaFree(x->dA);
@@ -495,8 +576,15 @@ static void finish_init(ca3dmm_engine_p e, int dst_srow, int dst_nrow, int dst_s
         ce->gemm_cycle = 1;
     }
     int gm;
-    GET_ENV_INT_VAR(gm, "CA3DMM_GEMM_MODE", "gemm_mode", 0, 0, 1);
+    GET_ENV_INT_VAR(gm, "CA3DMM_GEMM_MODE", "gemm_mode", 0, 0, 2);
     e->gemm_mode = gm;
+    int cm;
+    GET_ENV_INT_VAR(cm, "CA3DMM_CRT_MODULI", "crt_moduli", 0, 0, CA3DMM_CRT_MAX_MODULI);
+    e->crt_moduli = crt_resolve(e, cm);
+    if (e->gemm_mode == CA3DMM_GEMM_CRT && e->crt_moduli == 0) {
+        WARNING_PRINTF("CA3DMM_GEMM_MODE=2: no modulus count fits this k; using plain FP64\n");
+        e->gemm_mode = CA3DMM_GEMM_PLAIN;
+    }
     int sl;
     GET_ENV_INT_VAR(sl, "CA3DMM_OZAKI_SLICES", "ozaki_slices", 7, 2, 8);
     e->ozaki_slices = sl;
@@ -928,6 +1016,31 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
                                    w + pl->off_ozplan);
         if (rc) return rc;
     }
+    if (e->gemm_mode == CA3DMM_GEMM_CRT) {
+        const int ns = pl->crt_nsl;
+        for (int i = 0; i < 2 * ns; i++) {
+            pl->cs[i].base = NULL;
+            pl->cs[i].ld = i < ns ? ldA : ldB;
+            pl->cs[i].trans = i < ns ? e->trans_A : e->trans_B;
+            pl->cs[i].pad = 0;
+        }
+        for (int s2 = 0; s2 < ns; s2++) {
+            ca3dmm_crt_group_t *g = &pl->cg[s2];
+            if (ns > 1) {
+                g->C = (double *) (w + pl->off_slab) + (size_t) s2 * pl->slab_stride;
+                g->ldc = pl->slab_ld;
+            } else {
+                g->C = out;
+                g->ldc = ldo;
+            }
+            g->band = e->raster;
+        }
+        rc = ca3dmm_crt_plan_encode(&pl->crt, e->crt_moduli, ns, pl->cb, pl->cs, ns, pl->cb + ns,
+                                    pl->cs + ns, ns, pl->cg, w + pl->off_crt, pl->crt_bytes,
+                                    h + pl->off_crtplan, w + pl->off_crtplan);
+        if (rc) return rc;
+        e->crt_bits = pl->crt.p_min;
+    }
     memset(h + pl->off_status, 0, 64);
     CA3DMM_CUDA_TRY(cudaMemcpyAsync(w, h, pl->stage_bytes, cudaMemcpyHostToDevice, st));
     pl->c_A = A; pl->c_B = B; pl->c_ldA = ldA; pl->c_ldB = ldB;
@@ -979,7 +1092,11 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
     }
     int timing = e->sync_exec && pl->events_ok;
     if (timing) cudaEventRecord(pl->ev[0], st);
-    if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
+    const int crt = e->gemm_mode == CA3DMM_GEMM_CRT;
+    if (crt) {
+        rc = ca3dmm_crt_run_pack(&pl->crt, src_A, src_B, st);
+        if (rc) return rc;
+    } else if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
         rc = ca3dmm_oz_run_pack(&pl->oz, src_A, src_B, st);
         if (rc) return rc;
     } else {
@@ -990,7 +1107,12 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
     }
     if (timing) cudaEventRecord(pl->ev[1], st);
     int *status_d = (int *) (w + pl->off_status);
-    if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
+    if (crt) {
+        rc = ca3dmm_crt_run_gemm(&pl->crt, NULL, status_d, 5.0, st);
+        if (!rc) rc = ca3dmm_crt_run_reconstruct(&pl->crt, 0, pl->crt_nsl, 0, INT32_MAX, st);
+        if (!rc) rc = ca3dmm_crt_run_nonfinite(&pl->crt, 0, pl->crt_nsl, 0, INT32_MAX, src_A, src_B,
+                                               st);
+    } else if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
         rc = ca3dmm_oz_run_gemm(&pl->oz, status_d, 5.0, st);
         if (!rc) rc = ca3dmm_oz_run_nonfinite(&pl->oz, NULL, src_A, src_B, st);
     } else
@@ -1002,15 +1124,16 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
                 pl->dst_ncol == e->n;
     double *out = whole ? (double *) dst_C : (double *) (w + pl->off_cout);
     long long ldo = whole ? ldC : e->m;
-    const int nred = e->gemm_mode == CA3DMM_GEMM_OZAKI ? (pl->oz_fused ? 1 : e->kp)
-                                                      : (pl->plain_merged ? 1 : e->kp * pl->ksplit);
+    const int nred = crt ? pl->crt_nsl
+                         : e->gemm_mode == CA3DMM_GEMM_OZAKI ? (pl->oz_fused ? 1 : e->kp)
+                                                              : (pl->plain_merged ? 1 : e->kp * pl->ksplit);
     if (nred > 1) {
         rc = ca3dmm_reduce_slabs_launch((const double *) (w + pl->off_slab),
                                         (long long) pl->slab_stride, pl->slab_ld, nred, e->m,
                                         e->n, out, ldo, st);
         if (rc) return rc;
     }
-    if (pl->sym) {
+    if (pl->sym && !crt) {      /* the modular mode computes all of C */
         rc = ca3dmm_mirror_upper_launch(out, ldo, e->m, st);
         if (rc) return rc;
     }
@@ -1121,6 +1244,56 @@ static int hx_create(ca3dmm_engine_p e, struct host_exec **out)
 /* Output row bands and, per band, the GEMM tile ranges and the descriptors
  * that pack or slice its op(A) rows.  Returns the band count (0 or 1: no
  * pipelining for this layout). */
+/* Bands of the modular mode: one group over all of C (a single k slab), whose
+ * work list numbers its items in bands of `raster` tile rows, so a band of
+ * output rows is one range; per band the residue descriptors of its op(A)
+ * rows. */
+static int hx_build_bands_crt(ca3dmm_engine_p e, struct host_exec *x, cudaStream_t st)
+{
+    plan_t *pl = (plan_t *) e->impl;
+    const int whole = pl->has_dst && pl->dst_srow == 0 && pl->dst_scol == 0 &&
+                      pl->dst_nrow == e->m && pl->dst_ncol == e->n;
+    if (e->is_BTB || !whole || pl->crt_nsl != 1 || e->m <= 0) return 0;
+    const int raster = e->raster > 0 ? e->raster : 8;
+    int band_rows = raster * 128;
+    while ((e->m + band_rows - 1) / band_rows > HX_MAX_BANDS) band_rows *= 2;
+    const size_t one = ca3dmm_oz_desc_bytes();
+    x->ndesc = 1;
+    x->desc_stride = align_up(one);
+    if (!x->desc_h) {
+        const size_t p1 = align_up(sizeof(ca3dmm_pack_desc_t) * (size_t) e->kp);
+        const size_t p2 = align_up(one * (size_t) e->kp);
+        const size_t cap = (p1 > p2 ? p1 : p2) * HX_MAX_BANDS;
+        if (cudaMallocHost(&x->desc_h, cap) != cudaSuccess) { x->desc_h = NULL; return 0; }
+        if (cudaMalloc(&x->desc_d, cap) != cudaSuccess) { x->desc_d = NULL; return 0; }
+    }
+    const char *hp = (const char *) pl->stage + pl->off_crtplan;
+    for (int r = 0; r < e->m; r += band_rows) {
+        const int c = x->nband++;
+        const int rend = r + band_rows < e->m ? r + band_rows : e->m;
+        x->r0[c] = r;
+        x->r1[c] = rend;
+        int begin = 0, count = 0, blk = 0;
+        if (ca3dmm_crt_group_items(hp, 0, r / 128, (rend + 127) / 128, &begin, &count) ||
+            ca3dmm_crt_encode_rows(hp, 1, &blk, 1, r, rend,
+                                   (char *) x->desc_h + (size_t) c * x->desc_stride, x->ntile[c])) {
+            x->nband = 0;
+            return 0;
+        }
+        ca3dmm_tile_ranges_t *rg = &x->rng[c];
+        memset(rg, 0, sizeof(*rg));
+        rg->n = 1;
+        rg->begin[0] = begin;
+        rg->len[0] = count;
+    }
+    if (cudaMemcpyAsync(x->desc_d, x->desc_h, x->desc_stride * (size_t) x->nband,
+                        cudaMemcpyHostToDevice, st) != cudaSuccess) {
+        x->nband = 0;
+        return 0;
+    }
+    return x->nband;
+}
+
 static int hx_build_bands(ca3dmm_engine_p e, struct host_exec *x, cudaStream_t st)
 {
     plan_t *pl = (plan_t *) e->impl;
@@ -1132,6 +1305,7 @@ static int hx_build_bands(ca3dmm_engine_p e, struct host_exec *x, cudaStream_t s
     x->built_mode = e->gemm_mode;
     x->built_slices = e->ozaki_slices;
     x->built_raster = e->raster;
+    if (e->gemm_mode == CA3DMM_GEMM_CRT) return hx_build_bands_crt(e, x, st);
     if (e->is_BTB || !whole || ((ozaki && pl->oz_fused) ? 1 : e->kp) * tnn > CA3DMM_MAX_RANGES ||
         (!ozaki && pl->ksplit > 1))
         return 0;
@@ -1258,11 +1432,15 @@ static int hx_btb_slabs(ca3dmm_engine_p e, struct host_exec *x, const void *B_h,
                         void *C_h, int ldC, cudaStream_t st)
 {
     plan_t *pl = (plan_t *) e->impl;
-    const int ozaki = e->gemm_mode == CA3DMM_GEMM_OZAKI;
+    const int crt = e->gemm_mode == CA3DMM_GEMM_CRT;
+    /* split precision (slices or residues) slices each arriving slab itself */
+    const int ozaki = e->gemm_mode == CA3DMM_GEMM_OZAKI || crt;
     const int kp = e->kp, n = e->n, ks = ozaki ? 1 : pl->ksplit;
     const int whole = pl->has_dst && pl->dst_srow == 0 && pl->dst_scol == 0 &&
                       pl->dst_nrow == e->m && pl->dst_ncol == e->n;
-    if (!e->is_BTB || kp < 2 || kp > HX_MAX_BANDS || !whole || (ozaki && pl->oz_fused)) return 1;
+    if (!e->is_BTB || kp < 2 || kp > HX_MAX_BANDS || !whole || (!crt && ozaki && pl->oz_fused) ||
+        (crt && pl->crt_nsl != kp))
+        return 1;
     for (int i = 0; !ozaki && i < pl->nA; i++)
         if (!pl->A[i].direct) return 1;
     for (int i = 0; !ozaki && i < pl->nB; i++)
@@ -1280,10 +1458,12 @@ static int hx_btb_slabs(ca3dmm_engine_p e, struct host_exec *x, const void *B_h,
             if (cudaMalloc(&x->desc_d, cap) != cudaSuccess) { x->desc_d = NULL; return 1; }
         }
         for (int j = 0; j < kp; j++) {
-            const int idx = pl->nA + j;
-            if (ca3dmm_oz_encode_blocks((char *) pl->stage + pl->off_ozplan, pl->ngroup, &idx, 1,
-                                        (char *) x->desc_h + (size_t) j * x->desc_stride,
-                                        x->ntile[j]))
+            char *dj = (char *) x->desc_h + (size_t) j * x->desc_stride;
+            const int idx = crt ? pl->crt_nsl + j : pl->nA + j;
+            if (crt ? ca3dmm_crt_encode_blocks((char *) pl->stage + pl->off_crtplan, pl->crt_nsl,
+                                               &idx, 1, dj, x->ntile[j])
+                    : ca3dmm_oz_encode_blocks((char *) pl->stage + pl->off_ozplan, pl->ngroup,
+                                              &idx, 1, dj, x->ntile[j]))
                 return 1;
         }
         CA3DMM_CUDA_TRY(cudaMemcpyAsync(x->desc_d, x->desc_h, x->desc_stride * (size_t) kp,
@@ -1304,7 +1484,7 @@ static int hx_btb_slabs(ca3dmm_engine_p e, struct host_exec *x, const void *B_h,
                                               cudaMemcpyHostToDevice, x->s_in));
         CA3DMM_CUDA_TRY(cudaEventRecord(x->ev_a[j], x->s_in));
     }
-    int rc = ozaki ? ca3dmm_oz_clear(&pl->oz, st) : CA3DMM_OK;
+    int rc = crt ? ca3dmm_crt_clear(&pl->crt, st) : ozaki ? ca3dmm_oz_clear(&pl->oz, st) : CA3DMM_OK;
     if (rc) return rc;
     int tile0 = 0;
     for (int j = 0; j < kp; j++) {
@@ -1322,7 +1502,18 @@ static int hx_btb_slabs(ca3dmm_engine_p e, struct host_exec *x, const void *B_h,
         rg.len[0] = count;
         tile0 += count;
         CA3DMM_CUDA_TRY(cudaStreamWaitEvent(st, x->ev_a[j], 0));
-        if (ozaki) {
+        if (crt) {
+            const void *dd = (const char *) x->desc_d + (size_t) j * x->desc_stride;
+            int ib = 0, ic = 0;
+            rc = ca3dmm_crt_group_items((char *) pl->stage + pl->off_crtplan, j, 0, INT32_MAX, &ib,
+                                        &ic);
+            rg.begin[0] = ib;
+            rg.len[0] = ic;
+            if (!rc) rc = ca3dmm_crt_pack_descs(&pl->crt, x->dB, dd, 1, x->ntile[j], st);
+            if (!rc) rc = ca3dmm_crt_run_gemm(&pl->crt, &rg, status_d, 5.0, st);
+            if (!rc) rc = ca3dmm_crt_run_reconstruct(&pl->crt, j, j + 1, 0, INT32_MAX, st);
+            if (!rc) rc = ca3dmm_crt_run_nonfinite(&pl->crt, j, j + 1, 0, INT32_MAX, x->dB, x->dB, st);
+        } else if (ozaki) {
             const void *dd = (const char *) x->desc_d + (size_t) j * x->desc_stride;
             rc = ca3dmm_oz_slice_descs(&pl->oz, x->dB, dd, 1, x->ntile[j], st);
             if (!rc) rc = ca3dmm_oz_run_gemm_ranges(&pl->oz, &rg, status_d, 5.0, st);
@@ -1420,8 +1611,12 @@ static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_
         CA3DMM_CUDA_TRY(cudaEventRecord(x->ev_a[c], x->s_in));
     }
     const int ozaki = e->gemm_mode == CA3DMM_GEMM_OZAKI;
+    const int crt = e->gemm_mode == CA3DMM_GEMM_CRT;
     CA3DMM_CUDA_TRY(cudaStreamWaitEvent(st, x->ev_b, 0));
-    if (ozaki) {
+    if (crt) {
+        rc = ca3dmm_crt_clear(&pl->crt, st);
+        if (!rc) rc = ca3dmm_crt_pack_side(&pl->crt, 1, x->dB, st);
+    } else if (ozaki) {
         rc = ca3dmm_oz_clear(&pl->oz, st);
         if (!rc) rc = ca3dmm_oz_slice_side(&pl->oz, 1, x->dB, st);
     } else {
@@ -1431,7 +1626,12 @@ static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_
     for (int c = 0; c < x->nband; c++) {
         const void *dd = (const char *) x->desc_d + (size_t) c * x->desc_stride;
         CA3DMM_CUDA_TRY(cudaStreamWaitEvent(st, x->ev_a[c], 0));
-        if (ozaki) {
+        if (crt) {
+            rc = ca3dmm_crt_pack_descs(&pl->crt, x->dA, dd, 1, x->ntile[c], st);
+            if (!rc) rc = ca3dmm_crt_run_gemm(&pl->crt, &x->rng[c], status_d, 5.0, st);
+            if (!rc) rc = ca3dmm_crt_run_reconstruct(&pl->crt, 0, 1, x->r0[c], x->r1[c], st);
+            if (!rc) rc = ca3dmm_crt_run_nonfinite(&pl->crt, 0, 1, x->r0[c], x->r1[c], x->dA, x->dB, st);
+        } else if (ozaki) {
             rc = ca3dmm_oz_slice_descs(&pl->oz, x->dA, dd, x->ndesc, x->ntile[c], st);
             if (!rc) rc = ca3dmm_oz_run_gemm_ranges(&pl->oz, &x->rng[c], status_d, 5.0, st);
             if (!rc) rc = ca3dmm_oz_run_nonfinite(&pl->oz, &x->rng[c], x->dA, x->dB, st);
@@ -1442,7 +1642,7 @@ static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_
                 rc = ca3dmm_dgemm_launch_ranges(w + pl->off_gemm, pl->ngroup, &x->rng[c],
                                                 pl->a_kmajor, status_d, 5.0, st);
         }
-        if (!rc && e->kp > 1 && !(ozaki && pl->oz_fused) && !(!ozaki && pl->plain_merged))
+        if (!rc && !crt && e->kp > 1 && !(ozaki && pl->oz_fused) && !(!ozaki && pl->plain_merged))
             rc = ca3dmm_reduce_slabs_launch((const double *) (w + pl->off_slab) + x->r0[c],
                                             (long long) pl->slab_stride, pl->slab_ld, e->kp,
                                             x->r1[c] - x->r0[c], e->n, x->dC + x->r0[c], x->ldc, st);
@@ -1537,12 +1737,16 @@ void ca3dmm_engine_set_stream(ca3dmm_engine_p e, void *stream, int sync)
 int ca3dmm_engine_set_gemm_mode(ca3dmm_engine_p e, int mode, int slices)
 {
     if (!e) return CA3DMM_EINVAL;
-    if (mode != CA3DMM_GEMM_PLAIN && mode != CA3DMM_GEMM_OZAKI) return CA3DMM_EINVAL;
+    if (mode != CA3DMM_GEMM_PLAIN && mode != CA3DMM_GEMM_OZAKI && mode != CA3DMM_GEMM_CRT)
+        return CA3DMM_EINVAL;
     if (mode == CA3DMM_GEMM_OZAKI && (slices < 2 || slices > 8)) return CA3DMM_EINVAL;
+    int nmod = 0;
+    if (mode == CA3DMM_GEMM_CRT && (nmod = crt_resolve(e, slices)) == 0) return CA3DMM_EINVAL;
     plan_t *pl = (plan_t *) e->impl;
-    int old_mode = e->gemm_mode, old_sl = e->ozaki_slices;
+    int old_mode = e->gemm_mode, old_sl = e->ozaki_slices, old_nm = e->crt_moduli;
     e->gemm_mode = mode;
     if (mode == CA3DMM_GEMM_OZAKI) e->ozaki_slices = slices;
+    if (mode == CA3DMM_GEMM_CRT) e->crt_moduli = nmod;
     size_t old_total = pl->total;
     plan_layout(e, pl);
     if (e->workbuf_d != NULL && pl->total > old_total) {
@@ -1550,6 +1754,7 @@ int ca3dmm_engine_set_gemm_mode(ca3dmm_engine_p e, int mode, int slices)
             /* the caller's buffer is too small: keep the old mode */
             e->gemm_mode = old_mode;
             e->ozaki_slices = old_sl;
+            e->crt_moduli = old_nm;
             plan_layout(e, pl);
             return CA3DMM_ENOMEM;
         }
@@ -1557,6 +1762,7 @@ int ca3dmm_engine_set_gemm_mode(ca3dmm_engine_p e, int mode, int slices)
         if (!nw) {
             e->gemm_mode = old_mode;
             e->ozaki_slices = old_sl;
+            e->crt_moduli = old_nm;
             plan_layout(e, pl);
             return CA3DMM_ENOMEM;
         }

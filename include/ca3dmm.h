@@ -36,6 +36,9 @@
 #define CA3DMM_GEMM_PLAIN 0   /* FP64 DMMA tensor-core GEMM (env CA3DMM_PLAIN_MERGE_SLABS=0 at
                                  init keeps the kp-slab sum order instead of one GEMM over k) */
 #define CA3DMM_GEMM_OZAKI 1   /* split precision: INT8 slices on tcgen05, FP64 recombination */
+#define CA3DMM_GEMM_CRT   2   /* split precision, modular: P-bit row / column integers, their exact
+                                 product from one INT8 tcgen05 GEMM per modulus (N moduli <= 256)
+                                 and the Chinese remainder theorem, rounded once to FP64 */
 
 struct ca3dmm_engine {
     int m, n, k;                    /* Size of op(A) (m*k), op(B) (k*n), C (m*n) */
@@ -121,6 +124,9 @@ struct ca3dmm_engine {
     int raster;                     /* GEMM tile rows per raster band (tuning knob) */
     int btb_symmetric;              /* B^T B: compute the upper block triangle only, mirror it
                                        (env CA3DMM_BTB_SYMMETRIC=1 at init_BTB) */
+    int crt_moduli;                 /* CA3DMM_GEMM_CRT: moduli (env CA3DMM_CRT_MODULI; 0 = the
+                                       fewest that give 51-bit integers for this k) */
+    int crt_bits;                   /* CA3DMM_GEMM_CRT: integer width P of the operands */
 };
 typedef struct ca3dmm_engine ca3dmm_engine_s;
 typedef struct ca3dmm_engine *ca3dmm_engine_p;
@@ -190,10 +196,12 @@ int ca3dmm_engine_last_error(ca3dmm_engine_p engine);
 /* Run exec on `stream` (cudaStream_t); sync = 0 makes exec asynchronous and
  * CUDA-graph capturable (the statistics are then not updated). */
 void ca3dmm_engine_set_stream(ca3dmm_engine_p engine, void *stream, int sync);
-/* Select the GEMM: CA3DMM_GEMM_PLAIN, or CA3DMM_GEMM_OZAKI with `slices`
- * INT8 slices per operand (2..8).  Must be called before attach_workbuf when
- * the caller allocates the work buffer (it changes *workbuf_bytes, which
- * ca3dmm_engine_workbuf_bytes reports). */
+/* Select the GEMM: CA3DMM_GEMM_PLAIN, CA3DMM_GEMM_OZAKI with `slices` INT8
+ * slices per operand (2..8), or CA3DMM_GEMM_CRT with `slices` moduli (8..18,
+ * 0 = the fewest whose product admits 51-bit operand integers at this k; the
+ * engine's crt_bits field then holds the integer width).  Must be called
+ * before attach_workbuf when the caller allocates the work buffer (it changes
+ * *workbuf_bytes, which ca3dmm_engine_workbuf_bytes reports). */
 int ca3dmm_engine_set_gemm_mode(ca3dmm_engine_p engine, int mode, int slices);
 size_t ca3dmm_engine_workbuf_bytes(ca3dmm_engine_p engine);
 /* Tile rows per raster band of the GEMM launches (4, 8 or 16; L2 reuse). */

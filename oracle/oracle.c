@@ -409,3 +409,185 @@ float orc_mlp_fwd_bwd(int B, int nin, int h1, int h2, const float *X, const floa
     free(a1); free(a2); free(d1); free(d2);
     return B > 0 ? (float) (loss / B) : 0.f;
 }
+
+/* ---------------------------------------------------------------------- */
+/* 8. Modular (CRT) split precision                                        */
+/*    Row i of op(A): E_i = frexp exponent of max_l |a_il| (max < 2^E_i,    */
+/*    0 for a zero row), a'_il = rint(a_il 2^(P - E_i)), |a'| <= 2^P; column */
+/*    j of op(B) likewise (F_j, b').  C'_ij = sum_l a'_il b'_lj exactly     */
+/*    (|C'| <= k 2^(2P)); the device obtains it from the residues of the    */
+/*    products modulo N pairwise coprime moduli <= 256 (one INT8 GEMM each) */
+/*    by the Chinese remainder theorem, which is exact while               */
+/*    k 2^(2P+1) < M = prod p_t.  C_ij = (C' rounded to double, round to   */
+/*    nearest even) 2^(E_i + F_j - 2P).  Rows / columns holding an Inf or a */
+/*    NaN are zero rows here too (orc_nonfinite_fixup gives their entries). */
+/* ---------------------------------------------------------------------- */
+static const int crt_mod_list[18] = {256, 255, 253, 251, 247, 241, 239, 233, 229,
+                                     227, 223, 217, 211, 199, 197, 193, 191, 181};
+
+int orc_crt_modulus(int t) { return (t >= 0 && t < 18) ? crt_mod_list[t] : 0; }
+
+/* Largest P <= 53 with k 2^(2P+1) < M_N (M_N the product of the first N moduli). */
+int orc_crt_bits(int nmod, long k)
+{
+    double lm = 0.0;
+    for (int t = 0; t < nmod && t < 18; t++) lm += log2((double) crt_mod_list[t]);
+    double lk = log2((double) (k > 1 ? k : 1));
+    int P = (int) floor((lm - 1.0 - lk - 1e-9) / 2.0);
+    return P > 53 ? 53 : P;
+}
+
+/* a' of one row / column: exponent from the largest magnitude, then rint of
+ * the scaled values (ldexp is exact; rint rounds half to even). */
+static int crt_row_ints(const double *v, long n, long stride, int P, long long *out)
+{
+    double mx = 0.0;
+    int fin = 1;
+    for (long l = 0; l < n; l++) {
+        double x = v[l * stride];
+        if (!isfinite(x)) fin = 0;
+        else if (fabs(x) > mx) mx = fabs(x);
+    }
+    int E = 0;
+    if (fin && mx > 0.0) frexp(mx, &E);
+    for (long l = 0; l < n; l++)
+        out[l] = fin ? (long long) rint(ldexp(v[l * stride], P - E)) : 0;
+    return E;
+}
+
+/* double of a signed integer below 2^127 in magnitude, rounded to nearest even,
+ * times 2^e: a 64-bit window with the leading bit at bit 63 and the bits below
+ * it ORed into bit 0, converted once, then scaled by a power of two (one more
+ * rounding only if the result leaves the normal range).  Same steps as the
+ * device. */
+static double crt_to_double(__int128 c, int e)
+{
+    int neg = c < 0;
+    unsigned __int128 mag = neg ? (unsigned __int128) (-c) : (unsigned __int128) c;
+    uint64_t hi = (uint64_t) (mag >> 64), lo = (uint64_t) mag;
+    double d;
+    if (hi == 0) {
+        d = (double) lo;     /* rounds to nearest even */
+    } else {
+        int lz = __builtin_clzll(hi);
+        int sh = 64 - lz;                       /* bits below the window */
+        unsigned __int128 top = mag >> sh;      /* < 2^64, leading bit at 63 */
+        uint64_t w = (uint64_t) top;
+        if ((mag & ((((unsigned __int128) 1) << sh) - 1)) != 0) w |= 1ull;
+        /* w has bit 63 set: round to 53 bits, nearest even (round bit 10,
+         * sticky bits 0-9) */
+        uint64_t m53 = w >> 11, rb = (w >> 10) & 1, st = (w & 0x3ffull) != 0;
+        if (rb && (st || (m53 & 1))) m53 += 1;
+        d = ldexp((double) m53, 11);
+        e += sh;
+    }
+    double r;
+    if (e >= -1022 && e <= 1023) r = d * ldexp(1.0, e);
+    else r = ldexp(d, e);
+    return neg ? -r : r;
+}
+
+/* The CRT scheme's result (m x n, column-major C), from the exact integer product. */
+void orc_crt_gemm(const double *A, long lda, int tA, const double *B, long ldb, int tB, int m,
+                  int n, int k, int P, double *C)
+{
+    long long *ai = (long long *) malloc(sizeof(long long) * (size_t) m * (k > 0 ? k : 1));
+    long long *bj = (long long *) malloc(sizeof(long long) * (size_t) n * (k > 0 ? k : 1));
+    int *ea = (int *) malloc(sizeof(int) * (size_t) (m > 0 ? m : 1));
+    int *fb = (int *) malloc(sizeof(int) * (size_t) (n > 0 ? n : 1));
+    for (long i = 0; i < m; i++)
+        ea[i] = crt_row_ints(tA ? A + i * lda : A + i, k, tA ? 1 : lda, P, ai + i * k);
+    for (long j = 0; j < n; j++)
+        fb[j] = crt_row_ints(tB ? B + j : B + j * ldb, k, tB ? ldb : 1, P, bj + j * k);
+    #pragma omp parallel for collapse(2) schedule(static)
+    for (long j = 0; j < n; j++)
+        for (long i = 0; i < m; i++) {
+            __int128 s = 0;
+            const long long *a = ai + i * k, *b = bj + j * k;
+            for (long l = 0; l < k; l++) s += (__int128) a[l] * b[l];
+            C[i + j * m] = crt_to_double(s, ea[i] + fb[j] - 2 * P);
+        }
+    free(ai); free(bj); free(ea); free(fb);
+}
+
+/* The modular route for the same integers, for small sizes: residues of a'
+ * and b' modulo each p_t in [-128, 127] (r = a' mod p in [0, p), minus p when
+ * r >= 128), the INT32 dot products of the residues reduced mod p_t, and a
+ * Garner (mixed radix) reconstruction in 128-bit integers, symmetric around
+ * 0.  Writes C'_ij (as two 64-bit halves, low first) so that a test can
+ * compare it with the direct integer product.  Returns 0, or 1 when the
+ * bound k 2^(2P+1) < M is not met. */
+static int crt_inv_mod(int a, int p)
+{
+    a %= p;
+    if (a < 0) a += p;
+    for (int x = 1; x < p; x++) if ((a * x) % p == 1) return x;
+    return 0;
+}
+
+int orc_crt_modular(const double *A, long lda, int tA, const double *B, long ldb, int tB, int m,
+                    int n, int k, int P, int nmod, long long *out_lo_hi)
+{
+    if (nmod < 2 || nmod > 18 || orc_crt_bits(nmod, k) < P) return 1;
+    long long *ai = (long long *) malloc(sizeof(long long) * (size_t) m * (k > 0 ? k : 1));
+    long long *bj = (long long *) malloc(sizeof(long long) * (size_t) n * (k > 0 ? k : 1));
+    for (long i = 0; i < m; i++)
+        crt_row_ints(tA ? A + i * lda : A + i, k, tA ? 1 : lda, P, ai + i * k);
+    for (long j = 0; j < n; j++)
+        crt_row_ints(tB ? B + j : B + j * ldb, k, tB ? ldb : 1, P, bj + j * k);
+    int u[18];
+    for (long j = 0; j < n; j++)
+        for (long i = 0; i < m; i++) {
+            for (int t = 0; t < nmod; t++) {
+                const long long p = crt_mod_list[t];
+                long long acc = 0;
+                for (long l = 0; l < k; l++) {
+                    long long ra = ((ai[i * k + l] % p) + p) % p, rb = ((bj[j * k + l] % p) + p) % p;
+                    if (ra >= 128) ra -= p;
+                    if (rb >= 128) rb -= p;
+                    acc += ra * rb;
+                }
+                u[t] = (int) (((acc % p) + p) % p);
+            }
+            /* Garner: x = v_0 + p_0 (v_1 + p_1 (v_2 + ...)) */
+            long long v[18];
+            for (int t = 0; t < nmod; t++) {
+                const int p = crt_mod_list[t];
+                long long x = 0, w = 1;
+                for (int s2 = 0; s2 < t; s2++) {
+                    x = (x + v[s2] % p * w) % p;
+                    w = w * crt_mod_list[s2] % p;
+                }
+                long long d = ((u[t] - x) % p + p) % p;
+                v[t] = d * crt_inv_mod((int) w, p) % p;
+            }
+            unsigned __int128 x = 0, w = 1, M = 1;
+            for (int t = 0; t < nmod; t++) { x += (unsigned __int128) v[t] * w; w *= crt_mod_list[t]; }
+            M = w;
+            __int128 c = x >= M / 2 ? (__int128) x - (__int128) M : (__int128) x;
+            out_lo_hi[2 * (i + j * m)] = (long long) (uint64_t) c;
+            out_lo_hi[2 * (i + j * m) + 1] = (long long) (c >> 64);
+        }
+    free(ai); free(bj);
+    return 0;
+}
+
+/* The exact integer product C'_ij (two 64-bit halves, low first). */
+void orc_crt_exact(const double *A, long lda, int tA, const double *B, long ldb, int tB, int m,
+                   int n, int k, int P, long long *out_lo_hi)
+{
+    long long *ai = (long long *) malloc(sizeof(long long) * (size_t) m * (k > 0 ? k : 1));
+    long long *bj = (long long *) malloc(sizeof(long long) * (size_t) n * (k > 0 ? k : 1));
+    for (long i = 0; i < m; i++)
+        crt_row_ints(tA ? A + i * lda : A + i, k, tA ? 1 : lda, P, ai + i * k);
+    for (long j = 0; j < n; j++)
+        crt_row_ints(tB ? B + j : B + j * ldb, k, tB ? ldb : 1, P, bj + j * k);
+    for (long j = 0; j < n; j++)
+        for (long i = 0; i < m; i++) {
+            __int128 s = 0;
+            for (long l = 0; l < k; l++) s += (__int128) ai[i * k + l] * bj[j * k + l];
+            out_lo_hi[2 * (i + j * m)] = (long long) (uint64_t) s;
+            out_lo_hi[2 * (i + j * m) + 1] = (long long) (s >> 64);
+        }
+    free(ai); free(bj);
+}

@@ -44,6 +44,15 @@ def lib():
         L.orc_ozaki_gemm.argtypes = [u8p, ip, u8p, ip, C.c_int, C.c_int, C.c_int, C.c_int, dp]
         L.orc_nonfinite_fixup.argtypes = [dp, C.c_long, C.c_int, dp, C.c_long, C.c_int, C.c_int,
                                           C.c_int, C.c_int, dp]
+        llp = C.POINTER(C.c_longlong)
+        L.orc_crt_modulus.argtypes = [C.c_int]
+        L.orc_crt_bits.argtypes = [C.c_int, C.c_long]
+        L.orc_crt_gemm.argtypes = [dp, C.c_long, C.c_int, dp, C.c_long, C.c_int, C.c_int,
+                                   C.c_int, C.c_int, C.c_int, dp]
+        L.orc_crt_modular.argtypes = [dp, C.c_long, C.c_int, dp, C.c_long, C.c_int, C.c_int,
+                                      C.c_int, C.c_int, C.c_int, C.c_int, llp]
+        L.orc_crt_exact.argtypes = [dp, C.c_long, C.c_int, dp, C.c_long, C.c_int, C.c_int,
+                                    C.c_int, C.c_int, C.c_int, llp]
         L.orc_ozaki_kchunk.argtypes = [C.c_int]
         L.orc_ozaki_kchunk.restype = C.c_int
         fp = C.POINTER(C.c_float)
@@ -218,6 +227,55 @@ def nonfinite_fixup(A, B, tA, tB, m, n, k, Cm):
     lib().orc_nonfinite_fixup(_d(A), A.shape[0], int(tA), _d(B), B.shape[0], int(tB), m, n, k,
                               _d(Cm))
     return Cm
+
+
+def crt_modulus(t):
+    """Modulus t of the modular scheme's list (pairwise coprime, <= 256)."""
+    return lib().orc_crt_modulus(int(t))
+
+
+def crt_bits(nmod, k):
+    """Integer width P of the modular scheme with nmod moduli and depth k."""
+    return lib().orc_crt_bits(int(nmod), int(k))
+
+
+def crt_gemm(A, B, tA, tB, m, n, k, P):
+    """The modular scheme's result C (m x n, Fortran order) from the exact
+    integer product of the P-bit row / column integers."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    B = np.asfortranarray(B, dtype=np.float64)
+    Cm = np.zeros((m, n), order="F")
+    lib().orc_crt_gemm(_d(A), A.shape[0], int(tA), _d(B), B.shape[0], int(tB), m, n, k, int(P),
+                       _d(Cm))
+    return Cm
+
+
+def _i128(buf, m, n):
+    lo = buf[0::2].astype(np.uint64).astype(object)
+    hi = buf[1::2].astype(object)
+    return np.array([int(h) * (1 << 64) + int(l) for l, h in zip(lo, hi)],
+                    dtype=object).reshape((m, n), order="F")
+
+
+def crt_exact_ints(A, B, tA, tB, m, n, k, P):
+    """C' = sum_l a'_il b'_lj as Python integers (m x n object array)."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    B = np.asfortranarray(B, dtype=np.float64)
+    buf = np.zeros(2 * m * n, dtype=np.int64)
+    lib().orc_crt_exact(_d(A), A.shape[0], int(tA), _d(B), B.shape[0], int(tB), m, n, k, int(P),
+                        buf.ctypes.data_as(C.POINTER(C.c_longlong)))
+    return _i128(buf, m, n)
+
+
+def crt_modular_ints(A, B, tA, tB, m, n, k, P, nmod):
+    """The same integers through residues modulo nmod moduli and a Garner
+    reconstruction (None when the modulus product is too small for P, k)."""
+    A = np.asfortranarray(A, dtype=np.float64)
+    B = np.asfortranarray(B, dtype=np.float64)
+    buf = np.zeros(2 * m * n, dtype=np.int64)
+    rc = lib().orc_crt_modular(_d(A), A.shape[0], int(tA), _d(B), B.shape[0], int(tB), m, n, k,
+                               int(P), int(nmod), buf.ctypes.data_as(C.POINTER(C.c_longlong)))
+    return None if rc else _i128(buf, m, n)
 
 
 # ---------------------------------------------------------------- CPU CA3DMM

@@ -65,3 +65,36 @@ def test_recombination_extreme_exponents():
     assert np.all(err <= k * U * ab + (4 * k + 64) * 2.0 ** -1074)
     for i, j in ((0, 0), (1, 0)):
         assert abs(C[i, j] - hi[i, j]) <= k * U * ab[i, j]
+
+
+@pytest.mark.parametrize("nmod,seed", [(8, 0), (12, 1), (15, 2), (16, 3), (18, 4)])
+def test_crt_modular_route_equals_exact_integers(nmod, seed):
+    """The modular restatement (residues of a', b' in [-128, 127], INT32 dot
+    products reduced mod p_t, Garner reconstruction) gives exactly the
+    integer product the scheme's result is rounded from."""
+    rng = np.random.default_rng(seed)
+    m, n = (int(x) for x in rng.integers(3, 12, 2))
+    k = int(rng.integers(1, 400))
+    A = orc.gen_signed_exp(seed + 7, m, k)
+    B = orc.gen_signed_exp(seed + 8, k, n)
+    P = orc.crt_bits(nmod, k)
+    assert P >= 2
+    exact = orc.crt_exact_ints(A, B, 0, 0, m, n, k, P)
+    modular = orc.crt_modular_ints(A, B, 0, 0, m, n, k, P, nmod)
+    assert modular is not None and (exact == modular).all()
+    assert max(abs(int(x)) for x in exact.ravel()) <= k * 2 ** (2 * P)
+
+
+def test_crt_bits_rule():
+    """P is the largest width <= 53 with k 2^(2P+1) < prod p_t."""
+    import math
+    for nmod in (8, 12, 15, 16, 18):
+        lm = sum(math.log2(orc.crt_modulus(t)) for t in range(nmod))
+        for k in (1, 100, 2667, 8000, 32768, 131072):
+            P = orc.crt_bits(nmod, k)
+            assert P <= 53
+            assert math.log2(k) + 2 * P + 1 < lm
+            if P < 53:
+                assert math.log2(k) + 2 * (P + 1) + 1 >= lm - 1e-9
+    assert [orc.crt_modulus(t) for t in range(4)] == [256, 255, 253, 251]
+    assert orc.crt_bits(15, 8000) == 51 and orc.crt_bits(16, 32768) == 53
