@@ -55,24 +55,17 @@ constexpr int DEFAULT_BAND = 8;
 // ------------------------------------------------------------------ moduli
 // Pairwise coprime moduli <= 256, largest first (256 = 2^8 and odd numbers
 // with disjoint prime factors), and per modulus the constants of the residue
-// arithmetic: 2^16, 2^18, 2^36 mod p, and 1/p rounded down.
+// arithmetic: 2^16, 2^18, 2^36 mod p, and floor(2^32 / p).
 constexpr int kModList[MAXMOD] = {256, 255, 253, 251, 247, 241, 239, 233, 229,
                                   227, 223, 217, 211, 199, 197, 193, 191, 181};
 
 struct ModConst {
     int p, c16, c18, c36;
-    float invp;      // <= 1/p
+    unsigned int mrec;   // floor(2^32 / p): floor(y mrec / 2^32) is floor(y / p) or one less (y < 2^28)
     int half;        // floor(p/2)
     int bias;        // a multiple of p above 2^15 * 255 (keeps the epilogue's sums >= 0)
     int off54;       // p - (2^54 mod p) (keeps the residue pass's sums >= 0)
 };
-
-constexpr float inv_down(int p)
-{
-    // 1/p rounded down to a float: for 128 < p <= 256, 1/p lies in [2^-8, 2^-7),
-    // where floats are the multiples of 2^-31, and floor(2^31 / p) < 2^24
-    return (float) ((1LL << 31) / p) * (1.0f / 2147483648.0f);
-}
 
 constexpr ModConst make_mod(int p)
 {
@@ -80,7 +73,7 @@ constexpr ModConst make_mod(int p)
                     (int) ((1LL << 16) % p),
                     (int) ((1LL << 18) % p),
                     (int) ((1ULL << 36) % (unsigned long long) p),
-                    inv_down(p),
+                    (unsigned int) ((1ULL << 32) / (unsigned long long) p),
                     p / 2,
                     (int) (((8650752LL + p - 1) / p) * p),   // a multiple of p >= 2^23 + 2^18
                     (int) (p - (int) ((1ULL << 54) % (unsigned long long) p))};
@@ -194,10 +187,12 @@ double log2_modprod(int nmod)
 // One row's 16 consecutive k elements -> their residues for every modulus.
 // v = a' + 2^54 > 0 is split into 18-bit pieces x0 + 2^18 x1 + 2^36 x2, so
 // y = x2 (2^36 mod p) + x1 (2^18 mod p) + x0 + (p - 2^54 mod p) + floor(p/2)
-// is below 2^27 and congruent to a' + floor(p/2); q = floor(y / p) from a
-// float estimate rounded down (too small by at most one), r = y - q p in
-// [0, 2p) folded once, and the residue byte is r - floor(p/2).
+// is below 2^28 and congruent to a' + floor(p/2); q = floor(y floor(2^32/p) / 2^32)
+// is floor(y / p) or one less, r = y - q p in [0, 2p) is folded once, and the
+// residue byte is r - floor(p/2).
 struct ResidueWriter {
+    // the pass is issue-bound: four blocks of 256 threads per SM hide latency
+    static constexpr int kMinBlocks = 4;
     static __device__ __forceinline__ void write16(const SliceDesc &d, unsigned char *__restrict__ work,
                                                    const unsigned long long *__restrict__ mwork,
                                                    int gr, int gl, const double (&x)[16])
@@ -231,7 +226,7 @@ struct ResidueWriter {
             for (int j = 0; j < 16; ++j) {
                 const unsigned int y = x2[j] * (unsigned int) mc.c36 + x1[j] * (unsigned int) mc.c18 +
                                        x0[j] + add;
-                const unsigned int q = __float2uint_rd(__fmul_rd(__uint2float_rd(y), mc.invp));
+                const unsigned int q = __umulhi(y, mc.mrec);
                 const unsigned int rr0 = y - q * (unsigned int) mc.p;
                 const unsigned int r1 = rr0 - (unsigned int) mc.p;
                 r[j] = (rr0 < r1 ? rr0 : r1) - (unsigned int) mc.half;   // min folds [p, 2p) down
@@ -324,13 +319,13 @@ __device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr)
 
 // int32 sum -> its residue mod p in [0, p): v = 2^16 h + l (h signed), so
 // y = h (2^16 mod p) + l + bias >= 0 is below 2^25 and congruent to v; the
-// float quotient rounded down is short by at most one.
+// quotient floor(y floor(2^32/p) / 2^32) is short by at most one.
 __device__ __forceinline__ unsigned int mod_i32(uint32_t vbits, const ModConst &mc)
 {
     const int v = (int) vbits;
     const int h = v >> 16;
     const unsigned int y = (unsigned int) (h * mc.c16 + (int) (vbits & 0xffffu) + mc.bias);
-    const unsigned int q = __float2uint_rd(__fmul_rd(__uint2float_rd(y), mc.invp));
+    const unsigned int q = __umulhi(y, mc.mrec);
     const unsigned int r0 = y - q * (unsigned int) mc.p;
     const unsigned int r1 = r0 - (unsigned int) mc.p;
     return r0 < r1 ? r0 : r1;
@@ -539,11 +534,28 @@ __device__ __forceinline__ double u128_to_double(unsigned long long hi, unsigned
     return __ull2double_rn(w);
 }
 
-template <int N>
+// 32-bit limbs that the modulus product M_N needs (known at compile time)
+constexpr int crt_limbs(int n)
+{
+    const CrtTable T = make_crt_table();
+    int l = LIMBS + 1;
+    while (l > 1 && T.M[n][l - 1] == 0u) --l;
+    return l;
+}
+
+// C' from its residues: S = sum_t u_t W_t (column sums of 32-bit limb
+// products), q = rint(S / M) from an FP64 estimate of S (|C'| < M / 2, and the
+// estimate is off by far less than the gap to a half-integer), then
+// C' = S - q M taken modulo 2^128, which holds it exactly in two's complement
+// because |C'| <= k 2^(2P) <= 2^123.  Only the limbs below 2^128 of S and q M
+// are formed; all W_t and M fit in L = crt_limbs(N) limbs (a template
+// argument, computed on the host).
+template <int N, int L>
 __global__ void __launch_bounds__(256)
 crt_reconstruct_kernel(const CrtGroup *__restrict__ groups, int g0, int r0, int r1,
                        const unsigned char *__restrict__ work)
 {
+    static_assert(L >= 2 && L <= LIMBS, "modulus product outside the limb range");
     const CrtGroup &G = groups[g0 + blockIdx.y];
     const int rb = max(r0, 0), re = min(r1, G.m);
     if (re <= rb) return;
@@ -560,97 +572,59 @@ crt_reconstruct_kernel(const CrtGroup *__restrict__ groups, int g0, int r0, int 
         for (int t = 0; t < N; ++t)
             u4[t] = __ldg(reinterpret_cast<const unsigned int *>(
                 work + G.pl_off + (long long) t * G.pl_bytes + (long long) j * G.pl_ld + i0));
-#pragma unroll 1
+#pragma unroll
         for (int e = 0; e < 4; ++e) {
             const int i = i0 + e;
-            if (i >= re) break;
-            // S = sum_t u_t W_t in five 64-bit column sums, then 32-bit limbs s0..s5
-            unsigned long long a[LIMBS] = {0, 0, 0, 0, 0};
+            if (i < re) {
+                unsigned long long a[L];
 #pragma unroll
-            for (int t = 0; t < N; ++t) {
-                const unsigned long long u = (u4[t] >> (8 * e)) & 0xffu;
+                for (int q = 0; q < L; ++q) a[q] = 0ull;
 #pragma unroll
-                for (int q = 0; q < LIMBS; ++q) a[q] += u * kCrt.W[N][t][q];
-            }
-            unsigned int s[6];
-            unsigned long long c = 0;
+                for (int t = 0; t < N; ++t) {
+                    const unsigned int u = (u4[t] >> (8 * e)) & 0xffu;
 #pragma unroll
-            for (int q = 0; q < LIMBS; ++q) {
-                const unsigned long long x = a[q] + c;
-                s[q] = (unsigned int) x;
-                c = x >> 32;
-            }
-            s[5] = (unsigned int) c;
-            // quotient estimate floor(S / M) (off by at most one), R = S - q M
-            const double sd = fma((double) s[5], 0x1p160,
-                              fma((double) s[4], 0x1p128,
-                              fma((double) s[3], 0x1p96, fma((double) s[2], 0x1p64,
-                                                             (double) s[1] * 0x1p32))));
-            const unsigned int qe = (unsigned int) (sd * kCrt.invM[N]);
-            unsigned int r[6];
-            unsigned long long pc = 0;
-            long long bor = 0;
-#pragma unroll
-            for (int q = 0; q < 6; ++q) {
-                const unsigned long long pm = (unsigned long long) qe * kCrt.M[N][q] + pc;
-                pc = pm >> 32;
-                const long long dd = (long long) s[q] - (long long) (unsigned int) pm - bor;
-                bor = dd < 0 ? 1 : 0;
-                r[q] = (unsigned int) (dd + (bor << 32));
-            }
-            if (bor) {
-                // R < 0: add M
-                unsigned long long cc = 0;
-#pragma unroll
-                for (int q = 0; q < 6; ++q) {
-                    const unsigned long long x = (unsigned long long) r[q] + kCrt.M[N][q] + cc;
-                    r[q] = (unsigned int) x;
-                    cc = x >> 32;
+                    for (int q = 0; q < L; ++q) a[q] += (unsigned long long) u * kCrt.W[N][t][q];
                 }
-            } else {
-                // R >= M: subtract M
-                bool ge = true;
+                // quotient: S = sum_q a_q 2^(32 q) in FP64 (each a_q < 2^46 exact)
+                double sd = (double) a[L - 1];
 #pragma unroll
-                for (int q = 5; q >= 0; --q) {
-                    // lexicographic compare from the top limb
-                    if (r[q] != kCrt.M[N][q]) { ge = r[q] > kCrt.M[N][q]; break; }
-                }
-                if (ge) {
-                    long long bb = 0;
-#pragma unroll
-                    for (int q = 0; q < 6; ++q) {
-                        const long long dd = (long long) r[q] - (long long) kCrt.M[N][q] - bb;
-                        bb = dd < 0 ? 1 : 0;
-                        r[q] = (unsigned int) (dd + (bb << 32));
-                    }
-                }
-            }
-            // symmetric: C' = R - M when R >= M / 2
-            bool neg = true;
-#pragma unroll
-            for (int q = 5; q >= 0; --q) {
-                if (r[q] != kCrt.H[N][q]) { neg = r[q] > kCrt.H[N][q]; break; }
-            }
-            unsigned int mg[4];
-            if (neg) {
-                long long bb = 0;
+                for (int q = L - 2; q >= 0; --q) sd = fma(sd, 4294967296.0, (double) a[q]);
+                const unsigned int qe = (unsigned int) __double2int_rn(sd * kCrt.invM[N]);
+                // low 128 bits of S and of q M, then C' = S - q M mod 2^128
+                unsigned int s4[4];
+                unsigned long long c = 0ull;
 #pragma unroll
                 for (int q = 0; q < 4; ++q) {
-                    const long long dd = (long long) kCrt.M[N][q] - (long long) r[q] - bb;
-                    bb = dd < 0 ? 1 : 0;
-                    mg[q] = (unsigned int) (dd + (bb << 32));
+                    const unsigned long long x = (q < L ? a[q] : 0ull) + c;
+                    s4[q] = (unsigned int) x;
+                    c = x >> 32;
                 }
-            } else {
+                unsigned int t4[4];
+                unsigned long long pc = 0ull;
 #pragma unroll
-                for (int q = 0; q < 4; ++q) mg[q] = r[q];
+                for (int q = 0; q < 4; ++q) {
+                    const unsigned long long pm = (unsigned long long) qe * kCrt.M[N][q] + pc;
+                    t4[q] = (unsigned int) pm;
+                    pc = pm >> 32;
+                }
+                const unsigned long long slo = ((unsigned long long) s4[1] << 32) | s4[0];
+                const unsigned long long shi = ((unsigned long long) s4[3] << 32) | s4[2];
+                const unsigned long long tlo = ((unsigned long long) t4[1] << 32) | t4[0];
+                const unsigned long long thi = ((unsigned long long) t4[3] << 32) | t4[2];
+                unsigned long long lo = slo - tlo;
+                unsigned long long hi = shi - thi - (slo < tlo ? 1ull : 0ull);
+                const bool neg = (long long) hi < 0;
+                if (neg) {
+                    lo = ~lo + 1ull;
+                    hi = ~hi + (lo == 0ull ? 1ull : 0ull);
+                }
+                int sh;
+                const double dv = u128_to_double(hi, lo, &sh);
+                const int eb = ework[G.ea_off + i];
+                const int Ei = eb ? eb - EXP_BIAS : 0;
+                const double val = scale2(dv, sh + Ei + Fj - 2 * G.P);
+                G.C[i + (long long) j * G.ldc] = neg ? -val : val;
             }
-            int sh;
-            const double dv = u128_to_double(((unsigned long long) mg[3] << 32) | mg[2],
-                                             ((unsigned long long) mg[1] << 32) | mg[0], &sh);
-            const int eb = ework[G.ea_off + i];
-            const int Ei = eb ? eb - EXP_BIAS : 0;
-            const double val = scale2(dv, sh + Ei + Fj - 2 * G.P);
-            G.C[i + (long long) j * G.ldc] = neg ? -val : val;
         }
     }
 }
@@ -1061,7 +1035,7 @@ extern "C" int ca3dmm_crt_run_reconstruct(const ca3dmm_crt_plan_t *pl, int g0, i
     switch (pl->nmod) {
 #define CA3DMM_CRT_CASE(N)                                                                          \
     case N:                                                                                         \
-        crt_reconstruct_kernel<N><<<grid, 256, 0, stream>>>(groups, g0, r0, r1, w);                \
+        crt_reconstruct_kernel<N, crt_limbs(N)><<<grid, 256, 0, stream>>>(groups, g0, r0, r1, w);  \
         break;
         CA3DMM_CRT_CASE(8) CA3DMM_CRT_CASE(9) CA3DMM_CRT_CASE(10) CA3DMM_CRT_CASE(11)
         CA3DMM_CRT_CASE(12) CA3DMM_CRT_CASE(13) CA3DMM_CRT_CASE(14) CA3DMM_CRT_CASE(15)

@@ -161,6 +161,7 @@ __device__ __forceinline__ void slice16(const SliceDesc &d, unsigned char *__res
 
 template <int S>
 struct SliceWriter {
+    static constexpr int kMinBlocks = 4;
     static __device__ __forceinline__ void write16(const SliceDesc &d, unsigned char *__restrict__ work,
                                                    const unsigned long long *__restrict__ mwork,
                                                    int gr, int gl, const double (&x)[16])

@@ -216,7 +216,8 @@ oz_exp_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ desc
 // Pass 2 over the flat list of slicing tiles of one shape (padding rows and k
 // included: they hold zero digits).  W::write16 turns one row's 16
 // consecutive k elements into the operand bytes of the GEMM that follows
-// (INT8 slices, or residues modulo the moduli of the modular scheme).
+// (INT8 slices, or residues modulo the moduli of the modular scheme);
+// W::kMinBlocks is the occupancy the kernel is compiled for.
 //
 // KC: 16 rows x 256 k per tile.  Warp w loads rows 2w and 2w + 1 with
 // coalesced 16-byte loads (512 contiguous bytes per instruction), the tile is
@@ -229,7 +230,7 @@ oz_exp_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ desc
 constexpr int KC_SLOT = 18;                           // doubles per staged chunk (16 + 2 of padding)
 constexpr int KC_ROW = (KC_SK / 16) * KC_SLOT + 4;    // doubles per staged row
 template <class W>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, W::kMinBlocks)
 slice_kc_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ descs, int ndesc,
                    int total_tiles, unsigned char *__restrict__ work,
                    const unsigned long long *__restrict__ mwork)
@@ -288,7 +289,7 @@ slice_kc_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ de
 }
 
 template <class W>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(256, W::kMinBlocks)
 slice_rc_kernel(const double *__restrict__ src, const SliceDesc *__restrict__ descs, int ndesc,
                    int total_tiles, unsigned char *__restrict__ work,
                    const unsigned long long *__restrict__ mwork)
