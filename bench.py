@@ -4,10 +4,12 @@ Workload (N=1): square FP64 GEMM M=N=K=8000, transA=0, transB=0, the
 reference's 24-rank virtual grid 4x2x3 (cuboid 2000x4000x2667), entries
 sign*(1+u)*2^e with e uniform in [-8,8] (seeded hash).  A step is one
 ca3dmm_engine_exec over device-resident A and B (512 MB each, larger than
-L2, so no flush is needed).  The headline leg is the split-precision
-(Ozaki INT8 on tcgen05) GEMM when available, with the plain FP64 DMMA leg
-measured beside it; both legs' errors against the double-double oracle are
-measured on sampled entries.
+L2, so no flush is needed).  Three legs are measured, each with its error
+against the double-double oracle on sampled entries: plain FP64 (DMMA), split
+precision by INT8 slices (7 slices) and split precision by the modular scheme
+(one INT8 GEMM per modulus, the count the engine chooses for this k).  The
+headline is the fastest split leg whose error is no worse than the plain
+leg's.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -660,15 +662,25 @@ def main():
     assert eng_plain.ok, "engine init failed"
     eng_plain.set_gemm_mode(cb.GEMM_PLAIN)
     oz_slices = int(os.environ.get("CA3DMM_BENCH_SLICES", "7"))
+    crt_moduli = int(os.environ.get("CA3DMM_BENCH_MODULI", "0"))   # 0: the engine's choice
     eng_oz = engine()
     if not (eng_oz.ok and eng_oz.set_gemm_mode(cb.GEMM_OZAKI, oz_slices) == 0 and
             eng_oz.exec(dA, lda, dB, ldb, dC, m) == 0):
         raise RuntimeError("split-precision engine failed")
+    eng_crt = engine()
+    if not (eng_crt.ok and eng_crt.set_gemm_mode(cb.GEMM_CRT, crt_moduli) == 0 and
+            eng_crt.exec(dA, lda, dB, ldb, dC, m) == 0):
+        raise RuntimeError("modular split-precision engine failed")
+    engines = {"plain": eng_plain, "ozaki": eng_oz, "crt": eng_crt}
     legs["plain"] = leg(eng_plain, 1, args.warmup)
     legs["plain"]["err"] = sampled_error(dC, wl)
     legs["ozaki"] = leg(eng_oz, 1, args.warmup)
     legs["ozaki"]["err"] = sampled_error(dC, wl)
     legs["ozaki"]["slices"] = oz_slices
+    legs["crt"] = leg(eng_crt, 1, args.warmup)
+    legs["crt"]["err"] = sampled_error(dC, wl)
+    legs["crt"]["moduli"] = eng_crt.s.crt_moduli
+    legs["crt"]["bits"] = eng_crt.s.crt_bits
     if not btb and not args.no_slice_sweep:
         # the other slice counts: time and error of each (one timed exec)
         sweep = {}
@@ -683,6 +695,18 @@ def main():
                 sweep[str(sc)] = r
             e2.free()
         legs["ozaki_slice_sweep"] = sweep
+        # the neighbouring modulus counts of the modular scheme
+        msweep = {}
+        for nm in sorted({max(8, eng_crt.s.crt_moduli - 1), min(18, eng_crt.s.crt_moduli + 1)}):
+            e2 = engine()
+            if e2.ok and e2.set_gemm_mode(cb.GEMM_CRT, nm) == 0:
+                r = leg(e2, 2, 1)
+                r["err"] = sampled_error(dC, wl)
+                r["tflops"] = flops / (r["ms_per_step"] * 1e-3) / 1e12
+                r["bits"] = e2.s.crt_bits
+                msweep[str(nm)] = r
+            e2.free()
+        legs["crt_moduli_sweep"] = msweep
     if btb:
         # reported separately: C = B^T B is symmetric, and with
         # CA3DMM_BTB_SYMMETRIC=1 only its upper block triangle is computed and
@@ -700,12 +724,17 @@ def main():
             es.free()
         os.environ.pop("CA3DMM_BTB_SYMMETRIC", None)
         legs["btb_symmetric"] = symlegs
-    # the split-precision leg is the headline only while its error stays within
-    # twice the plain FP64 error (normwise and relative to |A||B|)
-    eo, ep = legs["ozaki"]["err"], legs["plain"]["err"]
-    head = "ozaki" if (eo["normwise"] <= 2 * ep["normwise"] and
-                       eo["vs_absprod"] <= 2 * ep["vs_absprod"]) else "plain"
-    eng = eng_oz if head == "ozaki" else eng_plain
+    # the headline is the fastest split-precision leg whose error against the
+    # double-double truth is no worse than the plain FP64 leg's (normwise and
+    # relative to |A||B|); plain FP64 when neither is
+    ep = legs["plain"]["err"]
+    head = "plain"
+    for cand in ("ozaki", "crt"):
+        ec = legs[cand]["err"]
+        if ec["normwise"] <= ep["normwise"] and ec["vs_absprod"] <= ep["vs_absprod"] and (
+                head == "plain" or legs[cand]["ms_per_step"] < legs[head]["ms_per_step"]):
+            head = cand
+    eng = engines[head]
 
     # timed region (headline leg), clocks sampled meanwhile
     sampler = ClockSampler(local)
@@ -722,8 +751,9 @@ def main():
     clocks = sampler.stop(i0, sampler.mark())
     ms = max_over_ranks(res["ms_per_step"], world)
     value = whole_job_tflops(flops, world, ms)
-    other = "plain" if head == "ozaki" else "ozaki"
-    legs[other].update(leg(eng_plain if other == "plain" else eng_oz, max(2, args.steps // 2), 1))
+    for other in engines:
+        if other != head:
+            legs[other].update(leg(engines[other], max(2, args.steps // 2), 1))
     legs[head].update(res)
 
     # e2e: the same exec through the C ABI with host buffers
@@ -746,15 +776,21 @@ def main():
     peaks = measured_peaks()
     traffic = ncu_traffic().get(wl["label"], {})
     gemm_ms = res["gemm_ms"]
-    if head == "ozaki":
+    int8_peak = 2.0 * peaks.get("bf16_tflops", 1590.0)
+    int8_src = ("of measured: 2 x measured dense bf16 (dense INT8 rate is twice the bf16 rate)"
+                if "bf16_tflops" in peaks else "of fallback")
+    if head == "crt":
+        nm = eng.s.crt_moduli
+        ops = flops * nm                        # one INT8 product per modulus
+        roof = {"bound": "tensor", "kernel": "crt_gemm_kernel",
+                "achieved": ops / (gemm_ms * 1e-3) / 1e12, "peak": int8_peak, "unit": "TFLOP/s",
+                "peak_source": int8_src, "traffic": traffic.get("crt_gemm_kernel")}
+    elif head == "ozaki":
         s = eng.s.ozaki_slices
         ops = flops * s * (s + 1) / 2           # INT8 ops of the slice products
-        peak = 2.0 * peaks.get("bf16_tflops", 1590.0)
         roof = {"bound": "tensor", "kernel": "oz_gemm_kernel",
-                "achieved": ops / (gemm_ms * 1e-3) / 1e12, "peak": peak, "unit": "TFLOP/s",
-                "peak_source": "of measured: 2 x measured dense bf16 (dense INT8 rate is twice "
-                               "the bf16 rate)" if "bf16_tflops" in peaks else "of fallback",
-                "traffic": traffic.get("oz_gemm_kernel")}
+                "achieved": ops / (gemm_ms * 1e-3) / 1e12, "peak": int8_peak, "unit": "TFLOP/s",
+                "peak_source": int8_src, "traffic": traffic.get("oz_gemm_kernel")}
     else:
         sm_mhz = peaks.get("sm_max_mhz", 1965.0)
         peak = 148 * 128 * sm_mhz * 1e6 / 1e12
@@ -766,17 +802,21 @@ def main():
     in_bytes = (0 if dA is None else dA.numel() * 8) + dB.numel() * 8
     # the metric's comparison, split precision against plain FP64 at their
     # errors against the double-double truth, as top-level keys
-    eo, ep = legs["ozaki"]["err"], legs["plain"]["err"]
+    split = head if head != "plain" else "crt"
+    eo, ep = legs[split]["err"], legs["plain"]["err"]
     plain_tf = flops / (legs["plain"]["ms_per_step"] * 1e-3) / 1e12
-    split_tf = flops / (legs["ozaki"]["ms_per_step"] * 1e-3) / 1e12
+    split_tf = flops / (legs[split]["ms_per_step"] * 1e-3) / 1e12
     out = {
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic",
         "config": {"workload": wl["desc"], "l2": wl["l2"]},
-        "gemm": head, "ozaki_slices": eng_oz.s.ozaki_slices,
+        "gemm": head, "split_leg": split, "ozaki_slices": eng_oz.s.ozaki_slices,
+        "crt_moduli": eng_crt.s.crt_moduli, "crt_bits": eng_crt.s.crt_bits,
         "plain_tflops": plain_tf, "split_tflops": split_tf,
+        "ozaki_tflops": flops / (legs["ozaki"]["ms_per_step"] * 1e-3) / 1e12,
+        "crt_tflops": flops / (legs["crt"]["ms_per_step"] * 1e-3) / 1e12,
         "split_over_plain": split_tf / plain_tf,
         "err_normwise_split": eo["normwise"], "err_normwise_plain": ep["normwise"],
         "err_vs_absprod_split": eo["vs_absprod"], "err_vs_absprod_plain": ep["vs_absprod"],

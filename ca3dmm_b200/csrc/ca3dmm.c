@@ -94,6 +94,10 @@ typedef struct {
     ca3dmm_oz_src_t *cs;
     ca3dmm_crt_group_t *cg;
     size_t off_crtplan, crt_plan_bytes, off_crt, crt_bytes;
+    int crt_band;                 /* tile rows per band of the device exec's CRT work list
+                                     (env CA3DMM_CRT_BAND, default 32 -- measured best at
+                                     8000^3; 0: all tile rows in one band) */
+    int upload_for_host;          /* the plan being uploaded serves exec_host's row bands */
     struct host_exec *hx;         /* state of ca3dmm_engine_exec_host (lazily created) */
 } plan_t;
 
@@ -332,6 +336,7 @@ static int plan_build(ca3dmm_engine_p e)
     int merge;
     GET_ENV_INT_VAR(merge, "CA3DMM_PLAIN_MERGE_SLABS", "plain_merge_slabs", 1, 0, 1);
     pl->merge_allowed = merge;
+    GET_ENV_INT_VAR(pl->crt_band, "CA3DMM_CRT_BAND", "crt_band", 32, 0, 1 << 20);
     pl->gd = (ca3dmm_dgemm_desc_t *) calloc((size_t) pl->ngroup * (size_t) pl->ksplit,
                                             sizeof(ca3dmm_dgemm_desc_t));
     pl->ob = (ca3dmm_oz_blk_t *) calloc((size_t) (pl->nA + pl->nB), sizeof(ca3dmm_oz_blk_t));
@@ -1033,7 +1038,11 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
                 g->C = out;
                 g->ldc = ldo;
             }
-            g->band = e->raster;
+            /* host-buffer exec: bands of the pipeline's rows; device exec: wide
+             * bands, so that one modulus' residues of op(A) stay in L2 while
+             * the tile columns stream through */
+            g->band = pl->upload_for_host ? e->raster
+                                          : (pl->crt_band > 0 ? pl->crt_band : (e->m + 127) / 128);
         }
         rc = ca3dmm_crt_plan_encode(&pl->crt, e->crt_moduli, ns, pl->cb, pl->cs, ns, pl->cb + ns,
                                     pl->cs + ns, ns, pl->cg, w + pl->off_crt, pl->crt_bytes,
@@ -1109,9 +1118,6 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
     int *status_d = (int *) (w + pl->off_status);
     if (crt) {
         rc = ca3dmm_crt_run_gemm(&pl->crt, NULL, status_d, 5.0, st);
-        if (!rc) rc = ca3dmm_crt_run_reconstruct(&pl->crt, 0, pl->crt_nsl, 0, INT32_MAX, st);
-        if (!rc) rc = ca3dmm_crt_run_nonfinite(&pl->crt, 0, pl->crt_nsl, 0, INT32_MAX, src_A, src_B,
-                                               st);
     } else if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
         rc = ca3dmm_oz_run_gemm(&pl->oz, status_d, 5.0, st);
         if (!rc) rc = ca3dmm_oz_run_nonfinite(&pl->oz, NULL, src_A, src_B, st);
@@ -1120,6 +1126,14 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
                                  pl->a_kmajor, status_d, 5.0, st);
     if (rc) return rc;
     if (timing) cudaEventRecord(pl->ev[2], st);
+    if (crt) {
+        /* the modular mode's reconstruction of C (with the slab sum below, the
+         * "reduce" phase of the timers) */
+        rc = ca3dmm_crt_run_reconstruct(&pl->crt, 0, pl->crt_nsl, 0, INT32_MAX, st);
+        if (!rc) rc = ca3dmm_crt_run_nonfinite(&pl->crt, 0, pl->crt_nsl, 0, INT32_MAX, src_A, src_B,
+                                               st);
+        if (rc) return rc;
+    }
     int whole = pl->has_dst && pl->dst_srow == 0 && pl->dst_scol == 0 && pl->dst_nrow == e->m &&
                 pl->dst_ncol == e->n;
     double *out = whole ? (double *) dst_C : (double *) (w + pl->off_cout);
@@ -1564,7 +1578,9 @@ static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_
     /* device plan for the staging buffers (rebuilt only when they change) */
     if (!pl->plan_valid || pl->c_A != dAsrc || pl->c_B != x->dB || pl->c_ldA != ldAsrc ||
         pl->c_ldB != x->ldb || pl->c_dst != x->dC || pl->c_ldC != x->ldc) {
+        pl->upload_for_host = 1;
         rc = plan_upload(e, dAsrc, (int) ldAsrc, x->dB, (int) x->ldb, x->dC, (int) x->ldc, st);
+        pl->upload_for_host = 0;
         if (rc) return rc;
         x->built_mode = -1;
         x->slab_built = 0;
