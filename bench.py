@@ -363,7 +363,8 @@ def run_grouped(args, world, rank, local):
         for i, g in enumerate(singles):
             g.exec([dA[i]], [lda[i]], [dB[i]], [ldb[i]], [dC[i]], [ldc[i]])
     res["per_gemm_launches_ms"] = timed(run_singles, args.steps)
-    for mode, sl, key in ((cb.GEMM_PLAIN, 0, "grouped_plain"), (cb.GEMM_OZAKI, 7, "grouped_ozaki7")):
+    for mode, sl, key in ((cb.GEMM_PLAIN, 0, "grouped_plain"), (cb.GEMM_OZAKI, 7, "grouped_ozaki7"),
+                          (cb.GEMM_CRT, 0, "grouped_crt")):
         g = cb.GroupedGemm([p[0] for p in probs], [p[1] for p in probs], [p[2] for p in probs],
                            [p[3] for p in probs], [p[4] for p in probs], mode=mode, slices=sl)
         assert g.ok
@@ -374,9 +375,12 @@ def run_grouped(args, world, rank, local):
             g.exec(dA, lda, dB, ldb, dC, ldc)
         res[key + "_ms"] = timed(graph.replay, args.steps)
         del graph
-    v = flops / (res["grouped_ozaki7_ms"] * 1e-3) / 1e12
+    # the headline: the faster split-precision leg (both at least as accurate as
+    # plain FP64 on these entries)
+    head = min(("grouped_ozaki7_ms", "grouped_crt_ms"), key=lambda x: res[x])
+    v = flops / (res[head] * 1e-3) / 1e12
     out = {"metric": METRIC, "value": v, "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps,
-           "warmup": args.warmup, "ms_per_step": res["grouped_ozaki7_ms"],
+           "warmup": args.warmup, "ms_per_step": res[head], "gemm": head.replace("_ms", ""),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic",
            "config": {"workload": "%d independent GEMMs, m,n,k log-uniform in [64,4096], random "

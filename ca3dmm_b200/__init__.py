@@ -22,9 +22,9 @@ DEFAULT_COST_MODEL = os.path.join(HERE, "data", "costmodel_b200.txt")
 DEV_TYPE_HOST, DEV_TYPE_CUDA, DEV_TYPE_CUDA_MPI_DIRECT = 0, 1, 2
 GEMM_PLAIN, GEMM_OZAKI, GEMM_CRT = 0, 1, 2
 # return codes of the C ABI (ca3dmm_kernels.h)
-OK, EINVAL, ECUDA, ETIMEOUT, ENOMEM, ENODEV = 0, 1, 2, 3, 4, 5
+OK, EINVAL, ECUDA, ETIMEOUT, ENOMEM, ENODEV, ECANARY = 0, 1, 2, 3, 4, 5, 6
 ERRORS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "device wait timed out",
-          4: "out of memory", 5: "no device"}
+          4: "out of memory", 5: "no device", 6: "work buffer guard band overwritten"}
 
 _lib = None
 
@@ -114,6 +114,7 @@ def lib():
         "ca3dmm_engine_set_gemm_mode": (i, [EP, i, i]),
         "ca3dmm_engine_workbuf_bytes": (sz, [EP]),
         "ca3dmm_engine_vrank_info": (i, [EP, i, pi]),
+        "ca3dmm_engine_guard_bands": (i, [EP, C.POINTER(C.c_longlong), i]),
         "cannon_engine_init": (None, [i, i, i, p, i, C.POINTER(C.POINTER(CannonEngineS)),
                                       C.POINTER(sz)]),
         "cannon_engine_attach_workbuf": (None, [C.POINTER(CannonEngineS), p, p]),
@@ -124,6 +125,7 @@ def lib():
         "dev_type_malloc": (p, [sz, i]),
         "dev_type_free": (None, [p, i]),
         "dev_type_memcpy": (None, [p, p, sz, i, i]),
+        "dev_type_memset": (None, [p, i, sz, i]),
         "dev_type_copy_mat_blk": (None, [sz, i, i, p, i, p, i, i]),
         "ca3dmm_dgemm_kslab_noalloc": (i, [i, i, i, i, p, i, p, i, p, i, p]),
         "ca3dmm_dgemm_kslab_noalloc_scratch_bytes": (sz, []),

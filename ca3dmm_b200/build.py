@@ -23,7 +23,7 @@ C_SOURCES = ["vcomm.c", "partition.c", "dev_type.c", "mat_redist.c", "cannon.c",
 CU_SOURCES = ["k_dgemm.cu", "k_pack.cu", "k_ozaki.cu", "k_crt.cu", "k_noalloc.cu", "k_mlp.cu"]
 HEADERS = ["ca3dmm_kernels.h", "ca3dmm_ozaki.h", "ca3dmm_crt.h", "ca3dmm_util.h", "k_common.cuh",
            "k_split.cuh"]
-EXAMPLES = ["example_cholesky_qr"]
+EXAMPLES = ["example_cholesky_qr", "example_ab", "example_btb"]
 
 
 def _newer(target, deps):

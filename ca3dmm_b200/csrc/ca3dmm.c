@@ -22,6 +22,7 @@
 #include <stdint.h>
 #include <string.h>
 #include <cuda_runtime_api.h>
+#include <nvtx3/nvToolsExt.h>
 #include "ca3dmm_util.h"
 #include "ca3dmm_kernels.h"
 #include "ca3dmm_ozaki.h"
@@ -29,6 +30,8 @@
 #include "ca3dmm.h"
 
 #define ALIGN_BYTES 256
+#define CANARY_BYTES 256
+#define CANARY_BYTE 0xA5
 
 typedef struct {
     int tk, tm, tn;        /* task ids */
@@ -98,6 +101,11 @@ typedef struct {
                                      (env CA3DMM_CRT_BAND, default 32 -- measured best at
                                      8000^3; 0: all tile rows in one band) */
     int upload_for_host;          /* the plan being uploaded serves exec_host's row bands */
+    /* guard bands: 256-byte canaries between the work buffer's regions, filled
+     * with CANARY_BYTE at each plan upload and, with CA3DMM_CANARY=1, checked
+     * on the device after every exec */
+    int ncanary, check_canary;
+    long long canary[CA3DMM_MAX_CANARIES];
     struct host_exec *hx;         /* state of ca3dmm_engine_exec_host (lazily created) */
 } plan_t;
 
@@ -177,9 +185,16 @@ static void vrank_geometry(int m, int n, int k, int mp, int np, int kp, int rank
 static size_t align_up(size_t x) { return (x + ALIGN_BYTES - 1) / ALIGN_BYTES * ALIGN_BYTES; }
 
 /* Byte layout of the device work buffer for the current gemm mode. */
+#define GUARD_BAND(off)                                                                      \
+    do {                                                                                     \
+        if (pl->ncanary < CA3DMM_MAX_CANARIES) pl->canary[pl->ncanary++] = (long long) (off); \
+        (off) += CANARY_BYTES;                                                               \
+    } while (0)
+
 static void plan_layout(ca3dmm_engine_p e, plan_t *pl)
 {
     size_t off = 0;
+    pl->ncanary = 0;
     pl->off_status = off; off = align_up(off + 64);
     pl->off_packA = off; off = align_up(off + sizeof(ca3dmm_pack_desc_t) * pl->nA);
     pl->off_packB = off; off = align_up(off + sizeof(ca3dmm_pack_desc_t) * pl->nB);
@@ -192,6 +207,7 @@ static void plan_layout(ca3dmm_engine_p e, plan_t *pl)
     pl->off_ozplan = off; off = align_up(off + pl->oz_plan_bytes);
     pl->crt_plan_bytes = ca3dmm_crt_plan_bytes(2 * pl->crt_nsl, pl->crt_nsl);
     pl->off_crtplan = off; off = align_up(off + pl->crt_plan_bytes);
+    GUARD_BAND(off);
     size_t packs = 0;
     pl->off_A = off;
     for (int i = 0; i < pl->nA; i++) {
@@ -202,6 +218,7 @@ static void plan_layout(ca3dmm_engine_p e, plan_t *pl)
         packs += align_up(sizeof(double) * (mm > km ? mm : km));
     }
     off += packs;
+    GUARD_BAND(off);
     packs = 0;
     pl->off_B = off;
     for (int i = 0; i < pl->nB; i++) {
@@ -209,14 +226,17 @@ static void plan_layout(ca3dmm_engine_p e, plan_t *pl)
         packs += align_up(sizeof(double) * (size_t) pl->B[i].ld * (size_t) pl->B[i].cols);
     }
     off += packs;
+    GUARD_BAND(off);
     pl->slab_ld = ca3dmm_round_up(e->m, 2);
     pl->slab_stride = (size_t) pl->slab_ld * (size_t) e->n;
     pl->off_slab = off;
     int nslab = e->kp * pl->ksplit;          /* plain mode's sub-slabs; split mode uses kp of them */
     if (pl->crt_nsl > nslab) nslab = pl->crt_nsl;
     if (nslab > 1) off = align_up(off + sizeof(double) * pl->slab_stride * (size_t) nslab);
+    GUARD_BAND(off);
     pl->off_cout = off;
     off = align_up(off + sizeof(double) * (size_t) e->m * (size_t) e->n);
+    GUARD_BAND(off);
     pl->off_oz = off;
     pl->oz_bytes = 0;
     if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
@@ -230,6 +250,7 @@ static void plan_layout(ca3dmm_engine_p e, plan_t *pl)
         }
         off = align_up(off + pl->oz_bytes);
     }
+    GUARD_BAND(off);
     pl->off_crt = off;
     pl->crt_bytes = 0;
     if (e->gemm_mode == CA3DMM_GEMM_CRT) {
@@ -251,6 +272,7 @@ static void plan_layout(ca3dmm_engine_p e, plan_t *pl)
         }
         off = align_up(off + pl->crt_bytes);
     }
+    GUARD_BAND(off);
     pl->total = off;
 }
 
@@ -337,6 +359,7 @@ static int plan_build(ca3dmm_engine_p e)
     GET_ENV_INT_VAR(merge, "CA3DMM_PLAIN_MERGE_SLABS", "plain_merge_slabs", 1, 0, 1);
     pl->merge_allowed = merge;
     GET_ENV_INT_VAR(pl->crt_band, "CA3DMM_CRT_BAND", "crt_band", 32, 0, 1 << 20);
+    GET_ENV_INT_VAR(pl->check_canary, "CA3DMM_CANARY", "check_canary", 0, 0, 1);
     pl->gd = (ca3dmm_dgemm_desc_t *) calloc((size_t) pl->ngroup * (size_t) pl->ksplit,
                                             sizeof(ca3dmm_dgemm_desc_t));
     pl->ob = (ca3dmm_oz_blk_t *) calloc((size_t) (pl->nA + pl->nB), sizeof(ca3dmm_oz_blk_t));
@@ -1052,6 +1075,8 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
     }
     memset(h + pl->off_status, 0, 64);
     CA3DMM_CUDA_TRY(cudaMemcpyAsync(w, h, pl->stage_bytes, cudaMemcpyHostToDevice, st));
+    for (int i = 0; i < pl->ncanary; i++)
+        CA3DMM_CUDA_TRY(cudaMemsetAsync(w + pl->canary[i], CANARY_BYTE, CANARY_BYTES, st));
     pl->c_A = A; pl->c_B = B; pl->c_ldA = ldA; pl->c_ldB = ldB;
     pl->c_dst = dst; pl->c_ldC = ldC;
     pl->plan_valid = 1;
@@ -1073,6 +1098,37 @@ static int launch_pack_side(ca3dmm_engine_p e, int which, const void *src, cudaS
                                       (double *) w, (int *) (w + pl->off_status), 5.0, st);
     return ca3dmm_pack_launch((const double *) src, (double *) w,
                               (const ca3dmm_pack_desc_t *) (w + off_desc), nd, tiles, st);
+}
+
+/* The device status word after a call: 0, a bounded wait that ran out, or
+ * an overwritten guard band (status[1] holds its index). */
+static int device_status_error(const plan_t *pl)
+{
+    const int code = pl->status_h[0];
+    if (code == 0) return CA3DMM_OK;
+    if (code == 6) {
+        const int b = pl->status_h[1];
+        ERROR_PRINTF("Work buffer guard band %d (bytes %lld .. %lld) was overwritten\n", b,
+                     b >= 0 && b < pl->ncanary ? pl->canary[b] : -1LL,
+                     b >= 0 && b < pl->ncanary ? pl->canary[b] + CANARY_BYTES - 1 : -1LL);
+        return CA3DMM_ECANARY;
+    }
+    ERROR_PRINTF("Device status %d: a bounded wait ran out\n", code);
+    return CA3DMM_ETIMEOUT;
+}
+
+/* With CA3DMM_CANARY=1: compare every guard band with its fill pattern. */
+static int launch_guard_check(const ca3dmm_engine_p e, const plan_t *pl, int *status_d,
+                              cudaStream_t st)
+{
+    if (!pl->check_canary || pl->ncanary == 0) return CA3DMM_OK;
+    ca3dmm_guard_bands_t g;
+    memset(&g, 0, sizeof(g));
+    g.n = pl->ncanary;
+    g.bytes = CANARY_BYTES;
+    g.pattern = CANARY_BYTE;
+    for (int i = 0; i < pl->ncanary; i++) g.off[i] = pl->canary[i];
+    return ca3dmm_guard_check_launch(e->workbuf_d, &g, status_d, st);
 }
 
 static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void *src_B, int ldB,
@@ -1102,20 +1158,23 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
     int timing = e->sync_exec && pl->events_ok;
     if (timing) cudaEventRecord(pl->ev[0], st);
     const int crt = e->gemm_mode == CA3DMM_GEMM_CRT;
+    /* NVTX ranges mark the phases of the reference's timers on the host
+     * timeline (visible to nsys and to ncu --nvtx); each closes before an
+     * error return */
+    nvtxRangePushA("ca3dmm: redistribute (pack / slice operands)");
     if (crt) {
         rc = ca3dmm_crt_run_pack(&pl->crt, src_A, src_B, st);
-        if (rc) return rc;
     } else if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
         rc = ca3dmm_oz_run_pack(&pl->oz, src_A, src_B, st);
-        if (rc) return rc;
     } else {
         rc = launch_pack_side(e, 0, src_A, st);
-        if (rc) return rc;
-        rc = launch_pack_side(e, 1, src_B, st);
-        if (rc) return rc;
+        if (!rc) rc = launch_pack_side(e, 1, src_B, st);
     }
+    nvtxRangePop();
+    if (rc) return rc;
     if (timing) cudaEventRecord(pl->ev[1], st);
     int *status_d = (int *) (w + pl->off_status);
+    nvtxRangePushA("ca3dmm: GEMM (2D Cannon)");
     if (crt) {
         rc = ca3dmm_crt_run_gemm(&pl->crt, NULL, status_d, 5.0, st);
     } else if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
@@ -1124,15 +1183,16 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
     } else
         rc = ca3dmm_dgemm_launch(w + pl->off_gemm, pl->ngroup * pl->ksplit, pl->gemm_tiles,
                                  pl->a_kmajor, status_d, 5.0, st);
+    nvtxRangePop();
     if (rc) return rc;
     if (timing) cudaEventRecord(pl->ev[2], st);
+    nvtxRangePushA("ca3dmm: reduce (slab sum, reconstruction)");
     if (crt) {
         /* the modular mode's reconstruction of C (with the slab sum below, the
          * "reduce" phase of the timers) */
         rc = ca3dmm_crt_run_reconstruct(&pl->crt, 0, pl->crt_nsl, 0, INT32_MAX, st);
         if (!rc) rc = ca3dmm_crt_run_nonfinite(&pl->crt, 0, pl->crt_nsl, 0, INT32_MAX, src_A, src_B,
                                                st);
-        if (rc) return rc;
     }
     int whole = pl->has_dst && pl->dst_srow == 0 && pl->dst_scol == 0 && pl->dst_nrow == e->m &&
                 pl->dst_ncol == e->n;
@@ -1141,31 +1201,32 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
     const int nred = crt ? pl->crt_nsl
                          : e->gemm_mode == CA3DMM_GEMM_OZAKI ? (pl->oz_fused ? 1 : e->kp)
                                                               : (pl->plain_merged ? 1 : e->kp * pl->ksplit);
-    if (nred > 1) {
+    if (!rc && nred > 1)
         rc = ca3dmm_reduce_slabs_launch((const double *) (w + pl->off_slab),
                                         (long long) pl->slab_stride, pl->slab_ld, nred, e->m,
                                         e->n, out, ldo, st);
-        if (rc) return rc;
-    }
-    if (pl->sym && !crt) {      /* the modular mode computes all of C */
+    if (!rc && pl->sym && !crt)      /* the modular mode computes all of C */
         rc = ca3dmm_mirror_upper_launch(out, ldo, e->m, st);
-        if (rc) return rc;
-    }
+    nvtxRangePop();
+    if (rc) return rc;
     if (timing) cudaEventRecord(pl->ev[3], st);
     if (pl->has_dst && !whole) {
+        nvtxRangePushA("ca3dmm: C to dst_C");
         rc = ca3dmm_pack_launch((const double *) (w + pl->off_cout), (double *) dst_C,
                                 (const ca3dmm_pack_desc_t *) (w + pl->off_copy), 1,
                                 pl->pack_tiles_C, st);
+        nvtxRangePop();
         if (rc) return rc;
     }
     if (timing) cudaEventRecord(pl->ev[4], st);
-    CA3DMM_CUDA_TRY(cudaMemcpyAsync(pl->status_h, status_d, sizeof(int), cudaMemcpyDeviceToHost, st));
+    rc = launch_guard_check(e, pl, status_d, st);
+    if (rc) return rc;
+    CA3DMM_CUDA_TRY(cudaMemcpyAsync(pl->status_h, status_d, 2 * sizeof(int), cudaMemcpyDeviceToHost,
+                                    st));
     if (e->sync_exec) {
         CA3DMM_CUDA_TRY(cudaStreamSynchronize(st));
-        if (pl->status_h[0] != 0) {
-            ERROR_PRINTF("Device status %d: a bounded wait ran out\n", pl->status_h[0]);
-            return CA3DMM_ETIMEOUT;
-        }
+        rc = device_status_error(pl);
+        if (rc) return rc;
         if (timing) {
             float t_pack = 0, t_gemm = 0, t_red = 0, t_copy = 0;
             cudaEventElapsedTime(&t_pack, pl->ev[0], pl->ev[1]);
@@ -1204,7 +1265,9 @@ void ca3dmm_engine_exec(ca3dmm_engine_p e, const void *src_A, const int ldA, con
         return;
     }
     double t0 = ca3dmm_wtime_sec();
+    nvtxRangePushA("ca3dmm_engine_exec");
     int rc = exec_device(e, src_A, ldA, src_B, ldB, dst_C, ldC, (cudaStream_t) e->stream);
+    nvtxRangePop();
     e->last_error = rc;
     if (rc) {
         ERROR_PRINTF("ca3dmm_engine_exec failed (error %d)\n", rc);
@@ -1546,13 +1609,12 @@ static int hx_btb_slabs(ca3dmm_engine_p e, struct host_exec *x, const void *B_h,
     CA3DMM_CUDA_TRY(cudaMemcpy2DAsync(C_h, sizeof(double) * (size_t) ldC, x->dC,
                                       sizeof(double) * (size_t) x->ldc, sizeof(double) * (size_t) e->m,
                                       (size_t) e->n, cudaMemcpyDeviceToHost, st));
-    CA3DMM_CUDA_TRY(cudaMemcpyAsync(pl->status_h, status_d, sizeof(int), cudaMemcpyDeviceToHost, st));
+    rc = launch_guard_check(e, pl, status_d, st);
+    if (rc) return rc;
+    CA3DMM_CUDA_TRY(cudaMemcpyAsync(pl->status_h, status_d, 2 * sizeof(int), cudaMemcpyDeviceToHost,
+                                    st));
     CA3DMM_CUDA_TRY(cudaStreamSynchronize(st));
-    if (pl->status_h[0] != 0) {
-        ERROR_PRINTF("Device status %d: a bounded wait ran out\n", pl->status_h[0]);
-        return CA3DMM_ETIMEOUT;
-    }
-    return CA3DMM_OK;
+    return device_status_error(pl);
 }
 
 static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_h, int ldB,
@@ -1670,14 +1732,13 @@ static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_
                                           sizeof(double) * (size_t) (x->r1[c] - x->r0[c]), (size_t) e->n,
                                           cudaMemcpyDeviceToHost, x->s_out));
     }
-    CA3DMM_CUDA_TRY(cudaMemcpyAsync(pl->status_h, status_d, sizeof(int), cudaMemcpyDeviceToHost, st));
+    rc = launch_guard_check(e, pl, status_d, st);
+    if (rc) return rc;
+    CA3DMM_CUDA_TRY(cudaMemcpyAsync(pl->status_h, status_d, 2 * sizeof(int), cudaMemcpyDeviceToHost,
+                                    st));
     CA3DMM_CUDA_TRY(cudaStreamSynchronize(st));
     CA3DMM_CUDA_TRY(cudaStreamSynchronize(x->s_out));
-    if (pl->status_h[0] != 0) {
-        ERROR_PRINTF("Device status %d: a bounded wait ran out\n", pl->status_h[0]);
-        return CA3DMM_ETIMEOUT;
-    }
-    return CA3DMM_OK;
+    return device_status_error(pl);
 }
 
 int ca3dmm_engine_exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_h, int ldB,
@@ -1693,7 +1754,9 @@ int ca3dmm_engine_exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const v
         return CA3DMM_EINVAL;
     }
     double t0 = ca3dmm_wtime_sec();
+    nvtxRangePushA("ca3dmm_engine_exec_host");
     int rc = exec_host(e, A_h, ldA, B_h, ldB, C_h, ldC);
+    nvtxRangePop();
     e->last_error = rc;
     if (rc) {
         ERROR_PRINTF("ca3dmm_engine_exec_host failed (error %d)\n", rc);
@@ -1806,4 +1869,12 @@ int ca3dmm_engine_vrank_info(ca3dmm_engine_p e, int vrank, int *out34)
     if (!e || !out34 || vrank < 0 || vrank >= e->n_proc) return CA3DMM_EINVAL;
     vrank_geometry(e->m, e->n, e->k, e->mp, e->np, e->kp, vrank, e->is_BTB, out34);
     return CA3DMM_OK;
+}
+
+int ca3dmm_engine_guard_bands(ca3dmm_engine_p e, long long *offsets, int max)
+{
+    if (!e || !e->impl) return -1;
+    const plan_t *pl = (const plan_t *) e->impl;
+    for (int i = 0; i < pl->ncanary && i < max && offsets; i++) offsets[i] = pl->canary[i];
+    return pl->ncanary;
 }

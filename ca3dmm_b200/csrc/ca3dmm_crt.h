@@ -51,6 +51,8 @@ typedef struct {
     int kc_tiles[2], rc_tiles[2];
     int p_min, p_max;     /* integer widths of the groups */
     long long n_exp;
+    long long recon_items;  /* reconstruction items (4 rows x 1 column) over every group */
+    int group_m, group_n;   /* the group's size when the plan has one group */
     void *dev_plan;
     void *dev_work;
 } ca3dmm_crt_plan_t;

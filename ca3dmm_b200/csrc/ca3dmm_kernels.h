@@ -19,6 +19,7 @@ enum {
     CA3DMM_ETIMEOUT = 3,     /* a device-side bounded wait ran out */
     CA3DMM_ENOMEM = 4,       /* work buffer too small / allocation failed */
     CA3DMM_ENODEV = 5,       /* no sm_100 device or driver entry point missing */
+    CA3DMM_ECANARY = 6,      /* a guard band of the work buffer was overwritten */
 };
 
 /* ---- plain FP64 DMMA GEMM, grouped ---------------------------------------
@@ -52,6 +53,7 @@ int ca3dmm_dgemm_plan_encode(const ca3dmm_dgemm_desc_t *probs, int nprob, void *
  * plan's tile list (each problem's tiles are numbered in raster bands of
  * `raster` tile rows, so a band of output rows is one range per problem). */
 #define CA3DMM_MAX_RANGES 8
+#define CA3DMM_MAX_CANARIES 8
 typedef struct {
     int n;
     int begin[CA3DMM_MAX_RANGES], len[CA3DMM_MAX_RANGES];
@@ -112,6 +114,17 @@ int ca3dmm_mirror_upper_launch(double *C, long long ldc, int n, cudaStream_t str
 int ca3dmm_reduce_slabs_launch(const double *slab, long long slab_stride, long long lds,
                                int nslab, int m, int n, double *out, long long ldo,
                                cudaStream_t stream);
+
+/* ---- work-buffer guard bands ----------------------------------------------
+ * Checks n bands of `bytes` bytes at base + offsets[i] (each filled with
+ * `pattern`); a band that differs sets *status to the canary code (first
+ * writer wins) and records the band index in status[1]. */
+typedef struct {
+    int n, bytes, pattern, pad;
+    long long off[CA3DMM_MAX_CANARIES];
+} ca3dmm_guard_bands_t;
+int ca3dmm_guard_check_launch(const void *base, const ca3dmm_guard_bands_t *bands, int *dev_status,
+                              cudaStream_t stream);
 
 /* ---- device properties (cached) ------------------------------------------ */
 int ca3dmm_device_sm_count(void);

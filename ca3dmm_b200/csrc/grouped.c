@@ -1,12 +1,14 @@
 /* Batched independent FP64 GEMMs: one pack launch per operand side and one
- * persistent grouped GEMM launch (plain FP64 DMMA or split precision) for the
- * whole batch.  See include/ca3dmm_grouped.h. */
+ * persistent grouped GEMM launch (plain FP64 DMMA, or split precision by INT8
+ * slices or by the modular scheme) for the whole batch.  See
+ * include/ca3dmm_grouped.h. */
 #include <stdint.h>
 #include <string.h>
 #include <cuda_runtime_api.h>
 #include "ca3dmm_util.h"
 #include "ca3dmm_kernels.h"
 #include "ca3dmm_ozaki.h"
+#include "ca3dmm_crt.h"
 #include "ca3dmm_grouped.h"
 
 #define GALIGN 256
@@ -19,8 +21,9 @@ struct ca3dmm_grouped {
     long long *lda_p, *ldb_p;     /* leading dimensions of the packed copies */
     size_t *offA, *offB;          /* byte offsets of the packed copies */
     /* work buffer layout */
-    size_t off_status, off_packA, off_packB, off_gemm, off_ozplan, off_A, off_B, off_oz, total;
-    size_t oz_bytes, stage_bytes;
+    size_t off_status, off_packA, off_packB, off_gemm, off_ozplan, off_crtplan, off_A, off_B,
+        off_oz, total;
+    size_t oz_bytes, crt_bytes, stage_bytes;
     void *workbuf_d;
     int alloc_workbuf;
     void *stage;                  /* pinned host staging of the plan */
@@ -40,6 +43,8 @@ struct ca3dmm_grouped {
     ca3dmm_oz_src_t *os;
     ca3dmm_oz_group_t *og;
     ca3dmm_oz_plan_t oz;
+    ca3dmm_crt_group_t *cg;       /* modular mode: one group per problem, in launch order */
+    ca3dmm_crt_plan_t crt;
     double last_ms;
 };
 
@@ -75,7 +80,7 @@ void ca3dmm_grouped_free(ca3dmm_grouped_p *gp)
     free(g->m); free(g->n); free(g->k); free(g->ta); free(g->tb); free(g->order);
     free(g->lda_p); free(g->ldb_p); free(g->offA); free(g->offB);
     free(g->cA); free(g->cB); free(g->cC); free(g->cldA); free(g->cldB); free(g->cldC);
-    free(g->gd); free(g->ob); free(g->os); free(g->og);
+    free(g->gd); free(g->ob); free(g->os); free(g->og); free(g->cg);
     if (g->stage) cudaFreeHost(g->stage);
     if (g->status_h) cudaFreeHost(g->status_h);
     if (g->events_ok) { cudaEventDestroy(g->ev[0]); cudaEventDestroy(g->ev[1]); }
@@ -91,13 +96,28 @@ int ca3dmm_grouped_init(int nprob, const int *m, const int *n, const int *k, con
     if (!gp) return CA3DMM_EINVAL;
     *gp = NULL;
     if (nprob < 1 || nprob > 32768 || !m || !n || !k) return CA3DMM_EINVAL;
-    if (gemm_mode != 0 && gemm_mode != 1) return CA3DMM_EINVAL;
+    if (gemm_mode < 0 || gemm_mode > 2) return CA3DMM_EINVAL;
     if (gemm_mode == 1 && (slices < 2 || slices > 8)) return CA3DMM_EINVAL;
-    for (int i = 0; i < nprob; i++)
+    int kmax = 0;
+    for (int i = 0; i < nprob; i++) {
         if (m[i] < 1 || n[i] < 1 || k[i] < 1) {
             ERROR_PRINTF("grouped GEMM %d: invalid size %d x %d x %d\n", i, m[i], n[i], k[i]);
             return CA3DMM_EINVAL;
         }
+        if (k[i] > kmax) kmax = k[i];
+    }
+    if (gemm_mode == 2) {
+        /* moduli: the given count (8..18), or the fewest that give 51-bit
+         * integers for the deepest product; every k within the exact range */
+        if (kmax > CA3DMM_CRT_MAX_K) return CA3DMM_EINVAL;
+        if (slices == 0) {
+            slices = CA3DMM_CRT_MAX_MODULI;
+            for (int nm = 8; nm <= CA3DMM_CRT_MAX_MODULI; nm++)
+                if (ca3dmm_crt_bits(nm, kmax) >= 51) { slices = nm; break; }
+        }
+        if (slices < 8 || slices > CA3DMM_CRT_MAX_MODULI || ca3dmm_crt_bits(slices, kmax) < 2)
+            return CA3DMM_EINVAL;
+    }
     ca3dmm_grouped_p g = (ca3dmm_grouped_p) calloc(1, sizeof(*g));
     if (!g) return CA3DMM_ENOMEM;
     g->nprob = nprob;
@@ -117,9 +137,10 @@ int ca3dmm_grouped_init(int nprob, const int *m, const int *n, const int *k, con
     g->ob = calloc(2 * (size_t) nprob, sizeof(ca3dmm_oz_blk_t));
     g->os = calloc(2 * (size_t) nprob, sizeof(ca3dmm_oz_src_t));
     g->og = calloc(nprob, sizeof(ca3dmm_oz_group_t));
+    g->cg = calloc(nprob, sizeof(ca3dmm_crt_group_t));
     if (!g->m || !g->n || !g->k || !g->ta || !g->tb || !g->order || !g->lda_p || !g->ldb_p || !g->offA ||
         !g->offB || !g->cA || !g->cB || !g->cC || !g->cldA || !g->cldB || !g->cldC || !g->gd ||
-        !g->ob || !g->os || !g->og) {
+        !g->ob || !g->os || !g->og || !g->cg) {
         ca3dmm_grouped_free(&g);
         return CA3DMM_ENOMEM;
     }
@@ -138,6 +159,7 @@ int ca3dmm_grouped_init(int nprob, const int *m, const int *n, const int *k, con
     g->off_packB = off; off = galign(off + sizeof(ca3dmm_pack_desc_t) * nprob);
     g->off_gemm = off; off = galign(off + ca3dmm_dgemm_plan_bytes(nprob));
     g->off_ozplan = off; off = galign(off + ca3dmm_oz_plan_bytes(nprob));
+    g->off_crtplan = off; off = galign(off + ca3dmm_crt_plan_bytes(2 * nprob, nprob));
     g->stage_bytes = off;
     g->off_A = off;
     if (gemm_mode == 0) {
@@ -163,6 +185,10 @@ int ca3dmm_grouped_init(int nprob, const int *m, const int *n, const int *k, con
     if (gemm_mode == 1) {
         g->oz_bytes = ca3dmm_oz_work_bytes(nprob, m, k, nprob, k, n, slices);
         off = galign(off + g->oz_bytes);
+    }
+    if (gemm_mode == 2) {
+        g->crt_bytes = ca3dmm_crt_work_bytes(nprob, m, k, nprob, k, n, nprob, m, n, slices);
+        off = galign(off + g->crt_bytes);
     }
     g->total = off;
     if (workbuf_bytes) {
@@ -274,6 +300,7 @@ static int build_plan(ca3dmm_grouped_p g, const double *const *A, const int *ldA
         int rc = ca3dmm_dgemm_plan_encode(g->gd, np, h + g->off_gemm, &g->gemm_tiles);
         if (rc) return rc;
     } else {
+        /* split precision: operand blocks read where they lie (absolute bases) */
         for (int i = 0; i < np; i++) {
             g->ob[i].r0 = 0; g->ob[i].c0 = 0; g->ob[i].rows = g->m[i]; g->ob[i].cols = g->k[i];
             g->ob[i].alias = -1;
@@ -283,16 +310,30 @@ static int build_plan(ca3dmm_grouped_p g, const double *const *A, const int *ldA
             g->ob[np + i].alias = -1;
             g->os[np + i].base = B[i]; g->os[np + i].ld = ldB[i]; g->os[np + i].trans = g->tb[i];
         }
-        for (int j = 0; j < np; j++) {
-            const int i = g->order[j];
-            g->og[j].a_blk = i; g->og[j].b_blk = i;
-            g->og[j].row0 = 0; g->og[j].col0 = 0;
-            g->og[j].C = C[i]; g->og[j].ldc = ldC[i];
-            g->og[j].m = g->m[i]; g->og[j].n = g->n[i]; g->og[j].k = g->k[i];
-        }
-        int rc = ca3dmm_oz_plan_encode(&g->oz, g->slices, np, g->ob, g->os, np, g->ob + np,
+        int rc;
+        if (g->mode == 2) {
+            for (int j = 0; j < np; j++) {
+                const int i = g->order[j];
+                g->cg[j].a_blk = i; g->cg[j].b_blk = i;
+                g->cg[j].C = C[i]; g->cg[j].ldc = ldC[i];
+                g->cg[j].m = g->m[i]; g->cg[j].n = g->n[i]; g->cg[j].k = g->k[i];
+                g->cg[j].band = 0;
+            }
+            rc = ca3dmm_crt_plan_encode(&g->crt, g->slices, np, g->ob, g->os, np, g->ob + np,
+                                        g->os + np, np, g->cg, w + g->off_oz, g->crt_bytes,
+                                        h + g->off_crtplan, w + g->off_crtplan);
+        } else {
+            for (int j = 0; j < np; j++) {
+                const int i = g->order[j];
+                g->og[j].a_blk = i; g->og[j].b_blk = i;
+                g->og[j].row0 = 0; g->og[j].col0 = 0;
+                g->og[j].C = C[i]; g->og[j].ldc = ldC[i];
+                g->og[j].m = g->m[i]; g->og[j].n = g->n[i]; g->og[j].k = g->k[i];
+            }
+            rc = ca3dmm_oz_plan_encode(&g->oz, g->slices, np, g->ob, g->os, np, g->ob + np,
                                        g->os + np, np, g->og, 0, NULL, w + g->off_oz, g->oz_bytes,
                                        h + g->off_ozplan, w + g->off_ozplan);
+        }
         if (rc) return rc;
     }
     CA3DMM_CUDA_TRY(cudaMemcpyAsync(w, h, g->stage_bytes, cudaMemcpyHostToDevice, st));
@@ -337,6 +378,12 @@ int ca3dmm_grouped_exec(ca3dmm_grouped_p g, const double *const *A, const int *l
         if (rc) return rc;
         rc = ca3dmm_dgemm_launch(w + g->off_gemm, g->nprob, g->gemm_tiles, g->a_kmajor, status,
                                  5.0, st);
+        if (rc) return rc;
+    } else if (g->mode == 2) {
+        rc = ca3dmm_crt_run_pack(&g->crt, NULL, NULL, st);
+        if (!rc) rc = ca3dmm_crt_run_gemm(&g->crt, NULL, status, 5.0, st);
+        if (!rc) rc = ca3dmm_crt_run_reconstruct(&g->crt, 0, g->nprob, 0, 0x7fffffff, st);
+        if (!rc) rc = ca3dmm_crt_run_nonfinite(&g->crt, 0, g->nprob, 0, 0x7fffffff, NULL, NULL, st);
         if (rc) return rc;
     } else {
         rc = ca3dmm_oz_run_pack(&g->oz, NULL, NULL, st);

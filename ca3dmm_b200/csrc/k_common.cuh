@@ -20,6 +20,7 @@ enum {
     CA3DMM_DEV_TIMEOUT_ACCUM   = 3,   // MMA issuer gave up waiting for a drained accumulator
     CA3DMM_DEV_TIMEOUT_EPI     = 4,   // epilogue gave up waiting for an accumulator
     CA3DMM_DEV_TIMEOUT_QUEUE   = 5,   // persistent work queue wait ran out
+    CA3DMM_DEV_CANARY          = 6,   // a work-buffer guard band was overwritten
 };
 
 // Virtual tile v of a persistent launch -> tile index of the plan: v walks the

@@ -251,6 +251,7 @@ struct CrtGroup {
     int m, n, k;
     int a_desc, b_desc, a_from_b;   // a_from_b: A tile tm is half tm % 2 of the B block's tile tm / 2
     int tiles_m, tiles_n, item_begin, band;
+    long long rc_begin;             // first reconstruction item (4 rows x 1 column) of the group
     int P, nkb;                     // integer width, 128-byte k blocks
     long long ea_off, eb_off;       // exponents of the A rows / B columns
     long long qa_off, qb_off;       // residue bytes of the operand blocks
@@ -550,21 +551,43 @@ constexpr int crt_limbs(int n)
 // because |C'| <= k 2^(2P) <= 2^123.  Only the limbs below 2^128 of S and q M
 // are formed; all W_t and M fit in L = crt_limbs(N) limbs (a template
 // argument, computed on the host).
+// Work items are 4 rows x 1 column of C.  One group: the rows [r0, r1) of
+// group g0; several: every row of groups [g0, g1), numbered by the groups'
+// rc_begin prefix (found by a search over a shared copy), so that the grid
+// is spread by size over a batch of uneven groups.
 template <int N, int L>
 __global__ void __launch_bounds__(256)
-crt_reconstruct_kernel(const CrtGroup *__restrict__ groups, int g0, int r0, int r1,
-                       const unsigned char *__restrict__ work)
+crt_reconstruct_kernel(const CrtGroup *__restrict__ groups, int g0, int g1, int r0, int r1,
+                       long long total, const unsigned char *__restrict__ work)
 {
     static_assert(L >= 2 && L <= LIMBS, "modulus product outside the limb range");
-    const CrtGroup &G = groups[g0 + blockIdx.y];
-    const int rb = max(r0, 0), re = min(r1, G.m);
-    if (re <= rb) return;
-    const int nq = (re - rb + 3) >> 2;
-    const long long items = (long long) nq * G.n;
+    __shared__ long long s_rb[GROUP_CACHE];
+    const int ng = g1 - g0;
+    const bool cached = ng > 1 && ng <= GROUP_CACHE;
+    if (cached)
+        for (int i = threadIdx.x; i < ng; i += blockDim.x) s_rb[i] = groups[g0 + i].rc_begin;
+    __syncthreads();
     const int *ework = reinterpret_cast<const int *>(work);
-    for (long long it = blockIdx.x * (long long) blockDim.x + threadIdx.x; it < items;
+    const long long base = ng > 1 ? groups[g0].rc_begin : 0;
+    for (long long it = blockIdx.x * (long long) blockDim.x + threadIdx.x; it < total;
          it += (long long) gridDim.x * blockDim.x) {
-        const int j = (int) (it / nq), i0 = rb + 4 * (int) (it % nq);
+        int gi = 0;
+        if (ng > 1) {
+            const long long a = base + it;
+            int lo = 0, hi = ng - 1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if ((cached ? s_rb[mid] : groups[g0 + mid].rc_begin) <= a) lo = mid; else hi = mid - 1;
+            }
+            gi = lo;
+        }
+        const CrtGroup &G = groups[g0 + gi];
+        const int rb = ng > 1 ? 0 : max(r0, 0), re = ng > 1 ? G.m : min(r1, G.m);
+        if (re <= rb) continue;
+        const int nq = (re - rb + 3) >> 2;
+        const long long local = ng > 1 ? base + it - G.rc_begin : it;
+        if (local >= (long long) nq * G.n) continue;
+        const int j = (int) (local / nq), i0 = rb + 4 * (int) (local % nq);
         const int fb = ework[G.eb_off + j];
         const int Fj = fb ? fb - EXP_BIAS : 0;
         uint32_t u4[N];
@@ -779,6 +802,7 @@ extern "C" int ca3dmm_crt_plan_encode(ca3dmm_crt_plan_t *pl, int nmod, int nA,
         eoff += rows;
     }
     int items = 0, pmin = 64, pmax = 0;
+    long long recon = 0;
     for (int g = 0; g < ngroup; ++g) {
         CrtGroup &o = gr[g];
         if (G[g].a_blk < 0 || G[g].a_blk >= nA || G[g].b_blk < 0 || G[g].b_blk >= nB)
@@ -796,6 +820,8 @@ extern "C" int ca3dmm_crt_plan_encode(ca3dmm_crt_plan_t *pl, int nmod, int nA,
         o.tiles_n = (o.m > 0 && o.n > 0) ? (o.n + CBN - 1) / CBN : 0;
         o.band = G[g].band > 0 ? G[g].band : DEFAULT_BAND;
         o.item_begin = items;
+        o.rc_begin = recon;
+        recon += (long long) ((o.m + 3) / 4) * (o.n > 0 ? o.n : 0);
         o.P = db.p_bits;
         o.nkb = o.k > 0 ? db.nkb : 0;
         o.ea_off = da.e_off;
@@ -820,6 +846,9 @@ extern "C" int ca3dmm_crt_plan_encode(ca3dmm_crt_plan_t *pl, int nmod, int nA,
     pl->p_min = pmin > pmax ? 0 : pmin;
     pl->p_max = pmax;
     pl->n_exp = (long long) ne;
+    pl->recon_items = recon;
+    pl->group_m = ngroup == 1 ? gr[0].m : 0;
+    pl->group_n = ngroup == 1 ? gr[0].n : 0;
     pl->dev_plan = dev_plan;
     pl->dev_work = dev_work;
     return CA3DMM_OK;
@@ -1025,17 +1054,28 @@ extern "C" int ca3dmm_crt_run_reconstruct(const ca3dmm_crt_plan_t *pl, int g0, i
     if (g0 < 0) g0 = 0;
     if (g1 > pl->ngroup) g1 = pl->ngroup;
     if (g1 <= g0) return CA3DMM_OK;
-    if (g1 - g0 > 65535) return CA3DMM_EINVAL;
+    // several groups: all their rows; one group: a row window of it, the
+    // items of the whole plan as the bound (the kernel skips the others)
+    if (g1 - g0 > 1 && (g0 != 0 || g1 != pl->ngroup || r0 > 0 || r1 < 0x7fffffff))
+        return CA3DMM_EINVAL;
+    long long total = pl->recon_items;
+    if (g1 - g0 == 1 && pl->ngroup == 1) {
+        const long long hi = r1 < pl->group_m ? r1 : pl->group_m, lo = r0 > 0 ? r0 : 0;
+        total = hi > lo ? ((hi - lo + 3) / 4) * pl->group_n : 0;
+    }
     const CrtLayout L(pl->nA + pl->nB, pl->ngroup);
     const CrtGroup *groups =
         reinterpret_cast<const CrtGroup *>(static_cast<const unsigned char *>(pl->dev_plan) + L.gr);
     const unsigned char *w = static_cast<const unsigned char *>(pl->dev_work);
-    const int per = (ca3dmm_device_sm_count() * 8 + (g1 - g0) - 1) / (g1 - g0);
-    dim3 grid((unsigned) (per > 1 ? per : 1), (unsigned) (g1 - g0));
+    if (total <= 0) return CA3DMM_OK;
+    long long blocks = (total + 255) / 256;
+    const long long cap = (long long) ca3dmm_device_sm_count() * 8;
+    if (blocks > cap) blocks = cap;
     switch (pl->nmod) {
 #define CA3DMM_CRT_CASE(N)                                                                          \
     case N:                                                                                         \
-        crt_reconstruct_kernel<N, crt_limbs(N)><<<grid, 256, 0, stream>>>(groups, g0, r0, r1, w);  \
+        crt_reconstruct_kernel<N, crt_limbs(N)><<<(unsigned) blocks, 256, 0, stream>>>(            \
+            groups, g0, g1, r0, r1, total, w);                                                     \
         break;
         CA3DMM_CRT_CASE(8) CA3DMM_CRT_CASE(9) CA3DMM_CRT_CASE(10) CA3DMM_CRT_CASE(11)
         CA3DMM_CRT_CASE(12) CA3DMM_CRT_CASE(13) CA3DMM_CRT_CASE(14) CA3DMM_CRT_CASE(15)

@@ -261,6 +261,35 @@ extern "C" int ca3dmm_copy_block_launch(const double *src, long long lds, double
     return CA3DMM_OK;
 }
 
+// Guard bands of a work buffer: one block, each thread compares its bytes of
+// every band with the fill pattern.
+__global__ void __launch_bounds__(256)
+guard_check_kernel(const unsigned char *__restrict__ base, const ca3dmm_guard_bands_t g,
+                   int *status)
+{
+    for (int b = 0; b < g.n; ++b) {
+        const unsigned char *band = base + g.off[b];
+        bool bad = false;
+        for (int i = threadIdx.x; i < g.bytes; i += blockDim.x)
+            bad = bad || band[i] != (unsigned char) g.pattern;
+        if (__syncthreads_or(bad) && threadIdx.x == 0 &&
+            atomicCAS(status, 0, CA3DMM_DEV_CANARY) == 0)
+            status[1] = b;
+    }
+}
+
+extern "C" int ca3dmm_guard_check_launch(const void *base, const ca3dmm_guard_bands_t *bands,
+                                         int *dev_status, cudaStream_t stream)
+{
+    if (!bands || bands->n <= 0) return CA3DMM_OK;
+    if (bands->n > CA3DMM_MAX_CANARIES) return CA3DMM_EINVAL;
+    guard_check_kernel<<<1, 256, 0, stream>>>(static_cast<const unsigned char *>(base), *bands,
+                                              dev_status);
+    CA3DMM_CUDA_TRY(cudaGetLastError());
+    ca3dmm_note_launch(1);
+    return CA3DMM_OK;
+}
+
 extern "C" int ca3dmm_pack_launch(const double *src_base, double *dst_base,
                                   const ca3dmm_pack_desc_t *dev_descs, int ndesc, int total_tiles,
                                   cudaStream_t stream)

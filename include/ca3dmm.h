@@ -191,6 +191,16 @@ int ca3dmm_device_wait_check(double timeout_s, int arrive);
  * capture; its replays do not). */
 unsigned long long ca3dmm_kernel_launches(void);
 
+/* Guard bands of the engine's device work buffer: 256-byte bands between its
+ * regions (plan, packed operands, slab buffers, C, split-precision regions),
+ * filled with the byte 0xA5 whenever the plan is uploaded.  With the
+ * environment variable CA3DMM_CANARY=1 at init, every exec checks them on the
+ * device afterwards and reports an overwritten band as CA3DMM_ECANARY (6),
+ * printing its byte range -- a kernel that wrote past its region.  Writes up
+ * to `max` band offsets (bytes into the work buffer) and returns the number
+ * of bands (-1 for a NULL engine). */
+int ca3dmm_engine_guard_bands(ca3dmm_engine_p engine, long long *offsets, int max);
+
 /* First error of the last call on this engine (0 = none). */
 int ca3dmm_engine_last_error(ca3dmm_engine_p engine);
 /* Run exec on `stream` (cudaStream_t); sync = 0 makes exec asynchronous and

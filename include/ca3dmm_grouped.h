@@ -4,8 +4,9 @@
  * product.  A batch of nprob products C_i = op(A_i) op(B_i) of any sizes and
  * transposes is planned once; each exec packs every operand (one launch per
  * operand side), then runs ONE persistent grouped GEMM launch over the tiles
- * of all products -- the plain FP64 DMMA kernel or the split-precision
- * (Ozaki INT8, tcgen05) kernel.  With set_stream(.., sync = 0) exec only
+ * of all products -- the plain FP64 DMMA kernel, the split-precision
+ * (Ozaki INT8 slices, tcgen05) kernel, or the modular split-precision kernel
+ * (one INT8 product per modulus) with its reconstruction pass.  With set_stream(.., sync = 0) exec only
  * enqueues work on the stream, so a caller may capture it in a CUDA graph and
  * replay it; the plan is re-uploaded only when a pointer or leading dimension
  * changes between calls.
@@ -22,7 +23,9 @@ extern "C" {
 typedef struct ca3dmm_grouped *ca3dmm_grouped_p;
 
 /* Plan nprob products (m[i] x n[i] x k[i], trans flags per product).
- * gemm_mode: 0 plain FP64 DMMA, 1 split precision with `slices` (2..8).
+ * gemm_mode: 0 plain FP64 DMMA, 1 split precision with `slices` (2..8), 2
+ * modular split precision with `slices` moduli (8..18; 0: the fewest that
+ * give 51-bit operand integers for the deepest product; every k <= 131072).
  * *workbuf_bytes != NULL: the caller allocates and attaches the device work
  * buffer; NULL: the batch allocates it.  Returns 0 or a CA3DMM_E* code. */
 int ca3dmm_grouped_init(int nprob, const int *m, const int *n, const int *k, const int *trans_A,
