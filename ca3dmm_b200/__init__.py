@@ -20,7 +20,7 @@ LIB_PATH = os.path.join(HERE, "libca3dmm_b200.so")
 DEFAULT_COST_MODEL = os.path.join(HERE, "data", "costmodel_b200.txt")
 
 DEV_TYPE_HOST, DEV_TYPE_CUDA, DEV_TYPE_CUDA_MPI_DIRECT = 0, 1, 2
-GEMM_PLAIN, GEMM_OZAKI, GEMM_CRT = 0, 1, 2
+GEMM_PLAIN, GEMM_OZAKI, GEMM_CRT, GEMM_AUTO = 0, 1, 2, 3
 # return codes of the C ABI (ca3dmm_kernels.h)
 OK, EINVAL, ECUDA, ETIMEOUT, ENOMEM, ENODEV, ECANARY = 0, 1, 2, 3, 4, 5, 6
 ERRORS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "device wait timed out",
@@ -56,15 +56,31 @@ class Ca3dmmEngineS(C.Structure):
         ("ozaki_slices", C.c_int), ("last_error", C.c_int), ("stream", C.c_void_p),
         ("sync_exec", C.c_int), ("workbuf_bytes", C.c_size_t), ("impl", C.c_void_p),
         ("raster", C.c_int), ("btb_symmetric", C.c_int), ("crt_moduli", C.c_int),
-        ("crt_bits", C.c_int)]
+        ("crt_bits", C.c_int), ("gemm_auto", C.c_int), ("tune_ms", C.c_double)]
 
 
 class TuneCfg(C.Structure):
     """Mirror of ca3dmm_tune_cfg_t (include/ca3dmm_tune.h)."""
-    _fields_ = [("gemm_mode", C.c_int), ("slices", C.c_int), ("kp", C.c_int), ("raster", C.c_int)]
+    _fields_ = [("gemm_mode", C.c_int), ("slices", C.c_int), ("kp", C.c_int), ("raster", C.c_int),
+                ("tile_n", C.c_int)]
+
+    def tuple(self):
+        return (self.gemm_mode, self.slices, self.kp, self.raster, self.tile_n)
 
 
-NFEAT = 12
+def _cfg(c):
+    """(mode, slices, kp, raster[, tile_n]) -> TuneCfg"""
+    c = tuple(c)
+    return TuneCfg(*(c + (0,) * (5 - len(c))))
+
+
+NFEAT = 14
+
+
+class Transport(C.Structure):
+    """Mirror of ca3dmm_transport_t (include/ca3dmm_dist.h)."""
+    _fields_ = [("rank", C.c_int), ("size", C.c_int), ("device_buffers", C.c_int),
+                ("ctx", C.c_void_p), ("allgather_ll", C.c_void_p), ("alltoallv_d", C.c_void_p)]
 
 
 class CannonEngineS(C.Structure):
@@ -141,10 +157,27 @@ def lib():
         "ca3dmm_tune_measure": (i, [i, i, i, i, i, p, i, p, i, p, i, C.POINTER(TuneCfg), i,
                                     C.POINTER(C.c_float)]),
         "ca3dmm_autotune": (i, [i, i, i, i, i, p, i, p, i, p, i, C.POINTER(TuneCfg), i, C.c_float,
-                                p, i, i, pi, C.POINTER(C.c_float)]),
+                                p, i, i, pi, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
+        "ca3dmm_engine_set_tune": (i, [EP, C.POINTER(TuneCfg)]),
+        "ca3dmm_transport_threads_create": (i, [i, C.POINTER(Transport)]),
+        "ca3dmm_transport_threads_free": (None, [C.POINTER(Transport)]),
+        "ca3dmm_nccl_unique_id": (i, [C.POINTER(C.c_ubyte)]),
+        "ca3dmm_transport_nccl_create": (i, [i, i, C.POINTER(C.c_ubyte), C.POINTER(Transport)]),
+        "ca3dmm_transport_nccl_free": (None, [C.POINTER(Transport)]),
+        "ca3dmm_dist_engine_init": (i, [i] * 18 + [pi, C.POINTER(Transport), i, i, C.POINTER(p)]),
+        "ca3dmm_dist_engine_exec": (i, [p, p, i, p, i, p, i]),
+        "ca3dmm_dist_engine_info": (i, [p, pi]),
+        "ca3dmm_dist_engine_counts": (i, [p] + [C.POINTER(C.c_longlong)] * 4),
+        "ca3dmm_dist_engine_stats": (i, [p, C.POINTER(C.c_double)]),
+        "ca3dmm_dist_engine_free": (None, [C.POINTER(p)]),
+        "ca3dmm_engine_get_tune": (i, [EP, C.POINTER(TuneCfg)]),
+        "ca3dmm_engine_autotune": (i, [EP, p, i, p, i, p, i, i, C.POINTER(TuneCfg)]),
+        "ca3dmm_engine_tune_report": (i, [EP, C.POINTER(TuneCfg), C.POINTER(C.c_float),
+                                          C.POINTER(C.c_float), i]),
         "ca3dmm_mlp_create": (i, [i, i, i, C.c_ulonglong, C.POINTER(p)]),
         "ca3dmm_mlp_free": (None, [C.POINTER(p)]),
         "ca3dmm_mlp_nparams": (i, [p]),
+        "ca3dmm_mlp_inputs": (i, [p]),
         "ca3dmm_mlp_get_params": (i, [p, C.POINTER(C.c_float)]),
         "ca3dmm_mlp_set_params": (i, [p, C.POINTER(C.c_float)]),
         "ca3dmm_mlp_set_normalisation": (i, [p, C.POINTER(C.c_float), C.POINTER(C.c_float)]),
@@ -287,6 +320,34 @@ class Ca3dmmEngine:
         """Tile rows per raster band of the GEMM tile order (L2 reuse)."""
         return lib().ca3dmm_engine_set_raster(self.e, int(raster))
 
+    def set_tune(self, cfg):
+        """ca3dmm_engine_set_tune: (mode, slices, kp, raster[, tile_n])."""
+        c = _cfg(cfg)
+        return lib().ca3dmm_engine_set_tune(self.e, C.byref(c))
+
+    def get_tune(self):
+        c = TuneCfg()
+        lib().ca3dmm_engine_get_tune(self.e, C.byref(c))
+        return c.tuple()
+
+    def autotune(self, A, ldA, B, ldB, Cout, ldC, how=1):
+        """ca3dmm_engine_autotune (how: 0 off, 1 model, 2 exhaustive); returns
+        (rc, chosen configuration)."""
+        c = TuneCfg()
+        rc = lib().ca3dmm_engine_autotune(self.e, _ptr(A), int(ldA), _ptr(B), int(ldB),
+                                          _ptr(Cout), int(ldC), int(how), C.byref(c))
+        return rc, c.tuple()
+
+    def tune_report(self):
+        """[(configuration, ms, guard error)] of the last tuning (ms -1 not
+        timed, -2 rejected by the accuracy guard)."""
+        n = 32
+        cf = (TuneCfg * n)()
+        ms = (C.c_float * n)()
+        er = (C.c_float * n)()
+        got = lib().ca3dmm_engine_tune_report(self.e, cf, ms, er, n)
+        return [(cf[i].tuple(), ms[i], er[i]) for i in range(max(0, min(got, n)))]
+
     def required_workbuf_bytes(self):
         return lib().ca3dmm_engine_workbuf_bytes(self.e)
 
@@ -317,6 +378,74 @@ class Ca3dmmEngine:
     def free(self):
         if self.e:
             lib().ca3dmm_engine_free(C.byref(self.e))
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class ThreadTransports:
+    """ca3dmm_transport_threads_create: `size` transports for ranks that are
+    threads of this process (host-staged exchange)."""
+
+    def __init__(self, size):
+        self.arr = (Transport * size)()
+        self.rc = lib().ca3dmm_transport_threads_create(int(size), self.arr)
+
+    def __getitem__(self, r):
+        return self.arr[r]
+
+    def free(self):
+        if self.rc == 0 and self.arr[0].ctx:
+            lib().ca3dmm_transport_threads_free(self.arr)
+
+
+class DistEngine:
+    """Python mirror of ca3dmm_dist_engine_{init,exec,info,counts,stats,free}:
+    one rank of the multi-GPU engine over a ca3dmm_transport_t.  Rectangles
+    are (srow, nrow, scol, ncol)."""
+
+    def __init__(self, m, n, k, ta, tb, src_A, src_B, dst_C, transport, proc_grid=None,
+                 btb=False, gemm_mode=GEMM_PLAIN, slices=0):
+        self.h = C.c_void_p()
+        self.size = transport.size
+        grid = (C.c_int * 3)(*proc_grid) if proc_grid is not None else None
+        a = list(src_A) if src_A is not None else [0, 0, 0, 0]
+        self.rc = lib().ca3dmm_dist_engine_init(int(m), int(n), int(k), int(ta), int(tb),
+                                                int(bool(btb)), *[int(x) for x in a],
+                                                *[int(x) for x in src_B],
+                                                *[int(x) for x in dst_C], grid,
+                                                C.byref(transport), int(gemm_mode), int(slices),
+                                                C.byref(self.h))
+
+    @property
+    def ok(self):
+        return self.rc == 0 and bool(self.h)
+
+    def exec(self, A, ldA, B, ldB, Cout, ldC):
+        return lib().ca3dmm_dist_engine_exec(self.h, _ptr(A), int(ldA), _ptr(B), int(ldB),
+                                             _ptr(Cout), int(ldC))
+
+    def info(self):
+        out = (C.c_int * 10)()
+        lib().ca3dmm_dist_engine_info(self.h, out)
+        return list(out)
+
+    def counts(self):
+        arrs = [(C.c_longlong * self.size)() for _ in range(4)]
+        lib().ca3dmm_dist_engine_counts(self.h, *arrs)
+        return [list(a) for a in arrs]
+
+    def stats(self):
+        out = (C.c_double * 4)()
+        n = lib().ca3dmm_dist_engine_stats(self.h, out)
+        return n, list(out)
+
+    def free(self):
+        if self.h:
+            lib().ca3dmm_dist_engine_free(C.byref(self.h))
 
     def __del__(self):
         try:
@@ -449,7 +578,7 @@ def _fp(a):
 def tune_features(m, n, k, ta, tb, cfg, spread):
     import numpy as np
     out = np.zeros(NFEAT, dtype=np.float32)
-    c = TuneCfg(*cfg)
+    c = _cfg(cfg)
     rc = lib().ca3dmm_tune_features(m, n, k, ta, tb, C.byref(c), float(spread),
                                     out.ctypes.data_as(C.POINTER(C.c_float)))
     if rc:
@@ -534,24 +663,27 @@ class CostModel:
 
 
 def autotune(m, n, k, ta, tb, A, ldA, B, ldB, Cm, ldC, cands, spread=0.0, model=None, topk=2,
-             reps=2):
-    """Run ca3dmm_autotune; returns (best index, measured ms per candidate or -1)."""
+             reps=2, with_err=False):
+    """Run ca3dmm_autotune; returns (best index, ms per candidate: -1 not
+    timed, -2 rejected by the accuracy guard[, guard errors])."""
     import numpy as np
-    arr = (TuneCfg * len(cands))(*[TuneCfg(*c) for c in cands])
+    arr = (TuneCfg * len(cands))(*[_cfg(c) for c in cands])
     best = C.c_int()
     ms = np.zeros(len(cands), dtype=np.float32)
+    er = np.zeros(len(cands), dtype=np.float32)
     rc = lib().ca3dmm_autotune(m, n, k, ta, tb, _ptr(A), ldA, _ptr(B), ldB, _ptr(Cm), ldC, arr,
                                len(cands), float(spread), model.h if model is not None else None,
                                int(topk), int(reps), C.byref(best),
-                               ms.ctypes.data_as(C.POINTER(C.c_float)))
+                               ms.ctypes.data_as(C.POINTER(C.c_float)),
+                               er.ctypes.data_as(C.POINTER(C.c_float)))
     if rc:
         raise RuntimeError("autotune failed: %d" % rc)
-    return best.value, ms
+    return (best.value, ms, er) if with_err else (best.value, ms)
 
 
 def measure(m, n, k, ta, tb, A, ldA, B, ldB, Cm, ldC, cfg, reps=2):
     t = C.c_float()
-    c = TuneCfg(*cfg)
+    c = _cfg(cfg)
     rc = lib().ca3dmm_tune_measure(m, n, k, ta, tb, _ptr(A), ldA, _ptr(B), ldB, _ptr(Cm), ldC,
                                    C.byref(c), int(reps), C.byref(t))
     return (t.value if rc == 0 else None)

@@ -19,11 +19,12 @@ NVCC = os.path.join(CUDA, "bin", "nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 
 C_SOURCES = ["vcomm.c", "partition.c", "dev_type.c", "mat_redist.c", "cannon.c", "ca3dmm.c",
-             "grouped.c", "autotune.c"]
-CU_SOURCES = ["k_dgemm.cu", "k_pack.cu", "k_ozaki.cu", "k_crt.cu", "k_noalloc.cu", "k_mlp.cu"]
+             "grouped.c", "autotune.c", "dist.c", "transport.c"]
+CU_SOURCES = ["k_dgemm.cu", "k_pack.cu", "k_ozaki.cu", "k_crt.cu", "k_noalloc.cu", "k_mlp.cu",
+              "k_tune_guard.cu"]
 HEADERS = ["ca3dmm_kernels.h", "ca3dmm_ozaki.h", "ca3dmm_crt.h", "ca3dmm_util.h", "k_common.cuh",
-           "k_split.cuh"]
-EXAMPLES = ["example_cholesky_qr", "example_ab", "example_btb"]
+           "k_split.cuh", "ca3dmm_tune_guard.h", "ca3dmm_tune_internal.h"]
+EXAMPLES = ["example_cholesky_qr", "example_ab", "example_btb", "example_ab_dist"]
 
 
 def _newer(target, deps):
@@ -61,7 +62,8 @@ def build(verbose=False):
             _run([NVCC] + ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
                                   "-I", INC, "-I", CSRC, "-c", s, "-o", o])
     if _newer(LIB, objs):
-        _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs + ["-lm"])
+        _run([NVCC] + ARCH + ["-shared", "-cudart", "static", "-o", LIB] + objs +
+             ["-lm", "-lpthread", "-ldl"])
     # the static archive beside the shared library, as the reference installs both
     # (src/common.make:1-2, 56-66); link with -lcudart_static -lstdc++ -ldl -lpthread -lrt
     if _newer(ARCHIVE, objs):
@@ -75,7 +77,7 @@ def build(verbose=False):
         if _newer(b, [s, LIB] + hdrs):
             _run(["gcc", "-O2", "-std=gnu11", "-I", INC, "-I", os.path.join(CUDA, "include"), s,
                   "-o", b, "-L", HERE, "-lca3dmm_b200", "-Wl,-rpath,$ORIGIN/..",
-                  "-L", os.path.join(CUDA, "lib64"), "-lcudart", "-lm"])
+                  "-L", os.path.join(CUDA, "lib64"), "-lcudart", "-lm", "-lpthread"])
     if verbose:
         print("built", LIB)
     return LIB

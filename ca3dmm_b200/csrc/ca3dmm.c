@@ -21,6 +21,7 @@
 #include <math.h>
 #include <stdint.h>
 #include <string.h>
+#include <strings.h>
 #include <cuda_runtime_api.h>
 #include <nvtx3/nvToolsExt.h>
 #include "ca3dmm_util.h"
@@ -28,6 +29,7 @@
 #include "ca3dmm_ozaki.h"
 #include "ca3dmm_crt.h"
 #include "ca3dmm.h"
+#include "ca3dmm_tune_internal.h"
 
 #define ALIGN_BYTES 256
 #define CANARY_BYTES 256
@@ -100,6 +102,8 @@ typedef struct {
     int crt_band;                 /* tile rows per band of the device exec's CRT work list
                                      (env CA3DMM_CRT_BAND, default 32 -- measured best at
                                      8000^3; 0: all tile rows in one band) */
+    int crt_band_env;             /* crt_band as the environment set it */
+    int crt_tile_n;               /* CRT GEMM tile columns, 128 or 256 (env CA3DMM_CRT_TILE_N) */
     int upload_for_host;          /* the plan being uploaded serves exec_host's row bands */
     /* guard bands: 256-byte canaries between the work buffer's regions, filled
      * with CANARY_BYTE at each plan upload and, with CA3DMM_CANARY=1, checked
@@ -107,6 +111,7 @@ typedef struct {
     int ncanary, check_canary;
     long long canary[CA3DMM_MAX_CANARIES];
     struct host_exec *hx;         /* state of ca3dmm_engine_exec_host (lazily created) */
+    ca3dmm_tune_report_t report;  /* the candidates of the last tuning */
 } plan_t;
 
 /* ca3dmm_engine_exec_host: device staging of A, B and C and the row-band
@@ -359,6 +364,9 @@ static int plan_build(ca3dmm_engine_p e)
     GET_ENV_INT_VAR(merge, "CA3DMM_PLAIN_MERGE_SLABS", "plain_merge_slabs", 1, 0, 1);
     pl->merge_allowed = merge;
     GET_ENV_INT_VAR(pl->crt_band, "CA3DMM_CRT_BAND", "crt_band", 32, 0, 1 << 20);
+    pl->crt_band_env = pl->crt_band;
+    GET_ENV_INT_VAR(pl->crt_tile_n, "CA3DMM_CRT_TILE_N", "crt_tile_n", 256, 128, 256);
+    if (pl->crt_tile_n != 128) pl->crt_tile_n = 256;
     GET_ENV_INT_VAR(pl->check_canary, "CA3DMM_CANARY", "check_canary", 0, 0, 1);
     pl->gd = (ca3dmm_dgemm_desc_t *) calloc((size_t) pl->ngroup * (size_t) pl->ksplit,
                                             sizeof(ca3dmm_dgemm_desc_t));
@@ -576,6 +584,78 @@ static void fill_rank0_fields(ca3dmm_engine_p e)
 }
 
 /* Shared tail of both init functions: plan, sizes, optional allocation. */
+/* ---------------------------------------------------------------------------
+ * Tuning support: the candidate configurations of this engine and the work
+ * buffer each needs. */
+
+int ca3dmm_engine_crt_resolve(ca3dmm_engine_p e, int want) { return crt_resolve(e, want); }
+
+size_t ca3dmm_engine_layout_bytes(ca3dmm_engine_p e, int mode, int count)
+{
+    plan_t *pl = (plan_t *) e->impl;
+    const int om = e->gemm_mode, os = e->ozaki_slices, oc = e->crt_moduli;
+    const size_t kept = pl->total;
+    e->gemm_mode = mode;
+    if (mode == CA3DMM_GEMM_OZAKI) e->ozaki_slices = count;
+    if (mode == CA3DMM_GEMM_CRT) e->crt_moduli = crt_resolve(e, count);
+    size_t need = 0;
+    if (mode != CA3DMM_GEMM_CRT || e->crt_moduli > 0) {
+        plan_layout(e, pl);
+        need = pl->total;
+    }
+    e->gemm_mode = om;
+    e->ozaki_slices = os;
+    e->crt_moduli = oc;
+    plan_layout(e, pl);
+    if (pl->total < kept) pl->total = kept;
+    return need;
+}
+
+/* Plain FP64 at raster 8 and 16; 7 and 8 INT8 slices; the modular mode at the
+ * fewest moduli for 51-bit integers with 256- and 128-column tiles and bands
+ * of 32 and 8 tile rows, and two moduli more (for operands whose exponent
+ * spread the accuracy guard rejects at the fewest).  Candidate 0 is the plain
+ * GEMM, the guard's reference. */
+int ca3dmm_engine_candidates(ca3dmm_engine_p e, ca3dmm_tune_cfg_t *c, int max)
+{
+    ca3dmm_tune_cfg_t l[CA3DMM_TUNE_MAX_CANDS];
+    int n = 0;
+#define CA3DMM_CAND(md, sl, r, tn)                                                           \
+    do {                                                                                     \
+        l[n].gemm_mode = (md); l[n].slices = (sl); l[n].kp = e->kp;                          \
+        l[n].raster = (r); l[n].tile_n = (tn); n++;                                          \
+    } while (0)
+    CA3DMM_CAND(CA3DMM_GEMM_PLAIN, 0, 8, 0);
+    CA3DMM_CAND(CA3DMM_GEMM_PLAIN, 0, 16, 0);
+    CA3DMM_CAND(CA3DMM_GEMM_OZAKI, 7, 8, 0);
+    CA3DMM_CAND(CA3DMM_GEMM_OZAKI, 7, 16, 0);
+    CA3DMM_CAND(CA3DMM_GEMM_OZAKI, 8, 8, 0);
+    const int nm = crt_resolve(e, 0);
+    if (nm > 0) {
+        CA3DMM_CAND(CA3DMM_GEMM_CRT, nm, 32, 256);
+        CA3DMM_CAND(CA3DMM_GEMM_CRT, nm, 8, 256);
+        CA3DMM_CAND(CA3DMM_GEMM_CRT, nm, 32, 128);
+        CA3DMM_CAND(CA3DMM_GEMM_CRT, nm, 8, 128);
+        const int nm2 = nm + 2 <= CA3DMM_CRT_MAX_MODULI ? nm + 2 : CA3DMM_CRT_MAX_MODULI;
+        if (nm2 != nm && crt_resolve(e, nm2) == nm2) CA3DMM_CAND(CA3DMM_GEMM_CRT, nm2, 32, 256);
+    }
+#undef CA3DMM_CAND
+    for (int i = 0; i < n && i < max && c; i++) c[i] = l[i];
+    return n;
+}
+
+static size_t auto_bytes(ca3dmm_engine_p e)
+{
+    ca3dmm_tune_cfg_t c[CA3DMM_TUNE_MAX_CANDS];
+    const int n = ca3dmm_engine_candidates(e, c, CA3DMM_TUNE_MAX_CANDS);
+    size_t mx = 0;
+    for (int i = 0; i < n; i++) {
+        const size_t b = ca3dmm_engine_layout_bytes(e, c[i].gemm_mode, c[i].slices);
+        if (b > mx) mx = b;
+    }
+    return mx;
+}
+
 static void finish_init(ca3dmm_engine_p e, int dst_srow, int dst_nrow, int dst_scol, int dst_ncol,
                         ca3dmm_engine_p *engine_, size_t *workbuf_bytes, double t0)
 {
@@ -604,7 +684,15 @@ static void finish_init(ca3dmm_engine_p e, int dst_srow, int dst_nrow, int dst_s
         ce->gemm_cycle = 1;
     }
     int gm;
-    GET_ENV_INT_VAR(gm, "CA3DMM_GEMM_MODE", "gemm_mode", 0, 0, 2);
+    const char *gms = getenv("CA3DMM_GEMM_MODE");
+    if (gms && strcasecmp(gms, "auto") == 0) {
+        INFO_PRINTF("Overriding parameter gemm_mode: 0 (default) --> auto (runtime)\n");
+        gm = CA3DMM_GEMM_AUTO;
+    } else {
+        GET_ENV_INT_VAR(gm, "CA3DMM_GEMM_MODE", "gemm_mode", 0, 0, 3);
+    }
+    e->gemm_auto = gm == CA3DMM_GEMM_AUTO ? 1 : 0;
+    if (gm == CA3DMM_GEMM_AUTO) gm = CA3DMM_GEMM_PLAIN;   /* until the tuner chooses */
     e->gemm_mode = gm;
     int cm;
     GET_ENV_INT_VAR(cm, "CA3DMM_CRT_MODULI", "crt_moduli", 0, 0, CA3DMM_CRT_MAX_MODULI);
@@ -643,6 +731,11 @@ static void finish_init(ca3dmm_engine_p e, int dst_srow, int dst_nrow, int dst_s
         pl->dst_scol = dst_scol; pl->dst_ncol = dst_ncol;
     }
     e->n_group = pl->ngroup;
+    if (e->gemm_auto) {
+        /* a work buffer that holds every candidate of the tuner */
+        const size_t need = auto_bytes(e);
+        if (pl->total < need) pl->total = need;
+    }
     e->workbuf_bytes = pl->total;
     e->self_workbuf_bytes = pl->total;
     GET_ENV_INT_VAR(e->print_timing, "CA3DMM_PRINT_TIMING", "engine->print_timing", 0, 0, 1);
@@ -1066,6 +1159,7 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
              * the tile columns stream through */
             g->band = pl->upload_for_host ? e->raster
                                           : (pl->crt_band > 0 ? pl->crt_band : (e->m + 127) / 128);
+            g->tile_n = pl->crt_tile_n;
         }
         rc = ca3dmm_crt_plan_encode(&pl->crt, e->crt_moduli, ns, pl->cb, pl->cs, ns, pl->cb + ns,
                                     pl->cs + ns, ns, pl->cg, w + pl->off_crt, pl->crt_bytes,
@@ -1263,6 +1357,15 @@ void ca3dmm_engine_exec(ca3dmm_engine_p e, const void *src_A, const int ldA, con
         ERROR_PRINTF("ca3dmm_engine has no device work buffer attached\n");
         e->last_error = CA3DMM_EINVAL;
         return;
+    }
+    if (e->gemm_auto == 1) {
+        /* CA3DMM_GEMM_AUTO: tune on this exec's operands first */
+        int rc = ca3dmm_engine_autotune_env(e, src_A, ldA, src_B, ldB, dst_C, ldC);
+        if (rc) {
+            e->last_error = rc;
+            ERROR_PRINTF("ca3dmm_engine_exec: tuning failed (error %d)\n", rc);
+            return;
+        }
     }
     double t0 = ca3dmm_wtime_sec();
     nvtxRangePushA("ca3dmm_engine_exec");
@@ -1637,6 +1740,24 @@ static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_
     cudaStream_t st = (cudaStream_t) e->stream;
     const double *dAsrc = e->is_BTB ? x->dB : x->dA;
     const long long ldAsrc = e->is_BTB ? x->ldb : x->lda;
+    if (e->gemm_auto == 1) {
+        /* CA3DMM_GEMM_AUTO: tune on device copies of the whole operands */
+        const int a_cols = e->trans_A ? e->m : e->k, b_cols = e->trans_B ? e->k : e->n;
+        if (!e->is_BTB)
+            CA3DMM_CUDA_TRY(cudaMemcpy2DAsync(x->dA, sizeof(double) * x->lda, A_h,
+                                              sizeof(double) * (size_t) ldA,
+                                              sizeof(double) * (size_t) a_rows, a_cols,
+                                              cudaMemcpyHostToDevice, st));
+        CA3DMM_CUDA_TRY(cudaMemcpy2DAsync(x->dB, sizeof(double) * x->ldb, B_h,
+                                          sizeof(double) * (size_t) ldB,
+                                          sizeof(double) * (size_t) b_rows, b_cols,
+                                          cudaMemcpyHostToDevice, st));
+        CA3DMM_CUDA_TRY(cudaStreamSynchronize(st));
+        rc = ca3dmm_engine_autotune_env(e, dAsrc, (int) ldAsrc, x->dB, (int) x->ldb, x->dC,
+                                        (int) x->ldc);
+        if (rc) return rc;
+        pl->plan_valid = 0;   /* the row-band pipeline needs its own plan */
+    }
     /* device plan for the staging buffers (rebuilt only when they change) */
     if (!pl->plan_valid || pl->c_A != dAsrc || pl->c_B != x->dB || pl->c_ldA != ldAsrc ||
         pl->c_ldB != x->ldb || pl->c_dst != x->dC || pl->c_ldC != x->ldc) {
@@ -1800,7 +1921,14 @@ void ca3dmm_engine_print_stat(ca3dmm_engine_p e)
     double gf = 2.0 * (double) e->m * (double) e->n * (double) e->k / (e->cannon_ms / e->n_exec) /
                 1e6;
     printf("* GEMM throughput        : %.2f GFlops (%s)\n", gf,
-           e->gemm_mode == CA3DMM_GEMM_OZAKI ? "split precision" : "FP64 DMMA");
+           e->gemm_mode == CA3DMM_GEMM_OZAKI ? "split precision"
+           : e->gemm_mode == CA3DMM_GEMM_CRT ? "split precision, modular" : "FP64 DMMA");
+    if (e->gemm_auto == 2) {
+        ca3dmm_tune_cfg_t c;
+        ca3dmm_engine_get_tune(e, &c);
+        printf("* Tuned (auto mode)      : mode %d, %d slices / moduli, raster %d, tile %d "
+               "(%.0f ms to tune)\n", c.gemm_mode, c.slices, c.raster, c.tile_n, e->tune_ms);
+    }
     printf("============================================================\n");
 }
 
@@ -1813,44 +1941,145 @@ void ca3dmm_engine_set_stream(ca3dmm_engine_p e, void *stream, int sync)
     e->sync_exec = sync ? 1 : 0;
 }
 
+/* Make the work buffer at least `need` bytes: the engine's own buffer is
+ * replaced, a caller's buffer that is too small is an error. */
+static int grow_workbuf(ca3dmm_engine_p e, plan_t *pl, size_t need, size_t have)
+{
+    if (e->workbuf_d == NULL || need <= have) return CA3DMM_OK;
+    if (!e->alloc_workbuf) return CA3DMM_ENOMEM;
+    void *nw = dev_type_malloc(need, DEV_TYPE_CUDA);
+    if (!nw) return CA3DMM_ENOMEM;
+    dev_type_free(e->workbuf_d, DEV_TYPE_CUDA);
+    pl->total = need;
+    ca3dmm_engine_attach_workbuf(e, NULL, nw);
+    return CA3DMM_OK;
+}
+
 int ca3dmm_engine_set_gemm_mode(ca3dmm_engine_p e, int mode, int slices)
 {
     if (!e) return CA3DMM_EINVAL;
+    plan_t *pl = (plan_t *) e->impl;
+    if (mode == CA3DMM_GEMM_AUTO) {
+        const size_t old_total = pl->total, need = auto_bytes(e);
+        if (pl->total < need) pl->total = need;
+        int rc = grow_workbuf(e, pl, pl->total, old_total);
+        if (rc) {
+            pl->total = old_total;
+            return rc;
+        }
+        e->workbuf_bytes = pl->total;
+        e->gemm_auto = 1;
+        return CA3DMM_OK;
+    }
     if (mode != CA3DMM_GEMM_PLAIN && mode != CA3DMM_GEMM_OZAKI && mode != CA3DMM_GEMM_CRT)
         return CA3DMM_EINVAL;
     if (mode == CA3DMM_GEMM_OZAKI && (slices < 2 || slices > 8)) return CA3DMM_EINVAL;
     int nmod = 0;
     if (mode == CA3DMM_GEMM_CRT && (nmod = crt_resolve(e, slices)) == 0) return CA3DMM_EINVAL;
-    plan_t *pl = (plan_t *) e->impl;
     int old_mode = e->gemm_mode, old_sl = e->ozaki_slices, old_nm = e->crt_moduli;
     e->gemm_mode = mode;
     if (mode == CA3DMM_GEMM_OZAKI) e->ozaki_slices = slices;
     if (mode == CA3DMM_GEMM_CRT) e->crt_moduli = nmod;
     size_t old_total = pl->total;
     plan_layout(e, pl);
-    if (e->workbuf_d != NULL && pl->total > old_total) {
-        if (!e->alloc_workbuf) {
-            /* the caller's buffer is too small: keep the old mode */
-            e->gemm_mode = old_mode;
-            e->ozaki_slices = old_sl;
-            e->crt_moduli = old_nm;
-            plan_layout(e, pl);
-            return CA3DMM_ENOMEM;
-        }
-        void *nw = dev_type_malloc(pl->total, DEV_TYPE_CUDA);
-        if (!nw) {
-            e->gemm_mode = old_mode;
-            e->ozaki_slices = old_sl;
-            e->crt_moduli = old_nm;
-            plan_layout(e, pl);
-            return CA3DMM_ENOMEM;
-        }
-        dev_type_free(e->workbuf_d, DEV_TYPE_CUDA);
-        ca3dmm_engine_attach_workbuf(e, NULL, nw);
+    int rc = grow_workbuf(e, pl, pl->total, old_total);
+    if (rc) {
+        /* the caller's buffer is too small, or no memory: keep the old mode */
+        e->gemm_mode = old_mode;
+        e->ozaki_slices = old_sl;
+        e->crt_moduli = old_nm;
+        plan_layout(e, pl);
+        if (pl->total < old_total) pl->total = old_total;
+        return rc;
     }
     if (pl->total < old_total) pl->total = old_total;   /* keep the larger layout's size */
     e->workbuf_bytes = pl->total;
+    e->gemm_auto = 0;
     pl->plan_valid = 0;
+    return CA3DMM_OK;
+}
+
+int ca3dmm_engine_set_tune(ca3dmm_engine_p e, const ca3dmm_tune_cfg_t *c)
+{
+    if (!e || !c) return CA3DMM_EINVAL;
+    plan_t *pl = (plan_t *) e->impl;
+    if (c->gemm_mode == CA3DMM_GEMM_CRT) {
+        if ((c->tile_n != 0 && c->tile_n != 128 && c->tile_n != 256) || c->raster < 0 ||
+            c->raster > 1024)
+            return CA3DMM_EINVAL;
+    } else if (c->tile_n != 0 ||
+               (c->raster != 0 && c->raster != 4 && c->raster != 8 && c->raster != 16)) {
+        return CA3DMM_EINVAL;
+    }
+    int rc = ca3dmm_engine_set_gemm_mode(e, c->gemm_mode, c->slices);
+    if (rc) return rc;
+    if (c->gemm_mode == CA3DMM_GEMM_CRT) {
+        pl->crt_band = c->raster ? c->raster : pl->crt_band_env;
+        pl->crt_tile_n = c->tile_n ? c->tile_n : 256;
+    } else {
+        e->raster = c->raster ? c->raster : 8;
+    }
+    pl->plan_valid = 0;
+    return CA3DMM_OK;
+}
+
+int ca3dmm_engine_get_tune(ca3dmm_engine_p e, ca3dmm_tune_cfg_t *c)
+{
+    if (!e || !c) return CA3DMM_EINVAL;
+    const plan_t *pl = (const plan_t *) e->impl;
+    c->gemm_mode = e->gemm_mode;
+    c->slices = e->gemm_mode == CA3DMM_GEMM_OZAKI ? e->ozaki_slices
+                : e->gemm_mode == CA3DMM_GEMM_CRT ? e->crt_moduli : 0;
+    c->kp = e->kp;
+    c->raster = e->gemm_mode == CA3DMM_GEMM_CRT ? pl->crt_band : e->raster;
+    c->tile_n = e->gemm_mode == CA3DMM_GEMM_CRT ? pl->crt_tile_n : 0;
+    return CA3DMM_OK;
+}
+
+ca3dmm_tune_report_t *ca3dmm_engine_report_slot(ca3dmm_engine_p e)
+{
+    return e && e->impl ? &((plan_t *) e->impl)->report : NULL;
+}
+
+int ca3dmm_engine_tune_report(ca3dmm_engine_p e, ca3dmm_tune_cfg_t *cfgs, float *ms, float *err,
+                              int max)
+{
+    const ca3dmm_tune_report_t *r = ca3dmm_engine_report_slot(e);
+    if (!r) return -1;
+    for (int i = 0; i < r->n && i < max; i++) {
+        if (cfgs) cfgs[i] = r->cfg[i];
+        if (ms) ms[i] = r->ms[i];
+        if (err) err[i] = r->err[i];
+    }
+    return r->n;
+}
+
+static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void *src_B, int ldB,
+                       void *dst_C, int ldC, cudaStream_t st);
+
+int ca3dmm_engine_exec_reps(ca3dmm_engine_p e, const void *A, int ldA, const void *B, int ldB,
+                            void *C, int ldC, int reps, float *ms)
+{
+    const int sync = e->sync_exec;
+    e->sync_exec = 1;
+    const double t0 = e->redist_ms + e->cannon_ms + e->reduce_ms;
+    int rc = CA3DMM_OK;
+    for (int r = 0; r < reps && !rc; r++)
+        rc = exec_device(e, A, ldA, B, ldB, C, ldC, (cudaStream_t) e->stream);
+    e->sync_exec = sync;
+    if (!rc && ms && reps > 0)
+        *ms = (float) ((e->redist_ms + e->cannon_ms + e->reduce_ms - t0) / reps);
+    return rc;
+}
+
+int ca3dmm_engine_full_c(ca3dmm_engine_p e, void *dst_C, int ldC, const double **C,
+                         long long *ld)
+{
+    const plan_t *pl = (const plan_t *) e->impl;
+    const int whole = pl->has_dst && pl->dst_srow == 0 && pl->dst_scol == 0 &&
+                      pl->dst_nrow == e->m && pl->dst_ncol == e->n;
+    *C = whole ? (const double *) dst_C : (const double *) ((char *) e->workbuf_d + pl->off_cout);
+    *ld = whole ? ldC : e->m;
     return CA3DMM_OK;
 }
 

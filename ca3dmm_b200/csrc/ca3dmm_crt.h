@@ -42,6 +42,7 @@ typedef struct {
     long long ldc;
     int m, n, k;
     int band;
+    int tile_n;     /* GEMM tile columns: 128 or 256 (0 = 256); the same in every group */
 } ca3dmm_crt_group_t;
 
 typedef struct {
@@ -53,6 +54,7 @@ typedef struct {
     long long n_exp;
     long long recon_items;  /* reconstruction items (4 rows x 1 column) over every group */
     int group_m, group_n;   /* the group's size when the plan has one group */
+    int tile_n;             /* GEMM tile columns of every group */
     void *dev_plan;
     void *dev_work;
 } ca3dmm_crt_plan_t;

@@ -41,11 +41,21 @@
 namespace {
 
 constexpr int MAXMOD = CA3DMM_CRT_MAX_MODULI;
-constexpr int CBM = 128, CBN = 256, CKB = 128;   // tile rows, tile cols, k bytes per stage
+// B residue blocks are stored in 256-column tiles (CBN); a GEMM tile is CBM rows
+// by TN = 256 or 128 columns (a 128-column tile reads one half of a stored
+// 256-row block, 16 KiB per k block, as the A side of B^T B already does).
+constexpr int CBM = 128, CBN = 256, CKB = 128;   // tile rows, stored B tile rows, k bytes per stage
 constexpr int CA_BYTES = CBM * CKB;              // 16 KiB
 constexpr int CB_BYTES = CBN * CKB;              // 32 KiB
-constexpr int CSTAGE_BYTES = CA_BYTES + CB_BYTES;
-constexpr int CNSTAGE = 4;
+
+template <int TN>
+struct CrtTile {
+    static constexpr int kBBytes = TN * CKB;                    // B bytes per stage
+    static constexpr int kStageBytes = CA_BYTES + kBBytes;
+    static constexpr int kStages = TN == 256 ? 4 : 6;          // 192 KiB of stages either way
+    static constexpr int kTmemCols = 2 * TN;                    // two accumulators
+    static constexpr size_t kSmem = (size_t) kStages * kStageBytes + (2 * kStages + 4) * 8 + 1024;
+};
 constexpr int C_THREADS = 352;                   // 11 warps
 constexpr int C_ISSUERS = 2;
 constexpr int C_EPI_WARPS = 8;
@@ -251,6 +261,7 @@ struct CrtGroup {
     int m, n, k;
     int a_desc, b_desc, a_from_b;   // a_from_b: A tile tm is half tm % 2 of the B block's tile tm / 2
     int tiles_m, tiles_n, item_begin, band;
+    int tile_n, pad_;               // GEMM tile columns (128 or 256; the same in every group)
     long long rc_begin;             // first reconstruction item (4 rows x 1 column) of the group
     int P, nkb;                     // integer width, 128-byte k blocks
     long long ea_off, eb_off;       // exponents of the A rows / B columns
@@ -333,6 +344,7 @@ __device__ __forceinline__ unsigned int mod_i32(uint32_t vbits, const ModConst &
 }
 
 // ------------------------------------------------------------------ GEMM
+template <int TN>
 __global__ void __launch_bounds__(C_THREADS, 1)
 crt_gemm_kernel(const CrtGroup *__restrict__ groups, int ngroup, int nmod,
                 const ca3dmm_tile_ranges_t rg, int total_items,
@@ -341,6 +353,8 @@ crt_gemm_kernel(const CrtGroup *__restrict__ groups, int ngroup, int nmod,
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    using T = CrtTile<TN>;
+    constexpr int CNSTAGE = T::kStages, CSTAGE_BYTES = T::kStageBytes;
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + CNSTAGE * CSTAGE_BYTES);
     uint64_t *empty = full + CNSTAGE;
     uint64_t *acc_full = empty + CNSTAGE;       // [2]
@@ -368,7 +382,7 @@ crt_gemm_kernel(const CrtGroup *__restrict__ groups, int ngroup, int nmod,
     if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&tmem_slot)),
-                     "r"(512)
+                     "r"(T::kTmemCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -379,7 +393,7 @@ crt_gemm_kernel(const CrtGroup *__restrict__ groups, int ngroup, int nmod,
     if (warp >= 3 && warp <= 6) {
         // zero both accumulators (the MMAs only accumulate)
         const uint32_t lane_base = (uint32_t) ((warp & 3) * 32) << 16;
-        for (int c = 0; c < 2 * CBN; c += 32) tmem_zero32(tmem_base + lane_base + (uint32_t) c);
+        for (int c = 0; c < T::kTmemCols; c += 32) tmem_zero32(tmem_base + lane_base + (uint32_t) c);
         tmem_wait_st();
     }
     tc_fence_before();
@@ -401,8 +415,11 @@ crt_gemm_kernel(const CrtGroup *__restrict__ groups, int ngroup, int nmod,
                                      (long long) (tm >> 1) * G.nkb * CB_BYTES + (tm & 1) * CA_BYTES
                                : work + G.qa_off + t * G.qa_tstride + (long long) tm * G.nkb * CA_BYTES;
                 const long long a_step = G.a_from_b ? CB_BYTES : CA_BYTES;
+                // a 128-column tile: half tn % 2 of stored 256-row tile tn / 2
                 const unsigned char *qb =
-                    work + G.qb_off + t * G.qb_tstride + (long long) tn * G.nkb * CB_BYTES;
+                    TN == CBN ? work + G.qb_off + t * G.qb_tstride + (long long) tn * G.nkb * CB_BYTES
+                              : work + G.qb_off + t * G.qb_tstride +
+                                    (long long) (tn >> 1) * G.nkb * CB_BYTES + (tn & 1) * T::kBBytes;
                 for (int kb = 0; kb < G.nkb; ++kb, ++it) {
                     const uint32_t s = it % CNSTAGE, ph = (it / CNSTAGE) & 1u;
                     if (!mbar_wait_bounded(&empty[s], ph ^ 1u, &abort_flag, status,
@@ -413,7 +430,7 @@ crt_gemm_kernel(const CrtGroup *__restrict__ groups, int ngroup, int nmod,
                     uint8_t *sA = smem + s * CSTAGE_BYTES;
                     mbar_arrive_expect_tx(&full[s], CSTAGE_BYTES);
                     bulk_load(sA, qa + (long long) kb * a_step, CA_BYTES, &full[s]);
-                    bulk_load(sA + CA_BYTES, qb + (long long) kb * CB_BYTES, CB_BYTES, &full[s]);
+                    bulk_load(sA + CA_BYTES, qb + (long long) kb * CB_BYTES, T::kBBytes, &full[s]);
                 }
             }
             // drain copies in flight (bounded, abort flag ignored)
@@ -428,7 +445,7 @@ crt_gemm_kernel(const CrtGroup *__restrict__ groups, int ngroup, int nmod,
         // ------------------------------------------------------ MMA issuers
         if (lane == 0) {
             const int half = warp - 1;          // k steps 2 half, 2 half + 1 of each stage
-            const uint32_t idesc = idesc_i8(CBN, CBM);
+            const uint32_t idesc = idesc_i8(TN, CBM);
             uint32_t it = 0, ai = 0;
             bool ok = true;
             for (int v = blockIdx.x; v < total_items && ok; v += gridDim.x, ++ai) {
@@ -441,7 +458,7 @@ crt_gemm_kernel(const CrtGroup *__restrict__ groups, int ngroup, int nmod,
                     break;
                 }
                 tc_fence_after();
-                const uint32_t tacc = tmem_base + buf * CBN;
+                const uint32_t tacc = tmem_base + buf * TN;
                 for (int kb = 0; kb < G.nkb; ++kb, ++it) {
                     const uint32_t s = it % CNSTAGE, ph = (it / CNSTAGE) & 1u;
                     if (!mbar_wait_bounded(&full[s], ph, &abort_flag, status,
@@ -473,7 +490,7 @@ crt_gemm_kernel(const CrtGroup *__restrict__ groups, int ngroup, int nmod,
     } else {
         // ------------------------------------------------------ epilogue
         const int q = warp & 3;                       // TMEM lane quarter of this warp
-        const int h = (warp - 3) >> 2;                // accumulator columns 128 h .. 128 h + 127
+        const int h = (warp - 3) >> 2;                // accumulator columns TN/2 h .. TN/2 (h + 1) - 1
         uint32_t ai = 0;
         for (int v = blockIdx.x; v < total_items; v += gridDim.x, ++ai) {
             const int item = range_tile(rg, v);
@@ -489,13 +506,13 @@ crt_gemm_kernel(const CrtGroup *__restrict__ groups, int ngroup, int nmod,
             const int row = tm * CBM + q * 32 + lane;
             unsigned char *plane = work + G.pl_off + (long long) t * G.pl_bytes + row;
 #pragma unroll 1
-            for (int cb = 0; cb < 4; ++cb) {
-                const int c0 = h * 128 + cb * 32;
+            for (int cb = 0; cb < TN / 64; ++cb) {
+                const int c0 = h * (TN / 2) + cb * 32;
                 uint32_t vv[32];
-                const uint32_t ta = tmem_base + ((uint32_t) (q * 32) << 16) + buf * CBN + (uint32_t) c0;
+                const uint32_t ta = tmem_base + ((uint32_t) (q * 32) << 16) + buf * TN + (uint32_t) c0;
                 tmem_ld32(ta, vv);
                 tmem_zero32(ta);
-                unsigned char *pc = plane + (long long) (tn * CBN + c0) * G.pl_ld;
+                unsigned char *pc = plane + (long long) (tn * TN + c0) * G.pl_ld;
 #pragma unroll
                 for (int j = 0; j < 32; ++j)
                     pc[(long long) j * G.pl_ld] = (unsigned char) mod_i32(vv[j], mc);
@@ -511,7 +528,7 @@ crt_gemm_kernel(const CrtGroup *__restrict__ groups, int ngroup, int nmod,
     if (warp == 1) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem_base),
-                     "r"(512)
+                     "r"(T::kTmemCols)
                      : "memory");
     }
 }
@@ -817,7 +834,9 @@ extern "C" int ca3dmm_crt_plan_encode(ca3dmm_crt_plan_t *pl, int nmod, int nA,
         o.b_desc = nA + G[g].b_blk;
         o.a_from_b = al >= 0 ? 1 : 0;
         o.tiles_m = (o.m > 0 && o.n > 0) ? (o.m + CBM - 1) / CBM : 0;
-        o.tiles_n = (o.m > 0 && o.n > 0) ? (o.n + CBN - 1) / CBN : 0;
+        o.tile_n = G[g].tile_n == 128 ? 128 : CBN;
+        if (o.tile_n != (G[0].tile_n == 128 ? 128 : CBN)) return CA3DMM_EINVAL;
+        o.tiles_n = (o.m > 0 && o.n > 0) ? (o.n + o.tile_n - 1) / o.tile_n : 0;
         o.band = G[g].band > 0 ? G[g].band : DEFAULT_BAND;
         o.item_begin = items;
         o.rc_begin = recon;
@@ -847,6 +866,7 @@ extern "C" int ca3dmm_crt_plan_encode(ca3dmm_crt_plan_t *pl, int nmod, int nA,
     pl->p_max = pmax;
     pl->n_exp = (long long) ne;
     pl->recon_items = recon;
+    pl->tile_n = G[0].tile_n == 128 ? 128 : CBN;
     pl->group_m = ngroup == 1 ? gr[0].m : 0;
     pl->group_n = ngroup == 1 ? gr[0].n : 0;
     pl->dev_plan = dev_plan;
@@ -1035,14 +1055,23 @@ extern "C" int ca3dmm_crt_run_gemm(const ca3dmm_crt_plan_t *pl, const ca3dmm_til
     const CrtLayout L(pl->nA + pl->nB, pl->ngroup);
     const CrtGroup *groups =
         reinterpret_cast<const CrtGroup *>(static_cast<const unsigned char *>(pl->dev_plan) + L.gr);
-    const size_t smem = (size_t) CNSTAGE * CSTAGE_BYTES + (2 * CNSTAGE + 4) * 8 + 1024;
     int grid = ca3dmm_device_sm_count();
     if (grid > vitems) grid = vitems;
-    CA3DMM_CUDA_TRY(cudaFuncSetAttribute(crt_gemm_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int) smem));
-    crt_gemm_kernel<<<grid, C_THREADS, smem, stream>>>(
-        groups, pl->ngroup, pl->nmod, rg, vitems, static_cast<unsigned char *>(pl->dev_work),
-        dev_status, (unsigned long long) (timeout_s * 1e9));
+    unsigned char *w = static_cast<unsigned char *>(pl->dev_work);
+    const unsigned long long lim = (unsigned long long) (timeout_s * 1e9);
+    if (pl->tile_n == 128) {
+        const size_t smem = CrtTile<128>::kSmem;
+        CA3DMM_CUDA_TRY(cudaFuncSetAttribute(crt_gemm_kernel<128>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        crt_gemm_kernel<128><<<grid, C_THREADS, smem, stream>>>(groups, pl->ngroup, pl->nmod, rg,
+                                                                vitems, w, dev_status, lim);
+    } else {
+        const size_t smem = CrtTile<256>::kSmem;
+        CA3DMM_CUDA_TRY(cudaFuncSetAttribute(crt_gemm_kernel<256>,
+                                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int) smem));
+        crt_gemm_kernel<256><<<grid, C_THREADS, smem, stream>>>(groups, pl->ngroup, pl->nmod, rg,
+                                                                vitems, w, dev_status, lim);
+    }
     CA3DMM_CUDA_TRY(cudaGetLastError());
     ca3dmm_note_launch(1);
     return CA3DMM_OK;

@@ -237,6 +237,8 @@ extern "C" void ca3dmm_mlp_free(ca3dmm_mlp_p *mp)
 
 extern "C" int ca3dmm_mlp_nparams(ca3dmm_mlp_p m) { return m ? m->np : 0; }
 
+extern "C" int ca3dmm_mlp_inputs(ca3dmm_mlp_p m) { return m ? m->nin : 0; }
+
 extern "C" int ca3dmm_mlp_get_params(ca3dmm_mlp_p m, float *host)
 {
     if (!m || !host) return CA3DMM_EINVAL;

@@ -39,6 +39,10 @@
 #define CA3DMM_GEMM_CRT   2   /* split precision, modular: P-bit row / column integers, their exact
                                  product from one INT8 tcgen05 GEMM per modulus (N moduli <= 256)
                                  and the Chinese remainder theorem, rounded once to FP64 */
+#define CA3DMM_GEMM_AUTO  3   /* chosen at the first exec by the autotuner among plain, slice and
+                                 modular configurations, split precision only where it passes
+                                 the accuracy guard (include/ca3dmm_tune.h; env CA3DMM_AUTOTUNE,
+                                 CA3DMM_TUNE_CACHE; CA3DMM_GEMM_MODE=auto at init) */
 
 struct ca3dmm_engine {
     int m, n, k;                    /* Size of op(A) (m*k), op(B) (k*n), C (m*n) */
@@ -127,6 +131,9 @@ struct ca3dmm_engine {
     int crt_moduli;                 /* CA3DMM_GEMM_CRT: moduli (env CA3DMM_CRT_MODULI; 0 = the
                                        fewest that give 51-bit integers for this k) */
     int crt_bits;                   /* CA3DMM_GEMM_CRT: integer width P of the operands */
+    int gemm_auto;                  /* CA3DMM_GEMM_AUTO: 1 until tuned, 2 after (gemm_mode then
+                                       holds the choice) */
+    double tune_ms;                 /* wall time of the tuning at the first exec */
 };
 typedef struct ca3dmm_engine ca3dmm_engine_s;
 typedef struct ca3dmm_engine *ca3dmm_engine_p;
@@ -207,9 +214,11 @@ int ca3dmm_engine_last_error(ca3dmm_engine_p engine);
  * CUDA-graph capturable (the statistics are then not updated). */
 void ca3dmm_engine_set_stream(ca3dmm_engine_p engine, void *stream, int sync);
 /* Select the GEMM: CA3DMM_GEMM_PLAIN, CA3DMM_GEMM_OZAKI with `slices` INT8
- * slices per operand (2..8), or CA3DMM_GEMM_CRT with `slices` moduli (8..18,
+ * slices per operand (2..8), CA3DMM_GEMM_CRT with `slices` moduli (8..18,
  * 0 = the fewest whose product admits 51-bit operand integers at this k; the
- * engine's crt_bits field then holds the integer width).  Must be called
+ * engine's crt_bits field then holds the integer width), or CA3DMM_GEMM_AUTO
+ * (tuned at the next exec; the work buffer then covers every candidate;
+ * `slices` ignored).  Must be called
  * before attach_workbuf when the caller allocates the work buffer (it changes
  * *workbuf_bytes, which ca3dmm_engine_workbuf_bytes reports). */
 int ca3dmm_engine_set_gemm_mode(ca3dmm_engine_p engine, int mode, int slices);

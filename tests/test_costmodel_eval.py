@@ -1,9 +1,11 @@
 """The shipped cost model (ca3dmm_b200/data/costmodel_b200.txt) against
-exhaustive autotuning on the 500 held-out shapes of the B200 study.
+exhaustive autotuning on the 400 held-out shapes of the B200 study.
 
 tests/golden/costmodel_timings_b200.npz holds the study's exhaustive timings
-(every one of the 18 candidates on every shape, ms) and features, written by
-  python -m ca3dmm_b200.costmodel --train 2000 --test 500 --epochs 300 --out DIR
+(every one of the 16 candidates -- plain, INT8-slice and modular
+configurations with their k splits, rasters / bands and tile widths -- on
+every shape, ms) and features, written by
+  python -m ca3dmm_b200.costmodel --train 1600 --test 400 --epochs 300 --out DIR
 on one B200.  The network is evaluated here with the oracle's FP32 forward.
 What the network gains is measured against the tuner without it: the untuned
 default, the best single configuration of the training shapes, and linear /
@@ -76,7 +78,7 @@ def lstsq_predictor(study, quadratic):
 
 def test_model_layout():
     nin, h1, h2, mu, sd, params = load_model()
-    assert (nin, h1, h2) == (12, 64, 64)
+    assert (nin, h1, h2) == (14, 64, 64)
     assert params.size == h1 * nin + h1 + h2 * h1 + h2 + h2 + 1
     assert np.all(sd > 0)
 
@@ -85,10 +87,10 @@ def test_held_out_regret_and_search_time(study):
     T = study["Tte"]
     P = study["mlp"](study["Fte"])
     r1, r2 = regret(P, T, 1), regret(P, T, 2)
-    assert len(r1) == 500
+    assert len(r1) == 400
     assert r1.mean() <= 0.03 and np.median(r1) <= 0.01, (r1.mean(), np.median(r1))
     assert r2.mean() <= 0.015 and np.median(r2) == 0.0, (r2.mean(), np.median(r2))
-    # timing the model's top 2 instead of all 18 candidates
+    # timing the model's top 2 instead of all 16 candidates
     order = np.argsort(P, axis=1)[:, :2]
     saved = 1.0 - np.take_along_axis(T, order, 1).sum(1) / T.sum(1)
     assert saved.mean() >= 0.85, saved.mean()
@@ -104,7 +106,7 @@ def test_network_beats_the_tuner_without_it(study):
     fixed = regret(np.tile(np.arange(ncand) != fixed_cfg, (len(T), 1)).astype(float), T).mean()
     linear = regret(lstsq_predictor(study, False), T).mean()
     quad = regret(lstsq_predictor(study, True), T).mean()
-    print("\nmean top-1 regret on 500 held-out shapes: mlp %.4f, quadratic %.4f, linear %.4f, "
+    print("\nmean top-1 regret on 400 held-out shapes: mlp %.4f, quadratic %.4f, linear %.4f, "
           "best fixed (cfg %d) %.4f, untuned default %.4f" % (r_mlp, quad, linear, fixed_cfg,
                                                                fixed, default))
     assert default >= 0.5

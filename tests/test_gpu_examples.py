@@ -46,10 +46,11 @@ def test_help_without_gpu():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("mode", ["0", "1", "2"])
+@pytest.mark.parametrize("mode", ["0", "1", "2", "auto"])
 def test_example_ab_2048_on_four_ranks(cuda, mode):
     """The 2048^3 example on 4 virtual ranks: the reference's grid 2 x 1 x 2,
-    cuboid 1024 x 2048 x 1024, and 0 errors in every GEMM mode."""
+    cuboid 1024 x 2048 x 1024, and 0 errors in every GEMM mode (auto: tuned at
+    the warm-up exec)."""
     rc, out = run("example_ab", 2048, 2048, 2048, 0, 0, 1, 3, 1,
                   env={"CA3DMM_VRANKS": "4", "CA3DMM_GEMM_MODE": mode})
     assert rc == 0, out

@@ -7,7 +7,7 @@ import pytest
 
 import ca3dmm_b200 as cb
 from oracle import oracle as orc
-from tests._util import dev_zeros, to_dev
+from tests._util import dev_zeros, from_dev, to_dev
 
 pytestmark = pytest.mark.gpu
 
@@ -47,13 +47,192 @@ def test_autotune_exhaustive_and_model(cuda):
     dA, lda = to_dev(A)
     dB, ldb = to_dev(B)
     dC = dev_zeros(m * n)
-    cands = [(0, 0, 1, 8), (0, 0, 2, 8), (0, 0, 4, 4), (1, 7, 1, 8), (1, 7, 2, 16)]
-    best, ms = cb.autotune(m, n, k, 0, 0, dA, lda, dB, ldb, dC, m, cands)
-    assert np.all(ms > 0)
-    assert best == int(np.argmin(ms))
+    cands = [(0, 0, 1, 8, 0), (0, 0, 2, 8, 0), (0, 0, 4, 4, 0), (1, 7, 1, 8, 0),
+             (1, 7, 2, 16, 0), (2, 0, 1, 32, 256), (2, 0, 1, 8, 128)]
+    best, ms, err = cb.autotune(m, n, k, 0, 0, dA, lda, dB, ldb, dC, m, cands, with_err=True)
+    # every candidate ran; split ones are timed or rejected by the guard
+    assert np.all((ms > 0) | (ms == -2)) and np.all(err >= 0)
+    assert np.all(ms[[0, 1, 2]] > 0)
+    assert best == int(np.argmin(np.where(ms > 0, ms, np.inf)))
     cm = cb.CostModel(seed=11)
     best2, ms2 = cb.autotune(m, n, k, 0, 0, dA, lda, dB, ldb, dC, m, cands, model=cm, topk=2)
     assert int(np.sum(ms2 > 0)) == 2 and ms2[best2] > 0
+
+
+def _oracle_c(A, B, m, n, k, cfg):
+    """C of an engine configuration (1 x 1 x 1 grid): bit-exact oracles for the
+    split modes, None for the plain mode (checked against the DD bound)."""
+    mode, sl = cfg[0], cfg[1]
+    if mode == cb.GEMM_CRT:
+        P = orc.crt_bits(sl, k)
+        c = orc.crt_gemm(np.asfortranarray(A), np.asfortranarray(B), 0, 0, m, n, k, P)
+        return orc.nonfinite_fixup(np.asfortranarray(A), np.asfortranarray(B), 0, 0, m, n, k, c)
+    if mode == cb.GEMM_OZAKI:
+        qa, ea = orc.ozaki_slices_rows(np.asfortranarray(A), 0, m, k, sl)
+        qb, eb = orc.ozaki_slices_cols(np.asfortranarray(B), 0, k, n, sl)
+        return orc.ozaki_gemm(qa, ea, qb, eb, m, n, k, sl)
+    return None
+
+
+@pytest.mark.parametrize("tile", [128, 256])
+def test_crt_tile_widths_bitexact(cuda, tile):
+    """Both modular GEMM tile widths give the oracle's C bit for bit (edge tiles
+    in both dimensions, bands of 8 and 32 tile rows)."""
+    m, n, k = 1100, 700, 900
+    A = orc.gen_signed_exp(31, m, k)
+    B = orc.gen_signed_exp(32, k, n)
+    dA, lda = to_dev(A)
+    dB, ldb = to_dev(B)
+    want = _oracle_c(A, B, m, n, k, (cb.GEMM_CRT, 15))
+    for band in (8, 32):
+        dC = dev_zeros(m * n)
+        e = cb.Ca3dmmEngine(m, n, k)
+        assert e.set_tune((cb.GEMM_CRT, 15, 1, band, tile)) == 0
+        assert e.get_tune() == (cb.GEMM_CRT, 15, 1, band, tile)
+        assert e.exec(dA, lda, dB, ldb, dC, m) == 0
+        got = from_dev(dC, m, n)
+        e.free()
+        assert np.array_equal(got, want), (band, np.max(np.abs(got - want)))
+
+
+def test_set_tune_refusals(cuda):
+    e = cb.Ca3dmmEngine(256, 256, 256)
+    assert e.set_tune((cb.GEMM_CRT, 15, 1, 8, 64)) != 0        # no 64-column modular tile
+    assert e.set_tune((cb.GEMM_PLAIN, 0, 1, 8, 128)) != 0      # the plain GEMM has one tile
+    assert e.set_tune((cb.GEMM_PLAIN, 0, 1, 5, 0)) != 0        # raster 4, 8 or 16
+    assert e.set_tune((cb.GEMM_OZAKI, 9, 1, 8, 0)) != 0        # 2..8 slices
+    assert e.set_tune((cb.GEMM_PLAIN, 0, 1, 16, 0)) == 0
+    assert e.get_tune() == (cb.GEMM_PLAIN, 0, 1, 16, 0)
+
+
+@pytest.mark.parametrize("how", [0, 1, 2])
+def test_engine_auto_picks_the_tuned_config_and_matches_the_oracle(cuda, how):
+    """An engine in auto mode tunes at its first exec: the configuration it
+    keeps is the fastest admissible one of its report (exhaustive, model:
+    among the timed ones; off: the model's first admissible), and its C is the
+    oracle's for that configuration."""
+    m, n, k = 1000, 900, 1200
+    A = orc.gen_signed_exp(41, m, k, emin=-2, emax=2)
+    B = orc.gen_signed_exp(42, k, n, emin=-2, emax=2)
+    dA, lda = to_dev(A)
+    dB, ldb = to_dev(B)
+    dC = dev_zeros(m * n)
+    e = cb.Ca3dmmEngine(m, n, k)
+    assert e.set_gemm_mode(cb.GEMM_AUTO) == 0 and e.s.gemm_auto == 1
+    import os
+    old = os.environ.get("CA3DMM_AUTOTUNE")
+    os.environ["CA3DMM_AUTOTUNE"] = ("off", "model", "exhaustive")[how]
+    try:
+        assert e.exec(dA, lda, dB, ldb, dC, m) == 0
+    finally:
+        if old is None:
+            del os.environ["CA3DMM_AUTOTUNE"]
+        else:
+            os.environ["CA3DMM_AUTOTUNE"] = old
+    assert e.s.gemm_auto == 2 and e.s.tune_ms > 0
+    rep = e.tune_report()
+    chosen = e.get_tune()
+    timed = [(ms, c) for c, ms, _ in rep if ms > 0]
+    if how == 0:
+        assert not timed
+    else:
+        assert timed and chosen == min(timed)[1]
+        if how == 2:
+            assert all(ms > 0 or ms == -2 for _, ms, _ in rep)
+    # at this mild exponent spread every split candidate passes the guard
+    assert all(ms != -2 for _, ms, _ in rep)
+    got = from_dev(dC, m, n)
+    want = _oracle_c(A, B, m, n, k, chosen)
+    if want is not None:
+        assert np.array_equal(got, want)
+    else:
+        hi, lo, ab = orc.dd_gemm(A, B, 0, 0, m, n, k)
+        assert np.all(np.abs(got - hi) <= k * 2.0 ** -53 * ab + 1e-300)
+    # later execs reuse the choice without tuning
+    assert e.exec(dA, lda, dB, ldb, dC, m) == 0 and e.get_tune() == chosen and e.s.n_exec == 2
+    e.free()
+
+
+def test_guard_rejects_split_precision_where_it_loses_accuracy(cuda):
+    """Rows whose one large entry meets a zero row of B: their C entries come
+    from entries 2^40 below the row maximum, which P-bit rounding below the
+    maximum wipes out.  The guard rejects every split candidate; the engine
+    keeps the plain GEMM."""
+    m, n, k = 512, 384, 640
+    rng = np.random.default_rng(5)
+    A = rng.uniform(-1, 1, (m, k))
+    B = rng.uniform(-1, 1, (k, n))
+    spiky = rng.choice(m, 16, replace=False)
+    A[spiky, 0] = 2.0 ** 40
+    B[0, :] = 0.0
+    dA, lda = to_dev(A)
+    dB, ldb = to_dev(B)
+    dC = dev_zeros(m * n)
+    e = cb.Ca3dmmEngine(m, n, k)
+    rc, chosen = e.autotune(dA, lda, dB, ldb, dC, m, how=2)
+    assert rc == 0
+    rep = e.tune_report()
+    assert all(ms == -2 for c, ms, _ in rep if c[0] != cb.GEMM_PLAIN), rep
+    assert chosen[0] == cb.GEMM_PLAIN
+    assert e.exec(dA, lda, dB, ldb, dC, m) == 0
+    hi, lo, ab = orc.dd_gemm(A, B, 0, 0, m, n, k)
+    got = from_dev(dC, m, n)
+    assert np.all(np.abs(got - hi) <= k * 2.0 ** -53 * ab + 1e-300)
+    e.free()
+
+
+def test_guard_rejects_split_on_nonfinite_operands(cuda):
+    m, n, k = 256, 256, 300
+    A = orc.gen_uniform(3, m, k)
+    B = orc.gen_uniform(4, k, n)
+    A[7, 11] = np.inf
+    dA, lda = to_dev(A)
+    dB, ldb = to_dev(B)
+    dC = dev_zeros(m * n)
+    e = cb.Ca3dmmEngine(m, n, k)
+    rc, chosen = e.autotune(dA, lda, dB, ldb, dC, m, how=2)
+    assert rc == 0 and chosen[0] == cb.GEMM_PLAIN
+    assert all(ms == -2 for c, ms, _ in e.tune_report() if c[0] != cb.GEMM_PLAIN)
+    e.free()
+
+
+def test_tune_cache_and_host_exec(cuda, tmp_path, monkeypatch):
+    """CA3DMM_GEMM_MODE=auto with CA3DMM_TUNE_CACHE: the first engine tunes and
+    appends its choice; a second engine of the same problem takes it from the
+    cache (one report entry, no timing), here through exec_host."""
+    import torch
+    cache = tmp_path / "tune.txt"
+    monkeypatch.setenv("CA3DMM_GEMM_MODE", "auto")
+    monkeypatch.setenv("CA3DMM_TUNE_CACHE", str(cache))
+    monkeypatch.setenv("CA3DMM_AUTOTUNE", "exhaustive")
+    m, n, k = 700, 500, 800
+    A = orc.gen_signed_exp(21, m, k, emin=-2, emax=2)
+    B = orc.gen_signed_exp(22, k, n, emin=-2, emax=2)
+    dA, lda = to_dev(A)
+    dB, ldb = to_dev(B)
+    dC = dev_zeros(m * n)
+    e1 = cb.Ca3dmmEngine(m, n, k, p=4)
+    assert e1.s.gemm_auto == 1
+    assert e1.exec(dA, lda, dB, ldb, dC, m) == 0
+    first = e1.get_tune()
+    assert len(e1.tune_report()) > 1
+    e1.free()
+    line = cache.read_text().strip().splitlines()
+    assert len(line) == 1 and line[0].startswith("v1 700 500 800 0 0 0 0 ")
+    e2 = cb.Ca3dmmEngine(m, n, k, p=4)
+    hA = torch.from_numpy(np.asfortranarray(A).ravel(order="F").copy()).pin_memory()
+    hB = torch.from_numpy(np.asfortranarray(B).ravel(order="F").copy()).pin_memory()
+    hC = torch.zeros(m * n, dtype=torch.float64).pin_memory()
+    assert e2.exec_host(hA, m, hB, k, hC, m) == 0
+    assert e2.s.gemm_auto == 2 and e2.get_tune() == first
+    assert len(e2.tune_report()) == 1
+    got = np.asfortranarray(hC.numpy().reshape((m, n), order="F"))
+    want = _oracle_c(A, B, m, n, k, first)
+    if want is not None and e2.s.kp == 1:
+        assert np.array_equal(got, want)
+    hi, lo, ab = orc.dd_gemm(A, B, 0, 0, m, n, k)
+    assert np.all(np.abs(got - hi) <= 2 * k * 2.0 ** -53 * ab + 1e-300)
+    e2.free()
 
 
 def test_shipped_model_predicts_like_the_oracle(cuda):
