@@ -54,6 +54,9 @@ def parse():
                     help="square workload entries: sign*(1+u)*2^e, e in [-8,8] (8000^3), or "
                          "uniform in [-1,1) (the 2048^3 example workload)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--gemm", default="auto", choices=["auto", "plain", "ozaki", "crt"],
+                    help="leg timed as the headline (auto: the fastest split leg whose error is "
+                         "no worse than plain's); a fixed leg keeps profiling captures on one path")
     ap.add_argument("--workload", default="square", choices=["square", "grouped", "btb"],
                     help="square: the headline 8000^3 engine exec; grouped: 256 uneven "
                          "independent GEMMs in one graph-captured launch; btb: B^T B of a "
@@ -738,6 +741,8 @@ def main():
         if ec["normwise"] <= ep["normwise"] and ec["vs_absprod"] <= ep["vs_absprod"] and (
                 head == "plain" or legs[cand]["ms_per_step"] < legs[head]["ms_per_step"]):
             head = cand
+    if args.gemm != "auto":
+        head = args.gemm
     eng = engines[head]
 
     # timed region (headline leg), clocks sampled meanwhile
