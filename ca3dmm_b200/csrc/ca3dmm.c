@@ -51,6 +51,8 @@ typedef struct {
     long long direct_ld;
 } blk_t;
 
+#define CRT_MAX_BANDS 16
+
 typedef struct {
     int ngroup, nA, nB;
     int tmn, tnn;             /* row / column blocks of the internal grouping (1: merged) */
@@ -103,6 +105,11 @@ typedef struct {
                                      (env CA3DMM_CRT_BAND, default 32 -- measured best at
                                      8000^3; 0: all tile rows in one band) */
     int crt_band_env;             /* crt_band as the environment set it */
+    int crt_overlap;              /* device exec: reconstruct band b beside the GEMM of band b + 1
+                                     (env CA3DMM_CRT_OVERLAP=1) */
+    cudaStream_t st_aux;          /* the reconstruction stream of the overlapped exec */
+    cudaEvent_t ev_band[CRT_MAX_BANDS], ev_join;
+    int aux_ok;
     int crt_tile_n;               /* CRT GEMM tile columns, 128 or 256 (env CA3DMM_CRT_TILE_N) */
     int upload_for_host;          /* the plan being uploaded serves exec_host's row bands */
     /* guard bands: 256-byte canaries between the work buffer's regions, filled
@@ -366,6 +373,7 @@ static int plan_build(ca3dmm_engine_p e)
     GET_ENV_INT_VAR(pl->crt_band, "CA3DMM_CRT_BAND", "crt_band", 32, 0, 1 << 20);
     pl->crt_band_env = pl->crt_band;
     GET_ENV_INT_VAR(pl->crt_tile_n, "CA3DMM_CRT_TILE_N", "crt_tile_n", 256, 128, 256);
+    GET_ENV_INT_VAR(pl->crt_overlap, "CA3DMM_CRT_OVERLAP", "crt_overlap", 0, 0, 1);
     if (pl->crt_tile_n != 128) pl->crt_tile_n = 256;
     GET_ENV_INT_VAR(pl->check_canary, "CA3DMM_CANARY", "check_canary", 0, 0, 1);
     pl->gd = (ca3dmm_dgemm_desc_t *) calloc((size_t) pl->ngroup * (size_t) pl->ksplit,
@@ -492,6 +500,11 @@ static void plan_free(plan_t *pl)
     if (pl->status_h) cudaFreeHost(pl->status_h);
     if (pl->events_ok)
         for (int i = 0; i < 5; i++) cudaEventDestroy(pl->ev[i]);
+    if (pl->aux_ok) {
+        cudaStreamDestroy(pl->st_aux);
+        for (int i = 0; i < CRT_MAX_BANDS; i++) cudaEventDestroy(pl->ev_band[i]);
+        cudaEventDestroy(pl->ev_join);
+    }
     free(pl);
 }
 
@@ -1225,6 +1238,67 @@ static int launch_guard_check(const ca3dmm_engine_p e, const plan_t *pl, int *st
     return ca3dmm_guard_check_launch(e->workbuf_d, &g, status_d, st);
 }
 
+/* Modular mode, device exec of one group: the bands of its work list (crt_band
+ * tile rows each) run as one GEMM launch per band on `st`, and the
+ * reconstruction of band b runs on the auxiliary stream as soon as band b's
+ * residue planes are complete -- beside the GEMM of band b + 1 (two blocks per
+ * SM fit next to the GEMM's CTA: 2 x 256 x 48 registers and 2 x 4 KB of shared
+ * memory, with the same shared-memory carveout).  Returns the number of bands
+ * so run (0: not overlapped). */
+static int crt_overlapped_gemm(ca3dmm_engine_p e, plan_t *pl, int *status_d, cudaStream_t st,
+                               int *rc_out)
+{
+    *rc_out = CA3DMM_OK;
+    if (!pl->crt_overlap || pl->crt_nsl != 1 || pl->upload_for_host || e->m <= 0) return 0;
+    const int tiles_m = (e->m + 127) / 128;
+    const int band = pl->crt_band > 0 ? pl->crt_band : tiles_m;
+    int per = band, nb = (tiles_m + band - 1) / band;
+    while (nb > CRT_MAX_BANDS) {              /* several work-list bands per launch */
+        per += band;
+        nb = (tiles_m + per - 1) / per;
+    }
+    if (nb < 2) return 0;
+    if (!pl->aux_ok) {
+        if (cudaStreamCreateWithFlags(&pl->st_aux, cudaStreamNonBlocking) != cudaSuccess) return 0;
+        for (int i = 0; i < CRT_MAX_BANDS; i++)
+            cudaEventCreateWithFlags(&pl->ev_band[i], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&pl->ev_join, cudaEventDisableTiming);
+        pl->aux_ok = 1;
+    }
+    const char *hp = (const char *) pl->stage + pl->off_crtplan;
+    const int sms = ca3dmm_device_sm_count();
+    int rc = CA3DMM_OK;
+    for (int b = 0; b < nb && !rc; b++) {
+        const int lo = b * per, hi = lo + per < tiles_m ? lo + per : tiles_m;
+        int begin = 0, count = 0;
+        rc = ca3dmm_crt_group_items(hp, 0, lo, hi, &begin, &count);
+        if (rc) break;
+        ca3dmm_tile_ranges_t rg;
+        memset(&rg, 0, sizeof(rg));
+        rg.n = 1;
+        rg.begin[0] = begin;
+        rg.len[0] = count;
+        rc = ca3dmm_crt_run_gemm(&pl->crt, &rg, status_d, 5.0, st);
+        if (rc) break;
+        if (cudaEventRecord(pl->ev_band[b], st) != cudaSuccess ||
+            cudaStreamWaitEvent(pl->st_aux, pl->ev_band[b], 0) != cudaSuccess) {
+            rc = CA3DMM_ECUDA;
+            break;
+        }
+        /* two blocks per SM beside the next band's GEMM; the last band alone */
+        const int r1 = hi * 128 < e->m ? hi * 128 : e->m;
+        rc = ca3dmm_crt_run_reconstruct_capped(&pl->crt, 0, 1, lo * 128, r1,
+                                               b + 1 < nb ? 2 * sms : 0, pl->st_aux);
+    }
+    if (rc) {
+        /* nothing of this exec may still run on the auxiliary stream after it returns */
+        cudaEventRecord(pl->ev_join, pl->st_aux);
+        cudaStreamWaitEvent(st, pl->ev_join, 0);
+    }
+    *rc_out = rc;
+    return nb;
+}
+
 static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void *src_B, int ldB,
                        void *dst_C, int ldC, cudaStream_t st)
 {
@@ -1269,8 +1343,10 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
     if (timing) cudaEventRecord(pl->ev[1], st);
     int *status_d = (int *) (w + pl->off_status);
     nvtxRangePushA("ca3dmm: GEMM (2D Cannon)");
+    int crt_bands = 0;
     if (crt) {
-        rc = ca3dmm_crt_run_gemm(&pl->crt, NULL, status_d, 5.0, st);
+        crt_bands = crt_overlapped_gemm(e, pl, status_d, st, &rc);
+        if (!crt_bands && !rc) rc = ca3dmm_crt_run_gemm(&pl->crt, NULL, status_d, 5.0, st);
     } else if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
         rc = ca3dmm_oz_run_gemm(&pl->oz, status_d, 5.0, st);
         if (!rc) rc = ca3dmm_oz_run_nonfinite(&pl->oz, NULL, src_A, src_B, st);
@@ -1283,8 +1359,15 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
     nvtxRangePushA("ca3dmm: reduce (slab sum, reconstruction)");
     if (crt) {
         /* the modular mode's reconstruction of C (with the slab sum below, the
-         * "reduce" phase of the timers) */
-        rc = ca3dmm_crt_run_reconstruct(&pl->crt, 0, pl->crt_nsl, 0, INT32_MAX, st);
+         * "reduce" phase of the timers); overlapped: what is left of it after
+         * the last GEMM band */
+        if (crt_bands) {
+            if (cudaEventRecord(pl->ev_join, pl->st_aux) != cudaSuccess ||
+                cudaStreamWaitEvent(st, pl->ev_join, 0) != cudaSuccess)
+                rc = CA3DMM_ECUDA;
+        } else {
+            rc = ca3dmm_crt_run_reconstruct(&pl->crt, 0, pl->crt_nsl, 0, INT32_MAX, st);
+        }
         if (!rc) rc = ca3dmm_crt_run_nonfinite(&pl->crt, 0, pl->crt_nsl, 0, INT32_MAX, src_A, src_B,
                                                st);
     }

@@ -100,6 +100,10 @@ int ca3dmm_crt_run_gemm(const ca3dmm_crt_plan_t *pl, const ca3dmm_tile_ranges_t 
 /* C from the residue planes, for groups [g0, g1) and rows [r0, r1) of each. */
 int ca3dmm_crt_run_reconstruct(const ca3dmm_crt_plan_t *pl, int g0, int g1, int r0, int r1,
                                cudaStream_t stream);
+/* The same with at most max_blocks blocks of 256 threads (0: 8 per SM), so
+ * that it can share the SMs with a GEMM launch running beside it. */
+int ca3dmm_crt_run_reconstruct_capped(const ca3dmm_crt_plan_t *pl, int g0, int g1, int r0, int r1,
+                                      int max_blocks, cudaStream_t stream);
 /* IEEE values of the entries in rows / columns holding an Inf or a NaN, for
  * groups [g0, g1) and rows [r0, r1); after the reconstruction.  Returns at once
  * on the device when no row or column was flagged. */

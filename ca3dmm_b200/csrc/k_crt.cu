@@ -1080,6 +1080,13 @@ extern "C" int ca3dmm_crt_run_gemm(const ca3dmm_crt_plan_t *pl, const ca3dmm_til
 extern "C" int ca3dmm_crt_run_reconstruct(const ca3dmm_crt_plan_t *pl, int g0, int g1, int r0,
                                           int r1, cudaStream_t stream)
 {
+    return ca3dmm_crt_run_reconstruct_capped(pl, g0, g1, r0, r1, 0, stream);
+}
+
+extern "C" int ca3dmm_crt_run_reconstruct_capped(const ca3dmm_crt_plan_t *pl, int g0, int g1,
+                                                 int r0, int r1, int max_blocks,
+                                                 cudaStream_t stream)
+{
     if (g0 < 0) g0 = 0;
     if (g1 > pl->ngroup) g1 = pl->ngroup;
     if (g1 <= g0) return CA3DMM_OK;
@@ -1098,11 +1105,16 @@ extern "C" int ca3dmm_crt_run_reconstruct(const ca3dmm_crt_plan_t *pl, int g0, i
     const unsigned char *w = static_cast<const unsigned char *>(pl->dev_work);
     if (total <= 0) return CA3DMM_OK;
     long long blocks = (total + 255) / 256;
-    const long long cap = (long long) ca3dmm_device_sm_count() * 8;
+    const long long cap = max_blocks > 0 ? max_blocks : (long long) ca3dmm_device_sm_count() * 8;
     if (blocks > cap) blocks = cap;
+    // the same shared-memory carveout as the GEMM, so that blocks of this
+    // kernel can share an SM with a GEMM CTA running beside it
     switch (pl->nmod) {
 #define CA3DMM_CRT_CASE(N)                                                                          \
     case N:                                                                                         \
+        CA3DMM_CUDA_TRY(cudaFuncSetAttribute(crt_reconstruct_kernel<N, crt_limbs(N)>,              \
+                                             cudaFuncAttributePreferredSharedMemoryCarveout,      \
+                                             (int) cudaSharedmemCarveoutMaxShared));              \
         crt_reconstruct_kernel<N, crt_limbs(N)><<<(unsigned) blocks, 256, 0, stream>>>(            \
             groups, g0, g1, r0, r1, total, w);                                                     \
         break;
