@@ -106,7 +106,8 @@ typedef struct {
                                      8000^3; 0: all tile rows in one band) */
     int crt_band_env;             /* crt_band as the environment set it */
     int crt_overlap;              /* device exec: reconstruct band b beside the GEMM of band b + 1
-                                     (env CA3DMM_CRT_OVERLAP=1) */
+                                     (env CA3DMM_CRT_OVERLAP, default 1) */
+    int crt_overlap_blocks;       /* reconstruction blocks per SM beside the GEMM (1 or 2) */
     cudaStream_t st_aux;          /* the reconstruction stream of the overlapped exec */
     cudaEvent_t ev_band[CRT_MAX_BANDS], ev_join;
     int aux_ok;
@@ -373,7 +374,8 @@ static int plan_build(ca3dmm_engine_p e)
     GET_ENV_INT_VAR(pl->crt_band, "CA3DMM_CRT_BAND", "crt_band", 32, 0, 1 << 20);
     pl->crt_band_env = pl->crt_band;
     GET_ENV_INT_VAR(pl->crt_tile_n, "CA3DMM_CRT_TILE_N", "crt_tile_n", 256, 128, 256);
-    GET_ENV_INT_VAR(pl->crt_overlap, "CA3DMM_CRT_OVERLAP", "crt_overlap", 0, 0, 1);
+    GET_ENV_INT_VAR(pl->crt_overlap, "CA3DMM_CRT_OVERLAP", "crt_overlap", 1, 0, 1);
+    GET_ENV_INT_VAR(pl->crt_overlap_blocks, "CA3DMM_CRT_OVERLAP_BLOCKS", "crt_overlap_blocks", 2, 1, 2);
     if (pl->crt_tile_n != 128) pl->crt_tile_n = 256;
     GET_ENV_INT_VAR(pl->check_canary, "CA3DMM_CANARY", "check_canary", 0, 0, 1);
     pl->gd = (ca3dmm_dgemm_desc_t *) calloc((size_t) pl->ngroup * (size_t) pl->ksplit,
@@ -1285,10 +1287,11 @@ static int crt_overlapped_gemm(ca3dmm_engine_p e, plan_t *pl, int *status_d, cud
             rc = CA3DMM_ECUDA;
             break;
         }
-        /* two blocks per SM beside the next band's GEMM; the last band alone */
+        /* one or two blocks per SM beside the next band's GEMM; the last band alone */
         const int r1 = hi * 128 < e->m ? hi * 128 : e->m;
         rc = ca3dmm_crt_run_reconstruct_capped(&pl->crt, 0, 1, lo * 128, r1,
-                                               b + 1 < nb ? 2 * sms : 0, pl->st_aux);
+                                               b + 1 < nb ? pl->crt_overlap_blocks * sms : 0,
+                                               pl->st_aux);
     }
     if (rc) {
         /* nothing of this exec may still run on the auxiliary stream after it returns */
