@@ -1108,13 +1108,18 @@ extern "C" int ca3dmm_crt_run_reconstruct_capped(const ca3dmm_crt_plan_t *pl, in
     const long long cap = max_blocks > 0 ? max_blocks : (long long) ca3dmm_device_sm_count() * 8;
     if (blocks > cap) blocks = cap;
     // the same shared-memory carveout as the GEMM, so that blocks of this
-    // kernel can share an SM with a GEMM CTA running beside it
+    // kernel can share an SM with a GEMM CTA running beside it (set once per
+    // instantiation and process)
+    static bool carveout_set[MAXMOD + 1] = {};
     switch (pl->nmod) {
 #define CA3DMM_CRT_CASE(N)                                                                          \
     case N:                                                                                         \
-        CA3DMM_CUDA_TRY(cudaFuncSetAttribute(crt_reconstruct_kernel<N, crt_limbs(N)>,              \
-                                             cudaFuncAttributePreferredSharedMemoryCarveout,      \
-                                             (int) cudaSharedmemCarveoutMaxShared));              \
+        if (!carveout_set[N]) {                                                                     \
+            CA3DMM_CUDA_TRY(cudaFuncSetAttribute(crt_reconstruct_kernel<N, crt_limbs(N)>,          \
+                                                 cudaFuncAttributePreferredSharedMemoryCarveout,  \
+                                                 (int) cudaSharedmemCarveoutMaxShared));          \
+            carveout_set[N] = true;                                                                 \
+        }                                                                                           \
         crt_reconstruct_kernel<N, crt_limbs(N)><<<(unsigned) blocks, 256, 0, stream>>>(            \
             groups, g0, g1, r0, r1, total, w);                                                     \
         break;
