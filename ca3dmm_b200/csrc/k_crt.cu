@@ -74,7 +74,10 @@ struct ModConst {
     unsigned int mrec;   // floor(2^32 / p): floor(y mrec / 2^32) is floor(y / p) or one less (y < 2^28)
     int half;        // floor(p/2)
     int bias;        // a multiple of p above 2^15 * 255 (keeps the epilogue's sums >= 0)
-    int off54;       // p - (2^54 mod p) (keeps the residue pass's sums >= 0)
+    int off54;       // p - (2^54 mod p)
+    double c27;      // 2^27 mod p (the residue pass, in FP64)
+    double inv;      // 1 / p rounded to double
+    double pd;       // p
 };
 
 constexpr ModConst make_mod(int p)
@@ -86,7 +89,10 @@ constexpr ModConst make_mod(int p)
                     (unsigned int) ((1ULL << 32) / (unsigned long long) p),
                     p / 2,
                     (int) (((8650752LL + p - 1) / p) * p),   // a multiple of p >= 2^23 + 2^18
-                    (int) (p - (int) ((1ULL << 54) % (unsigned long long) p))};
+                    (int) (p - (int) ((1ULL << 54) % (unsigned long long) p)),
+                    (double) ((1LL << 27) % p),
+                    1.0 / (double) p,
+                    (double) p};
 }
 
 struct ModTable {
@@ -200,9 +206,18 @@ double log2_modprod(int nmod)
 // is below 2^28 and congruent to a' + floor(p/2); q = floor(y floor(2^32/p) / 2^32)
 // is floor(y / p) or one less, r = y - q p in [0, 2p) is folded once, and the
 // residue byte is r - floor(p/2).
+// The residues of the row / column integers a' = rint(a 2^(P - E)) (|a'| <=
+// 2^53), as signed bytes in [-(p-1)/2, (p-1)/2] (p odd) and [-128, 127]
+// (p = 256).  They are formed in FP64, whose pipe the integer multiply-add
+// path of the other passes leaves idle: a' = h 2^27 + l with |h|, |l| <= 2^26,
+// then per odd modulus y = h (2^27 mod p) + l (|y| < 2^35, exact), q = the
+// nearest integer to y / p (y (1/p) is within 2^-23 of y / p, which is never
+// closer than 1 / (2p) to a half-integer for odd p), r = y - q p exact; the
+// low bits of r + 1.5 2^52 are r in two's complement.  For p = 256 the byte is
+// the low byte of l (a' = l mod 256).  Every value is the unique representative
+// of a' mod p in that range, so the bytes equal the integer formulation's.
 struct ResidueWriter {
-    // the pass is issue-bound: four blocks of 256 threads per SM hide latency
-    static constexpr int kMinBlocks = 4;
+    static constexpr int kMinBlocks = 2;
     static __device__ __forceinline__ void write16(const SliceDesc &d, unsigned char *__restrict__ work,
                                                    const unsigned long long *__restrict__ mwork,
                                                    int gr, int gl, const double (&x)[16])
@@ -215,14 +230,14 @@ struct ResidueWriter {
             reinterpret_cast<int *>(work)[d.e_off + gr] = (fin && mr) ? E + EXP_BIAS : 0;
         const int sh = d.p_bits - E;
         const double up1 = ldexp(1.0, sh / 2), up2 = ldexp(1.0, sh - sh / 2);
-        unsigned int x0[16], x1[16], x2[16];
+        constexpr double MAGIC = 6755399441055744.0;          // 1.5 2^52
+        double hh[16], lm[16];
 #pragma unroll
         for (int j = 0; j < 16; ++j) {
-            const long long a = __double2ll_rn((fin ? x[j] : 0.0) * up1 * up2);
-            const unsigned long long v = (unsigned long long) a + (1ull << 54);
-            x0[j] = (unsigned int) (v & 0x3ffffu);
-            x1[j] = (unsigned int) ((v >> 18) & 0x3ffffu);
-            x2[j] = (unsigned int) (v >> 36);
+            const double a = rint((fin ? x[j] : 0.0) * up1 * up2);
+            const double h = (a * 0x1p-27 + MAGIC) - MAGIC;   // nearest integer, |h| <= 2^26
+            hh[j] = h;
+            lm[j] = fma(-h, 0x1p27, a) + MAGIC;              // l + 1.5 2^52, exact
         }
         const int rt = gr / d.tile_rows, rr = gr % d.tile_rows;
         const int kb = gl >> 7, chunk = (gl & 127) >> 4;
@@ -230,16 +245,17 @@ struct ResidueWriter {
                              rr * CKB + ((chunk ^ (rr & 7)) << 4);
         for (int t = 0; t < d.nmod; ++t) {
             const ModConst mc = kMod.m[t];
-            const unsigned int add = (unsigned int) (mc.off54 + mc.half);
             unsigned int r[16];
+            if (mc.p == 256) {
 #pragma unroll
-            for (int j = 0; j < 16; ++j) {
-                const unsigned int y = x2[j] * (unsigned int) mc.c36 + x1[j] * (unsigned int) mc.c18 +
-                                       x0[j] + add;
-                const unsigned int q = __umulhi(y, mc.mrec);
-                const unsigned int rr0 = y - q * (unsigned int) mc.p;
-                const unsigned int r1 = rr0 - (unsigned int) mc.p;
-                r[j] = (rr0 < r1 ? rr0 : r1) - (unsigned int) mc.half;   // min folds [p, 2p) down
+                for (int j = 0; j < 16; ++j) r[j] = (unsigned int) __double2loint(lm[j]);
+            } else {
+#pragma unroll
+                for (int j = 0; j < 16; ++j) {
+                    const double yb = fma(hh[j], mc.c27, lm[j]);      // y + 1.5 2^52
+                    const double q = fma(yb - MAGIC, mc.inv, MAGIC) - MAGIC;
+                    r[j] = (unsigned int) __double2loint(fma(-q, mc.pd, yb));
+                }
             }
             uint32_t out[4];
 #pragma unroll
