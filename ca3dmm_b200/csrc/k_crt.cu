@@ -68,6 +68,7 @@ constexpr int DEFAULT_BAND = 8;
 // arithmetic: 2^16, 2^18, 2^36 mod p, and floor(2^32 / p).
 constexpr int kModList[MAXMOD] = {256, 255, 253, 251, 247, 241, 239, 233, 229,
                                   227, 223, 217, 211, 199, 197, 193, 191, 181};
+static_assert(kModList[0] == 256, "the residue pass takes modulus 0 as the byte of the integer");
 
 struct ModConst {
     int p, c16, c18, c36;
@@ -243,18 +244,19 @@ struct ResidueWriter {
         const int kb = gl >> 7, chunk = (gl & 127) >> 4;
         unsigned char *dst = work + d.q_off + ((long long) rt * d.nkb + kb) * d.tile_rows * CKB +
                              rr * CKB + ((chunk ^ (rr & 7)) << 4);
+        // modulus 0 is 256 (kModList), the others are odd
         for (int t = 0; t < d.nmod; ++t) {
-            const ModConst mc = kMod.m[t];
             unsigned int r[16];
-            if (mc.p == 256) {
+            if (t == 0) {
 #pragma unroll
                 for (int j = 0; j < 16; ++j) r[j] = (unsigned int) __double2loint(lm[j]);
             } else {
+                const double c27 = kMod.m[t].c27, inv = kMod.m[t].inv, pd = kMod.m[t].pd;
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
-                    const double yb = fma(hh[j], mc.c27, lm[j]);      // y + 1.5 2^52
-                    const double q = fma(yb - MAGIC, mc.inv, MAGIC) - MAGIC;
-                    r[j] = (unsigned int) __double2loint(fma(-q, mc.pd, yb));
+                    const double yb = fma(hh[j], c27, lm[j]);      // y + 1.5 2^52
+                    const double q = fma(yb - MAGIC, inv, MAGIC) - MAGIC;
+                    r[j] = (unsigned int) __double2loint(fma(-q, pd, yb));
                 }
             }
             uint32_t out[4];
