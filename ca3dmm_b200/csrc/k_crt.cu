@@ -5,26 +5,29 @@
 //  2. slice_kc/rc_kernel<ResidueWriter> -- E = frexp exponent of the row max,
 //                         a' = rint(x 2^(P-E)) (|a'| <= 2^P), and for every
 //                         modulus p_t the residue a' mod p_t as a signed byte in
-//                         [-floor(p/2), ceil(p/2) - 1], written straight into the
-//                         GEMM's shared-memory image: per modulus, 128-row (A) /
+//                         [-floor(p/2), ceil(p/2) - 1] (computed in FP64), written
+//                         straight into the GEMM's shared-memory image: per
+//                         modulus, 128-row (A) /
 //                         256-row (B) tile and 128-byte k block, a K-major tile
 //                         with the 128-byte swizzle (16-byte chunk ^= row & 7).
-//  3. crt_gemm_kernel  -- per modulus, the INT8 product of the residues on the
-//                         tcgen05 tensor cores: 128 x 256 output tiles, K = 32 per
-//                         MMA, S32 accumulators in TMEM (two 256-column buffers, so
-//                         the epilogue of one tile overlaps the next tile's MMAs).
+//  3. crt_gemm_kernel<TN> -- per modulus, the INT8 product of the residues on the
+//                         tcgen05 tensor cores: 128 x TN output tiles (TN = 256 or
+//                         128), K = 32 per MMA, S32 accumulators in TMEM (two
+//                         TN-column buffers, so the epilogue of one tile overlaps
+//                         the next tile's MMAs).
 //                         The sums are exact (k 2^14 < 2^31); the epilogue reduces
 //                         each mod p_t into a byte plane of C's residues.
-//  4. crt_reconstruct_kernel<N> -- per C entry, C' from its N residues by the
-//                         Chinese remainder theorem in 160-bit integer arithmetic
-//                         (weights in constant memory), rounded once to double
-//                         and scaled by 2^(E_i + F_j - 2P).
+//  4. crt_reconstruct_kernel<N, L> -- per C entry, C' from its N residues by the
+//                         Chinese remainder theorem: limb sums of the weights (in
+//                         constant memory), an FP64 quotient estimate, the low 128
+//                         bits exact; rounded once to double and scaled by
+//                         2^(E_i + F_j - 2P).
 //  5. crt_nonfinite_kernel -- rows / columns holding an Inf or a NaN were zero rows;
 //                         writes their entries' IEEE value.
 // Warp roles of the GEMM: warp 0 bulk-copy producer, warps 1-2 MMA issuers (two
 // of the four k steps of each stage each: one issuing thread alone does not keep
 // the tensor pipe busy), warps 3-10 epilogue (warp w reads TMEM lanes
-// 32 (w % 4) .. +31, columns 0-127 or 128-255 of the accumulator).  The MMAs only
+// 32 (w % 4) .. +31, columns 0 .. TN/2-1 or TN/2 .. TN-1 of the accumulator).  The MMAs only
 // accumulate; the epilogue zeroes each accumulator after reading it.  Every wait
 // is bounded; on timeout the kernel records a status, drains, frees TMEM, returns.
 #include <cuda.h>
