@@ -5,9 +5,9 @@
  * (src/ca3dmm.h:114-200; examples/example_AB.c:85-98 passes 1D column
  * blocks).  ca3dmm_dist_engine_* is that call with the communicator replaced
  * by a transport: two collectives the engine needs, as function pointers, so
- * that an MPI caller passes MPI_Allgather / MPI_Alltoallv (INTEGRATION.md
- * shows the ten-line adapter), a C caller without MPI uses the built-in NCCL
- * transport, and ranks that are threads of one process use the built-in
+ * that an MPI caller passes MPI_Allgather / MPI_Alltoallv_c through two
+ * wrapper functions of a few lines, a C caller without MPI uses the built-in
+ * NCCL transport, and ranks that are threads of one process use the built-in
  * thread transport.
  *
  * Each rank computes the reference's grid and every rank's cuboid for
