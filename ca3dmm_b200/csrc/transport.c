@@ -2,7 +2,9 @@
  * process exchanging through host memory, and NCCL loaded at run time. */
 #define _GNU_SOURCE
 #include <dlfcn.h>
+#include <errno.h>
 #include <pthread.h>
+#include <time.h>
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -16,11 +18,53 @@
 
 typedef struct {
     int size;
-    pthread_barrier_t bar;
+    pthread_mutex_t mu;         /* a barrier with a time limit: a rank that never */
+    pthread_cond_t cv;          /* arrives fails the others' collective instead of */
+    int arrived;                /* hanging them (CA3DMM_DIST_TIMEOUT seconds, 300) */
+    unsigned long long phase;
+    int broken;
+    double limit_s;
     const void **ptr;           /* per rank: its send buffer / contribution */
     const long long **cnt, **dsp;
     int n;                      /* allgather: values per rank */
 } thr_shared_t;
+
+/* 0 when every rank arrived; nonzero when the limit passed first (the
+ * exchange area is then broken and every later collective fails at once) */
+static int thr_barrier(thr_shared_t *s)
+{
+    pthread_mutex_lock(&s->mu);
+    if (s->broken) {
+        pthread_mutex_unlock(&s->mu);
+        return 1;
+    }
+    const unsigned long long ph = s->phase;
+    if (++s->arrived == s->size) {
+        s->arrived = 0;
+        s->phase++;
+        pthread_cond_broadcast(&s->cv);
+        pthread_mutex_unlock(&s->mu);
+        return 0;
+    }
+    struct timespec dl;
+    clock_gettime(CLOCK_REALTIME, &dl);
+    const double lim = s->limit_s;
+    dl.tv_sec += (time_t) lim;
+    dl.tv_nsec += (long) ((lim - (double) (time_t) lim) * 1e9);
+    if (dl.tv_nsec >= 1000000000L) { dl.tv_sec++; dl.tv_nsec -= 1000000000L; }
+    int rc = 0;
+    while (s->phase == ph && !s->broken) {
+        if (pthread_cond_timedwait(&s->cv, &s->mu, &dl) == ETIMEDOUT && s->phase == ph) {
+            s->broken = 1;
+            pthread_cond_broadcast(&s->cv);
+            ERROR_PRINTF("thread transport: a rank did not arrive within %.0f s\n", lim);
+            break;
+        }
+    }
+    if (s->phase == ph) rc = 1;
+    pthread_mutex_unlock(&s->mu);
+    return rc;
+}
 
 typedef struct {
     thr_shared_t *sh;
@@ -32,11 +76,10 @@ static int thr_allgather(void *ctx, const long long *mine, int n, long long *all
     thr_rank_t *t = (thr_rank_t *) ctx;
     thr_shared_t *s = t->sh;
     s->ptr[t->rank] = mine;
-    pthread_barrier_wait(&s->bar);
+    if (thr_barrier(s)) return 1;
     for (int r = 0; r < s->size; r++)
         memcpy(all + (size_t) r * n, s->ptr[r], sizeof(long long) * (size_t) n);
-    pthread_barrier_wait(&s->bar);   /* no rank leaves while a peer still reads its values */
-    return 0;
+    return thr_barrier(s);           /* no rank leaves while a peer still reads its values */
 }
 
 static int thr_alltoallv(void *ctx, const double *send, const long long *scounts,
@@ -50,7 +93,7 @@ static int thr_alltoallv(void *ctx, const double *send, const long long *scounts
     s->ptr[me] = send;
     s->cnt[me] = scounts;
     s->dsp[me] = sdispls;
-    pthread_barrier_wait(&s->bar);
+    if (thr_barrier(s)) return 1;
     int bad = 0;
     for (int q = 0; q < s->size; q++) {
         const long long c = s->cnt[q][me];
@@ -62,7 +105,7 @@ static int thr_alltoallv(void *ctx, const double *send, const long long *scounts
             memcpy(recv + rdispls[q], (const double *) s->ptr[q] + s->dsp[q][me],
                    sizeof(double) * (size_t) c);
     }
-    pthread_barrier_wait(&s->bar);
+    if (thr_barrier(s)) return 1;
     return bad;
 }
 
@@ -76,10 +119,15 @@ int ca3dmm_transport_threads_create(int size, ca3dmm_transport_t *per_rank)
     s->ptr = (const void **) calloc((size_t) size, sizeof(void *));
     s->cnt = (const long long **) calloc((size_t) size, sizeof(void *));
     s->dsp = (const long long **) calloc((size_t) size, sizeof(void *));
-    if (!s->ptr || !s->cnt || !s->dsp || pthread_barrier_init(&s->bar, NULL, (unsigned) size)) {
+    if (!s->ptr || !s->cnt || !s->dsp) {
         free(s->ptr); free(s->cnt); free(s->dsp); free(s); free(ranks);
         return CA3DMM_ENOMEM;
     }
+    pthread_mutex_init(&s->mu, NULL);
+    pthread_cond_init(&s->cv, NULL);
+    int lim;
+    GET_ENV_INT_VAR(lim, "CA3DMM_DIST_TIMEOUT", "dist_timeout", 300, 1, 1 << 20);
+    s->limit_s = (double) lim;
     for (int r = 0; r < size; r++) {
         ranks[r].sh = s;
         ranks[r].rank = r;
@@ -99,7 +147,8 @@ void ca3dmm_transport_threads_free(ca3dmm_transport_t *per_rank)
     thr_rank_t *ranks = (thr_rank_t *) per_rank[0].ctx;
     thr_shared_t *s = ranks[0].sh;
     const int size = s->size;
-    pthread_barrier_destroy(&s->bar);
+    pthread_mutex_destroy(&s->mu);
+    pthread_cond_destroy(&s->cv);
     free(s->ptr); free(s->cnt); free(s->dsp); free(s);
     free(ranks);
     for (int r = 0; r < size; r++) per_rank[r].ctx = NULL;

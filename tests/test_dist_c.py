@@ -131,3 +131,36 @@ def test_uncovered_panel_fails():
         return rc
 
     assert all(rc != 0 for rc in _run_ranks(p, make))
+
+
+def test_a_rank_that_never_arrives_fails_the_others(monkeypatch):
+    """Failure on the host: rank 2 of 3 never joins the init's allgather.  The
+    thread transport's barrier has a time limit (CA3DMM_DIST_TIMEOUT), so ranks
+    0 and 1 fail instead of hanging, and a later collective fails at once."""
+    import time
+    monkeypatch.setenv("CA3DMM_DIST_TIMEOUT", "1")
+    p = 3
+    tr = cb.ThreadTransports(p)
+    assert tr.rc == 0
+    out = [None] * p
+
+    def body(r):
+        sa, sb, dc = _column_layout(120, 90, 70, 0, 0, p, r)
+        t0 = time.time()
+        e = cb.DistEngine(120, 90, 70, 0, 0, sa, sb, dc, tr[r])
+        out[r] = (e.rc, time.time() - t0)
+        e.free()
+
+    th = [threading.Thread(target=body, args=(r,)) for r in (0, 1)]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(30)
+    assert not any(t.is_alive() for t in th)
+    for r in (0, 1):
+        rc, dt = out[r]
+        assert rc != 0 and dt < 10, out[r]
+    # the exchange area stays broken: rank 2 arriving late fails at once
+    body(2)
+    assert out[2][0] != 0 and out[2][1] < 1.0
+    tr.free()
