@@ -220,6 +220,9 @@ double log2_modprod(int nmod)
 // low bits of r + 1.5 2^52 are r in two's complement.  For p = 256 the byte is
 // the low byte of l (a' = l mod 256).  Every value is the unique representative
 // of a' mod p in that range, so the bytes equal the integer formulation's.
+// NM: the modulus count, a template argument so that the modulus loop unrolls
+// (the constants become immediate operands and consecutive moduli interleave).
+template <int NM>
 struct ResidueWriter {
     static constexpr int kMinBlocks = 2;
     static __device__ __forceinline__ void write16(const SliceDesc &d, unsigned char *__restrict__ work,
@@ -248,7 +251,8 @@ struct ResidueWriter {
         unsigned char *dst = work + d.q_off + ((long long) rt * d.nkb + kb) * d.tile_rows * CKB +
                              rr * CKB + ((chunk ^ (rr & 7)) << 4);
         // modulus 0 is 256 (kModList), the others are odd
-        for (int t = 0; t < d.nmod; ++t) {
+#pragma unroll
+        for (int t = 0; t < NM; ++t) {
             unsigned int r[16];
             if (t == 0) {
 #pragma unroll
@@ -941,17 +945,27 @@ static int crt_residues(const ca3dmm_crt_plan_t *pl, const void *src, const Slic
         reinterpret_cast<const unsigned long long *>(w + exp_bytes(pl->n_exp));
     const int cap = ca3dmm_device_sm_count() * 4;
     const double *x = static_cast<const double *>(src);
-    if (nkc > 0) {
-        slice_kc_kernel<ResidueWriter><<<nkc < cap ? nkc : cap, 256, 0, stream>>>(x, descs, ndesc,
-                                                                                 nkc, w, mwork);
-        CA3DMM_CUDA_TRY(cudaGetLastError());
-        ca3dmm_note_launch(1);
-    }
-    if (nrc > 0) {
-        slice_rc_kernel<ResidueWriter><<<nrc < cap ? nrc : cap, 256, 0, stream>>>(x, descs, ndesc,
-                                                                                 nrc, w, mwork);
-        CA3DMM_CUDA_TRY(cudaGetLastError());
-        ca3dmm_note_launch(1);
+    switch (pl->nmod) {
+#define CA3DMM_RES_CASE(N)                                                                          \
+    case N:                                                                                         \
+        if (nkc > 0) {                                                                              \
+            slice_kc_kernel<ResidueWriter<N>><<<nkc < cap ? nkc : cap, 256, 0, stream>>>(          \
+                x, descs, ndesc, nkc, w, mwork);                                                    \
+            CA3DMM_CUDA_TRY(cudaGetLastError());                                                    \
+            ca3dmm_note_launch(1);                                                                  \
+        }                                                                                           \
+        if (nrc > 0) {                                                                              \
+            slice_rc_kernel<ResidueWriter<N>><<<nrc < cap ? nrc : cap, 256, 0, stream>>>(          \
+                x, descs, ndesc, nrc, w, mwork);                                                    \
+            CA3DMM_CUDA_TRY(cudaGetLastError());                                                    \
+            ca3dmm_note_launch(1);                                                                  \
+        }                                                                                           \
+        break;
+        CA3DMM_RES_CASE(8) CA3DMM_RES_CASE(9) CA3DMM_RES_CASE(10) CA3DMM_RES_CASE(11)
+        CA3DMM_RES_CASE(12) CA3DMM_RES_CASE(13) CA3DMM_RES_CASE(14) CA3DMM_RES_CASE(15)
+        CA3DMM_RES_CASE(16) CA3DMM_RES_CASE(17) CA3DMM_RES_CASE(18)
+#undef CA3DMM_RES_CASE
+        default: return CA3DMM_EINVAL;
     }
     return CA3DMM_OK;
 }
