@@ -247,3 +247,32 @@ def test_shipped_model_predicts_like_the_oracle(cuda):
     Xn = ((X - mu) / sd).astype(np.float32)
     _, want, _ = orc.mlp_fwd_bwd(params, Xn, np.zeros(len(Xn), np.float32), nin, h1, h2)
     assert np.allclose(got, want, rtol=1e-4, atol=1e-4), np.max(np.abs(got - want))
+
+
+def test_engine_auto_btb(cuda):
+    """B^T B in auto mode: the tuner sees op(A) = B^T (the guard samples B's
+    columns on both sides) and the result stays within the plain GEMM's bound
+    (the kept configuration passed the guard)."""
+    n, k = 300, 20000
+    Bm = orc.gen_btb(77, k, n)
+    dB, ldb = to_dev(Bm)
+    dC = dev_zeros(n * n)
+    e = cb.Ca3dmmEngine(n, n, k, p=8, btb=True)
+    assert e.set_gemm_mode(cb.GEMM_AUTO) == 0
+    import os
+    old = os.environ.get("CA3DMM_AUTOTUNE")
+    os.environ["CA3DMM_AUTOTUNE"] = "exhaustive"
+    try:
+        assert e.exec(None, 0, dB, ldb, dC, n) == 0
+    finally:
+        if old is None:
+            del os.environ["CA3DMM_AUTOTUNE"]
+        else:
+            os.environ["CA3DMM_AUTOTUNE"] = old
+    assert e.s.gemm_auto == 2
+    rep = e.tune_report()
+    assert len(rep) > 1 and all(ms > 0 or ms == -2 for _, ms, _ in rep)
+    got = from_dev(dC, n, n)
+    hi, lo, ab = orc.dd_gemm(Bm, Bm, 1, 0, n, n, k)
+    assert np.all(np.abs(got - hi) <= 2 * k * 2.0 ** -53 * ab + 1e-300)
+    e.free()
