@@ -380,11 +380,12 @@ static int prepare(struct ca3dmm_dist_engine *e)
     const int me = e->me;
     int rc = CA3DMM_OK;
     const rect_t c = e->cblk[me];
-    if (e->active[me] && c.nr > 0 && c.nc > 0 && e->kz[me] > 0) {
+    /* idempotent: a retry after a failed attempt reuses what was made */
+    if (!e->local && e->active[me] && c.nr > 0 && c.nc > 0 && e->kz[me] > 0) {
         int pm[2];
         rect_t pr[2];
         panels_of(e, me, pm, pr);
-        if (ca3dmm_vcomm_create(1, &e->local_comm)) return CA3DMM_EINVAL;
+        if (!e->local_comm && ca3dmm_vcomm_create(1, &e->local_comm)) return CA3DMM_EINVAL;
         const int ar = pr[0].nr, ac = pr[0].nc, br = pr[1].nr, bc = pr[1].nc;
         ca3dmm_engine_init(c.nr, c.nc, e->kz[me], e->ta, e->tb, 0, ar, 0, ac, 0, br, 0, bc, 0, c.nr,
                            0, c.nc, NULL, e->local_comm, DEV_TYPE_CUDA, &e->local, NULL);
@@ -399,9 +400,11 @@ static int prepare(struct ca3dmm_dist_engine *e)
     }
 #define DALLOC(p, n)                                                                        \
     do {                                                                                    \
-        if (cudaMalloc((void **) &(p), sizeof(double) * (size_t) ((n) > 0 ? (n) : 1)) !=    \
-            cudaSuccess)                                                                    \
+        if (!(p) && cudaMalloc((void **) &(p), sizeof(double) * (size_t) ((n) > 0 ? (n) : 1)) != \
+                        cudaSuccess) {                                                      \
+            (p) = NULL;                                                                     \
             return CA3DMM_ENOMEM;                                                           \
+        }                                                                                   \
     } while (0)
     DALLOC(e->d_send, e->stot);
     DALLOC(e->d_recv, e->rtot);
@@ -411,7 +414,7 @@ static int prepare(struct ca3dmm_dist_engine *e)
     DALLOC(e->d_crecv, e->crtot);
     DALLOC(e->d_layers, (long long) e->kp * area(e->dstC[me]));
 #undef DALLOC
-    if (!e->tr.device_buffers) {
+    if (!e->tr.device_buffers && !e->h_send) {
         size_t hb = sizeof(double) * (size_t) (1 + (e->stot > e->cstot ? e->stot : e->cstot));
         size_t rb = sizeof(double) * (size_t) (1 + (e->rtot > e->crtot ? e->rtot : e->crtot));
         if (cudaMallocHost((void **) &e->h_send, hb) != cudaSuccess ||
@@ -433,21 +436,21 @@ static int prepare(struct ca3dmm_dist_engine *e)
         }
     }
     for (int i = 0; i < e->nsend; i++) rm(e->send[i].x, moff(e, e->send[i].mat), dr + 4 * i);
-    if (e->nmy > 0 && e->nsend > 0)
+    if (e->nmy > 0 && e->nsend > 0 && !e->pack_ab)
         rc = mat_redist_layouts_init(e->nmy, sr, e->nsend, dr, &e->pack_ab);
     for (int i = 0; !rc && i < e->nrecv; i++) rm(e->recv[i].x, moff(e, e->recv[i].mat), sr + 4 * i);
     for (int u = 0; !rc && u < e->nuniq; u++) rm(e->urect[u], moff(e, e->umat[u]), dr + 4 * u);
-    if (!rc && e->nrecv > 0 && e->nuniq > 0 && area(e->urect[0]) > 0)
+    if (!rc && e->nrecv > 0 && e->nuniq > 0 && area(e->urect[0]) > 0 && !e->unpack_ab)
         rc = mat_redist_layouts_init(e->nrecv, sr, e->nuniq, dr, &e->unpack_ab);
     /* C: my C_2dmm block -> send pieces; received pieces -> slab layers of dst_C */
     const rect_t d = e->dstC[me];
     const int layers = e->kp > 1 ? e->kp : 1;
-    if (!rc && e->active[me] && area(c) > 0 && e->ncsend > 0) {
+    if (!rc && e->active[me] && area(c) > 0 && e->ncsend > 0 && !e->pack_c) {
         rm(c, 0, sr);
         for (int i = 0; i < e->ncsend; i++) rm(e->csend[i].x, 0, dr + 4 * i);
         rc = mat_redist_layouts_init(1, sr, e->ncsend, dr, &e->pack_c);
     }
-    if (!rc && area(d) > 0 && e->ncrecv > 0) {
+    if (!rc && area(d) > 0 && e->ncrecv > 0 && !e->unpack_c) {
         int *s2 = (int *) xcalloc(4 * (size_t) e->ncrecv, sizeof(int));
         int *d2 = (int *) xcalloc(4 * (size_t) layers, sizeof(int));
         if (!s2 || !d2) rc = CA3DMM_ENOMEM;

@@ -230,12 +230,26 @@ std::vector<int> pick(const std::vector<double> &st, int R, int K, int want)
 
 }  // namespace
 
+static int guard_build(ca3dmm_guard_t *g, int m, int n, int k, int trans_A, int trans_B,
+                       const double *A, int ldA, const double *B, int ldB, int samples,
+                       void *stream_);
+
 extern "C" int ca3dmm_guard_create(ca3dmm_guard_t *g, int m, int n, int k, int trans_A,
                                    int trans_B, const double *A, int ldA, const double *B,
                                    int ldB, int samples, void *stream_)
 {
-    if (!g || m < 1 || n < 1 || k < 1 || !A || !B || samples < 2) return CA3DMM_EINVAL;
+    if (!g) return CA3DMM_EINVAL;
     memset(g, 0, sizeof(*g));
+    const int rc = guard_build(g, m, n, k, trans_A, trans_B, A, ldA, B, ldB, samples, stream_);
+    if (rc) ca3dmm_guard_free(g);        /* nothing half-made stays allocated */
+    return rc;
+}
+
+static int guard_build(ca3dmm_guard_t *g, int m, int n, int k, int trans_A, int trans_B,
+                       const double *A, int ldA, const double *B, int ldB, int samples,
+                       void *stream_)
+{
+    if (m < 1 || n < 1 || k < 1 || !A || !B || samples < 2) return CA3DMM_EINVAL;
     cudaStream_t stream = (cudaStream_t) stream_;
     g->m = m; g->n = n; g->k = k;
     // op(A)(i, l) and op(B)(l, j) as rows of a strided matrix
