@@ -646,7 +646,7 @@ crt_reconstruct_kernel(const CrtGroup *__restrict__ groups, int g0, int g1, int 
                 for (int q = 0; q < L; ++q) a[q] = 0ull;
 #pragma unroll
                 for (int t = 0; t < N; ++t) {
-                    const unsigned int u = (u4[t] >> (8 * e)) & 0xffu;
+                    const unsigned int u = __byte_perm(u4[t], 0u, 0x4440u | (unsigned int) e);
 #pragma unroll
                     for (int q = 0; q < L; ++q) a[q] += (unsigned long long) u * kCrt.W[N][t][q];
                 }
