@@ -2,9 +2,10 @@
 that do not need the whole product on the CPU.
 
 * split precision: sampled rows x sampled columns of C equal, bit for bit, the
-  oracle's slicing and recombination of those rows of op(A) and columns of
-  op(B), slab by slab in slab order (each row's exponent depends on that row
-  alone, so a row subset is sliced exactly as inside the full block);
+  oracle's slicing and recombination (INT8 slices) or its 128-bit integer
+  product (modular scheme) of those rows of op(A) and columns of op(B), slab
+  by slab in slab order (each row's exponent depends on that row alone, so a
+  row subset is scaled exactly as inside the full block);
 * plain FP64: the same sampled entries within k u |A||B| of the double-double
   truth;
 * B^T B: the split-precision C is exactly symmetric.
@@ -75,6 +76,18 @@ def _oracle_split(ra, cb_, k, kp, s):
     return out
 
 
+def _oracle_crt(ra, cb_, k, nslab, nmod):
+    """Modular oracle for rows ra and columns cb_, slab by slab (nslab k slabs)."""
+    out = None
+    for sl in range(nslab):
+        k0, kz = orc.block_spos_size(k, nslab, sl)
+        a = np.asfortranarray(ra[:, k0:k0 + kz])
+        b = np.asfortranarray(cb_[k0:k0 + kz, :])
+        c = orc.crt_gemm(a, b, 0, 0, a.shape[0], b.shape[1], kz, orc.crt_bits(nmod, kz))
+        out = c if out is None else out + c
+    return out
+
+
 def _dd_ok(got, ra, cb_, k):
     hi, lo, ab = orc.dd_gemm(np.asfortranarray(ra), cb_, 0, 0, ra.shape[0], cb_.shape[1], k)
     err = orc.errors(np.asfortranarray(got).ravel(order="F"), hi.ravel(order="F"),
@@ -88,10 +101,14 @@ def _engine_run(m, n, k, ta, A, B, p, grid, mode, slices=7, btb=False):
     assert e.ok
     if mode == cb.GEMM_OZAKI:
         assert e.set_gemm_mode(mode, slices) == 0
+    if mode == cb.GEMM_CRT:
+        assert e.set_gemm_mode(mode, 0) == 0            # the engine's modulus count
     C = torch.empty(m * n, dtype=torch.float64, device="cuda")
     lda = 0 if btb else (k if ta else m)
     assert e.exec(None if btb else A, lda, B, k, C, m) == 0
     kp = e.s.kp
+    if mode == cb.GEMM_CRT:
+        kp = (kp, e.s.crt_moduli)
     e.free()
     return C, kp
 
@@ -107,24 +124,27 @@ def _check_square(n, ta, p, grid, gen, seed, nsel, mode):
     got = C.view(n, n).T[ri][:, cj].cpu().numpy()       # C(ri, cj)
     if mode == cb.GEMM_OZAKI:
         assert np.array_equal(got, _oracle_split(ra, cbm, n, kp, 7))
+    elif mode == cb.GEMM_CRT:
+        # one k slab below 131072, whatever the grid's kp
+        assert np.array_equal(got, _oracle_crt(ra, cbm, n, 1, kp[1]))
     else:
         _dd_ok(got, ra, cbm, n)
 
 
-@pytest.mark.parametrize("mode", [cb.GEMM_OZAKI, cb.GEMM_PLAIN])
+@pytest.mark.parametrize("mode", [cb.GEMM_CRT, cb.GEMM_OZAKI, cb.GEMM_PLAIN])
 @pytest.mark.parametrize("ta", [0, 1])
 def test_8000cube_grid_4x2x3(cuda, mode, ta):
     """The headline configuration: 8000^3 on 24 virtual ranks, grid 4 x 2 x 3."""
     _check_square(8000, ta, 24, (4, 2, 3), _signed_exp, 101 + ta, 40, mode)
 
 
-@pytest.mark.parametrize("mode", [cb.GEMM_OZAKI, cb.GEMM_PLAIN])
+@pytest.mark.parametrize("mode", [cb.GEMM_CRT, cb.GEMM_OZAKI, cb.GEMM_PLAIN])
 def test_2048cube_4_ranks(cuda, mode):
     """2048^3 on 4 virtual ranks with the reference's own grid choice (2 x 1 x 2)."""
     _check_square(2048, 0, 4, None, _uniform, 201, 64, mode)
 
 
-@pytest.mark.parametrize("mode", [cb.GEMM_OZAKI, cb.GEMM_PLAIN])
+@pytest.mark.parametrize("mode", [cb.GEMM_CRT, cb.GEMM_OZAKI, cb.GEMM_PLAIN])
 def test_btb_1048576x512_grid_1x1x32(cuda, mode):
     """B^T B with B of 1,048,576 x 512 (columns N(0,1) 10^u, u in [-3, 3]) on grid 1x1x32."""
     import torch
@@ -136,6 +156,9 @@ def test_btb_1048576x512_grid_1x1x32(cuda, mode):
     B.mul_(torch.pow(10.0, u)[:, None])
     B = B.reshape(-1)                                   # column-major K x N
     C, kp = _engine_run(N, N, K, 0, None, B, 32, (1, 1, 32), mode, btb=True)
+    nmod = 0
+    if mode == cb.GEMM_CRT:
+        kp, nmod = kp
     assert kp == 32
     sel = _sample(N, 16, 7)
     cols = _cols(B, K, N, sel, 0)                       # K x len(sel) columns of B
@@ -144,11 +167,14 @@ def test_btb_1048576x512_grid_1x1x32(cuda, mode):
     if mode == cb.GEMM_OZAKI:
         assert np.array_equal(got, _oracle_split(np.ascontiguousarray(cols.T), cols, K, kp, 7))
         assert torch.equal(Cm, Cm.T)
+    elif mode == cb.GEMM_CRT:
+        # the modular B^T B keeps the reference's kp slabs
+        assert np.array_equal(got, _oracle_crt(np.ascontiguousarray(cols.T), cols, K, kp, nmod))
     else:
         _dd_ok(got, np.ascontiguousarray(cols.T), cols, K)
 
 
-@pytest.mark.parametrize("mode", [cb.GEMM_OZAKI, cb.GEMM_PLAIN])
+@pytest.mark.parametrize("mode", [cb.GEMM_CRT, cb.GEMM_OZAKI, cb.GEMM_PLAIN])
 def test_256_uneven_gemms(cuda, mode):
     """256 independent GEMMs, m, n, k log-uniform in [64, 4096], random transposes."""
     import torch
@@ -180,5 +206,10 @@ def test_256_uneven_gemms(cuda, mode):
         got = C[i].view(n, m).T[ri][:, cj].cpu().numpy()
         if mode == cb.GEMM_OZAKI:
             assert np.array_equal(got, _oracle_split(ra, cbm, k, 1, 7)), i
+        elif mode == cb.GEMM_CRT:
+            # one modulus count for the batch (the deepest product's), P per product
+            kmax = int(dims[:, 2].max())
+            nm = next(x for x in range(8, 19) if orc.crt_bits(x, kmax) >= 51)
+            assert np.array_equal(got, _oracle_crt(ra, cbm, k, 1, nm)), i
         else:
             _dd_ok(got, ra, cbm, k)
