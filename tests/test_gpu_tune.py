@@ -276,3 +276,28 @@ def test_engine_auto_btb(cuda):
     hi, lo, ab = orc.dd_gemm(Bm, Bm, 1, 0, n, n, k)
     assert np.all(np.abs(got - hi) <= 2 * k * 2.0 ** -53 * ab + 1e-300)
     e.free()
+
+
+@pytest.mark.parametrize("m,n,k,ta,tb,p", [(1, 1, 1, 0, 0, 1), (3, 700, 5, 1, 0, 2),
+                                           (130, 2, 900, 0, 1, 3), (257, 129, 64, 1, 1, 6),
+                                           (64, 64, 20000, 0, 0, 8)])
+def test_engine_auto_small_and_odd_shapes(cuda, m, n, k, ta, tb, p):
+    """Auto mode over degenerate and odd shapes: every candidate that runs
+    gives a result the guard can judge, the kept one is admissible, and C is
+    within the plain GEMM's bound."""
+    A = orc.gen_signed_exp(51 + m, *((k, m) if ta else (m, k)), emin=-3, emax=3)
+    B = orc.gen_signed_exp(52 + n, *((n, k) if tb else (k, n)), emin=-3, emax=3)
+    dA, lda = to_dev(A)
+    dB, ldb = to_dev(B)
+    dC = dev_zeros(m * n)
+    e = cb.Ca3dmmEngine(m, n, k, ta, tb, p=p)
+    assert e.set_gemm_mode(cb.GEMM_AUTO) == 0
+    rc, chosen = e.autotune(dA, lda, dB, ldb, dC, m, how=2)
+    assert rc == 0
+    rep = {c: ms for c, ms, _ in e.tune_report()}
+    assert rep[chosen] > 0
+    assert e.exec(dA, lda, dB, ldb, dC, m) == 0
+    got = from_dev(dC, m, n)
+    hi, lo, ab = orc.dd_gemm(A, B, ta, tb, m, n, k)
+    assert np.all(np.abs(got - hi) <= 2 * k * 2.0 ** -53 * ab + 1e-300)
+    e.free()
