@@ -346,6 +346,13 @@ int ca3dmm_engine_autotune(ca3dmm_engine_p e, const void *A, int ldA, const void
     ca3dmm_guard_free(&g);
     if (pick < 0) pick = 0;                     /* the plain GEMM is always admissible */
     if (!rc) rc = ca3dmm_engine_set_tune(e, &c[pick]);
+    if (rc) {
+        /* a failed tuning leaves the engine on the plain GEMM, still to be tuned */
+        ca3dmm_engine_set_tune(e, &c[0]);
+        e->gemm_auto = auto_state;
+        ca3dmm_engine_reset_stat(e);
+        return rc;
+    }
     e->gemm_auto = auto_state == 1 ? 2 : auto_state;
     if (chosen) *chosen = c[pick];
     ca3dmm_engine_reset_stat(e);
@@ -398,7 +405,12 @@ static int cache_verify(ca3dmm_engine_p e, const ca3dmm_tune_cfg_t *c, const voi
                         const void *B, int ldB, void *C, int ldC, int *ok)
 {
     *ok = 1;
-    if (c->gemm_mode == CA3DMM_GEMM_PLAIN) return CA3DMM_OK;
+    if (c->gemm_mode == CA3DMM_GEMM_PLAIN) {
+        /* a plain entry needs no guard, only to be valid for this engine */
+        const int rc = ca3dmm_engine_set_tune(e, c);
+        if (rc == CA3DMM_EINVAL || rc == CA3DMM_ENOMEM) *ok = 0;
+        return rc == CA3DMM_EINVAL || rc == CA3DMM_ENOMEM ? CA3DMM_OK : rc;
+    }
     int tA, tB;
     operands_of(e, &A, &ldA, B, ldB, &tA, &tB);
     ca3dmm_guard_t g;
@@ -409,8 +421,12 @@ static int cache_verify(ca3dmm_engine_p e, const ca3dmm_tune_cfg_t *c, const voi
     ca3dmm_tune_cfg_t plain = {CA3DMM_GEMM_PLAIN, 0, e->kp, 8, 0};
     float ms, er;
     rc = try_candidate(e, &plain, A, ldA, B, ldB, C, ldC, &g, &ref, 0, 1, &ms, &er);
-    if (!rc) rc = try_candidate(e, c, A, ldA, B, ldB, C, ldC, &g, &ref, 0, 1, &ms, &er);
-    if (!rc) *ok = ms != -2.f;
+    if (!rc) {
+        const int crc = try_candidate(e, c, A, ldA, B, ldB, C, ldC, &g, &ref, 0, 1, &ms, &er);
+        if (crc == CA3DMM_EINVAL || crc == CA3DMM_ENOMEM) *ok = 0;   /* not for this engine */
+        else if (crc) rc = crc;
+        else *ok = ms != -2.f;
+    }
     ca3dmm_guard_free(&g);
     return rc;
 }
@@ -443,7 +459,8 @@ int ca3dmm_engine_autotune_env(ca3dmm_engine_p e, const void *A, int ldA, const 
         int rc = cache_verify(e, &c, A, ldA, B, ldB, C, ldC, &ok);
         if (!rc && ok) rc = ca3dmm_engine_set_tune(e, &c);
         e->gemm_auto = auto_state;
-        if (rc) return rc;
+        if (rc == CA3DMM_EINVAL || rc == CA3DMM_ENOMEM) ok = 0;   /* an entry this engine cannot take */
+        else if (rc) return rc;
         if (ok) {
             ca3dmm_tune_report_t *rep = ca3dmm_engine_report_slot(e);
             rep->n = 1;

@@ -301,3 +301,30 @@ def test_engine_auto_small_and_odd_shapes(cuda, m, n, k, ta, tb, p):
     hi, lo, ab = orc.dd_gemm(A, B, ta, tb, m, n, k)
     assert np.all(np.abs(got - hi) <= 2 * k * 2.0 ** -53 * ab + 1e-300)
     e.free()
+
+
+def test_tune_cache_entry_this_engine_cannot_take(cuda, tmp_path, monkeypatch):
+    """A cache line that does not fit the engine (a modular tile width that does
+    not exist) is ignored: the engine tunes and appends its own choice."""
+    m, n, k = 300, 200, 400
+    e0 = cb.Ca3dmmEngine(m, n, k)
+    key = "v1 %d %d %d 0 0 0 0 %d %d %d" % (m, n, k, e0.s.mp, e0.s.np, e0.s.kp)
+    e0.free()
+    cache = tmp_path / "tune.txt"
+    cache.write_text(key + " : 2 15 32 64\n")
+    monkeypatch.setenv("CA3DMM_GEMM_MODE", "auto")
+    monkeypatch.setenv("CA3DMM_TUNE_CACHE", str(cache))
+    monkeypatch.setenv("CA3DMM_AUTOTUNE", "exhaustive")
+    A = orc.gen_signed_exp(61, m, k, emin=-2, emax=2)
+    B = orc.gen_signed_exp(62, k, n, emin=-2, emax=2)
+    dA, lda = to_dev(A)
+    dB, ldb = to_dev(B)
+    dC = dev_zeros(m * n)
+    e = cb.Ca3dmmEngine(m, n, k)
+    assert e.exec(dA, lda, dB, ldb, dC, m) == 0
+    assert e.s.gemm_auto == 2 and len(e.tune_report()) > 1
+    lines = cache.read_text().strip().splitlines()
+    assert len(lines) == 2 and lines[1].startswith(key)
+    hi, lo, ab = orc.dd_gemm(A, B, 0, 0, m, n, k)
+    assert np.all(np.abs(from_dev(dC, m, n) - hi) <= 2 * k * 2.0 ** -53 * ab + 1e-300)
+    e.free()
