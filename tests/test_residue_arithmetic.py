@@ -1,0 +1,84 @@
+"""The FP64 residue arithmetic of the modular scheme's residue pass, checked on
+the CPU with exact rational arithmetic (no GPU): for integers |a'| <= 2^53,
+
+  h = RN(a' 2^-27 + M) - M,  l = a' - h 2^27           (M = 1.5 2^52)
+  y = h (2^27 mod p) + l
+  q = RN(y RN(1/p) + M) - M,  r = y - q p
+
+gives the unique representative of a' mod p in [-(p-1)/2, (p-1)/2] for every
+odd modulus of the list, and every intermediate is exact in FP64 (|h|, |l| <=
+2^26, |y| < 2^35).  RN is round-to-nearest-even, which Python's float() of a
+Fraction performs exactly.  The device kernel evaluates the same expressions
+with FMAs (single roundings of the exact values written here)."""
+from fractions import Fraction
+
+import numpy as np
+import pytest
+
+MODULI = [256, 255, 253, 251, 247, 241, 239, 233, 229, 227, 223, 217, 211, 199, 197, 193, 191, 181]
+MAGIC = 6755399441055744.0          # 1.5 2^52
+
+
+def rn(x):
+    """Round an exact rational to the nearest double (ties to even)."""
+    return float(x)
+
+
+def residue(a, p):
+    assert abs(a) <= 2 ** 53
+    h = rn(Fraction(a) * Fraction(2) ** -27 + Fraction(MAGIC)) - MAGIC   # exact subtraction
+    h = int(h)
+    l = a - h * 2 ** 27
+    assert abs(h) <= 2 ** 26 and abs(l) <= 2 ** 26
+    c27 = (2 ** 27) % p
+    y = h * c27 + l
+    assert abs(y) < 2 ** 35
+    inv = rn(Fraction(1, p))
+    qm = rn(Fraction(y) * Fraction(inv) + Fraction(MAGIC))
+    q = int(qm - MAGIC)
+    r = y - q * p
+    return r
+
+
+def cases(seed, count):
+    rng = np.random.default_rng(seed)
+    out = [0, 1, -1, 2 ** 53, -(2 ** 53), 2 ** 53 - 1, 2 ** 27, -(2 ** 27), 2 ** 26, 2 ** 26 + 1,
+           -(2 ** 26) - 1]
+    for _ in range(count):
+        e = int(rng.integers(0, 54))
+        out.append(int(rng.integers(-(2 ** e), 2 ** e + 1)) if e < 63 else 0)
+    return out
+
+
+@pytest.mark.parametrize("p", [p for p in MODULI if p % 2 == 1])
+def test_centred_residue_for_every_odd_modulus(p):
+    half = (p - 1) // 2
+    for a in cases(p, 1500):
+        r = residue(a, p)
+        assert -half <= r <= half, (a, p, r)
+        assert (r - a) % p == 0, (a, p, r)
+
+
+def test_near_half_integer_quotients():
+    """Values of y whose y / p lies closest to a half-integer (the rounding
+    decision of q): y = (2j + 1)(p - 1) / 2 and neighbours, across the y range."""
+    for p in [p for p in MODULI if p % 2 == 1]:
+        for j in (0, 1, 7, 2 ** 20, 2 ** 26 - 3):
+            for d in (-2, -1, 0, 1, 2):
+                a = (2 * j + 1) * (p - 1) // 2 + d
+                for sgn in (1, -1):
+                    r = residue(sgn * a, p)
+                    assert -(p - 1) // 2 <= r <= (p - 1) // 2
+                    assert (r - sgn * a) % p == 0
+
+
+def test_modulus_256_is_the_low_byte():
+    """Modulus 256: the signed low byte of l is a' mod 256 in [-128, 127]."""
+    rng = np.random.default_rng(3)
+    for _ in range(5000):
+        a = int(rng.integers(-(2 ** 53), 2 ** 53))
+        h = int(rn(Fraction(a) * Fraction(2) ** -27 + Fraction(MAGIC)) - MAGIC)
+        l = a - h * 2 ** 27
+        byte = l & 0xFF
+        signed = byte - 256 if byte >= 128 else byte
+        assert (signed - a) % 256 == 0 and -128 <= signed <= 127
