@@ -82,3 +82,30 @@ def test_modulus_256_is_the_low_byte():
         byte = l & 0xFF
         signed = byte - 256 if byte >= 128 else byte
         assert (signed - a) % 256 == 0 and -128 <= signed <= 127
+
+
+def test_reconstruction_quotient_margin():
+    """The reconstruction takes q = rint(S / M) from an FP64 estimate of S / M,
+    off by less than 2^-38 (S < 18 * 256 * M).  It is the right quotient as
+    long as |C'| / M stays that far below 1/2.  The integer width P the library
+    picks (ca3dmm_crt_bits) keeps k 2^(2P) < M / 2 with a relative margin above
+    2^-30 for every modulus count and depth: checked here in exact integers."""
+    import ca3dmm_b200 as cb
+    L = cb.lib()
+    rng = np.random.default_rng(9)
+    ks = sorted(set([1, 2, 3, 100, 1000, 4096, 8000, 8192, 32768, 65536, 131071, 131072] +
+                    [int(x) for x in rng.integers(1, 131073, 300)]))
+    for nmod in range(8, 19):
+        M = 1
+        for p in MODULI[:nmod]:
+            M *= p
+        for k in ks:
+            P = L.ca3dmm_crt_bits(nmod, k)
+            if P < 2:
+                continue
+            bound = k * 2 ** (2 * P)          # |C'| <= k 2^(2P)
+            assert 2 * bound < M, (nmod, k, P)
+            margin = Fraction(M - 2 * bound, 2 * M)
+            assert margin > Fraction(1, 2 ** 30), (nmod, k, P, float(margin))
+            if P < 53:                          # and P is the largest width that fits
+                assert 2 * k * 2 ** (2 * (P + 1)) >= M or P + 1 > 53, (nmod, k, P)
