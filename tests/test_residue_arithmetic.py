@@ -1,5 +1,8 @@
-"""The FP64 residue arithmetic of the modular scheme's residue pass, checked on
-the CPU with exact rational arithmetic (no GPU): for integers |a'| <= 2^53,
+"""The integer arithmetic of the modular scheme, checked on the CPU (no GPU):
+the residue pass's FP64 expressions, the GEMM epilogue's reduction of INT32
+sums, and the margin the reconstruction's quotient estimate needs.
+
+Residue pass, with exact rational arithmetic: for integers |a'| <= 2^53,
 
   h = RN(a' 2^-27 + M) - M,  l = a' - h 2^27           (M = 1.5 2^52)
   y = h (2^27 mod p) + l
@@ -109,3 +112,33 @@ def test_reconstruction_quotient_margin():
             assert margin > Fraction(1, 2 ** 30), (nmod, k, P, float(margin))
             if P < 53:                          # and P is the largest width that fits
                 assert 2 * k * 2 ** (2 * (P + 1)) >= M or P + 1 > 53, (nmod, k, P)
+
+
+def _mod_i32(v, p):
+    """The GEMM epilogue's reduction of an INT32 sum v mod p, restated with
+    32-bit unsigned arithmetic: y = h (2^16 mod p) + (v mod 2^16) + bias with
+    h = v >> 16, q = umulhi(y, floor(2^32 / p)), r = y - q p folded once."""
+    c16 = (1 << 16) % p
+    bias = ((8650752 + p - 1) // p) * p
+    mrec = (1 << 32) // p
+    h = v >> 16                                   # arithmetic shift (numpy int64)
+    y = (h * c16 + (v & 0xFFFF) + bias).astype(np.uint64)
+    assert np.all(y < (1 << 25))
+    q = (y * np.uint64(mrec)) >> np.uint64(32)
+    r0 = (y - q * np.uint64(p)).astype(np.int64)
+    r = np.where(r0 >= p, r0 - p, r0)
+    return r
+
+
+@pytest.mark.parametrize("p", MODULI)
+def test_epilogue_reduction_of_int32_sums(p):
+    """Every INT32 sum the modular GEMM can form (|v| <= k 128^2 < 2^31 for
+    k <= 131072) reduces to v mod p in [0, p)."""
+    rng = np.random.default_rng(p)
+    lim = 131072 * 128 * 128
+    v = np.concatenate([rng.integers(-lim, lim + 1, 200000),
+                        np.array([0, 1, -1, lim, -lim, 2 ** 16, -(2 ** 16), 2 ** 16 - 1,
+                                  -(2 ** 31) + 1, 2 ** 31 - 1])]).astype(np.int64)
+    r = _mod_i32(v, p)
+    assert np.all((r >= 0) & (r < p))
+    assert np.all((r - v) % p == 0)
