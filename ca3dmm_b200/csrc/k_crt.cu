@@ -67,36 +67,29 @@ constexpr int DEFAULT_BAND = 8;
 
 // ------------------------------------------------------------------ moduli
 // Pairwise coprime moduli <= 256, largest first (256 = 2^8 and odd numbers
-// with disjoint prime factors), and per modulus the constants of the residue
-// arithmetic: 2^16, 2^18, 2^36 mod p, and floor(2^32 / p).
+// with disjoint prime factors), and per modulus the constants of the GEMM
+// epilogue's reduction (2^16 mod p, floor(2^32 / p), a bias) and of the
+// residue pass (2^27 mod p and 1/p in FP64).
 constexpr int kModList[MAXMOD] = {256, 255, 253, 251, 247, 241, 239, 233, 229,
                                   227, 223, 217, 211, 199, 197, 193, 191, 181};
 static_assert(kModList[0] == 256, "the residue pass takes modulus 0 as the byte of the integer");
 
 struct ModConst {
-    int p, c16, c18, c36;
+    int p, c16;          // p, 2^16 mod p
     unsigned int mrec;   // floor(2^32 / p): floor(y mrec / 2^32) is floor(y / p) or one less (y < 2^28)
-    int half;        // floor(p/2)
-    int bias;        // a multiple of p above 2^15 * 255 (keeps the epilogue's sums >= 0)
-    int off54;       // p - (2^54 mod p)
+    int bias;            // a multiple of p above 2^15 * 255 (keeps the epilogue's sums >= 0)
     double c27;      // 2^27 mod p (the residue pass, in FP64)
     double inv;      // 1 / p rounded to double
-    double pd;       // p
 };
 
 constexpr ModConst make_mod(int p)
 {
     return ModConst{p,
                     (int) ((1LL << 16) % p),
-                    (int) ((1LL << 18) % p),
-                    (int) ((1ULL << 36) % (unsigned long long) p),
                     (unsigned int) ((1ULL << 32) / (unsigned long long) p),
-                    p / 2,
                     (int) (((8650752LL + p - 1) / p) * p),   // a multiple of p >= 2^23 + 2^18
-                    (int) (p - (int) ((1ULL << 54) % (unsigned long long) p)),
                     (double) ((1LL << 27) % p),
-                    1.0 / (double) p,
-                    (double) p};
+                    1.0 / (double) p};
 }
 
 struct ModTable {
@@ -204,22 +197,21 @@ double log2_modprod(int nmod)
 }
 
 // ------------------------------------------------------------------ residues
-// One row's 16 consecutive k elements -> their residues for every modulus.
-// v = a' + 2^54 > 0 is split into 18-bit pieces x0 + 2^18 x1 + 2^36 x2, so
-// y = x2 (2^36 mod p) + x1 (2^18 mod p) + x0 + (p - 2^54 mod p) + floor(p/2)
-// is below 2^28 and congruent to a' + floor(p/2); q = floor(y floor(2^32/p) / 2^32)
-// is floor(y / p) or one less, r = y - q p in [0, 2p) is folded once, and the
-// residue byte is r - floor(p/2).
 // The residues of the row / column integers a' = rint(a 2^(P - E)) (|a'| <=
 // 2^53), as signed bytes in [-(p-1)/2, (p-1)/2] (p odd) and [-128, 127]
-// (p = 256).  They are formed in FP64, whose pipe the integer multiply-add
-// path of the other passes leaves idle: a' = h 2^27 + l with |h|, |l| <= 2^26,
-// then per odd modulus y = h (2^27 mod p) + l (|y| < 2^35, exact), q = the
-// nearest integer to y / p (y (1/p) is within 2^-23 of y / p, which is never
-// closer than 1 / (2p) to a half-integer for odd p), r = y - q p exact; the
-// low bits of r + 1.5 2^52 are r in two's complement.  For p = 256 the byte is
-// the low byte of l (a' = l mod 256).  Every value is the unique representative
-// of a' mod p in that range, so the bytes equal the integer formulation's.
+// (p = 256).  a' = h 2^27 + l with |h|, |l| <= 2^26 (h by rounding with
+// 1.5 2^52 added), then per odd modulus yb = h (2^27 mod p) + l + 1.5 2^52
+// (one FMA, exact: |y| < 2^35) and q = the nearest integer to y / p, from
+// y = yb - 1.5 2^52 and one FMA with 1.5 2^52 added (y (1/p) is within 2^-23
+// of y / p, which is never closer than 1 / (2p) to a half-integer for odd p).
+// The low words of yb and of that FMA are y and q modulo 2^32 (the low bits of
+// x + 1.5 2^52 are the integer x in two's complement), and r = y - q p is
+// small, so it is one 32-bit integer multiply-add modulo 2^32: three FP64
+// operations and one on the integer pipe per modulus (five FP64 operations
+// when r was formed in FP64: 119 -> 99 us per 4000 x 4000 operand).  For
+// p = 256 the byte is the low byte of l (a' = l mod 256).  Every value is the
+// unique representative of a' mod p in that range, so the bytes equal the
+// integer formulation's.
 // NM: the modulus count, a template argument so that the modulus loop unrolls
 // (the constants become immediate operands and consecutive moduli interleave).
 template <int NM>
@@ -258,12 +250,13 @@ struct ResidueWriter {
 #pragma unroll
                 for (int j = 0; j < 16; ++j) r[j] = (unsigned int) __double2loint(lm[j]);
             } else {
-                const double c27 = kMod.m[t].c27, inv = kMod.m[t].inv, pd = kMod.m[t].pd;
+                const double c27 = kMod.m[t].c27, inv = kMod.m[t].inv;
+                const unsigned int p = (unsigned int) kMod.m[t].p;
 #pragma unroll
                 for (int j = 0; j < 16; ++j) {
                     const double yb = fma(hh[j], c27, lm[j]);      // y + 1.5 2^52
-                    const double q = fma(yb - MAGIC, inv, MAGIC) - MAGIC;
-                    r[j] = (unsigned int) __double2loint(fma(-q, pd, yb));
+                    const double qm = fma(yb - MAGIC, inv, MAGIC);  // q + 1.5 2^52
+                    r[j] = (unsigned int) __double2loint(yb) - (unsigned int) __double2loint(qm) * p;
                 }
             }
             uint32_t out[4];

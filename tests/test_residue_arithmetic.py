@@ -5,14 +5,16 @@ sums, and the margin the reconstruction's quotient estimate needs.
 Residue pass, with exact rational arithmetic: for integers |a'| <= 2^53,
 
   h = RN(a' 2^-27 + M) - M,  l = a' - h 2^27           (M = 1.5 2^52)
-  y = h (2^27 mod p) + l
-  q = RN(y RN(1/p) + M) - M,  r = y - q p
+  yb = h (2^27 mod p) + l + M                          (y = yb - M)
+  qm = RN(y RN(1/p) + M),  q = qm - M,  r = y - q p
 
 gives the unique representative of a' mod p in [-(p-1)/2, (p-1)/2] for every
 odd modulus of the list, and every intermediate is exact in FP64 (|h|, |l| <=
 2^26, |y| < 2^35).  RN is round-to-nearest-even, which Python's float() of a
 Fraction performs exactly.  The device kernel evaluates the same expressions
-with FMAs (single roundings of the exact values written here)."""
+with FMAs (single roundings of the exact values written here) and forms r in
+32-bit integers from the low words of the doubles yb and qm:
+(lo(yb) - lo(qm) p) mod 2^32, read as a signed word."""
 from fractions import Fraction
 
 import numpy as np
@@ -37,10 +39,20 @@ def residue(a, p):
     y = h * c27 + l
     assert abs(y) < 2 ** 35
     inv = rn(Fraction(1, p))
+    yb = rn(Fraction(y) + Fraction(MAGIC))
+    assert yb - MAGIC == y                                  # exact
     qm = rn(Fraction(y) * Fraction(inv) + Fraction(MAGIC))
     q = int(qm - MAGIC)
     r = y - q * p
+    # the device's integer form: low words of yb and qm, arithmetic mod 2^32
+    rw = (low_word(yb) - low_word(qm) * p) % 2 ** 32
+    assert (rw - 2 ** 32 if rw >= 2 ** 31 else rw) == r
     return r
+
+
+def low_word(v):
+    """The low 32 bits of the IEEE bit pattern of the double v."""
+    return int(np.array([v], dtype=np.float64).view(np.uint64)[0]) & 0xFFFFFFFF
 
 
 def cases(seed, count):
