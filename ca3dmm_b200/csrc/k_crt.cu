@@ -334,6 +334,15 @@ __device__ __forceinline__ void item_decode(const CrtGroup &G, int nmod, int ite
     tn = r2 / rows;
 }
 
+// Columns of tile tn that the MMAs compute: TN, or for the last tile of a
+// group the columns of C it holds rounded up to 16 (an MMA N with M = 128);
+// the B rows past them are neither loaded nor multiplied.
+__device__ __forceinline__ int tile_cols(const CrtGroup &G, int tn, int TN)
+{
+    const int left = G.n - tn * TN;
+    return left >= TN ? TN : (left + 15) & ~15;
+}
+
 // K-major, SWIZZLE_128B shared-memory operand descriptor: rows of 128 bytes,
 // 8-row groups 1024 bytes apart (SBO), descriptor version 1, layout type 2.
 __device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr)
@@ -433,6 +442,7 @@ crt_gemm_kernel(const CrtGroup *__restrict__ groups, int ngroup, int nmod,
                                      (long long) (tm >> 1) * G.nkb * CB_BYTES + (tm & 1) * CA_BYTES
                                : work + G.qa_off + t * G.qa_tstride + (long long) tm * G.nkb * CA_BYTES;
                 const long long a_step = G.a_from_b ? CB_BYTES : CA_BYTES;
+                const uint32_t b_bytes = (uint32_t) tile_cols(G, tn, TN) * CKB;
                 // a 128-column tile: half tn % 2 of stored 256-row tile tn / 2
                 const unsigned char *qb =
                     TN == CBN ? work + G.qb_off + t * G.qb_tstride + (long long) tn * G.nkb * CB_BYTES
@@ -446,9 +456,9 @@ crt_gemm_kernel(const CrtGroup *__restrict__ groups, int ngroup, int nmod,
                         break;
                     }
                     uint8_t *sA = smem + s * CSTAGE_BYTES;
-                    mbar_arrive_expect_tx(&full[s], CSTAGE_BYTES);
+                    mbar_arrive_expect_tx(&full[s], CA_BYTES + b_bytes);
                     bulk_load(sA, qa + (long long) kb * a_step, CA_BYTES, &full[s]);
-                    bulk_load(sA + CA_BYTES, qb + (long long) kb * CB_BYTES, T::kBBytes, &full[s]);
+                    bulk_load(sA + CA_BYTES, qb + (long long) kb * CB_BYTES, b_bytes, &full[s]);
                 }
             }
             // drain copies in flight (bounded, abort flag ignored)
@@ -463,12 +473,14 @@ crt_gemm_kernel(const CrtGroup *__restrict__ groups, int ngroup, int nmod,
         // ------------------------------------------------------ MMA issuers
         if (lane == 0) {
             const int half = warp - 1;          // k steps 2 half, 2 half + 1 of each stage
-            const uint32_t idesc = idesc_i8(TN, CBM);
             uint32_t it = 0, ai = 0;
             bool ok = true;
             for (int v = blockIdx.x; v < total_items && ok; v += gridDim.x, ++ai) {
                 const int item = range_tile(rg, v);
                 const CrtGroup &G = groups[find_group(gb, groups, ngroup, item)];
+                int t, tm, tn;
+                item_decode(G, nmod, item, t, tm, tn);
+                const uint32_t idesc = idesc_i8(tile_cols(G, tn, TN), CBM);
                 const uint32_t buf = ai & 1u;
                 if (!mbar_wait_bounded(&acc_empty[buf], ((ai >> 1) & 1u) ^ 1u, &abort_flag, status,
                                        CA3DMM_DEV_TIMEOUT_ACCUM, limit_ns)) {
@@ -487,10 +499,13 @@ crt_gemm_kernel(const CrtGroup *__restrict__ groups, int ngroup, int nmod,
                     tc_fence_after();
                     const uint32_t sA = smem_u32(smem + s * CSTAGE_BYTES);
                     const uint32_t sB = sA + CA_BYTES;
+                    // k steps past the group's k hold zero residues: not issued
+                    const int kleft = G.k - kb * CKB;
 #pragma unroll
                     for (int kk = 2 * half; kk < 2 * half + 2; ++kk)
-                        tc_mma_i8(tacc, sdesc_sw128(sA + kk * 32), sdesc_sw128(sB + kk * 32),
-                                  idesc, 1u);
+                        if (kk * 32 < kleft)
+                            tc_mma_i8(tacc, sdesc_sw128(sA + kk * 32), sdesc_sw128(sB + kk * 32),
+                                      idesc, 1u);
                     tc_commit(&empty[s]);
                 }
                 if (!ok) break;
@@ -523,9 +538,13 @@ crt_gemm_kernel(const CrtGroup *__restrict__ groups, int ngroup, int nmod,
             const ModConst mc = kMod.m[t];
             const int row = tm * CBM + q * 32 + lane;
             unsigned char *plane = work + G.pl_off + (long long) t * G.pl_bytes + row;
+            // columns past tile_cols were not accumulated (still zero) and lie
+            // past the group's n (never read): skipped
+            const int ncols = tile_cols(G, tn, TN);
 #pragma unroll 1
             for (int cb = 0; cb < TN / 64; ++cb) {
                 const int c0 = h * (TN / 2) + cb * 32;
+                if (c0 >= ncols) break;
                 uint32_t vv[32];
                 const uint32_t ta = tmem_base + ((uint32_t) (q * 32) << 16) + buf * TN + (uint32_t) c0;
                 tmem_ld32(ta, vv);
