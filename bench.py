@@ -326,11 +326,17 @@ def grouped_problems(nprob, seed=2024):
 
 def run_grouped(args, world, rank, local):
     """256 uneven GEMMs: one persistent grouped launch (captured in a CUDA graph)
-    against one plain DMMA launch per GEMM."""
+    against one plain DMMA launch per GEMM.  With N ranks each GPU runs its own
+    replica of the batch (weak scaling): the time is the slowest rank's and the
+    value counts every rank's flops."""
     import torch
     import ca3dmm_b200 as cb
     from oracle import oracle as orc
     torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     probs = grouped_problems(args.nprob)
     flops = sum(2.0 * m * n * k for m, n, k, _, _ in probs)
     dA, dB, dC, lda, ldb, ldc = [], [], [], [], [], []
@@ -349,13 +355,17 @@ def run_grouped(args, world, rank, local):
             for _ in range(max(args.warmup, 1)):
                 fn()
             torch.cuda.synchronize()
+            if world > 1:
+                torch.distributed.barrier()
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record(stream)
             for _ in range(steps):
                 fn()
             e1.record(stream)
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1) / steps
+        if world > 1:
+            torch.distributed.barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / steps, world)
 
     # one plain DMMA launch (pack + GEMM) per product
     singles = [cb.GroupedGemm([m], [n], [k], [ta], [tb]) for m, n, k, ta, tb in probs]
@@ -381,8 +391,13 @@ def run_grouped(args, world, rank, local):
     # the headline: the faster split-precision leg (both at least as accurate as
     # plain FP64 on these entries)
     head = min(("grouped_ozaki7_ms", "grouped_crt_ms"), key=lambda x: res[x])
-    v = flops / (res[head] * 1e-3) / 1e12
-    out = {"metric": METRIC, "value": v, "unit": "TFLOP/s", "n_gpus": 1, "steps": args.steps,
+    v = whole_job_tflops(flops, world, res[head])
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if rank != 0:
+        return
+    out = {"metric": METRIC, "value": v, "unit": "TFLOP/s", "n_gpus": world, "steps": args.steps,
            "warmup": args.warmup, "ms_per_step": res[head], "gemm": head.replace("_ms", ""),
            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
            "data": "synthetic",
@@ -390,7 +405,8 @@ def run_grouped(args, world, rank, local):
                                   "trans, one grouped launch in a CUDA graph" % len(probs),
                       "total_flop": flops},
            "legs_ms": res,
-           "legs_tflops": {k.replace("_ms", ""): flops / (t * 1e-3) / 1e12 for k, t in res.items()}}
+           "legs_tflops": {k.replace("_ms", ""): whole_job_tflops(flops, world, t)
+                           for k, t in res.items()}}
     print(json.dumps(out), flush=True)
 
 
@@ -747,15 +763,19 @@ def main():
 
     # timed region (headline leg), clocks sampled meanwhile
     sampler = ClockSampler(local)
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
     sampler.start()
     time.sleep(0.3)
     i0 = sampler.mark()
+    # the timed steps, bracketed by a barrier and a device synchronisation on
+    # both sides (leg() synchronises before its first and after its last event)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
     l0 = cb.kernel_launches()
     res = leg(eng, args.steps, 0)
     launches = cb.kernel_launches() - l0
+    if world > 1:
+        torch.distributed.barrier()
     time.sleep(0.15)                      # the sample covering the region's end
     clocks = sampler.stop(i0, sampler.mark())
     ms = max_over_ranks(res["ms_per_step"], world)
@@ -822,8 +842,11 @@ def main():
     # errors against the double-double truth, as top-level keys
     split = head if head != "plain" else "crt"
     eo, ep = legs[split]["err"], legs["plain"]["err"]
-    plain_tf = flops / (legs["plain"]["ms_per_step"] * 1e-3) / 1e12
-    split_tf = flops / (legs[split]["ms_per_step"] * 1e-3) / 1e12
+    # whole-job rates of the three legs, each over its slowest rank (every rank
+    # takes these reductions in the same order)
+    leg_tf = {x: whole_job_tflops(flops, world, max_over_ranks(legs[x]["ms_per_step"], world))
+              for x in ("plain", "ozaki", "crt")}
+    plain_tf, split_tf = leg_tf["plain"], leg_tf[split]
     out = {
         "metric": METRIC, "value": value, "unit": "TFLOP/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -833,8 +856,7 @@ def main():
         "gemm": head, "split_leg": split, "ozaki_slices": eng_oz.s.ozaki_slices,
         "crt_moduli": eng_crt.s.crt_moduli, "crt_bits": eng_crt.s.crt_bits,
         "plain_tflops": plain_tf, "split_tflops": split_tf,
-        "ozaki_tflops": flops / (legs["ozaki"]["ms_per_step"] * 1e-3) / 1e12,
-        "crt_tflops": flops / (legs["crt"]["ms_per_step"] * 1e-3) / 1e12,
+        "ozaki_tflops": leg_tf["ozaki"], "crt_tflops": leg_tf["crt"],
         "split_over_plain": split_tf / plain_tf,
         "err_normwise_split": eo["normwise"], "err_normwise_plain": ep["normwise"],
         "err_vs_absprod_split": eo["vs_absprod"], "err_vs_absprod_plain": ep["vs_absprod"],
