@@ -423,8 +423,12 @@ static int prepare(struct ca3dmm_dist_engine *e)
     }
     /* operands: my blocks -> send pieces; received pieces -> my panels */
     const int nmats = e->btb ? 1 : 2;
-    int *sr = (int *) xcalloc(4 * (size_t) (2 + e->nsend + e->nrecv + 2), sizeof(int));
-    int *dr = (int *) xcalloc(4 * (size_t) (2 + e->nsend + e->nrecv + 2), sizeof(int));
+    /* rectangle lists of the four batched copies, in turn: my blocks (<= 2) /
+     * send pieces, received pieces / my panels (<= 2), my C block (1) / C
+     * send pieces */
+    const size_t nrect = (size_t) 2 + (size_t) e->nsend + (size_t) e->nrecv + (size_t) e->ncsend;
+    int *sr = (int *) xcalloc(4 * nrect, sizeof(int));
+    int *dr = (int *) xcalloc(4 * nrect, sizeof(int));
     if (!sr || !dr) { free(sr); free(dr); return CA3DMM_ENOMEM; }
     e->nmy = 0;
     for (int t = 0; t < nmats; t++) {

@@ -75,6 +75,23 @@ def test_crt_bitexact(cuda, m, n, k, ta, tb, p, grid, nmod):
     assert np.array_equal(got, want), np.max(np.abs(got - want))
 
 
+@pytest.mark.parametrize("tile_n", [256, 128])
+def test_crt_edge_tiles_bitexact(cuda, monkeypatch, tile_n):
+    """The last tile column holding 1 .. TN - 1 columns of C (the GEMM multiplies
+    only those, rounded up to 16) and k ending anywhere in the last 128-byte k
+    block (the k steps past k are not issued): bit-exact against the oracle."""
+    monkeypatch.setenv("CA3DMM_CRT_TILE_N", str(tile_n))
+    cases = [(130, 257, 1), (129, 256 + 15, 33), (128, 256 + 16, 64), (200, 256 + 17, 95),
+             (64, 511, 96), (100, 255, 127), (70, 1, 129), (33, 384 + 112, 200),
+             (260, 128 + 113, 32), (5, 16, 31)]
+    for i, (m, n, k) in enumerate(cases):
+        A = orc.gen_signed_exp(60 + i, m, k)
+        B = orc.gen_signed_exp(80 + i, k, n)
+        got, (nm, P) = _run(A, B, m, n, k, 0, 0, 1, None, 15)
+        want = _oracle(A, B, m, n, k, 0, 0, nm)
+        assert np.array_equal(got, want), (tile_n, m, n, k, np.max(np.abs(got - want)))
+
+
 def test_crt_automatic_count_and_refusals(cuda):
     e = cb.Ca3dmmEngine(8000, 64, 8000, p=1)
     assert e.ok

@@ -30,6 +30,11 @@ U = 2.0 ** -53
 def _blocks(m, n, k, ta, tb, p, r, irregular=False):
     ar, ac = (k, m) if ta else (m, k)
     br, bc = (n, k) if tb else (k, n)
+    if irregular == "root":
+        # rank 0 holds all of A and B, C in 1D column blocks
+        c0, cz = cb.calc_block_spos_size(n, p, r)
+        whole = lambda rows, cols: (0, rows, 0, cols) if r == 0 else (0, 0, 0, 0)
+        return whole(ar, ac), whole(br, bc), (0, m, c0, cz)
     if not irregular:
         a0, az = cb.calc_block_spos_size(ac, p, r)
         b0, bz = cb.calc_block_spos_size(bc, p, r)
@@ -130,6 +135,25 @@ def test_threads_match(cuda, m, n, k, ta, tb, p, grid, irregular, mode):
         assert np.array_equal(got, want), np.max(np.abs(got - want))
     else:
         hi, lo, ab = orc.dd_gemm(A, B, ta, tb, m, n, k)
+        assert np.all(np.abs(got - hi) <= k * U * ab + 1e-300)
+
+
+@pytest.mark.parametrize("mode", [cb.GEMM_PLAIN, cb.GEMM_OZAKI])
+def test_threads_operands_on_one_rank(cuda, mode):
+    """Rank 0 holds all of A and B and C is split in 1D column blocks on the
+    grid 1 x 1 x 8: every rank's C block (all of C for its slab) goes to all
+    eight ranks while the other ranks send no operand piece, so the C
+    exchange has more pieces than the operand exchange."""
+    m, n, k, p, grid = 96, 96, 4096, 8, (1, 1, 8)
+    A = orc.gen_signed_exp(91, m, k)
+    B = orc.gen_signed_exp(92, k, n)
+    slices = 7 if mode == cb.GEMM_OZAKI else 0
+    got, info = _dist_run(A, B, m, n, k, 0, 0, p, grid, mode, slices, "root")
+    assert tuple(info[:3]) == grid
+    if mode == cb.GEMM_OZAKI:
+        assert np.array_equal(got, _single(A, B, m, n, k, 0, 0, p, grid, mode, slices))
+    else:
+        hi, lo, ab = orc.dd_gemm(A, B, 0, 0, m, n, k)
         assert np.all(np.abs(got - hi) <= k * U * ab + 1e-300)
 
 
