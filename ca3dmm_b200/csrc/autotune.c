@@ -234,6 +234,10 @@ int ca3dmm_autotune(int m, int n, int k, int trans_A, int trans_B, const double 
     *best = -1;
     for (int i = 0; i < ncand; i++)
         if (ms[i] >= 0.f && (*best < 0 || ms[i] < ms[*best])) *best = i;
+    /* nothing timed: the first plain candidate in the model's order (the IEEE
+     * reference, admissible whatever the guard says), else the model's first */
+    for (int r = 0; r < ncand && *best < 0; r++)
+        if (cands[order[r]].gemm_mode == CA3DMM_GEMM_PLAIN && ms[order[r]] != -2.f) *best = order[r];
     if (*best < 0) *best = order[0];
     for (int i = 0; i < ncand; i++) {
         if (measured_ms) measured_ms[i] = ms[i];

@@ -75,7 +75,9 @@ typedef struct ca3dmm_mlp *ca3dmm_mlp_p;
  * admissible ones.  One engine per kp serves every candidate with that kp.
  * measured_ms[i] receives the time of candidate i, -1 if not timed, -2 if
  * the accuracy guard rejected it; guard_err[i] (may be NULL) its normwise
- * error on the guard's sample (-1 if not run).  *best: the chosen candidate. */
+ * error on the guard's sample (-1 if not run).  *best: the fastest timed
+ * candidate; when none could be timed, the first plain candidate in the
+ * model's order (the IEEE reference), else the model's first. */
 int ca3dmm_autotune(int m, int n, int k, int trans_A, int trans_B, const double *A, int ldA,
                     const double *B, int ldB, double *C, int ldC, const ca3dmm_tune_cfg_t *cands,
                     int ncand, float exp_spread, ca3dmm_mlp_p model, int topk, int reps,
