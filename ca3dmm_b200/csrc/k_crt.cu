@@ -1155,17 +1155,22 @@ extern "C" int ca3dmm_crt_run_reconstruct_capped(const ca3dmm_crt_plan_t *pl, in
     const long long cap = max_blocks > 0 ? max_blocks : (long long) ca3dmm_device_sm_count() * 8;
     if (blocks > cap) blocks = cap;
     // the same shared-memory carveout as the GEMM, so that blocks of this
-    // kernel can share an SM with a GEMM CTA running beside it (set once per
-    // instantiation and process)
-    static bool carveout_set[MAXMOD + 1] = {};
+    // kernel can share an SM with a GEMM CTA running beside it (a kernel
+    // attribute of each device: set once per instantiation, device and
+    // process; a bit per device ordinal below 64, set atomically, as ranks
+    // that are threads of one process may drive several devices)
+    static unsigned long long carveout_set[MAXMOD + 1] = {};
+    int dev = 0;
+    CA3DMM_CUDA_TRY(cudaGetDevice(&dev));
+    const unsigned long long dbit = dev < 64 ? 1ull << dev : 0ull;
     switch (pl->nmod) {
 #define CA3DMM_CRT_CASE(N)                                                                          \
     case N:                                                                                         \
-        if (!carveout_set[N]) {                                                                     \
+        if (!(__atomic_load_n(&carveout_set[N], __ATOMIC_ACQUIRE) & dbit)) {                        \
             CA3DMM_CUDA_TRY(cudaFuncSetAttribute(crt_reconstruct_kernel<N, crt_limbs(N)>,          \
                                                  cudaFuncAttributePreferredSharedMemoryCarveout,  \
                                                  (int) cudaSharedmemCarveoutMaxShared));          \
-            carveout_set[N] = true;                                                                 \
+            __atomic_fetch_or(&carveout_set[N], dbit, __ATOMIC_RELEASE);                            \
         }                                                                                           \
         crt_reconstruct_kernel<N, crt_limbs(N)><<<(unsigned) blocks, 256, 0, stream>>>(            \
             groups, g0, g1, r0, r1, total, w);                                                     \
