@@ -4,6 +4,7 @@
 #include "ca3dmm_util.h"
 #include "ca3dmm_kernels.h"
 #include "dev_type.h"
+#include "cuda_proxy.h"
 
 int is_dev_type_valid(dev_type_t dev_type)
 {
@@ -62,3 +63,33 @@ void dev_type_copy_mat_blk(size_t dt_size, const int nrow, const int ncol, const
     if (ca3dmm_copy_block_launch((const double *) src, lds, (double *) dst, ldd, ncol, nrow, 0))
         ERROR_PRINTF("dev_type_copy_mat_blk: copy launch failed\n");
 }
+
+/* ---------------------------------------------------------------- device choice */
+
+int ca3dmm_mpi_local_rank_env(void)
+{
+    static const char *const vars[] = {"MPI_LOCALRANKID", "MV2_COMM_WORLD_LOCAL_RANK",
+                                       "OMPI_COMM_WORLD_NODE_RANK", "SLURM_LOCALID",
+                                       "PBS_O_VNODENUM"};
+    for (size_t i = 0; i < sizeof(vars) / sizeof(vars[0]); i++) {
+        const char *v = getenv(vars[i]);
+        if (v) {                                  /* the first one set decides */
+            const long r = strtol(v, NULL, 10);
+            return r >= 0 && r < (1L << 30) ? (int) r : 0;
+        }
+    }
+    return -1;
+}
+
+void select_cuda_device_by_mpi_local_rank(void)
+{
+    int local = ca3dmm_mpi_local_rank_env();
+    if (local < 0) local = 0;
+    int ndev = 0;
+    cudaError_t err = cudaGetDeviceCount(&ndev);
+    if (err == cudaSuccess && ndev > 0) err = cudaSetDevice(local % ndev);
+    if (err != cudaSuccess || ndev <= 0)
+        ERROR_PRINTF("select_cuda_device_by_mpi_local_rank: no device selected (%s)\n",
+                     err != cudaSuccess ? cudaGetErrorString(err) : "no CUDA device");
+}
+

@@ -23,6 +23,7 @@
 #include <string.h>
 #include <cuda_runtime_api.h>
 #include "ca3dmm.h"
+#include "cuda_proxy.h"
 
 static int get_int_param(int argc, char **argv, int argi, int default_val, int min_val,
                          int max_val)
@@ -58,6 +59,9 @@ int main(int argc, char **argv)
         grid[2] = atoi(argv[11]);
         proc_grid = grid;
     }
+    /* one process per GPU under an MPI launcher: this process' GPU, as the
+     * reference's drivers choose it (examples/example_AB.c:43-46) */
+    select_cuda_device_by_mpi_local_rank();
     const char *pv = getenv("CA3DMM_VRANKS");
     int n_proc = pv ? atoi(pv) : (proc_grid ? grid[0] * grid[1] * grid[2] : 1);
     if (n_proc < 1) n_proc = 1;

@@ -17,6 +17,7 @@
 #include <string.h>
 #include <cuda_runtime_api.h>
 #include "ca3dmm.h"
+#include "cuda_proxy.h"
 
 static int get_int_param(int argc, char **argv, int argi, int default_val, int min_val,
                          int max_val)
@@ -42,6 +43,9 @@ int main(int argc, char **argv)
     int n_test = get_int_param(argc, argv, 4, 10, 1, 100);
     dev_type_t dev_type = get_int_param(argc, argv, 5, DEV_TYPE_CUDA, DEV_TYPE_CUDA,
                                         DEV_TYPE_CUDA_MPI_DIRECT);
+    /* one process per GPU under an MPI launcher: this process' GPU, as the
+     * reference's drivers choose it (examples/example_AB.c:43-46) */
+    select_cuda_device_by_mpi_local_rank();
     const char *pv = getenv("CA3DMM_VRANKS");
     int n_proc = pv ? atoi(pv) : 1;
     if (n_proc < 1) n_proc = 1;

@@ -17,6 +17,7 @@
 #include <string.h>
 #include <cuda_runtime_api.h>
 #include "ca3dmm.h"
+#include "cuda_proxy.h"
 
 static double uniform(uint64_t i, uint64_t j)
 {
@@ -99,6 +100,7 @@ int main(int argc, char **argv)
     CK(cudaMemcpy(dB, hB, sizeof(double) * nb, cudaMemcpyHostToDevice));
 
     MPI_Comm comm;
+    select_cuda_device_by_mpi_local_rank();   /* as examples/example_CholeskyQR.c does */
     if (ca3dmm_vcomm_create(p, &comm)) return 1;
     /* S = B^T B */
     ca3dmm_engine_p ce_S;

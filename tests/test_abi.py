@@ -64,3 +64,25 @@ def test_static_archive_defines_every_symbol_and_links():
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stderr[-2000:]
     assert subprocess.run([exe]).returncode == 0
+
+
+def test_local_rank_env_precedence(monkeypatch):
+    """select_cuda_device_by_mpi_local_rank's local rank: the first set of the
+    launchers' variables, in the reference's order (src/cuda_proxy.cu), -1 when
+    none is set, 0 for a value that is not a non-negative number."""
+    L = ctypes.CDLL(cb.LIB_PATH)
+    names = ["MPI_LOCALRANKID", "MV2_COMM_WORLD_LOCAL_RANK", "OMPI_COMM_WORLD_NODE_RANK",
+             "SLURM_LOCALID", "PBS_O_VNODENUM"]
+    for n in names:
+        monkeypatch.delenv(n, raising=False)
+    assert L.ca3dmm_mpi_local_rank_env() == -1
+    monkeypatch.setenv("PBS_O_VNODENUM", "9")
+    assert L.ca3dmm_mpi_local_rank_env() == 9
+    monkeypatch.setenv("SLURM_LOCALID", "5")
+    assert L.ca3dmm_mpi_local_rank_env() == 5
+    monkeypatch.setenv("OMPI_COMM_WORLD_NODE_RANK", "3")
+    assert L.ca3dmm_mpi_local_rank_env() == 3
+    monkeypatch.setenv("MV2_COMM_WORLD_LOCAL_RANK", "2")
+    assert L.ca3dmm_mpi_local_rank_env() == 2
+    monkeypatch.setenv("MPI_LOCALRANKID", "x")
+    assert L.ca3dmm_mpi_local_rank_env() == 0

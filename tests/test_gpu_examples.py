@@ -84,3 +84,21 @@ def test_example_btb(cuda):
         rc, out = run("example_btb", 512, 40000, 1, 2, 1,
                       env={"CA3DMM_VRANKS": "8", "CA3DMM_GEMM_MODE": mode})
         assert rc == 0 and parse(out)["errors"] == 0, out
+
+
+@pytest.mark.gpu
+def test_select_device_by_local_rank(cuda, monkeypatch):
+    """select_cuda_device_by_mpi_local_rank (include/cuda_proxy.h), which the
+    drivers call first: device (local rank mod device count) becomes current."""
+    import ctypes
+    import torch
+    import ca3dmm_b200 as cb
+    L = ctypes.CDLL(cb.LIB_PATH)
+    ndev = torch.cuda.device_count()
+    for n in ("MPI_LOCALRANKID", "MV2_COMM_WORLD_LOCAL_RANK", "SLURM_LOCALID", "PBS_O_VNODENUM"):
+        monkeypatch.delenv(n, raising=False)
+    for rank in (ndev, 2 * ndev - 1):
+        monkeypatch.setenv("OMPI_COMM_WORLD_NODE_RANK", str(rank))
+        L.select_cuda_device_by_mpi_local_rank()
+        assert torch.cuda.current_device() == rank % ndev
+    torch.cuda.set_device(0)
