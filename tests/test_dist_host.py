@@ -1,11 +1,16 @@
-"""The multi-GPU engine's host logic (ca3dmm_b200.dist) on CPU gloo ranks: the
-reference's grid and cuboids for p = the group's size, the pieces each rank
-sends and receives in the two operand/C all-to-alls, the unpacking into panels
-and slab layers and the slab-ordered sum.  The device side is replaced by
-numpy copies and the oracle's GEMMs (test only), so the assembled C must equal
-the single-process oracle bit for bit in split precision (slab by slab, slab
-order) and within k u |A||B| in plain FP64, for several rank counts, grids,
-transposes, source/destination layouts and B^T B."""
+"""The multi-GPU exec on CPU gloo ranks, two ways:
+  * the model of tests/_dist_model.py runs the whole exchange -- the
+    reference's grid and cuboids for p = the group's size, the pieces each rank
+    sends and receives in the operand and C all-to-alls, the unpacking into
+    panels and slab layers and the slab-ordered sum -- with numpy copies and
+    the oracle's GEMMs for the device side (test only), so that the assembled C
+    must equal the single-process oracle bit for bit in split precision (slab
+    by slab, slab order) and within k u |A||B| in plain FP64;
+  * the product's C engine (ca3dmm_dist_engine_init over the torch.distributed
+    transport of ca3dmm_b200/dist.py; init makes no CUDA call) plans the same
+    exchanges: its per-peer element counts must equal the model's, case by
+    case.
+Several rank counts, grids, transposes, source/destination layouts and B^T B."""
 import os
 import socket
 import sys
@@ -159,7 +164,10 @@ def _worker(rank, world, port, cases, q):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world,
                             timeout=datetime.timedelta(seconds=60))
-    from ca3dmm_b200.dist import DistCa3dmmEngine
+    import ca3dmm_b200 as cb
+    from ca3dmm_b200.dist import TorchTransport
+    from tests._dist_model import DistModel
+    tt = TorchTransport()
     out = []
     for case in cases:
         m, n, k, ta, tb, grid, lay, mode, s, btb, seed = case
@@ -174,15 +182,22 @@ def _worker(rank, world, port, cases, q):
             return torch.from_numpy(blk.ravel(order="F").copy() if blk.size else np.zeros(1)), \
                 max(r[1], 1)
 
-        e = DistCa3dmmEngine(m, n, k, ta, tb, sa, sb, dc, proc_grid=grid, btb=btb, gemm_mode=mode,
-                             slices=s, ops=NumpyOps())
+        e = DistModel(m, n, k, ta, tb, sa, sb, dc, proc_grid=grid, btb=btb, gemm_mode=mode,
+                      slices=s, ops=NumpyOps())
+        # the C engine's plan of the same call (no exec: that needs a GPU)
+        ce = cb.DistEngine(m, n, k, ta, tb, None if btb else sa, sb, dc, tt.t, proc_grid=grid,
+                           btb=btb, gemm_mode=mode, slices=s if mode else 0)
+        plan_c = ce.counts() if ce.ok else ce.rc
+        ce.free()
+        plan_model = [list(e.send_counts), list(e.recv_counts), list(e.c_send_counts),
+                      list(e.c_recv_counts)]
         tA, lda = block(A, sa) if A is not None else (torch.zeros(1, dtype=torch.float64), 1)
         tB, ldb = block(B, sb)
         ldc = max(dc[1], 1) + 1                 # a padded leading dimension
         tC = torch.full((ldc * max(dc[3], 1),), -1.0, dtype=torch.float64)
         e.exec(tA, lda, tB, ldb, tC, ldc)
         Cloc = tC.numpy().reshape(max(dc[3], 1), ldc).T[:dc[1], :dc[3]].copy()
-        out.append((dc, Cloc, (e.mp, e.np_, e.kp, e.rp)))
+        out.append((dc, Cloc, (e.mp, e.np_, e.kp, e.rp), plan_c, plan_model))
     dist.barrier()
     dist.destroy_process_group()
     q.put((rank, out))
@@ -231,8 +246,9 @@ def _run(world, cases):
         cm = n if btb else m
         C = np.full((cm, n), np.nan)
         for r in range(world):
-            dc, Cloc, g = res[r][i]
+            dc, Cloc, g, plan_c, plan_model = res[r][i]
             C[dc[0]:dc[0] + dc[1], dc[2]:dc[2] + dc[3]] = Cloc
+            assert plan_c == plan_model, (case, r, plan_c, plan_model)
         kp = res[0][i][2][2]
         if grid is not None:
             assert res[0][i][2][:3] == tuple(grid)
@@ -306,27 +322,31 @@ def _bad_worker(rank, world, port, q):
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world,
                             timeout=datetime.timedelta(seconds=60))
-    from ca3dmm_b200.dist import DistCa3dmmEngine
+    import ca3dmm_b200 as cb
+    from ca3dmm_b200.dist import TorchTransport
+    from tests._dist_model import DistModel
+    tt = TorchTransport()
     m, n, k = 40, 30, 50
     cols = lambda nr, nc: _layout("cols", nr, nc, world, rank)
-    calls = {
+    args = {
         # rank 1 passes another m
-        "sizes": lambda: DistCa3dmmEngine(m + rank, n, k, 0, 0, cols(m, k), cols(k, n),
-                                          cols(m, n), ops=NumpyOps()),
+        "sizes": (m + rank, n, k, cols(m, k), cols(k, n), cols(m, n)),
         # rank 1 owns no part of A: rank panels are not covered
-        "cover": lambda: DistCa3dmmEngine(m, n, k, 0, 0, cols(m, k) if rank == 0 else (0, 0, 0, 0),
-                                          cols(k, n), cols(m, n), ops=NumpyOps()),
+        "cover": (m, n, k, cols(m, k) if rank == 0 else (0, 0, 0, 0), cols(k, n), cols(m, n)),
         # a source rectangle beyond the matrix
-        "bounds": lambda: DistCa3dmmEngine(m, n, k, 0, 0, cols(m, k), (0, k + 1, 0, n),
-                                           cols(m, n), ops=NumpyOps()),
+        "bounds": (m, n, k, cols(m, k), (0, k + 1, 0, n), cols(m, n)),
     }
     out = {}
-    for name, fn in calls.items():
+    for name, (mm, nn, kk, sa, sb, dc) in args.items():
         try:
-            fn()
+            DistModel(mm, nn, kk, 0, 0, sa, sb, dc, ops=NumpyOps())
             out[name] = None
         except ValueError as exc:
             out[name] = str(exc)
+        # the C engine refuses the same call on every rank
+        ce = cb.DistEngine(mm, nn, kk, 0, 0, sa, sb, dc, tt.t)
+        out[name + "_c"] = ce.rc
+        ce.free()
     dist.barrier()
     dist.destroy_process_group()
     q.put((rank, out))
@@ -334,7 +354,9 @@ def _bad_worker(rank, world, port, q):
 
 def test_dist_engine_rejects_inconsistent_calls_on_every_rank():
     """Inconsistent arguments, uncovered panels and out-of-range blocks raise
-    ValueError on every rank before any exchange (no rank is left waiting)."""
+    ValueError on every rank before any exchange (no rank is left waiting) in
+    the model, and make ca3dmm_dist_engine_init return CA3DMM_EINVAL on every
+    rank."""
     import queue
     import time
     ctx = mp.get_context("spawn")
@@ -358,3 +380,4 @@ def test_dist_engine_rejects_inconsistent_calls_on_every_rank():
         assert "disagree" in res[r]["sizes"]
         assert "do not cover" in res[r]["cover"]
         assert "outside" in res[r]["bounds"]
+        assert res[r]["sizes_c"] == res[r]["cover_c"] == res[r]["bounds_c"] == 1

@@ -1,11 +1,13 @@
-"""The multi-GPU engine (ca3dmm_b200.dist) with its device side: batched
-rectangle copies (mat_redist_layouts), the single-GPU engine for each rank's
-cuboid and the slab-ordered sum kernel.  Only one GPU is visible, so the ranks
-are processes sharing it over gloo, which stages the exchanged pieces through
-host memory (the reference's DEV_TYPE_CUDA); no kernel waits on another rank.
-One rank over NCCL runs the device-direct exchange (DEV_TYPE_CUDA_MPI_DIRECT).
-Split precision must equal the single-GPU engine on the same grid bit for
-bit; plain FP64 stays within k u |A||B| of the exact product."""
+"""The multi-GPU engine from Python (ca3dmm_b200.dist: the C engine of
+include/ca3dmm_dist.h over a torch.distributed transport) with its device
+side: batched rectangle copies, the single-GPU engine for each rank's cuboid
+and the slab-ordered sum kernel.  Only one GPU is visible, so the ranks are
+processes sharing it over gloo, which stages the exchanged pieces through host
+memory (the reference's DEV_TYPE_CUDA); no kernel waits on another rank.  One
+rank over NCCL runs the device-direct exchange (DEV_TYPE_CUDA_MPI_DIRECT).
+INT8-slice split precision must equal the single-GPU engine on the same grid
+bit for bit; plain FP64 and the modular mode stay within 2 k u |A||B| of the
+exact product."""
 import os
 import sys
 
@@ -115,7 +117,8 @@ def test_dist_engine_three_ranks_host_staged(cuda):
     _run(3, "gloo", [(300, 200, 700, 0, 0, None, "cols", 1, 7, False, 51),
                      (256, 384, 512, 1, 1, (1, 1, 3), "rows", 1, 6, False, 52),
                      (180, 180, 2000, 0, 0, None, "cols", 1, 7, True, 53),
-                     (200, 300, 400, 0, 1, (3, 1, 1), "blocks", 0, 0, False, 54)])
+                     (200, 300, 400, 0, 1, (3, 1, 1), "blocks", 0, 0, False, 54),
+                     (300, 200, 700, 1, 0, None, "rows", 2, 0, False, 55)])
 
 
 def test_dist_engine_four_ranks_host_staged(cuda):
