@@ -34,74 +34,6 @@ def _area(r):
     return r[1] * r[3] if r is not None else 0
 
 
-class _CudaOps:
-    """The device side on a GPU: batched rectangle copies (mat_redist_layouts),
-    the single-GPU engine for the local GEMM and the ordered slab sum (the
-    engine's kp-slab reduction kernel), on the caller's current torch stream."""
-
-    def _stream(self):
-        return self.torch.cuda.current_stream(self.device).cuda_stream
-
-    def __init__(self, device):
-        import torch
-        self.torch = torch
-        self.device = device
-
-    def empty(self, count):
-        return self.torch.empty(max(int(count), 1), dtype=self.torch.float64, device=self.device)
-
-    def zeros(self, count):
-        return self.torch.zeros(max(int(count), 1), dtype=self.torch.float64, device=self.device)
-
-    def copier(self, src_rects, dst_rects):
-        """A reusable batched copy: every intersection of a source rectangle
-        with a destination rectangle (stacked coordinates, see _rm)."""
-        if not src_rects or not dst_rects:
-            return None
-        L = cb.RedistLayouts([_rm(r) for r in src_rects], [_rm(r) for r in dst_rects])
-        if not L.ok:
-            raise RuntimeError("mat_redist_layouts_init failed")
-        return L
-
-    def copy(self, L, srcs, dsts):
-        """srcs, dsts: lists of (tensor, element offset, ld) beside the rects."""
-        if L is None:
-            return
-        sp = [t.data_ptr() + 8 * off for t, off, _ in srcs]
-        dp = [t.data_ptr() + 8 * off for t, off, _ in dsts]
-        rc = L.exec(sp, [max(ld, 1) for _, _, ld in srcs], dp, [max(ld, 1) for _, _, ld in dsts],
-                    self._stream())
-        if rc:
-            raise RuntimeError("mat_redist_layouts_exec failed: %s" % cb.ERRORS.get(rc, rc))
-
-    def gemm_engine(self, m, n, k, ta, tb, mode, slices):
-        e = cb.Ca3dmmEngine(m, n, k, ta, tb, p=1)
-        if not e.ok:
-            raise RuntimeError("local engine init failed")
-        if e.set_gemm_mode(mode, slices) != 0:
-            raise RuntimeError("local engine: GEMM mode unavailable")
-        return e
-
-    def gemm(self, e, A, lda, B, ldb, C, ldc):
-        e.set_stream(self._stream(), 1)
-        rc = e.exec(A, lda, B, ldb, C, ldc)
-        if rc:
-            raise RuntimeError("local exec failed: %s" % cb.ERRORS.get(rc, rc))
-
-    def ordered_sum(self, layers, kp, nr, nc, out, ldo):
-        L = cb.lib()
-        import ctypes as C
-        rc = L.ca3dmm_reduce_slabs_launch(C.c_void_p(layers.data_ptr()), C.c_longlong(nr * nc),
-                                          C.c_longlong(max(nr, 1)), kp, nr, nc,
-                                          C.c_void_p(out.data_ptr()), C.c_longlong(ldo),
-                                          C.c_void_p(self._stream()))
-        if rc:
-            raise RuntimeError("slab sum failed: %s" % cb.ERRORS.get(rc, rc))
-
-    def sync(self):
-        self.torch.cuda.synchronize(self.device)
-
-
 def _rm(r):
     """A column-major rectangle of layer/matrix `r[4]` as the row-major rectangle
     of the transposed matrix that mat_redist_layouts works on, stacked by the
@@ -121,8 +53,7 @@ class DistModel:
     takes this rank's blocks as flat float64 device tensors (column-major)."""
 
     def __init__(self, m, n, k, trans_A, trans_B, src_A, src_B, dst_C, proc_grid=None,
-                 group=None, btb=False, gemm_mode=cb.GEMM_PLAIN, slices=7, device=None,
-                 ops=None):
+                 group=None, btb=False, gemm_mode=cb.GEMM_PLAIN, slices=7, ops=None):
         import torch
         import torch.distributed as dist
         self.dist, self.torch = dist, torch
@@ -133,11 +64,10 @@ class DistModel:
         self.m, self.n, self.k = (n if btb else m), n, k
         self.ta, self.tb = (1 if btb else int(trans_A)), (0 if btb else int(trans_B))
         self.direct = dist.get_backend(group) == "nccl"
-        if device is None:
-            device = getattr(ops, "device", None) or torch.device("cuda",
-                                                                   torch.cuda.current_device())
-        self.ops = ops if ops is not None else _CudaOps(device)
-        self.comm_device = device if self.direct else torch.device("cpu")
+        if ops is None:
+            raise ValueError("the model needs its device-side stand-in (ops)")
+        self.ops = ops
+        self.comm_device = ops.device if self.direct else torch.device("cpu")
         # every rank's rectangles
         # every rank's rectangles and call arguments: each rank checks all of
         # them, so an inconsistent call raises on every rank before any exchange
