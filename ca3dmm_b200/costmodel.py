@@ -8,10 +8,11 @@ transposes, entries sign * (1 + u) * 2^e with e uniform in [-E, E], E drawn
 per shape from {0, 4, 8} (the exponent-spread feature).  Candidates
 (ca3dmm_tune_cfg_t: mode, slices or moduli, kp, raster or band, tile
 columns): plain FP64 DMMA with k-slab splits kp in {1, 2, 4} and raster
-bands of 8 or 16 tile rows; 7 INT8 slices with kp in {1, 2} and raster 8 or
-16, and 8 slices; the modular mode at the fewest moduli for 51-bit integers
-with 256- or 128-column tiles and bands of 32 or 8 tile rows, and at two
-moduli more (16 configurations).  Every candidate is timed on every shape on
+bands of 8 or 16 tile rows on 128-column tiles, and on 64-column tiles with
+raster 8; 7 INT8 slices with kp in {1, 2} and raster 8 or 16, and 8 slices;
+the modular mode at the fewest moduli for 51-bit integers with 256- or
+128-column tiles and bands of 32 or 8 tile rows, and at two moduli more (19
+configurations).  Every candidate is timed on every shape on
 one engine per kp (ca3dmm_engine_set_tune between candidates: one warm-up,
 then the mean of `reps` execs from the engine's device events).  The MLP is
 trained on log2(ms) of the training shapes and evaluated on the held-out
@@ -34,6 +35,7 @@ import ca3dmm_b200 as cb
 
 AUTO, AUTO2 = 0, -2    # the fewest moduli for 51-bit integers; two more
 CANDS = ([(0, 0, kp, r, 0) for kp in (1, 2, 4) for r in (8, 16)] +
+         [(0, 0, kp, 8, 64) for kp in (1, 2, 4)] +
          [(1, 7, kp, r, 0) for kp in (1, 2) for r in (8, 16)] + [(1, 8, 1, 8, 0)] +
          [(2, AUTO, 1, band, tn) for tn in (256, 128) for band in (32, 8)] +
          [(2, AUTO2, 1, 32, 256)])

@@ -38,11 +38,11 @@ int ca3dmm_tune_features(int m, int n, int k, int trans_A, int trans_B,
 {
     if (!cfg || !f || m < 1 || n < 1 || k < 1) return CA3DMM_EINVAL;
     const int mode = cfg->gemm_mode;
-    /* the tile each GEMM kernel computes: DMMA 128 x 128, slices 128 x 64,
-     * modular 128 x tile_n */
+    /* the tile each GEMM kernel computes: DMMA 128 x 128 or 128 x 64, slices
+     * 128 x 64, modular 128 x tile_n */
     const int rows = 128;
     const int cols = mode == CA3DMM_GEMM_CRT ? (cfg->tile_n == 128 ? 128 : 256)
-                     : mode == CA3DMM_GEMM_OZAKI ? 64 : 128;
+                     : mode == CA3DMM_GEMM_OZAKI ? 64 : (cfg->tile_n == 64 ? 64 : 128);
     const int raster = cfg->raster > 0 ? cfg->raster : (mode == CA3DMM_GEMM_CRT ? 32 : 8);
     f[0] = (float) log2((double) m);
     f[1] = (float) log2((double) n);

@@ -112,6 +112,10 @@ typedef struct {
     cudaEvent_t ev_band[CRT_MAX_BANDS], ev_join;
     int aux_ok;
     int crt_tile_n;               /* CRT GEMM tile columns, 128 or 256 (env CA3DMM_CRT_TILE_N) */
+    int plain_tile_n;             /* plain DMMA GEMM tile columns, 128 or 64 (env
+                                     CA3DMM_PLAIN_TILE_N; 128 for the symmetric B^T B plan,
+                                     whose tiles follow 128-row block rows) */
+    int plain_tile_n_env;
     int upload_for_host;          /* the plan being uploaded serves exec_host's row bands */
     /* guard bands: 256-byte canaries between the work buffer's regions, filled
      * with CANARY_BYTE at each plan upload and, with CA3DMM_CANARY=1, checked
@@ -374,6 +378,9 @@ static int plan_build(ca3dmm_engine_p e)
     GET_ENV_INT_VAR(pl->crt_band, "CA3DMM_CRT_BAND", "crt_band", 32, 0, 1 << 20);
     pl->crt_band_env = pl->crt_band;
     GET_ENV_INT_VAR(pl->crt_tile_n, "CA3DMM_CRT_TILE_N", "crt_tile_n", 256, 128, 256);
+    GET_ENV_INT_VAR(pl->plain_tile_n, "CA3DMM_PLAIN_TILE_N", "plain_tile_n", 128, 64, 128);
+    if (pl->plain_tile_n != 64 || pl->sym) pl->plain_tile_n = 128;
+    pl->plain_tile_n_env = pl->plain_tile_n;
     GET_ENV_INT_VAR(pl->crt_overlap, "CA3DMM_CRT_OVERLAP", "crt_overlap", 1, 0, 1);
     GET_ENV_INT_VAR(pl->crt_overlap_blocks, "CA3DMM_CRT_OVERLAP_BLOCKS", "crt_overlap_blocks", 2, 1, 2);
     if (pl->crt_tile_n != 128) pl->crt_tile_n = 256;
@@ -640,8 +647,10 @@ int ca3dmm_engine_candidates(ca3dmm_engine_p e, ca3dmm_tune_cfg_t *c, int max)
         l[n].gemm_mode = (md); l[n].slices = (sl); l[n].kp = e->kp;                          \
         l[n].raster = (r); l[n].tile_n = (tn); n++;                                          \
     } while (0)
+    const plan_t *pl = (const plan_t *) e->impl;
     CA3DMM_CAND(CA3DMM_GEMM_PLAIN, 0, 8, 0);
     CA3DMM_CAND(CA3DMM_GEMM_PLAIN, 0, 16, 0);
+    if (!pl->sym) CA3DMM_CAND(CA3DMM_GEMM_PLAIN, 0, 8, 64);
     CA3DMM_CAND(CA3DMM_GEMM_OZAKI, 7, 8, 0);
     CA3DMM_CAND(CA3DMM_GEMM_OZAKI, 7, 16, 0);
     CA3DMM_CAND(CA3DMM_GEMM_OZAKI, 8, 8, 0);
@@ -1083,7 +1092,8 @@ static int plan_upload(ca3dmm_engine_p e, const void *A, int ldA, const void *B,
             q->a_kmajor = pl->a_kmajor;
         }
     }
-    int rc = ca3dmm_dgemm_plan_encode(gd, pl->ngroup * ks, h + pl->off_gemm, &pl->gemm_tiles);
+    int rc = ca3dmm_dgemm_plan_encode_tn(gd, pl->ngroup * ks, h + pl->off_gemm, &pl->gemm_tiles,
+                                         pl->plain_tile_n);
     if (rc) return rc;
     if (e->gemm_mode == CA3DMM_GEMM_OZAKI) {
         ca3dmm_oz_blk_t *ob = pl->ob;
@@ -1354,8 +1364,8 @@ static int exec_device(ca3dmm_engine_p e, const void *src_A, int ldA, const void
         rc = ca3dmm_oz_run_gemm(&pl->oz, status_d, 5.0, st);
         if (!rc) rc = ca3dmm_oz_run_nonfinite(&pl->oz, NULL, src_A, src_B, st);
     } else
-        rc = ca3dmm_dgemm_launch(w + pl->off_gemm, pl->ngroup * pl->ksplit, pl->gemm_tiles,
-                                 pl->a_kmajor, status_d, 5.0, st);
+        rc = ca3dmm_dgemm_launch_tn(w + pl->off_gemm, pl->ngroup * pl->ksplit, pl->gemm_tiles,
+                                    pl->a_kmajor, status_d, 5.0, st, pl->plain_tile_n);
     nvtxRangePop();
     if (rc) return rc;
     if (timing) cudaEventRecord(pl->ev[2], st);
@@ -1576,7 +1586,7 @@ static int hx_build_bands(ca3dmm_engine_p e, struct host_exec *x, cudaStream_t s
         (!ozaki && pl->ksplit > 1))
         return 0;
     const int raster = e->raster > 0 ? e->raster : 8;
-    const int bn = ozaki ? 64 : 128;
+    const int bn = ozaki ? 64 : pl->plain_tile_n;
     /* tile numbering of the GEMM plans: per group (plain) or per unit of
      * (task_m, task_n) with its kp slabs chained (split precision) */
     int *tb = (int *) malloc(sizeof(int) * (size_t) pl->ngroup);
@@ -1759,7 +1769,8 @@ static int hx_btb_slabs(ca3dmm_engine_p e, struct host_exec *x, const void *B_h,
         for (int g = j * gps; g < (j + 1) * gps; g++) {
             const group_t *gg = &pl->groups[g];
             if (gg->mz <= 0 || gg->nz <= 0) continue;
-            count += ks * ((gg->mz + 127) / 128) * (ozaki ? (gg->nz + 63) / 64 : (gg->nz + 127) / 128);
+            const int bn = ozaki ? 64 : pl->plain_tile_n;
+            count += ks * ((gg->mz + 127) / 128) * ((gg->nz + bn - 1) / bn);
         }
         ca3dmm_tile_ranges_t rg;
         memset(&rg, 0, sizeof(rg));
@@ -1785,8 +1796,8 @@ static int hx_btb_slabs(ca3dmm_engine_p e, struct host_exec *x, const void *B_h,
             if (!rc) rc = ca3dmm_oz_run_gemm_ranges(&pl->oz, &rg, status_d, 5.0, st);
             if (!rc) rc = ca3dmm_oz_run_nonfinite(&pl->oz, &rg, x->dB, x->dB, st);
         } else {
-            rc = ca3dmm_dgemm_launch_ranges(w + pl->off_gemm, pl->ngroup * pl->ksplit, &rg,
-                                            pl->a_kmajor, status_d, 5.0, st);
+            rc = ca3dmm_dgemm_launch_ranges_tn(w + pl->off_gemm, pl->ngroup * pl->ksplit, &rg,
+                                               pl->a_kmajor, status_d, 5.0, st, pl->plain_tile_n);
         }
         if (rc) return rc;
     }
@@ -1924,8 +1935,9 @@ static int exec_host(ca3dmm_engine_p e, const void *A_h, int ldA, const void *B_
             rc = ca3dmm_pack_launch(x->dA, (double *) w, (const ca3dmm_pack_desc_t *) dd, x->ndesc,
                                     x->ntile[c][0], st);
             if (!rc)
-                rc = ca3dmm_dgemm_launch_ranges(w + pl->off_gemm, pl->ngroup, &x->rng[c],
-                                                pl->a_kmajor, status_d, 5.0, st);
+                rc = ca3dmm_dgemm_launch_ranges_tn(w + pl->off_gemm, pl->ngroup, &x->rng[c],
+                                                   pl->a_kmajor, status_d, 5.0, st,
+                                                   pl->plain_tile_n);
         }
         if (!rc && !crt && e->kp > 1 && !(ozaki && pl->oz_fused) && !(!ozaki && pl->plain_merged))
             rc = ca3dmm_reduce_slabs_launch((const double *) (w + pl->off_slab) + x->r0[c],
@@ -2093,8 +2105,13 @@ int ca3dmm_engine_set_tune(ca3dmm_engine_p e, const ca3dmm_tune_cfg_t *c)
         if ((c->tile_n != 0 && c->tile_n != 128 && c->tile_n != 256) || c->raster < 0 ||
             c->raster > 1024)
             return CA3DMM_EINVAL;
-    } else if (c->tile_n != 0 ||
-               (c->raster != 0 && c->raster != 4 && c->raster != 8 && c->raster != 16)) {
+    } else if (c->raster != 0 && c->raster != 4 && c->raster != 8 && c->raster != 16) {
+        return CA3DMM_EINVAL;
+    } else if (c->gemm_mode == CA3DMM_GEMM_PLAIN) {
+        /* 128- or 64-column DMMA tiles; the symmetric B^T B plan takes 128 */
+        if ((c->tile_n != 0 && c->tile_n != 64 && c->tile_n != 128) || (c->tile_n == 64 && pl->sym))
+            return CA3DMM_EINVAL;
+    } else if (c->tile_n != 0) {
         return CA3DMM_EINVAL;
     }
     int rc = ca3dmm_engine_set_gemm_mode(e, c->gemm_mode, c->slices);
@@ -2104,6 +2121,8 @@ int ca3dmm_engine_set_tune(ca3dmm_engine_p e, const ca3dmm_tune_cfg_t *c)
         pl->crt_tile_n = c->tile_n ? c->tile_n : 256;
     } else {
         e->raster = c->raster ? c->raster : 8;
+        if (c->gemm_mode == CA3DMM_GEMM_PLAIN)
+            pl->plain_tile_n = c->tile_n ? c->tile_n : pl->plain_tile_n_env;
     }
     pl->plan_valid = 0;
     return CA3DMM_OK;
@@ -2118,7 +2137,9 @@ int ca3dmm_engine_get_tune(ca3dmm_engine_p e, ca3dmm_tune_cfg_t *c)
                 : e->gemm_mode == CA3DMM_GEMM_CRT ? e->crt_moduli : 0;
     c->kp = e->kp;
     c->raster = e->gemm_mode == CA3DMM_GEMM_CRT ? pl->crt_band : e->raster;
-    c->tile_n = e->gemm_mode == CA3DMM_GEMM_CRT ? pl->crt_tile_n : 0;
+    c->tile_n = e->gemm_mode == CA3DMM_GEMM_CRT ? pl->crt_tile_n
+                : (e->gemm_mode == CA3DMM_GEMM_PLAIN && pl->plain_tile_n != 128) ? pl->plain_tile_n
+                : 0;
     return CA3DMM_OK;
 }
 

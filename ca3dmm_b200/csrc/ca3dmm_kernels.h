@@ -49,6 +49,10 @@ size_t ca3dmm_dgemm_plan_bytes(int nprob);
  * repeats. */
 int ca3dmm_dgemm_plan_encode(const ca3dmm_dgemm_desc_t *probs, int nprob, void *host_plan,
                              int *total_tiles);
+/* The same with output tiles of 128 x tile_n (tile_n = 128, the default, or
+ * 64); the launch must be given the same tile_n. */
+int ca3dmm_dgemm_plan_encode_tn(const ca3dmm_dgemm_desc_t *probs, int nprob, void *host_plan,
+                                int *total_tiles, int tile_n);
 /* Up to CA3DMM_MAX_RANGES contiguous ranges [begin, begin + len) of a grouped
  * plan's tile list (each problem's tiles are numbered in raster bands of
  * `raster` tile rows, so a band of output rows is one range per problem). */
@@ -66,6 +70,13 @@ int ca3dmm_dgemm_launch(const void *dev_plan, int nprob, int total_tiles, int a_
 int ca3dmm_dgemm_launch_ranges(const void *dev_plan, int nprob, const ca3dmm_tile_ranges_t *ranges,
                                int a_kmajor, int *dev_status, double timeout_s,
                                cudaStream_t stream);
+/* Both for a plan encoded with tile_n (ca3dmm_dgemm_plan_encode_tn). */
+int ca3dmm_dgemm_launch_tn(const void *dev_plan, int nprob, int total_tiles, int a_kmajor,
+                           int *dev_status, double timeout_s, cudaStream_t stream, int tile_n);
+int ca3dmm_dgemm_launch_ranges_tn(const void *dev_plan, int nprob,
+                                  const ca3dmm_tile_ranges_t *ranges, int a_kmajor,
+                                  int *dev_status, double timeout_s, cudaStream_t stream,
+                                  int tile_n);
 
 /* ---- pack / transpose ----------------------------------------------------
  * Batched block copies between column-major matrices.  Descriptor j copies a

@@ -37,14 +37,24 @@
 
 namespace {
 
-constexpr int BM = 128, BN = 128, BK = 16;
-constexpr int STAGES = 5;
-constexpr int STAGE_BYTES = (BM + BN) * BK * 8;      // 32 KiB
+constexpr int BM = 128, BK = 16;
 constexpr int A_BYTES = BM * BK * 8;                 // 16 KiB
 constexpr int CONSUMER_WARPS = 8;
 constexpr int THREADS = CONSUMER_WARPS * 32;         // thread 0 also issues the TMA loads
 constexpr int GROUP_M = 8;
-constexpr size_t SMEM_BYTES = (size_t) STAGES * STAGE_BYTES + 2 * STAGES * 8 + 1024;
+
+// The output tile is BM x TBN, TBN = 128 or 64 columns.  Each warp computes
+// 16 MI rows x 32 columns (MI m16 tiles x 4 n8 tiles): the 8 warps stand
+// WM x WN = 2 x 4 over a 128-column tile and 4 x 2 over a 64-column one, so
+// the fragment layout of a warp is the same for both widths.
+template <int TBN>
+struct DTile {
+    static_assert(TBN == 128 || TBN == 64, "tile width");
+    static constexpr int WN = TBN / 32, WM = CONSUMER_WARPS / WN, MI = BM / (16 * WM);
+    static constexpr int STAGE_BYTES = A_BYTES + TBN * BK * 8;   // 32 or 24 KiB
+    static constexpr int STAGES = TBN == 128 ? 5 : 6;
+    static constexpr size_t SMEM_BYTES = (size_t) STAGES * STAGE_BYTES + 2 * STAGES * 8 + 1024;
+};
 
 struct alignas(16) DProb {
     double *C;
@@ -113,6 +123,7 @@ __device__ __forceinline__ void store_pair(const DProb &p, int m, int n, double 
 
 // Iterator over this CTA's (tile, k-tile) load sequence, used by the
 // producer thread.  Tiles with k == 0 carry no loads and are skipped.
+template <int TBN>
 struct LoadCursor {
     int tile, kt, ktiles, pi, m0, n0;   // tile: virtual index into the launch's ranges
     bool valid;
@@ -128,7 +139,7 @@ struct LoadCursor {
                 int tm, tn;
                 tile_coords(p, t, tm, tn);
                 m0 = tm * BM;
-                n0 = tn * BN;
+                n0 = tn * TBN;
                 valid = true;
                 return;
             }
@@ -152,19 +163,22 @@ __device__ __forceinline__ int sigma_row(int g) { return (g & 4) | ((g & 1) << 1
 
 // The k loop of one output tile: wait for each stage, run the 16-k block's
 // DMMAs, release the stage and (thread 0) refill it.  AK: A tile K-major.
-template <bool AK, class Issue>
+template <bool AK, int TBN, class Issue>
 __device__ __forceinline__ bool k_loop(const uint8_t *smem, uint64_t *full, uint64_t *empty,
-                                       int ktiles, uint32_t &it, double (&acc)[4][4][4],
+                                       int ktiles, uint32_t &it,
+                                       double (&acc)[DTile<TBN>::MI][4][4],
                                        volatile int *abort_flag, int *status,
                                        unsigned long long limit_ns, bool producer,
                                        Issue &issue_one, int wm, int wn, int g, int t, int lane)
 {
+    using T = DTile<TBN>;
+    constexpr int MI = T::MI;
     for (int kt = 0; kt < ktiles; ++kt, ++it) {
-        const uint32_t stage = it % STAGES, phase = (it / STAGES) & 1u;
+        const uint32_t stage = it % T::STAGES, phase = (it / T::STAGES) & 1u;
         if (!mbar_wait_bounded(&full[stage], phase, abort_flag, status,
                                CA3DMM_DEV_TIMEOUT_CONSUME, limit_ns))
             return false;
-        const uint8_t *sA = smem + stage * STAGE_BYTES;
+        const uint8_t *sA = smem + stage * T::STAGE_BYTES;
         const uint8_t *sB = sA + A_BYTES;
 #pragma unroll
         for (int q = 0; q < 2; ++q) {
@@ -177,12 +191,12 @@ __device__ __forceinline__ bool k_loop(const uint8_t *smem, uint64_t *full, uint
             }
             if (AK) {
 #pragma unroll
-                for (int ip = 0; ip < 2; ++ip) {
+                for (int ip = 0; ip < MI / 2; ++ip) {
                     double2 alo[2], ahi[2];
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
                         // K-major A: tile row of MMA row g of m16 tile i
-                        const int ra = wm * 64 + 2 * sigma_row(g) + 16 * (2 * ip + h);
+                        const int ra = wm * 16 * MI + 2 * sigma_row(g) + 16 * (2 * ip + h);
                         alo[h] = *reinterpret_cast<const double2 *>(
                             sA + ra * 128 + (((4 * q + t) ^ (ra & 7)) << 4));
                         ahi[h] = *reinterpret_cast<const double2 *>(
@@ -202,13 +216,13 @@ __device__ __forceinline__ bool k_loop(const uint8_t *smem, uint64_t *full, uint
 #pragma unroll
                 for (int b = 0; b < 2; ++b) {
                     const int kr = 8 * q + 2 * t + b;
-                    double2 af[4];
+                    double2 af[MI];
 #pragma unroll
-                    for (int i = 0; i < 4; ++i)
+                    for (int i = 0; i < MI; ++i)
                         af[i] = *reinterpret_cast<const double2 *>(
-                            sA + (wm * 4 + i) * 2048 + kr * 128 + ((g ^ (kr & 7)) << 4));
+                            sA + (wm * MI + i) * 2048 + kr * 128 + ((g ^ (kr & 7)) << 4));
 #pragma unroll
-                    for (int i = 0; i < 4; ++i)
+                    for (int i = 0; i < MI; ++i)
 #pragma unroll
                         for (int j = 0; j < 4; ++j)
                             dmma(acc[i][j], af[i].x, af[i].y, b ? bf[j].y : bf[j].x);
@@ -227,7 +241,7 @@ __device__ __forceinline__ bool k_loop(const uint8_t *smem, uint64_t *full, uint
 // of load L - STAGES.  Loads are issued STAGES-1 ahead of consumption, and the
 // refill after consuming load `it` waits on the release of load it - 1, which
 // every warp has usually finished, so the producer thread rarely stalls.
-template <bool AK>
+template <bool AK, int TBN>
 __global__ void __launch_bounds__(THREADS, 1)
 dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restrict__ probs,
                    int nprob, const ca3dmm_tile_ranges_t rg, int total_tiles, int *status,
@@ -236,6 +250,8 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
     extern __shared__ uint8_t smem_raw[];
     uint8_t *smem = reinterpret_cast<uint8_t *>(
         (reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    using T = DTile<TBN>;
+    constexpr int STAGES = T::STAGES, STAGE_BYTES = T::STAGE_BYTES, MI = T::MI;
     uint64_t *full = reinterpret_cast<uint64_t *>(smem + STAGES * STAGE_BYTES);
     uint64_t *empty = full + STAGES;
     __shared__ volatile int abort_flag;
@@ -258,7 +274,7 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
     }
     __syncthreads();
 
-    LoadCursor lc = {};
+    LoadCursor<TBN> lc = {};
     uint32_t issued = 0;
     int last_p = -1;
     // Issue load number `issued` at the cursor (producer thread only).
@@ -298,9 +314,9 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
     }
 
     const int g = lane >> 2, t = lane & 3;
-    const int wm = warp >> 2, wn = warp & 3;
+    const int wm = warp / T::WN, wn = warp % T::WN;
     uint32_t it = 0;   // loads consumed so far
-    double acc[4][4][4];
+    double acc[MI][4][4];
     bool ok = true;
 
     for (int v = blockIdx.x; v < total_tiles && ok; v += gridDim.x) {
@@ -311,20 +327,20 @@ dgemm_dmma_grouped(const CUtensorMap *__restrict__ tmaps, const DProb *__restric
         tile_coords(p, tile, tm, tn);
         const int ktiles = (p.k + BK - 1) / BK;
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < MI; ++i)
 #pragma unroll
             for (int j = 0; j < 4; ++j)
 #pragma unroll
                 for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.0;
 
-        ok = k_loop<AK>(smem, full, empty, ktiles, it, acc, &abort_flag, status, limit_ns,
+        ok = k_loop<AK, TBN>(smem, full, empty, ktiles, it, acc, &abort_flag, status, limit_ns,
                         producer, issue_one, wm, wn, g, t, lane);
         if (!ok) break;
 
-        const int mb = tm * BM + wm * 64 + 2 * (AK ? sigma_row(g) : g);
-        const int nb = tn * BN + wn * 32 + 8 * t;
+        const int mb = tm * BM + wm * 16 * MI + 2 * (AK ? sigma_row(g) : g);
+        const int nb = tn * TBN + wn * 32 + 8 * t;
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < MI; ++i)
 #pragma unroll
             for (int j = 0; j < 4; ++j) {
                 store_pair(p, mb + 16 * i, nb + j, acc[i][j][0], acc[i][j][2]);
@@ -440,6 +456,13 @@ extern "C" size_t ca3dmm_dgemm_plan_bytes(int nprob)
 extern "C" int ca3dmm_dgemm_plan_encode(const ca3dmm_dgemm_desc_t *probs, int nprob,
                                         void *host_plan, int *total_tiles)
 {
+    return ca3dmm_dgemm_plan_encode_tn(probs, nprob, host_plan, total_tiles, 128);
+}
+
+extern "C" int ca3dmm_dgemm_plan_encode_tn(const ca3dmm_dgemm_desc_t *probs, int nprob,
+                                           void *host_plan, int *total_tiles, int tile_n)
+{
+    if (tile_n != 128 && tile_n != 64) return CA3DMM_EINVAL;
     CUtensorMap *tm = reinterpret_cast<CUtensorMap *>(host_plan);
     DProb *dp = reinterpret_cast<DProb *>(tm + 2 * nprob);
     int tiles = 0;
@@ -461,7 +484,7 @@ extern "C" int ca3dmm_dgemm_plan_encode(const ca3dmm_dgemm_desc_t *probs, int np
             if (r) return r;
             r = ca3dmm_encode_tmap_2d(&tm[2 * i + 1], 8, q.B, (unsigned long long) q.k,
                                       (unsigned long long) q.n, (unsigned long long) q.ldb * 8,
-                                      16, BN, 1);
+                                      16, (unsigned) tile_n, 1);
             if (r) return r;
         }
         DProb &d = dp[i];
@@ -473,7 +496,7 @@ extern "C" int ca3dmm_dgemm_plan_encode(const ca3dmm_dgemm_desc_t *probs, int np
         // k == 0 still needs the beta-scaling pass; give it one tile per block
         // through the normal path (ktiles == 0 -> acc stays 0).
         d.tiles_m = (q.m > 0 && q.n > 0) ? (q.m + BM - 1) / BM : 0;
-        d.tiles_n = (q.m > 0 && q.n > 0) ? (q.n + BN - 1) / BN : 0;
+        d.tiles_n = (q.m > 0 && q.n > 0) ? (q.n + tile_n - 1) / tile_n : 0;
         d.tile_begin = tiles;
         d.vec_ok = ((reinterpret_cast<uintptr_t>(q.C) & 15) == 0) && ((q.ldc & 1) == 0);
         d.raster = q.raster > 0 ? q.raster : GROUP_M;
@@ -486,48 +509,90 @@ extern "C" int ca3dmm_dgemm_plan_encode(const ca3dmm_dgemm_desc_t *probs, int np
 extern "C" int ca3dmm_dgemm_launch(const void *dev_plan, int nprob, int total_tiles, int a_kmajor,
                                    int *dev_status, double timeout_s, cudaStream_t stream)
 {
+    return ca3dmm_dgemm_launch_tn(dev_plan, nprob, total_tiles, a_kmajor, dev_status, timeout_s,
+                                  stream, 128);
+}
+
+extern "C" int ca3dmm_dgemm_launch_tn(const void *dev_plan, int nprob, int total_tiles,
+                                      int a_kmajor, int *dev_status, double timeout_s,
+                                      cudaStream_t stream, int tile_n)
+{
     ca3dmm_tile_ranges_t rg;
     memset(&rg, 0, sizeof(rg));
     rg.n = 1;
     rg.len[0] = total_tiles;
-    return ca3dmm_dgemm_launch_ranges(dev_plan, nprob, &rg, a_kmajor, dev_status, timeout_s,
-                                      stream);
+    return ca3dmm_dgemm_launch_ranges_tn(dev_plan, nprob, &rg, a_kmajor, dev_status, timeout_s,
+                                         stream, tile_n);
 }
 
 extern "C" int ca3dmm_dgemm_launch_ranges(const void *dev_plan, int nprob,
                                           const ca3dmm_tile_ranges_t *ranges, int a_kmajor,
                                           int *dev_status, double timeout_s, cudaStream_t stream)
 {
+    return ca3dmm_dgemm_launch_ranges_tn(dev_plan, nprob, ranges, a_kmajor, dev_status, timeout_s,
+                                         stream, 128);
+}
+
+namespace {
+// the shared-memory limit of one instantiation, raised once per device (a bit
+// per device ordinal; two threads may both set it, which is harmless)
+template <bool AK, int TBN>
+cudaError_t dgemm_attr_once()
+{
+    static std::atomic<unsigned long long> done{0};
+    int dev = 0;
+    cudaError_t err = cudaGetDevice(&dev);
+    if (err != cudaSuccess) return err;
+    const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+    if (!bit || !(done.load(std::memory_order_acquire) & bit)) {
+        err = cudaFuncSetAttribute(dgemm_dmma_grouped<AK, TBN>,
+                                   cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int) DTile<TBN>::SMEM_BYTES);
+        if (err != cudaSuccess) return err;
+        done.fetch_or(bit, std::memory_order_release);
+    }
+    return cudaSuccess;
+}
+
+template <bool AK, int TBN>
+cudaError_t dgemm_launch_one(int grid, const CUtensorMap *tm, const DProb *dp, int nprob,
+                             const ca3dmm_tile_ranges_t &rg, int total_tiles, int *status,
+                             unsigned long long limit, cudaStream_t stream)
+{
+    cudaError_t err = dgemm_attr_once<AK, TBN>();
+    if (err != cudaSuccess) return err;
+    dgemm_dmma_grouped<AK, TBN><<<grid, THREADS, DTile<TBN>::SMEM_BYTES, stream>>>(
+        tm, dp, nprob, rg, total_tiles, status, limit);
+    return cudaGetLastError();
+}
+}  // namespace
+
+extern "C" int ca3dmm_dgemm_launch_ranges_tn(const void *dev_plan, int nprob,
+                                             const ca3dmm_tile_ranges_t *ranges, int a_kmajor,
+                                             int *dev_status, double timeout_s,
+                                             cudaStream_t stream, int tile_n)
+{
     if (!ranges || ranges->n < 0 || ranges->n > CA3DMM_MAX_RANGES) return CA3DMM_EINVAL;
+    if (tile_n != 128 && tile_n != 64) return CA3DMM_EINVAL;
     const int total_tiles = range_total(*ranges);
     if (total_tiles <= 0) return CA3DMM_OK;
-    // the shared-memory attribute is per device: one bit per device once set
-    // (two threads may both set it; that is harmless)
-    static std::atomic<unsigned long long> attr_done{0};
-    int dev = 0;
-    CA3DMM_CUDA_TRY(cudaGetDevice(&dev));
-    const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
-    if (!(attr_done.load(std::memory_order_acquire) & bit) || !bit) {
-        CA3DMM_CUDA_TRY(cudaFuncSetAttribute(dgemm_dmma_grouped<false>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int) SMEM_BYTES));
-        CA3DMM_CUDA_TRY(cudaFuncSetAttribute(dgemm_dmma_grouped<true>,
-                                             cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int) SMEM_BYTES));
-        attr_done.fetch_or(bit, std::memory_order_release);
-    }
     const CUtensorMap *tm = reinterpret_cast<const CUtensorMap *>(dev_plan);
     const DProb *dp = reinterpret_cast<const DProb *>(tm + 2 * nprob);
     int grid = ca3dmm_device_sm_count();
     if (grid > total_tiles) grid = total_tiles;
-    unsigned long long limit = (unsigned long long) (timeout_s * 1e9);
-    if (a_kmajor)
-        dgemm_dmma_grouped<true><<<grid, THREADS, SMEM_BYTES, stream>>>(
-            tm, dp, nprob, *ranges, total_tiles, dev_status, limit);
+    const unsigned long long limit = (unsigned long long) (timeout_s * 1e9);
+    cudaError_t err;
+    if (tile_n == 128)
+        err = a_kmajor ? dgemm_launch_one<true, 128>(grid, tm, dp, nprob, *ranges, total_tiles,
+                                                      dev_status, limit, stream)
+                       : dgemm_launch_one<false, 128>(grid, tm, dp, nprob, *ranges, total_tiles,
+                                                       dev_status, limit, stream);
     else
-        dgemm_dmma_grouped<false><<<grid, THREADS, SMEM_BYTES, stream>>>(
-            tm, dp, nprob, *ranges, total_tiles, dev_status, limit);
-    CA3DMM_CUDA_TRY(cudaGetLastError());
+        err = a_kmajor ? dgemm_launch_one<true, 64>(grid, tm, dp, nprob, *ranges, total_tiles,
+                                                     dev_status, limit, stream)
+                       : dgemm_launch_one<false, 64>(grid, tm, dp, nprob, *ranges, total_tiles,
+                                                      dev_status, limit, stream);
+    CA3DMM_CUDA_TRY(err);
     ca3dmm_note_launch(1);
     return CA3DMM_OK;
 }

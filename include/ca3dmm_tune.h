@@ -48,8 +48,10 @@ typedef struct {
                         tuner keeps the engine's grid and ignores it) */
     int raster;      /* modes 0, 1: tile rows per raster band (4, 8 or 16);
                         mode 2: tile rows per band of the work order (1 .. 1024) */
-    int tile_n;      /* GEMM tile columns: mode 2: 128 or 256 (0 = 256); modes 0 / 1 have
-                        one tile shape each (128 x 128 and 128 x 64) and take 0 */
+    int tile_n;      /* GEMM tile columns: mode 2: 128 or 256 (0 = 256); mode 0: 128 or
+                        64 (0 = 128, or CA3DMM_PLAIN_TILE_N; 64 is refused for the
+                        symmetric B^T B plan); mode 1 has one tile shape (128 x 64 per
+                        slice) and takes 0 */
 } ca3dmm_tune_cfg_t;
 
 #define CA3DMM_TUNE_NFEAT 14

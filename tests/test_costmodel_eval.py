@@ -2,7 +2,7 @@
 exhaustive autotuning on the 400 held-out shapes of the B200 study.
 
 tests/golden/costmodel_timings_b200.npz holds the study's exhaustive timings
-(every one of the 16 candidates -- plain, INT8-slice and modular
+(every one of the 19 candidates -- plain at two tile widths, INT8-slice and modular
 configurations with their k splits, rasters / bands and tile widths -- on
 every shape, ms) and features, written by
   python -m ca3dmm_b200.costmodel --train 1600 --test 400 --epochs 300 --out DIR
@@ -90,7 +90,7 @@ def test_held_out_regret_and_search_time(study):
     assert len(r1) == 400
     assert r1.mean() <= 0.03 and np.median(r1) <= 0.01, (r1.mean(), np.median(r1))
     assert r2.mean() <= 0.015 and np.median(r2) == 0.0, (r2.mean(), np.median(r2))
-    # timing the model's top 2 instead of all 16 candidates
+    # timing the model's top 2 instead of all 19 candidates
     order = np.argsort(P, axis=1)[:, :2]
     saved = 1.0 - np.take_along_axis(T, order, 1).sum(1) / T.sum(1)
     assert saved.mean() >= 0.85, saved.mean()

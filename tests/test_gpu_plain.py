@@ -263,3 +263,58 @@ def test_dev_type_copy_mat_blk(cuda, nrow, ncol, lds, ldd):
     d = dst.cpu().numpy().reshape(nrow, ldd)
     assert np.array_equal(d[:, :ncol], s[:, :ncol])
     assert np.all(d[:, ncol:] == -7.0)
+
+
+@pytest.mark.parametrize("m,n,k,ta,tb,p,grid,pad", [
+    (300, 200, 1000, 0, 0, 1, None, 0),
+    (129, 65, 77, 1, 0, 1, None, 0),            # K-major A read in place
+    (1000, 999, 1001, 0, 1, 6, None, 1),         # packed blocks (odd ldA)
+    (700, 333, 2500, 1, 1, 4, (1, 1, 4), 0),    # kp slabs (k split)
+    (3200, 3100, 1500, 0, 0, 2, (1, 1, 2), 0),  # slabs merged into one GEMM over k
+    (2049, 63, 640, 0, 0, 24, (4, 2, 3), 0),    # several task blocks, a thin C
+])
+def test_plain_64_column_tiles_match_128(cuda, monkeypatch, m, n, k, ta, tb, p, grid, pad):
+    """The DMMA GEMM with 128 x 64 output tiles (CA3DMM_PLAIN_TILE_N=64, or
+    set_tune tile_n = 64) gives the 128 x 128 tiles' bits: every C entry is
+    summed by one thread over the same k order either way.  The host-buffer
+    exec (row bands over the 64-column tile numbering) gives the same bits."""
+    import torch
+    A = orc.gen_signed_exp(71, *((k, m) if ta else (m, k)))
+    B = orc.gen_signed_exp(72, *((n, k) if tb else (k, n)))
+    dA, lda = to_dev(A, pad_ld=A.shape[0] + pad)
+    dB, ldb = to_dev(B)
+    outs = []
+    for tn in ("128", "64"):
+        monkeypatch.setenv("CA3DMM_PLAIN_TILE_N", tn)
+        e = cb.Ca3dmmEngine(m, n, k, ta, tb, p=p, proc_grid=grid)
+        assert e.ok
+        dC = dev_zeros(m * n)
+        assert e.exec(dA, lda, dB, ldb, dC, m) == 0
+        outs.append(from_dev(dC, m, n))
+        e.free()
+    assert np.array_equal(outs[0], outs[1])
+    _dd_check(outs[1], A, B, ta, tb, m, n, k, full=False)
+    # set_tune switches the width on a live engine; exec_host over row bands
+    monkeypatch.delenv("CA3DMM_PLAIN_TILE_N")
+    e = cb.Ca3dmmEngine(m, n, k, ta, tb, p=p, proc_grid=grid)
+    assert e.set_tune((cb.GEMM_PLAIN, 0, e.s.kp, 8, 64)) == 0
+    assert e.get_tune()[4] == 64
+    hA = np.zeros((lda, A.shape[1]), order="F")
+    hA[:A.shape[0], :] = A
+    hAt = torch.from_numpy(hA.ravel(order="F").copy()).pin_memory()
+    hBt = torch.from_numpy(np.asfortranarray(B).ravel(order="F").copy()).pin_memory()
+    hC = torch.zeros(m * n, dtype=torch.float64).pin_memory()
+    assert e.exec_host(hAt, lda, hBt, ldb, hC, m) == 0
+    assert np.array_equal(hC.numpy().reshape(n, m).T, outs[0])
+    e.free()
+
+
+def test_plain_64_column_tiles_refused_for_symmetric_btb(cuda, monkeypatch):
+    """The symmetric B^T B plan tiles C by 128-row block rows: a 64-column tile
+    is refused there (set_tune returns CA3DMM_EINVAL; the variable is ignored)."""
+    monkeypatch.setenv("CA3DMM_BTB_SYMMETRIC", "1")
+    e = cb.Ca3dmmEngine(256, 256, 1000, btb=True, p=1)
+    assert e.ok
+    assert e.set_tune((cb.GEMM_PLAIN, 0, 1, 8, 64)) == cb.EINVAL
+    assert e.set_tune((cb.GEMM_PLAIN, 0, 1, 8, 0)) == 0
+    e.free()

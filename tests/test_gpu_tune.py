@@ -98,7 +98,12 @@ def test_crt_tile_widths_bitexact(cuda, tile):
 def test_set_tune_refusals(cuda):
     e = cb.Ca3dmmEngine(256, 256, 256)
     assert e.set_tune((cb.GEMM_CRT, 15, 1, 8, 64)) != 0        # no 64-column modular tile
-    assert e.set_tune((cb.GEMM_PLAIN, 0, 1, 8, 128)) != 0      # the plain GEMM has one tile
+    assert e.set_tune((cb.GEMM_PLAIN, 0, 1, 8, 96)) != 0       # plain tiles: 128 or 64 columns
+    assert e.set_tune((cb.GEMM_OZAKI, 7, 1, 8, 64)) != 0       # the slice GEMM has one tile
+    assert e.set_tune((cb.GEMM_PLAIN, 0, 1, 8, 128)) == 0
+    assert e.get_tune() == (cb.GEMM_PLAIN, 0, 1, 8, 0)          # 0: the default width, 128
+    assert e.set_tune((cb.GEMM_PLAIN, 0, 1, 8, 64)) == 0
+    assert e.get_tune() == (cb.GEMM_PLAIN, 0, 1, 8, 64)
     assert e.set_tune((cb.GEMM_PLAIN, 0, 1, 5, 0)) != 0        # raster 4, 8 or 16
     assert e.set_tune((cb.GEMM_OZAKI, 9, 1, 8, 0)) != 0        # 2..8 slices
     assert e.set_tune((cb.GEMM_PLAIN, 0, 1, 16, 0)) == 0

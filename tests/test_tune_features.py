@@ -36,3 +36,11 @@ def test_tile_shapes_and_counts():
     L = cb.lib()
     assert L.ca3dmm_crt_bits(int(auto), 8000) >= 51 and L.ca3dmm_crt_bits(int(auto) - 1, 8000) < 51
     assert feats(1000, 3000, 8000, (2, 17, 1, 32, 256))[7] == 17.0
+
+
+def test_plain_tile_widths():
+    """The plain DMMA GEMM's two tiles: 128 x 128 (tile_n 0 or 128) and 128 x 64."""
+    full = feats(1000, 3000, 8000, (0, 0, 1, 8, 0))
+    half = feats(1000, 3000, 8000, (0, 0, 1, 8, 64))
+    assert full[10:12] == [128.0, 128.0] and half[10:12] == [128.0, 64.0]
+    assert abs(full[12] - math.log2(8 * 24)) < 1e-6 and abs(half[12] - math.log2(8 * 47)) < 1e-6
