@@ -6,13 +6,14 @@
 // (src/cannon.c:410-418, :651-676; src/cuda_proxy.cu:211-230).  All virtual
 // ranks' cuboid GEMMs of one ca3dmm exec run in this single launch.
 //
-// Layout (per stage, 32 KiB, 1024-byte aligned):
+// Layout (per stage, 32 KiB for 128-column tiles or 24 KiB for 64-column
+// ones, 1024-byte aligned):
 //   A tile: 128 (m) x 16 (k) doubles as 8 TMA boxes of 16 m x 16 k, each box
 //           16 rows (k) of 128 B (m), SWIZZLE_128B -- or, for a K-major A
 //           (a transposed operand read in place), 1 box of 128 rows (m) of
 //           128 B (k), like B.
-//   B tile: 128 (n) x 16 (k) doubles as 1 TMA box, 128 rows (n) of 128 B (k),
-//           SWIZZLE_128B.
+//   B tile: TBN (n) x 16 (k) doubles as 1 TMA box, TBN rows (n) of 128 B (k),
+//           SWIZZLE_128B (TBN = 128 or 64 output columns per tile).
 // Fragment ownership is permuted so every fragment load is one conflict-free
 // 128-bit LDS:
 //   * MMA row r of an m16 tile  -> tile row 2r (r < 8) or 2(r-8)+1, so a0/a1 of
