@@ -318,3 +318,27 @@ def test_plain_64_column_tiles_refused_for_symmetric_btb(cuda, monkeypatch):
     assert e.set_tune((cb.GEMM_PLAIN, 0, 1, 8, 64)) == cb.EINVAL
     assert e.set_tune((cb.GEMM_PLAIN, 0, 1, 8, 0)) == 0
     e.free()
+
+
+@pytest.mark.parametrize("n,k,grid", [(300, 2000, (1, 1, 4)), (257, 5000, None)])
+def test_plain_64_column_tiles_btb(cuda, monkeypatch, n, k, grid):
+    """B^T B with 128 x 64 tiles (the plan of kp slabs, the host-buffer exec
+    pipelined over them) gives the 128 x 128 tiles' bits."""
+    import torch
+    Bm = orc.gen_signed_exp(81, k, n)
+    dB, ldb = to_dev(Bm)
+    outs = []
+    for tn in ("128", "64"):
+        monkeypatch.setenv("CA3DMM_PLAIN_TILE_N", tn)
+        e = cb.Ca3dmmEngine(n, n, k, btb=True, p=grid[2] if grid else 4, proc_grid=grid)
+        assert e.ok
+        dC = dev_zeros(n * n)
+        assert e.exec(None, 0, dB, ldb, dC, n) == 0
+        outs.append(from_dev(dC, n, n))
+        if tn == "64":
+            hB = torch.from_numpy(np.asfortranarray(Bm).ravel(order="F").copy()).pin_memory()
+            hC = torch.zeros(n * n, dtype=torch.float64).pin_memory()
+            assert e.exec_host(None, 0, hB, ldb, hC, n) == 0
+            assert np.array_equal(hC.numpy().reshape(n, n).T, outs[0])
+        e.free()
+    assert np.array_equal(outs[0], outs[1])
