@@ -288,7 +288,7 @@ def test_engine_auto_btb(cuda):
                                            (64, 64, 20000, 0, 0, 8)])
 def test_engine_auto_small_and_odd_shapes(cuda, m, n, k, ta, tb, p):
     """Auto mode over degenerate and odd shapes: every candidate that runs
-    gives a result the guard can judge, the kept one is admissible, and C is
+    gives a result the guard can assess, the kept one is admissible, and C is
     within the plain GEMM's bound."""
     A = orc.gen_signed_exp(51 + m, *((k, m) if ta else (m, k)), emin=-3, emax=3)
     B = orc.gen_signed_exp(52 + n, *((n, k) if tb else (k, n)), emin=-3, emax=3)
